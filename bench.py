@@ -1,0 +1,291 @@
+"""Benchmark: the 30-qubit complex128 layered circuit (plain method) on B200.
+
+Workload (one step): |0...0> on 30 qubits (16 GiB complex128 state, larger than L2), then 10 layers
+of RX, RY, RZ on every qubit (angles U[0, 2pi), seeded) followed by a CNOT ladder q -> q+1 -- 1190
+gates.  The metric is the circuit's effective HBM bandwidth against the algorithmic 2 x 16 x 2^n
+bytes per gate (the reference's figure), i.e. gates x 2 x 16 x 2^n / circuit time, summed over
+ranks.  The end-to-end figure (``e2e``) runs the same circuit through the public API with the
+observable (256 Pauli strings of weight <= 6) and 1024-shot sampling, reading results back to the
+host, and reports the same unit against the circuit bytes.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--mode staged|gate_by_gate]
+
+Multi-GPU: replicas only (each rank runs its own 30-qubit state; no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_QUBITS = 30
+DEPTH = 10
+N_TERMS = 256
+N_SHOTS = 1024
+GATE_SEED, TERM_SEED, SHOT_SEED = 2124, 2125, 2126
+METRIC = "30q circuit time & HBM GB/s (plain c128 layered RX/RY/RZ+CNOT, depth 10)"
+
+
+def bytes_per_gate(n: int) -> int:
+    return 2 * 16 * (1 << n)
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.lines = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_reference_gbs(n: int, gates, budget_s: float, threads: int, state=None):
+    """Time the reference csim (oracle/_ref, else the oracle port) gate by gate on host cores."""
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    os.environ.setdefault("QULACS_NUM_THREADS", str(threads))
+    from oracle import oracle as O
+    sim = O.reference()
+    kind = "reference"
+    if sim is None:
+        sim, kind = O.port(), "port"
+        threads = 1
+    from qulacs_b200 import workloads as W
+    s = state
+    if s is None:
+        s = np.zeros(1 << n, dtype=np.complex128)
+        s[0] = 1.0
+        W.run_on_cpu(gates[:2], s, sim)  # first touch of every page, untimed
+    done, t0 = 0, time.perf_counter()
+    i = 2
+    while time.perf_counter() - t0 < budget_s or done < 2:
+        W.run_on_cpu([gates[i % len(gates)]], s, sim)
+        i += 1
+        done += 1
+    dt = time.perf_counter() - t0
+    return {"value": done * bytes_per_gate(n) / dt / 1e9, "unit": "GB/s", "cores": threads, "kind": kind,
+            "sample": f"{done} gates of the {n}-qubit layered circuit, gate by gate, {dt:.1f} s"}
+
+
+def run_reference(args, rank: int, world: int):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    os.environ.setdefault("QULACS_NUM_THREADS", str(threads))
+    from oracle import oracle as O
+    from qulacs_b200 import workloads as W
+    n = args.qubits
+    gates = W.layered_rotation_circuit(n, DEPTH, GATE_SEED)
+    sim = O.reference() or O.port()
+    s = np.zeros(1 << n, dtype=np.complex128)
+    s[0] = 1.0
+    W.run_on_cpu(gates[:2], s, sim)  # first touch of every page, untimed
+    per_step_s = 6.0
+    vals = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_reference_gbs(n, gates[(i * 7) % len(gates):] + gates, per_step_s, threads, state=s)
+        if i >= args.warmup:
+            vals.append(r)
+    value = statistics.median(v["value"] for v in vals)
+    cb = dict(vals[-1])
+    cb["value"] = value
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * bytes_per_gate(n) * len(gates) / (value * 1e9),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128 (f64)",
+            "data": "synthetic (seeded)", "config": {"workload": f"layered RX/RY/RZ+CNOT n={n} depth={DEPTH}, gate sample per step"},
+            "cpu_baseline": cb, "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--mode", default="staged", choices=["staged", "gate_by_gate"])
+    ap.add_argument("--qubits", type=int, default=N_QUBITS)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3  # timing rule: at least 3 untimed warm-up steps
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    import qulacs_b200 as Q
+    from qulacs_b200 import _lib
+    from qulacs_b200 import workloads as W
+
+    n = args.qubits
+    stream = torch.cuda.current_stream()
+    Q.set_default_stream(stream.cuda_stream)
+    lib = _lib.load()
+    gates = W.layered_rotation_circuit(n, DEPTH, GATE_SEED)
+    terms = W.random_pauli_terms(n, N_TERMS, 1, 6, TERM_SEED)
+    circ = W.to_circuit(gates, n)
+    obs = W.to_observable(terms, n)
+    state = Q.QuantumState(n)
+    mode = args.mode
+
+    def step():
+        state.set_zero_state()
+        circ.update_quantum_state(state, mode=mode)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = lib.qs_launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    launches = lib.qs_launch_count() - l0
+    ms = ev0.elapsed_time(ev1) / args.steps
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    gb_per_step = len(gates) * bytes_per_gate(n) / 1e9
+    value = world * gb_per_step / (ms / 1e3)
+
+    # dominant kernel roofline: one HBM pass = 2 x 16 x 2^n algorithmic bytes
+    passes = circ.pass_count() if mode == "staged" else len(gates)
+    per_launch_ms = ms / max(1, passes)
+    hbm_peak, peak_kind = peaks()
+    achieved = bytes_per_gate(n) / 1e9 / (per_launch_ms / 1e3)
+
+    # end to end through the public API: host gate list already built into the circuit, observable
+    # masks and uniforms from host, results (term values + samples) back to the host
+    e2e_steps = max(1, min(args.steps, 3))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    energy = None
+    for i in range(e2e_steps):
+        state.set_zero_state()
+        circ.update_quantum_state(state, mode=mode)
+        energy = obs.get_expectation_value(state)
+        samples = state.sampling(N_SHOTS, SHOT_SEED + i)
+    torch.cuda.synchronize()
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / e2e_steps
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    h2d = N_TERMS * (8 + 8 + 4) + N_SHOTS * 8 + len(gates) * 64
+    d2h = N_TERMS * 8 + N_SHOTS * 8
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu = cpu_reference_gbs(n, gates, 12.0, os.cpu_count() or 1)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c128 (f64)", "data": "synthetic (seeded)",
+            "config": {"workload": f"layered RX/RY/RZ+CNOT n={n} depth={DEPTH} ({len(gates)} gates), c128",
+                       "exec_mode": mode, "hbm_passes": passes, "l2": "state 16 GiB > L2 (no flush needed)",
+                       "parallelism": f"replicas x{world}"},
+            "circuit_s": ms / 1e3,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                         "frac": achieved / hbm_peak, "peak_kind": peak_kind, "traffic": None,
+                         "kernel": "one HBM pass over the state (2 x 16 x 2^n B)"},
+            "e2e": {"value": world * gb_per_step / (e2e_ms / 1e3), "unit": "GB/s", "ms_per_step": e2e_ms,
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "includes": "set_zero_state + circuit + <H> (256 strings) + 1024-shot sampling"},
+            "energy": energy,
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,256 @@
+/*
+ * qulacs_b200.h -- C ABI of the B200 (sm_100a) state-update library.
+ *
+ * Drop-in boundary for the reference's csim / gpusim operator layer.  Every entry point keeps the
+ * csim name and argument order (src/csim/update_ops.hpp, src/csim/stat_ops.hpp,
+ * src/csim/update_ops_dm.hpp, src/csim/stat_ops_dm.hpp), prefixed `qs_`, and differs in three ways:
+ *   - `state` is a DEVICE pointer to `dim` complex128 amplitudes ((re, im) doubles, the layout of
+ *     csim's CTYPE = std::complex<double>), as gpusim's `void* state` (src/gpusim/update_ops_cuda.h);
+ *   - a trailing `void* stream` (a cudaStream_t; NULL = the legacy default stream) replaces gpusim's
+ *     `(void* stream, UINT device_number)`: the device is the current device of the calling thread;
+ *   - every function returns an int status (QS_OK or a QS_ERR_* code, message in
+ *     qs_get_last_error()) instead of void / exit(1) (src/gpusim/util.cuh:28-42).
+ * Matrices and index lists are HOST pointers, read before the call returns.  Gate calls are
+ * asynchronous on `stream`; calls that return a value to the host synchronise `stream`.
+ * Complex matrices are row-major arrays of interleaved doubles; for a k-target matrix, bit j of the
+ * row/column index refers to target_qubit_index_list[j] (src/csim/utility.cpp:77-93).
+ */
+#ifndef QULACS_B200_H_
+#define QULACS_B200_H_
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QS_API __attribute__((visibility("default")))
+
+typedef unsigned int QS_UINT;       /* csim UINT  (src/csim/type.hpp:14) */
+typedef unsigned long long QS_ITYPE; /* csim ITYPE (src/csim/type.hpp:29) */
+
+/* ---- status codes ---- */
+#define QS_OK 0
+#define QS_ERR_INVALID_ARGUMENT 1 /* bad qubit index, duplicate targets, dim not 2^n, k out of range */
+#define QS_ERR_OUT_OF_MEMORY 2    /* cudaMalloc failed (the reference calls exit(1), memory_ops.cpp:21-25) */
+#define QS_ERR_CUDA 3             /* any other CUDA runtime error */
+#define QS_ERR_TIMEOUT 4          /* a bounded device wait expired (persistent executor) */
+#define QS_ERR_NOT_SUPPORTED 5    /* valid request outside this build's limits */
+#define QS_ERR_NO_DEVICE 6        /* no CUDA device visible */
+#define QS_ERR_REJECTED 7         /* admission control refused a request (serving loop) */
+
+QS_API const char* qs_get_last_error(void);
+QS_API const char* qs_version(void);
+/* Number of kernels this library has launched in this process (diagnostic; no reference counterpart). */
+QS_API unsigned long long qs_launch_count(void);
+QS_API int qs_device_synchronize(void);
+QS_API int qs_stream_synchronize(void* stream);
+
+/* ---- memory and initialisation (src/csim/memory_ops.hpp, src/csim/init_ops.hpp) ---- */
+/* allocate_quantum_state (memory_ops.cpp:17-27): device buffer of dim complex128 amplitudes. */
+QS_API int qs_allocate_quantum_state(QS_ITYPE dim, void** state_out);
+/* complex64 variant for the reduced-precision (fused) path: dim (re, im) floats. */
+QS_API int qs_allocate_quantum_state_c64(QS_ITYPE dim, void** state_out);
+/* release_quantum_state (memory_ops.cpp:29-31). */
+QS_API int qs_release_quantum_state(void* state);
+/* initialize_quantum_state (init_ops_fill.cpp:10-23): |0...0>. */
+QS_API int qs_initialize_quantum_state(void* state, QS_ITYPE dim, void* stream);
+QS_API int qs_initialize_quantum_state_c64(void* state, QS_ITYPE dim, void* stream);
+/* set_computational_basis-style fill: |basis>. */
+QS_API int qs_set_computational_basis(QS_ITYPE basis, void* state, QS_ITYPE dim, void* stream);
+/* Host <-> device copies of a whole state (cppsim QuantumStateGpu::load / duplicate_data_cpp). */
+QS_API int qs_load_state(const void* host_src, void* state, QS_ITYPE dim, void* stream);
+QS_API int qs_get_state(const void* state, void* host_dst, QS_ITYPE dim, void* stream);
+/* complex128 -> complex64 and back (rounding to nearest). */
+QS_API int qs_state_to_c64(const void* state_c128, void* state_c64, QS_ITYPE dim, void* stream);
+QS_API int qs_state_to_c128(const void* state_c64, void* state_c128, QS_ITYPE dim, void* stream);
+
+/* ---- single-qubit gates (src/csim/update_ops.hpp) ---- */
+/* update_ops.hpp:720 single_qubit_dense_matrix_gate(UINT, const CTYPE[4], CTYPE*, ITYPE) */
+QS_API int qs_single_qubit_dense_matrix_gate(
+    QS_UINT target_qubit_index, const double matrix[8], void* state, QS_ITYPE dim, void* stream);
+/* update_ops.hpp:758 single_qubit_diagonal_matrix_gate */
+QS_API int qs_single_qubit_diagonal_matrix_gate(
+    QS_UINT target_qubit_index, const double diagonal_matrix[4], void* state, QS_ITYPE dim, void* stream);
+/* update_ops.hpp:793 single_qubit_phase_gate */
+QS_API int qs_single_qubit_phase_gate(
+    QS_UINT target_qubit_index, const double phase[2], void* state, QS_ITYPE dim, void* stream);
+/* update_ops.hpp:559/589/619 RX_gate / RY_gate / RZ_gate: exp(+i angle P / 2) */
+QS_API int qs_RX_gate(QS_UINT target_qubit_index, double angle, void* state, QS_ITYPE dim, void* stream);
+QS_API int qs_RY_gate(QS_UINT target_qubit_index, double angle, void* state, QS_ITYPE dim, void* stream);
+QS_API int qs_RZ_gate(QS_UINT target_qubit_index, double angle, void* state, QS_ITYPE dim, void* stream);
+/* update_ops.hpp:42-330 named one-qubit gates */
+QS_API int qs_X_gate(QS_UINT target_qubit_index, void* state, QS_ITYPE dim, void* stream);
+QS_API int qs_Y_gate(QS_UINT target_qubit_index, void* state, QS_ITYPE dim, void* stream);
+QS_API int qs_Z_gate(QS_UINT target_qubit_index, void* state, QS_ITYPE dim, void* stream);
+QS_API int qs_H_gate(QS_UINT target_qubit_index, void* state, QS_ITYPE dim, void* stream);
+QS_API int qs_S_gate(QS_UINT target_qubit_index, void* state, QS_ITYPE dim, void* stream);
+QS_API int qs_Sdag_gate(QS_UINT target_qubit_index, void* state, QS_ITYPE dim, void* stream);
+QS_API int qs_T_gate(QS_UINT target_qubit_index, void* state, QS_ITYPE dim, void* stream);
+QS_API int qs_Tdag_gate(QS_UINT target_qubit_index, void* state, QS_ITYPE dim, void* stream);
+QS_API int qs_sqrtX_gate(QS_UINT target_qubit_index, void* state, QS_ITYPE dim, void* stream);
+QS_API int qs_sqrtXdag_gate(QS_UINT target_qubit_index, void* state, QS_ITYPE dim, void* stream);
+QS_API int qs_sqrtY_gate(QS_UINT target_qubit_index, void* state, QS_ITYPE dim, void* stream);
+QS_API int qs_sqrtYdag_gate(QS_UINT target_qubit_index, void* state, QS_ITYPE dim, void* stream);
+QS_API int qs_P0_gate(QS_UINT target_qubit_index, void* state, QS_ITYPE dim, void* stream);
+QS_API int qs_P1_gate(QS_UINT target_qubit_index, void* state, QS_ITYPE dim, void* stream);
+
+/* ---- two-qubit and multi-qubit gates ---- */
+/* update_ops.hpp:343 CNOT_gate(UINT control, UINT target, CTYPE*, ITYPE) */
+QS_API int qs_CNOT_gate(QS_UINT control_qubit_index, QS_UINT target_qubit_index, void* state,
+    QS_ITYPE dim, void* stream);
+/* update_ops.hpp:373 CZ_gate */
+QS_API int qs_CZ_gate(QS_UINT control_qubit_index, QS_UINT target_qubit_index, void* state,
+    QS_ITYPE dim, void* stream);
+/* update_ops.hpp:403 SWAP_gate */
+QS_API int qs_SWAP_gate(QS_UINT target_qubit_index_0, QS_UINT target_qubit_index_1, void* state,
+    QS_ITYPE dim, void* stream);
+/* update_ops.hpp:1277 double_qubit_dense_matrix_gate_c (matrix bit 0 <-> t1, bit 1 <-> t2) */
+QS_API int qs_double_qubit_dense_matrix_gate_c(QS_UINT target_qubit_index1,
+    QS_UINT target_qubit_index2, const double matrix[32], void* state, QS_ITYPE dim, void* stream);
+/* update_ops.hpp:1330 multi_qubit_dense_matrix_gate; this build supports 1 <= count <= 6. */
+QS_API int qs_multi_qubit_dense_matrix_gate(const QS_UINT* target_qubit_index_list,
+    QS_UINT target_qubit_index_count, const double* matrix, void* state, QS_ITYPE dim, void* stream);
+/* update_ops.hpp:1459 multi_qubit_diagonal_matrix_gate; 1 <= count <= 20. */
+QS_API int qs_multi_qubit_diagonal_matrix_gate(const QS_UINT* target_qubit_index_list,
+    QS_UINT target_qubit_index_count, const double* diagonal_element, void* state, QS_ITYPE dim,
+    void* stream);
+/* update_ops.hpp:832 single_qubit_control_single_qubit_dense_matrix_gate */
+QS_API int qs_single_qubit_control_single_qubit_dense_matrix_gate(QS_UINT control_qubit_index,
+    QS_UINT control_value, QS_UINT target_qubit_index, const double matrix[8], void* state,
+    QS_ITYPE dim, void* stream);
+/* update_ops.hpp:880 multi_qubit_control_single_qubit_dense_matrix_gate */
+QS_API int qs_multi_qubit_control_single_qubit_dense_matrix_gate(
+    const QS_UINT* control_qubit_index_list, const QS_UINT* control_value_list,
+    QS_UINT control_qubit_index_count, QS_UINT target_qubit_index, const double matrix[8],
+    void* state, QS_ITYPE dim, void* stream);
+/* update_ops.hpp:1445 multi_qubit_control_multi_qubit_dense_matrix_gate; targets <= 6. */
+QS_API int qs_multi_qubit_control_multi_qubit_dense_matrix_gate(
+    const QS_UINT* control_qubit_index_list, const QS_UINT* control_value_list,
+    QS_UINT control_qubit_index_count, const QS_UINT* target_qubit_index_list,
+    QS_UINT target_qubit_index_count, const double* matrix, void* state, QS_ITYPE dim, void* stream);
+/* update_ops.hpp:1003 multi_qubit_Pauli_gate_partial_list (ids: 0=I 1=X 2=Y 3=Z) */
+QS_API int qs_multi_qubit_Pauli_gate_partial_list(const QS_UINT* target_qubit_index_list,
+    const QS_UINT* Pauli_operator_type_list, QS_UINT target_qubit_index_count, void* state,
+    QS_ITYPE dim, void* stream);
+/* update_ops.hpp:1191 multi_qubit_Pauli_rotation_gate_partial_list: exp(i angle P / 2) */
+QS_API int qs_multi_qubit_Pauli_rotation_gate_partial_list(const QS_UINT* target_qubit_index_list,
+    const QS_UINT* Pauli_operator_type_list, QS_UINT target_qubit_index_count, double angle,
+    void* state, QS_ITYPE dim, void* stream);
+
+/* ---- statistics (src/csim/stat_ops.hpp); results to host, stream synchronised ---- */
+/* stat_ops.hpp:5 state_norm_squared */
+QS_API int qs_state_norm_squared(const void* state, QS_ITYPE dim, void* stream, double* out);
+/* stat_ops.hpp:12 state_inner_product: sum conj(bra_i) ket_i -> out[0] + i out[1] */
+QS_API int qs_state_inner_product(const void* state_bra, const void* state_ket, QS_ITYPE dim,
+    void* stream, double out[2]);
+/* stat_ops.hpp:24/26/28 M0_prob, M1_prob, marginal_prob */
+QS_API int qs_M0_prob(QS_UINT target_qubit_index, const void* state, QS_ITYPE dim, void* stream, double* out);
+QS_API int qs_M1_prob(QS_UINT target_qubit_index, const void* state, QS_ITYPE dim, void* stream, double* out);
+QS_API int qs_marginal_prob(const QS_UINT* sorted_target_qubit_index_list, const QS_UINT* measured_value_list,
+    QS_UINT target_qubit_index_count, const void* state, QS_ITYPE dim, void* stream, double* out);
+/* stat_ops.hpp:38 expectation_value_multi_qubit_Pauli_operator_partial_list */
+QS_API int qs_expectation_value_multi_qubit_Pauli_operator_partial_list(
+    const QS_UINT* target_qubit_index_list, const QS_UINT* Pauli_operator_type_list,
+    QS_UINT target_qubit_index_count, const void* state, QS_ITYPE dim, void* stream, double* out);
+/* stat_ops.hpp:45 transition_amplitude_multi_qubit_Pauli_operator_partial_list: <bra|P|ket> */
+QS_API int qs_transition_amplitude_multi_qubit_Pauli_operator_partial_list(
+    const QS_UINT* target_qubit_index_list, const QS_UINT* Pauli_operator_type_list,
+    QS_UINT target_qubit_index_count, const void* state_bra, const void* state_ket, QS_ITYPE dim,
+    void* stream, double out[2]);
+/*
+ * Batched <P_k> for many Pauli strings in one call (GeneralQuantumOperator::get_expectation_value,
+ * cppsim/general_quantum_operator.cpp:105-141, without the coefficient).  Term k is given by its
+ * bit-flip mask x_masks[k], phase-flip mask z_masks[k] and Y count (src/csim/utility.cpp:12-43).
+ * Writes values[k] = <psi|P_k|psi> (real) for k < term_count.
+ */
+QS_API int qs_expectation_value_pauli_batch(const QS_ITYPE* x_masks, const QS_ITYPE* z_masks,
+    const QS_UINT* y_counts, QS_UINT term_count, const void* state, QS_ITYPE dim, void* stream,
+    double* values);
+/*
+ * cppsim QuantumStateCpu::sampling (cppsim/state.hpp:909-929) with caller-supplied uniforms in
+ * [0, 1): out[c] = lower_bound(stacked_prob, uniforms[c]) - 1 over the FP64 prefix sums of |a_i|^2
+ * (so 0 -> 2^64 - 1 and r > norm -> dim, as in the reference).
+ */
+QS_API int qs_state_sampling_with_uniforms(const void* state, QS_ITYPE dim, const double* uniforms,
+    QS_UINT sampling_count, QS_ITYPE* out, void* stream);
+/* Same, drawing the uniforms as the reference's Random does (cppsim/utility.hpp:54-80):
+ * std::mt19937_64 seeded with `random_seed`, std::uniform_real_distribution<double>(0, 1). */
+QS_API int qs_state_sampling(const void* state, QS_ITYPE dim, QS_UINT sampling_count,
+    QS_UINT random_seed, QS_ITYPE* out, void* stream);
+/* The uniforms qs_state_sampling draws for a seed (host only; cppsim/utility.hpp:54-80). */
+QS_API int qs_reference_uniforms(QS_UINT random_seed, QS_UINT count, double* out);
+
+/* ---- density matrix (src/csim/update_ops_dm.hpp, src/csim/stat_ops_dm.hpp) ----
+ * `rho` is a device pointer to dim*dim complex128 entries, row-major; dim = 2^n. */
+QS_API int qs_dm_allocate(QS_ITYPE dim, void** rho_out);
+QS_API int qs_dm_initialize_quantum_state(void* rho, QS_ITYPE dim, void* stream); /* |0><0| */
+QS_API int qs_dm_initialize_with_pure_state(void* rho, const void* pure_state, QS_ITYPE dim, void* stream);
+QS_API int qs_dm_single_qubit_dense_matrix_gate(
+    QS_UINT target_qubit_index, const double matrix[8], void* rho, QS_ITYPE dim, void* stream);
+QS_API int qs_dm_multi_qubit_dense_matrix_gate(const QS_UINT* target_qubit_index_list,
+    QS_UINT target_qubit_index_count, const double* matrix, void* rho, QS_ITYPE dim, void* stream);
+QS_API int qs_dm_CNOT_gate(QS_UINT control_qubit_index, QS_UINT target_qubit_index, void* rho,
+    QS_ITYPE dim, void* stream);
+QS_API int qs_dm_CZ_gate(QS_UINT control_qubit_index, QS_UINT target_qubit_index, void* rho,
+    QS_ITYPE dim, void* stream);
+QS_API int qs_dm_RX_gate(QS_UINT target_qubit_index, double angle, void* rho, QS_ITYPE dim, void* stream);
+QS_API int qs_dm_RY_gate(QS_UINT target_qubit_index, double angle, void* rho, QS_ITYPE dim, void* stream);
+QS_API int qs_dm_RZ_gate(QS_UINT target_qubit_index, double angle, void* rho, QS_ITYPE dim, void* stream);
+/* DepolarizingNoise(t, p) on a density matrix (cppsim/gate_factory.cpp:456-466 through the exact
+ * branch of cppsim/gate_general.hpp:265-285), in one pass. */
+QS_API int qs_dm_depolarizing_noise(QS_UINT target_qubit_index, double probability, void* rho,
+    QS_ITYPE dim, void* stream);
+/* TwoQubitDepolarizingNoise(t1, t2, p) (cppsim/gate_factory.cpp:471-500), in one pass. */
+QS_API int qs_dm_two_qubit_depolarizing_noise(QS_UINT target_qubit_index1,
+    QS_UINT target_qubit_index2, double probability, void* rho, QS_ITYPE dim, void* stream);
+/* stat_ops_dm.hpp dm_expectation_value_multi_qubit_Pauli_operator_partial_list (stat_ops_dm.cpp:164-191) */
+QS_API int qs_dm_expectation_value_multi_qubit_Pauli_operator_partial_list(
+    const QS_UINT* target_qubit_index_list, const QS_UINT* Pauli_operator_type_list,
+    QS_UINT target_qubit_index_count, const void* rho, QS_ITYPE dim, void* stream, double* out);
+/* DensityMatrixCpu::sampling (cppsim/state_dm.hpp:383-401) with supplied uniforms. */
+QS_API int qs_dm_sampling_with_uniforms(const void* rho, QS_ITYPE dim, const double* uniforms,
+    QS_UINT sampling_count, QS_ITYPE* out, void* stream);
+/* stat_ops_dm.hpp dm_state_norm_squared (trace) */
+QS_API int qs_dm_state_norm_squared(const void* rho, QS_ITYPE dim, void* stream, double* out);
+
+/* ---- circuits (cppsim QuantumCircuit, src/cppsim/circuit.hpp) ----
+ * A circuit is a host-side gate list plus its device-resident schedule.  update_quantum_state
+ * applies it to a complex128 state (or density matrix) in place, like
+ * QuantumCircuit::update_quantum_state (circuit.cpp:46-57). */
+typedef struct qs_circuit_s* qs_circuit_t;
+
+/* Gate kinds accepted by qs_circuit_add_gate. */
+#define QS_GATE_DENSE 0          /* matrix on targets (row-major 2^k x 2^k), optional controls */
+#define QS_GATE_DIAGONAL 1       /* diagonal entries on targets */
+#define QS_GATE_RX 2             /* params[0] = angle; csim RX_gate convention */
+#define QS_GATE_RY 3
+#define QS_GATE_RZ 4
+#define QS_GATE_CNOT 5           /* targets[0] = control, targets[1] = target */
+#define QS_GATE_CZ 6             /* targets[0] = control, targets[1] = target */
+#define QS_GATE_SWAP 7
+#define QS_GATE_PAULI 8          /* targets + pauli ids in params (as doubles) */
+#define QS_GATE_PAULI_ROTATION 9 /* targets + ids; angle in params[count] */
+#define QS_GATE_DEPOLARIZING 10  /* 1 or 2 targets, params[0] = probability (density matrix only) */
+
+/* Execution modes of qs_circuit_update_quantum_state. */
+#define QS_EXEC_GATE_BY_GATE 0 /* one kernel per gate: the reference's method */
+#define QS_EXEC_STAGED 1       /* several gates per HBM pass, identical arithmetic per gate */
+
+QS_API int qs_circuit_create(QS_UINT qubit_count, qs_circuit_t* out);
+QS_API int qs_circuit_destroy(qs_circuit_t circuit);
+QS_API int qs_circuit_add_gate(qs_circuit_t circuit, int kind, const QS_UINT* targets,
+    QS_UINT target_count, const QS_UINT* controls, const QS_UINT* control_values,
+    QS_UINT control_count, const double* params, QS_UINT param_count);
+QS_API int qs_circuit_gate_count(qs_circuit_t circuit, QS_UINT* out);
+QS_API int qs_circuit_update_quantum_state(
+    qs_circuit_t circuit, void* state, QS_ITYPE dim, int exec_mode, void* stream);
+/* Number of HBM passes (kernel launches over the whole state) the staged schedule uses. */
+QS_API int qs_circuit_pass_count(qs_circuit_t circuit, QS_ITYPE dim, QS_UINT* out);
+/* Apply to a density matrix (gates as U rho U^dagger, depolarizing channels exact). */
+QS_API int qs_circuit_update_density_matrix(
+    qs_circuit_t circuit, void* rho, QS_ITYPE dim, int exec_mode, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QULACS_B200_H_ */

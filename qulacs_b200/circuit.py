@@ -1,0 +1,93 @@
+"""QuantumCircuit over the C-ABI circuit object (cppsim/circuit.hpp, circuit.cpp)."""
+from __future__ import annotations
+
+import ctypes as C
+
+from . import _lib
+from . import gate as G
+from ._lib import call
+
+
+class QuantumCircuit:
+    """Gate list applied in order by ``update_quantum_state`` (cppsim circuit.cpp:46-57).
+
+    ``mode="gate_by_gate"`` launches one kernel per gate (the reference's method);
+    ``mode="staged"`` applies several gates per HBM pass with the same per-gate arithmetic.
+    """
+
+    def __init__(self, qubit_count: int):
+        _lib.load()
+        self.qubit_count = int(qubit_count)
+        h = C.c_void_p()
+        call("qs_circuit_create", self.qubit_count, C.byref(h))
+        self._h = h.value
+        self.gate_list = []
+
+    def get_qubit_count(self) -> int:
+        return self.qubit_count
+
+    def get_gate_count(self) -> int:
+        return len(self.gate_list)
+
+    def add_gate(self, gate: G.QuantumGateBase) -> None:
+        gate._add_to(self._h)
+        self.gate_list.append(gate)
+
+    add_gate_copy = add_gate
+
+    # convenience adders (cppsim circuit.hpp:130-600)
+    def add_X_gate(self, t): self.add_gate(G.X(t))
+    def add_Y_gate(self, t): self.add_gate(G.Y(t))
+    def add_Z_gate(self, t): self.add_gate(G.Z(t))
+    def add_H_gate(self, t): self.add_gate(G.H(t))
+    def add_S_gate(self, t): self.add_gate(G.S(t))
+    def add_T_gate(self, t): self.add_gate(G.T(t))
+    def add_RX_gate(self, t, a): self.add_gate(G.RX(t, a))
+    def add_RY_gate(self, t, a): self.add_gate(G.RY(t, a))
+    def add_RZ_gate(self, t, a): self.add_gate(G.RZ(t, a))
+    def add_RotX_gate(self, t, a): self.add_gate(G.RotX(t, a))
+    def add_RotY_gate(self, t, a): self.add_gate(G.RotY(t, a))
+    def add_RotZ_gate(self, t, a): self.add_gate(G.RotZ(t, a))
+    def add_U1_gate(self, t, l): self.add_gate(G.U1(t, l))
+    def add_U2_gate(self, t, p, l): self.add_gate(G.U2(t, p, l))
+    def add_U3_gate(self, t, th, p, l): self.add_gate(G.U3(t, th, p, l))
+    def add_CNOT_gate(self, c, t): self.add_gate(G.CNOT(c, t))
+    def add_CZ_gate(self, c, t): self.add_gate(G.CZ(c, t))
+    def add_SWAP_gate(self, a, b): self.add_gate(G.SWAP(a, b))
+    def add_dense_matrix_gate(self, targets, m): self.add_gate(G.DenseMatrix(targets, m))
+
+    def add_noise_gate(self, gate: G.QuantumGateBase, noise_type: str, prob: float) -> None:
+        """cppsim circuit.cpp:167-190: the gate, then depolarizing noise on its targets + controls."""
+        self.add_gate(gate)
+        qubits = gate.get_target_index_list() + gate.get_control_index_list()
+        if noise_type != "Depolarizing":
+            raise NotImplementedError(noise_type)
+        if len(qubits) == 1:
+            self.add_gate(G.DepolarizingNoise(qubits[0], prob))
+        elif len(qubits) == 2:
+            self.add_gate(G.TwoQubitDepolarizingNoise(qubits[0], qubits[1], prob))
+        else:
+            raise ValueError("depolarizing noise can be used up to 2 qubits")
+
+    def update_quantum_state(self, state, mode: str = "staged") -> None:
+        m = {"gate_by_gate": _lib.EXEC_GATE_BY_GATE, "staged": _lib.EXEC_STAGED}[mode]
+        if state.get_qubit_count() != self.qubit_count:
+            raise ValueError("state qubit count differs from the circuit's")
+        if state.is_state_vector():
+            call("qs_circuit_update_quantum_state", self._h, state.data_ptr(), state.dim, m, state.stream)
+        else:
+            call("qs_circuit_update_density_matrix", self._h, state.data_ptr(), state.dim, m, state.stream)
+
+    def pass_count(self) -> int:
+        out = C.c_uint()
+        call("qs_circuit_pass_count", self._h, 1 << self.qubit_count, C.byref(out))
+        return out.value
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            try:
+                _lib.load().qs_circuit_destroy(h)
+            except Exception:
+                pass
+            self._h = None

@@ -1,0 +1,463 @@
+// Reductions over a complex128 state: norm, inner product, probabilities, Pauli expectation values
+// and sampling.  All sums are FP64 and deterministic: a fixed per-thread order, a warp shuffle tree,
+// one partial per CTA written to scratch, then one CTA folds the partials in index order (no
+// floating-point atomics).
+#include <algorithm>
+#include <random>
+#include <vector>
+
+#include "qs_internal.cuh"
+
+namespace qs {
+
+constexpr int kRThreads = 256;
+constexpr int kMaxPartials = 4096;
+
+static unsigned reduce_blocks(ITYPE items) {
+    ITYPE b = (items + kRThreads - 1) / kRThreads;
+    ITYPE cap = std::min<ITYPE>((ITYPE)sm_count() * 8, kMaxPartials);
+    return (unsigned)std::max<ITYPE>(1, std::min(b, cap));
+}
+
+// Folds `count` partial vectors (each `width` doubles, partial p of value w at p * width + w)
+// into out[w], one CTA per value.
+__global__ void k_fold_partials(const double* __restrict__ part, int count, int width, double* __restrict__ out) {
+    __shared__ double sm[32];
+    const int w = blockIdx.x;
+    double v = 0.;
+    for (int p = threadIdx.x; p < count; p += blockDim.x) v += part[(size_t)p * width + w];
+    v = block_sum(v, sm);
+    if (threadIdx.x == 0) out[w] = v;
+}
+
+// ---------------------------------------------------------------- norm / probabilities
+// mode 0: sum |a|^2 ; mode 1: sum over bit t == 0 ; mode 2: bit t == 1 ;
+// mode 3: marginal (mask/value pair)
+__global__ void __launch_bounds__(kRThreads) k_prob_sum(
+    const double2* __restrict__ s, ITYPE dim, ITYPE mask, ITYPE value, double* __restrict__ part) {
+    __shared__ double sm[32];
+    double acc = 0.;
+    const ITYPE stride = (ITYPE)gridDim.x * kRThreads;
+    for (ITYPE i = (ITYPE)blockIdx.x * kRThreads + threadIdx.x; i < dim; i += stride)
+        if ((i & mask) == value) acc += norm2(ld_stream(s + i));
+    acc = block_sum(acc, sm);
+    if (threadIdx.x == 0) part[blockIdx.x] = acc;
+}
+
+__global__ void __launch_bounds__(kRThreads) k_inner(const double2* __restrict__ a, const double2* __restrict__ b,
+    ITYPE dim, double* __restrict__ part) {
+    __shared__ double sm[32];
+    double re = 0., im = 0.;
+    const ITYPE stride = (ITYPE)gridDim.x * kRThreads;
+    for (ITYPE i = (ITYPE)blockIdx.x * kRThreads + threadIdx.x; i < dim; i += stride) {
+        const double2 x = ld_stream(a + i), y = ld_stream(b + i);
+        re = fma(x.x, y.x, fma(x.y, y.y, re));
+        im = fma(x.x, y.y, fma(-x.y, y.x, im));
+    }
+    re = block_sum(re, sm);
+    im = block_sum(im, sm);
+    if (threadIdx.x == 0) {
+        part[2 * blockIdx.x] = re;
+        part[2 * blockIdx.x + 1] = im;
+    }
+}
+
+static int finish_reduce(double* part, unsigned blocks, int width, cudaStream_t st, double* host_out) {
+    double* fin = part + (size_t)blocks * width;
+    k_fold_partials<<<width, 256, 0, st>>>(part, (int)blocks, width, fin);
+    QS_TRY(check_launch("k_fold_partials"));
+    QS_CUDA_CHECK(cudaMemcpyAsync(host_out, fin, sizeof(double) * width, cudaMemcpyDeviceToHost, st));
+    QS_CUDA_CHECK(cudaStreamSynchronize(st));
+    return QS_OK;
+}
+
+int prob_sum(const double2* s, ITYPE dim, ITYPE mask, ITYPE value, cudaStream_t st, double* out) {
+    const unsigned blocks = reduce_blocks(dim);
+    void* buf;
+    QS_TRY(scratch(st, sizeof(double) * (blocks + 1), &buf));
+    k_prob_sum<<<blocks, kRThreads, 0, st>>>(s, dim, mask, value, (double*)buf);
+    QS_TRY(check_launch("k_prob_sum"));
+    return finish_reduce((double*)buf, blocks, 1, st, out);
+}
+
+// ---------------------------------------------------------------- Pauli expectation values
+struct PauliTerm {
+    ITYPE x, z;
+    UINT nrot, pivot;
+};
+
+__device__ __forceinline__ double phase_re_part(double2 v, UINT r) {
+    // Re(v * i^r)
+    switch (r & 3u) {
+        case 0: return v.x;
+        case 1: return -v.y;
+        case 2: return -v.x;
+        default: return v.y;
+    }
+}
+
+// One term with a bit flip: sum over pivot-0 indices b0 of 2 Re(a[b0] conj(a[b0 ^ x]) i^{nY + 2 par}),
+// stat_ops_expectation_value.cpp:352-373.
+__global__ void __launch_bounds__(kRThreads) k_ev_xz(const double2* __restrict__ s, ITYPE half, PauliTerm t,
+    double* __restrict__ part) {
+    __shared__ double sm[32];
+    double acc = 0.;
+    const ITYPE stride = (ITYPE)gridDim.x * kRThreads;
+    for (ITYPE p = (ITYPE)blockIdx.x * kRThreads + threadIdx.x; p < half; p += stride) {
+        const ITYPE b0 = insert0(p, t.pivot), b1 = b0 ^ t.x;
+        const double2 a0 = ld_stream(s + b0), a1 = ld_stream(s + b1);
+        const double2 v = cmul(a0, cconj(a1));
+        const UINT r = t.nrot + 2u * (UINT)(__popcll(b0 & t.z) & 1);
+        acc += 2.0 * phase_re_part(v, r);
+    }
+    acc = block_sum(acc, sm);
+    if (threadIdx.x == 0) part[blockIdx.x] = acc;
+}
+
+// All Z-only terms in one pass: values[w] = sum |a_i|^2 (-1)^{popcount(i & z_w)}
+// (stat_ops_expectation_value.cpp:467-482).  Partial p of term w at part[p * nz + w].
+template <int MAXZ>
+__global__ void __launch_bounds__(kRThreads) k_ev_z_batch(const double2* __restrict__ s, ITYPE dim,
+    const ITYPE* __restrict__ zmasks, int nz, double* __restrict__ part) {
+    __shared__ double sm[32];
+    __shared__ ITYPE zs[MAXZ];
+    for (int w = threadIdx.x; w < nz; w += kRThreads) zs[w] = zmasks[w];
+    __syncthreads();
+    double acc[MAXZ];
+#pragma unroll
+    for (int w = 0; w < MAXZ; ++w) acc[w] = 0.;
+    const ITYPE stride = (ITYPE)gridDim.x * kRThreads;
+    for (ITYPE i = (ITYPE)blockIdx.x * kRThreads + threadIdx.x; i < dim; i += stride) {
+        const double p = norm2(ld_stream(s + i));
+#pragma unroll
+        for (int w = 0; w < MAXZ; ++w)
+            if (w < nz) acc[w] += (__popcll(i & zs[w]) & 1) ? -p : p;
+    }
+    for (int w = 0; w < nz; ++w) {
+        const double v = block_sum(acc[w], sm);
+        if (threadIdx.x == 0) part[(size_t)blockIdx.x * nz + w] = v;
+    }
+}
+
+// Transition amplitude <bra|P|ket> = sum_i conj(bra[i ^ x]) ph(i) ket[i]  (stat_ops_transition_amplitude.cpp)
+__global__ void __launch_bounds__(kRThreads) k_transition(const double2* __restrict__ bra,
+    const double2* __restrict__ ket, ITYPE dim, PauliTerm t, double* __restrict__ part) {
+    __shared__ double sm[32];
+    double re = 0., im = 0.;
+    const ITYPE stride = (ITYPE)gridDim.x * kRThreads;
+    for (ITYPE i = (ITYPE)blockIdx.x * kRThreads + threadIdx.x; i < dim; i += stride) {
+        const UINT r = (t.nrot + 2u * (UINT)(__popcll(i & t.z) & 1)) & 3u;
+        const double2 ph = make_double2(r == 0 ? 1. : (r == 2 ? -1. : 0.), r == 1 ? 1. : (r == 3 ? -1. : 0.));
+        const double2 v = cmul(cconj(ld_stream(bra + (i ^ t.x))), cmul(ph, ld_stream(ket + i)));
+        re += v.x;
+        im += v.y;
+    }
+    re = block_sum(re, sm);
+    im = block_sum(im, sm);
+    if (threadIdx.x == 0) {
+        part[2 * blockIdx.x] = re;
+        part[2 * blockIdx.x + 1] = im;
+    }
+}
+
+static int pauli_term(const UINT* tl, const UINT* ids, UINT cnt, UINT n, PauliTerm* t) {
+    t->x = t->z = 0;
+    t->nrot = t->pivot = 0;
+    ITYPE seen = 0;
+    for (UINT i = 0; i < cnt; ++i) {
+        QS_TRY(check_target(tl[i], n, "Pauli operator"));
+        if (seen & (1ULL << tl[i])) return set_error(QS_ERR_INVALID_ARGUMENT, "Pauli operator: duplicated qubit");
+        seen |= 1ULL << tl[i];
+        const ITYPE b = 1ULL << tl[i];
+        switch (ids[i]) {
+            case 0: break;
+            case 1: t->x ^= b; t->pivot = tl[i]; break;
+            case 2: t->x ^= b; t->z ^= b; t->nrot++; t->pivot = tl[i]; break;
+            case 3: t->z ^= b; break;
+            default: return set_error(QS_ERR_INVALID_ARGUMENT, "Pauli id must be 0..3");
+        }
+    }
+    return QS_OK;
+}
+
+int ev_batch(const PauliTerm* terms, UINT count, const double2* s, ITYPE dim, cudaStream_t st, double* values) {
+    std::vector<int> zidx, xidx;
+    for (UINT k = 0; k < count; ++k) (terms[k].x == 0 ? zidx : xidx).push_back((int)k);
+    const unsigned blocks = reduce_blocks(dim);
+    constexpr int kZChunk = 16;
+    const size_t part_doubles = (size_t)blocks * std::max<size_t>(kZChunk, 1) + kZChunk + 64;
+    void* buf;
+    QS_TRY(scratch(st, sizeof(double) * part_doubles + sizeof(ITYPE) * kZChunk + 1024, &buf));
+    double* part = (double*)buf;
+    ITYPE* dz = (ITYPE*)((char*)buf + sizeof(double) * part_doubles);
+    // Z-only terms: kZChunk per pass.
+    for (size_t c0 = 0; c0 < zidx.size(); c0 += kZChunk) {
+        const int nz = (int)std::min<size_t>(kZChunk, zidx.size() - c0);
+        ITYPE hz[kZChunk];
+        for (int w = 0; w < nz; ++w) hz[w] = terms[zidx[c0 + w]].z;
+        QS_CUDA_CHECK(cudaMemcpyAsync(dz, hz, sizeof(ITYPE) * nz, cudaMemcpyHostToDevice, st));
+        k_ev_z_batch<kZChunk><<<blocks, kRThreads, 0, st>>>(s, dim, dz, nz, part);
+        QS_TRY(check_launch("k_ev_z_batch"));
+        double out[kZChunk];
+        QS_TRY(finish_reduce(part, blocks, nz, st, out));
+        for (int w = 0; w < nz; ++w) values[zidx[c0 + w]] = out[w];
+    }
+    const unsigned xblocks = reduce_blocks(dim / 2);
+    for (int k : xidx) {
+        k_ev_xz<<<xblocks, kRThreads, 0, st>>>(s, dim / 2, terms[k], part);
+        QS_TRY(check_launch("k_ev_xz"));
+        QS_TRY(finish_reduce(part, xblocks, 1, st, &values[k]));
+    }
+    return QS_OK;
+}
+
+// ---------------------------------------------------------------- sampling
+// Prefix structure: chunks of kChunk amplitudes; chunk sums (FP64, fixed order), then an inclusive
+// scan of the chunk sums by one CTA.  Per shot one warp binary-searches the chunk scan and re-scans
+// its chunk serially from the chunk's exclusive prefix, mirroring the reference's serial running
+// sum (cppsim/state.hpp:917-922) inside the chunk.
+constexpr int kChunk = 2048;
+
+// diag_stride: 0 = state vector (p_i = |a_i|^2); otherwise density matrix with p_i = |rho[i*(dim+1)]|.
+__device__ __forceinline__ double prob_at(const double2* s, ITYPE i, ITYPE diag_stride) {
+    if (diag_stride == 0) return norm2(s[i]);
+    const double2 v = s[i * diag_stride];
+    return sqrt(norm2(v));
+}
+
+__global__ void __launch_bounds__(256) k_chunk_sums(const double2* __restrict__ s, ITYPE dim, ITYPE diag_stride,
+    double* __restrict__ sums) {
+    __shared__ double sm[32];
+    const ITYPE c0 = (ITYPE)blockIdx.x * kChunk;
+    double acc = 0.;
+    for (int j = threadIdx.x; j < kChunk; j += 256)
+        if (c0 + j < dim) acc += prob_at(s, c0 + j, diag_stride);
+    acc = block_sum(acc, sm);
+    if (threadIdx.x == 0) sums[blockIdx.x] = acc;
+}
+
+// Inclusive scan of n values by one CTA of 1024 threads: thread t owns a contiguous range.
+__global__ void __launch_bounds__(1024) k_scan_sums(const double* __restrict__ sums, ITYPE n, double* __restrict__ incl) {
+    __shared__ double part[1024];
+    const ITYPE per = (n + 1023) / 1024;
+    const ITYPE lo = (ITYPE)threadIdx.x * per, hi = min(n, lo + per);
+    double acc = 0.;
+    for (ITYPE i = lo; i < hi; ++i) acc += sums[i];
+    part[threadIdx.x] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double run = 0.;
+        for (int t = 0; t < 1024; ++t) {
+            const double v = part[t];
+            part[t] = run;  // exclusive offset of thread t
+            run += v;
+        }
+    }
+    __syncthreads();
+    double run = part[threadIdx.x];
+    for (ITYPE i = lo; i < hi; ++i) {
+        run += sums[i];
+        incl[i] = run;
+    }
+}
+
+// One warp per shot.
+__global__ void k_sample(const double2* __restrict__ s, ITYPE dim, ITYPE diag_stride, const double* __restrict__ incl,
+    ITYPE nchunks, const double* __restrict__ uniforms, UINT count, ITYPE* __restrict__ out) {
+    const int lane = threadIdx.x & 31;
+    const UINT shot = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (shot >= count) return;
+    const double r = uniforms[shot];
+    if (!(r > 0.)) {  // lower_bound hits stacked_prob[0] = 0 -> index -1
+        if (lane == 0) out[shot] = ~0ULL;
+        return;
+    }
+    if (r > incl[nchunks - 1]) {  // past the total -> index dim
+        if (lane == 0) out[shot] = dim;
+        return;
+    }
+    // first chunk c with incl[c] >= r
+    ITYPE lo = 0, hi = nchunks - 1;
+    while (lo < hi) {
+        const ITYPE mid = lo + (hi - lo) / 2;
+        if (incl[mid] < r) lo = mid + 1;
+        else hi = mid;
+    }
+    const ITYPE c = lo;
+    const double base = c ? incl[c - 1] : 0.;
+    // lane-local sums of 64 consecutive probabilities, exclusive warp scan in lane order
+    const ITYPE c0 = c * kChunk + (ITYPE)lane * (kChunk / 32);
+    double lsum = 0.;
+    for (int j = 0; j < kChunk / 32; ++j)
+        if (c0 + j < dim) lsum += prob_at(s, c0 + j, diag_stride);
+    double excl = 0.;
+    for (int l = 0; l < 32; ++l) {
+        const double v = __shfl_sync(0xffffffffu, lsum, l);
+        if (l < lane) excl += v;
+    }
+    const double start = base + excl;
+    const double end = start + lsum;
+    // the first lane whose running end reaches r owns the answer
+    const unsigned ball = __ballot_sync(0xffffffffu, end >= r);
+    const int owner = ball ? __ffs(ball) - 1 : 31;
+    if (lane == owner) {
+        double run = start;
+        ITYPE idx = c0 + kChunk / 32 - 1;
+        for (int j = 0; j < kChunk / 32; ++j) {
+            if (c0 + j >= dim) break;
+            run += prob_at(s, c0 + j, diag_stride);
+            if (run >= r) {
+                idx = c0 + j;
+                break;
+            }
+        }
+        out[shot] = idx < dim ? idx : dim - 1;
+    }
+}
+
+int sample_with_uniforms(const double2* s, ITYPE dim, ITYPE diag_stride, const double* uniforms, UINT count,
+    ITYPE* out, cudaStream_t st) {
+    if (count == 0) return QS_OK;
+    const ITYPE nchunks = (dim + kChunk - 1) / kChunk;
+    const size_t bytes = sizeof(double) * (2 * nchunks + count) + sizeof(ITYPE) * count + 1024;
+    void* buf;
+    QS_TRY(scratch(st, bytes, &buf));
+    double* sums = (double*)buf;
+    double* incl = sums + nchunks;
+    double* du = incl + nchunks;
+    ITYPE* dout = (ITYPE*)(du + count);
+    QS_CUDA_CHECK(cudaMemcpyAsync(du, uniforms, sizeof(double) * count, cudaMemcpyHostToDevice, st));
+    k_chunk_sums<<<(unsigned)nchunks, 256, 0, st>>>(s, dim, diag_stride, sums);
+    QS_TRY(check_launch("k_chunk_sums"));
+    k_scan_sums<<<1, 1024, 0, st>>>(sums, nchunks, incl);
+    QS_TRY(check_launch("k_scan_sums"));
+    const unsigned threads = 256;
+    const unsigned blocks = (unsigned)(((ITYPE)count * 32 + threads - 1) / threads);
+    k_sample<<<blocks, threads, 0, st>>>(s, dim, diag_stride, incl, nchunks, du, count, dout);
+    QS_TRY(check_launch("k_sample"));
+    QS_CUDA_CHECK(cudaMemcpyAsync(out, dout, sizeof(ITYPE) * count, cudaMemcpyDeviceToHost, st));
+    QS_CUDA_CHECK(cudaStreamSynchronize(st));
+    return QS_OK;
+}
+
+// Reference RNG (cppsim/utility.hpp:54-80): mt19937_64 seeded with the seed, uniform_real_distribution(0, 1).
+void reference_uniforms(UINT seed, UINT count, std::vector<double>* u) {
+    std::mt19937_64 mt;
+    mt.seed(seed);
+    std::uniform_real_distribution<double> dist(0, 1);
+    u->resize(count);
+    for (UINT c = 0; c < count; ++c) (*u)[c] = dist(mt);
+}
+
+}  // namespace qs
+
+using namespace qs;
+
+extern "C" {
+
+QS_API int qs_state_norm_squared(const void* state, QS_ITYPE dim, void* stream, double* out) {
+    UINT n;
+    QS_TRY(check_dim(dim, &n));
+    return prob_sum((const double2*)state, dim, 0, 0, (cudaStream_t)stream, out);
+}
+QS_API int qs_M0_prob(QS_UINT t, const void* state, QS_ITYPE dim, void* stream, double* out) {
+    UINT n;
+    QS_TRY(check_dim(dim, &n));
+    QS_TRY(check_target(t, n, "M0_prob"));
+    return prob_sum((const double2*)state, dim, 1ULL << t, 0, (cudaStream_t)stream, out);
+}
+QS_API int qs_M1_prob(QS_UINT t, const void* state, QS_ITYPE dim, void* stream, double* out) {
+    UINT n;
+    QS_TRY(check_dim(dim, &n));
+    QS_TRY(check_target(t, n, "M1_prob"));
+    return prob_sum((const double2*)state, dim, 1ULL << t, 1ULL << t, (cudaStream_t)stream, out);
+}
+QS_API int qs_marginal_prob(const QS_UINT* tl, const QS_UINT* vals, QS_UINT cnt, const void* state,
+    QS_ITYPE dim, void* stream, double* out) {
+    UINT n;
+    QS_TRY(check_dim(dim, &n));
+    QS_TRY(check_distinct(tl, cnt, n, "marginal_prob"));
+    ITYPE mask = 0, value = 0;
+    for (UINT i = 0; i < cnt; ++i) {
+        if (vals[i] > 1) return set_error(QS_ERR_INVALID_ARGUMENT, "marginal_prob: value must be 0 or 1");
+        mask |= 1ULL << tl[i];
+        if (vals[i]) value |= 1ULL << tl[i];
+    }
+    return prob_sum((const double2*)state, dim, mask, value, (cudaStream_t)stream, out);
+}
+
+QS_API int qs_state_inner_product(const void* bra, const void* ket, QS_ITYPE dim, void* stream, double out[2]) {
+    UINT n;
+    QS_TRY(check_dim(dim, &n));
+    cudaStream_t st = (cudaStream_t)stream;
+    const unsigned blocks = reduce_blocks(dim);
+    void* buf;
+    QS_TRY(scratch(st, sizeof(double) * (2 * blocks + 2), &buf));
+    k_inner<<<blocks, kRThreads, 0, st>>>((const double2*)bra, (const double2*)ket, dim, (double*)buf);
+    QS_TRY(check_launch("k_inner"));
+    return finish_reduce((double*)buf, blocks, 2, st, out);
+}
+
+QS_API int qs_expectation_value_multi_qubit_Pauli_operator_partial_list(const QS_UINT* tl, const QS_UINT* ids,
+    QS_UINT cnt, const void* state, QS_ITYPE dim, void* stream, double* out) {
+    UINT n;
+    QS_TRY(check_dim(dim, &n));
+    PauliTerm t;
+    QS_TRY(pauli_term(tl, ids, cnt, n, &t));
+    return ev_batch(&t, 1, (const double2*)state, dim, (cudaStream_t)stream, out);
+}
+
+QS_API int qs_expectation_value_pauli_batch(const QS_ITYPE* x_masks, const QS_ITYPE* z_masks, const QS_UINT* y_counts,
+    QS_UINT term_count, const void* state, QS_ITYPE dim, void* stream, double* values) {
+    UINT n;
+    QS_TRY(check_dim(dim, &n));
+    std::vector<PauliTerm> terms(term_count);
+    for (UINT k = 0; k < term_count; ++k) {
+        if ((x_masks[k] | z_masks[k]) >> n)
+            return set_error(QS_ERR_INVALID_ARGUMENT, "expectation_value_pauli_batch: mask beyond qubit count");
+        terms[k].x = x_masks[k];
+        terms[k].z = z_masks[k];
+        terms[k].nrot = y_counts[k];
+        terms[k].pivot = x_masks[k] ? (UINT)(63 - __builtin_clzll(x_masks[k])) : 0;
+    }
+    return ev_batch(terms.data(), term_count, (const double2*)state, dim, (cudaStream_t)stream, values);
+}
+
+QS_API int qs_transition_amplitude_multi_qubit_Pauli_operator_partial_list(const QS_UINT* tl, const QS_UINT* ids,
+    QS_UINT cnt, const void* bra, const void* ket, QS_ITYPE dim, void* stream, double out[2]) {
+    UINT n;
+    QS_TRY(check_dim(dim, &n));
+    PauliTerm t;
+    QS_TRY(pauli_term(tl, ids, cnt, n, &t));
+    cudaStream_t st = (cudaStream_t)stream;
+    const unsigned blocks = reduce_blocks(dim);
+    void* buf;
+    QS_TRY(scratch(st, sizeof(double) * (2 * blocks + 2), &buf));
+    k_transition<<<blocks, kRThreads, 0, st>>>((const double2*)bra, (const double2*)ket, dim, t, (double*)buf);
+    QS_TRY(check_launch("k_transition"));
+    return finish_reduce((double*)buf, blocks, 2, st, out);
+}
+
+QS_API int qs_state_sampling_with_uniforms(const void* state, QS_ITYPE dim, const double* uniforms,
+    QS_UINT count, QS_ITYPE* out, void* stream) {
+    UINT n;
+    QS_TRY(check_dim(dim, &n));
+    return sample_with_uniforms((const double2*)state, dim, 0, uniforms, count, out, (cudaStream_t)stream);
+}
+
+QS_API int qs_state_sampling(const void* state, QS_ITYPE dim, QS_UINT count, QS_UINT seed, QS_ITYPE* out,
+    void* stream) {
+    std::vector<double> u;
+    reference_uniforms(seed, count, &u);
+    return qs_state_sampling_with_uniforms(state, dim, u.data(), count, out, stream);
+}
+
+QS_API int qs_reference_uniforms(QS_UINT seed, QS_UINT count, double* out) {
+    if (!out && count) return set_error(QS_ERR_INVALID_ARGUMENT, "null output pointer");
+    std::vector<double> u;
+    reference_uniforms(seed, count, &u);
+    for (UINT c = 0; c < count; ++c) out[c] = u[c];
+    return QS_OK;
+}
+
+}  // extern "C"

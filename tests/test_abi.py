@@ -1,0 +1,91 @@
+"""The C-ABI library loads, exports every declared symbol, and validates arguments on the host
+(these checks return before any CUDA call, so they run without a GPU)."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+from qulacs_b200 import _lib
+
+
+def declared_symbols():
+    names = []
+    for fn in sorted(os.listdir(os.path.join(ROOT, "include"))):
+        if fn.endswith(".h"):
+            txt = open(os.path.join(ROOT, "include", fn)).read()
+            names += re.findall(r"QS_API\s+[\w\s\*]+?\b(qs_\w+)\s*\(", txt)
+    return names
+
+
+def test_library_exports_every_declared_symbol(lib):
+    names = declared_symbols()
+    assert len(names) > 60
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_python_binding_covers_header():
+    names = set(declared_symbols())
+    assert names <= set(_lib.SIGNATURES), sorted(names - set(_lib.SIGNATURES))
+
+
+def test_version(lib):
+    assert b"sm_100a" in lib.qs_version()
+
+
+def test_invalid_dim_rejected_on_host(lib):
+    m = np.eye(2, dtype=np.complex128)
+    rc = lib.qs_single_qubit_dense_matrix_gate(0, m.ctypes.data_as(C.c_void_p), None, 3, None)
+    assert rc == 1  # QS_ERR_INVALID_ARGUMENT
+    assert b"power of two" in lib.qs_get_last_error()
+
+
+def test_target_out_of_range_rejected(lib):
+    m = np.eye(2, dtype=np.complex128)
+    rc = lib.qs_single_qubit_dense_matrix_gate(7, m.ctypes.data_as(C.c_void_p), None, 1 << 4, None)
+    assert rc == 1
+    assert b"qubit index 7" in lib.qs_get_last_error()
+
+
+def test_duplicate_targets_rejected(lib):
+    tl = np.array([1, 1], dtype=np.uint32)
+    m = np.eye(4, dtype=np.complex128)
+    rc = lib.qs_multi_qubit_dense_matrix_gate(tl.ctypes.data_as(C.c_void_p), 2, m.ctypes.data_as(C.c_void_p),
+                                              None, 1 << 4, None)
+    assert rc == 1
+    assert b"duplicated" in lib.qs_get_last_error()
+
+
+def test_dense_k_limit(lib):
+    tl = np.arange(7, dtype=np.uint32)
+    m = np.eye(128, dtype=np.complex128)
+    rc = lib.qs_multi_qubit_dense_matrix_gate(tl.ctypes.data_as(C.c_void_p), 7, m.ctypes.data_as(C.c_void_p),
+                                              None, 1 << 8, None)
+    assert rc == 5  # QS_ERR_NOT_SUPPORTED
+
+
+def test_circuit_host_validation(lib):
+    h = C.c_void_p()
+    assert lib.qs_circuit_create(4, C.byref(h)) == 0
+    t = np.array([0, 9], dtype=np.uint32)
+    rc = lib.qs_circuit_add_gate(h, 5, t.ctypes.data_as(C.c_void_p), 2, None, None, 0, None, 0)
+    assert rc == 1
+    t = np.array([0, 1], dtype=np.uint32)
+    assert lib.qs_circuit_add_gate(h, 5, t.ctypes.data_as(C.c_void_p), 2, None, None, 0, None, 0) == 0
+    cnt = C.c_uint()
+    assert lib.qs_circuit_gate_count(h, C.byref(cnt)) == 0 and cnt.value == 1
+    # wrong state dimension is refused before touching the device
+    assert lib.qs_circuit_update_quantum_state(h, None, 1 << 5, 0, None) == 1
+    assert lib.qs_circuit_destroy(h) == 0
+
+
+def test_python_errors_map_to_exceptions():
+    with pytest.raises(ValueError):
+        _lib.check(1, "x")
+    with pytest.raises(MemoryError):
+        _lib.check(2, "x")
+    with pytest.raises(NotImplementedError):
+        _lib.check(5, "x")

@@ -1,0 +1,88 @@
+"""Whole circuits on the B200: the 16-qubit layered circuit against the reference's golden fixture and
+the oracle, every execution mode, and size-independent properties at large n."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import AMP_TOL, BOUNDARY_EPS, EV_TOL, GOLDEN
+from qulacs_b200 import QuantumState
+from qulacs_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+MODES = ["gate_by_gate", "staged"]
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_config1_against_reference_golden(port, mode):
+    g = np.load(os.path.join(GOLDEN, "config1_n16.npz"))
+    n = int(g["n"])
+    gates = W.layered_rotation_circuit(n, int(g["depth"]), int(g["gate_seed"]))
+    circ = W.to_circuit(gates, n)
+    s = QuantumState(n)
+    circ.update_quantum_state(s, mode=mode)
+    v = s.get_vector()
+    assert np.max(np.abs(v[g["amp_index"]] - g["amps"])) <= AMP_TOL
+    # full state against the oracle
+    want = np.zeros(1 << n, dtype=np.complex128)
+    want[0] = 1
+    W.run_on_cpu(gates, want, port)
+    assert np.max(np.abs(v - want)) <= AMP_TOL
+    terms = W.random_pauli_terms(n, 64, 1, 4, int(g["term_seed"]))
+    obs = W.to_observable(terms, n)
+    assert np.max(np.abs(obs.term_values(s) - g["term_values"])) <= EV_TOL
+    assert abs(obs.get_expectation_value(s) - float(g["energy"])) <= EV_TOL
+    u = W.uniforms(1024, int(g["uniform_seed"]))
+    got = s.sampling_with_uniforms(u)
+    _, near = port.sampling_with_uniforms(want, u, eps=BOUNDARY_EPS)
+    assert np.all((got == g["samples"]) | near)
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_u3cz_full_state_golden(mode):
+    g = np.load(os.path.join(GOLDEN, "u3cz_n10.npz"))
+    n = int(g["n"])
+    circ = W.to_circuit(W.u3_cz_circuit(n, int(g["layers"]), int(g["gate_seed"])), n)
+    s = QuantumState(n)
+    circ.update_quantum_state(s, mode=mode)
+    assert np.max(np.abs(s.get_vector() - g["state"])) <= AMP_TOL
+
+
+@pytest.mark.parametrize("n", [5, 13, 19])
+@pytest.mark.parametrize("mode", MODES)
+def test_random_circuits_against_oracle(port, n, mode):
+    rng = np.random.default_rng(1000 + n)
+    gates = W.layered_rotation_circuit(n, 3, seed=n) + W.u3_cz_circuit(n, 3, seed=n + 1) + W.hea_circuit(n, 2, n + 2)
+    for _ in range(20):  # dense blocks on random qubits
+        k = int(rng.integers(2, min(6, n) + 1))
+        tl = tuple(int(x) for x in rng.choice(n, size=k, replace=False))
+        a = rng.normal(size=(1 << k, 1 << k)) + 1j * rng.normal(size=(1 << k, 1 << k))
+        q, _ = np.linalg.qr(a)
+        gates.append(("DENSE", tl, q))
+    circ = W.to_circuit(gates, n)
+    s = QuantumState(n)
+    circ.update_quantum_state(s, mode=mode)
+    want = np.zeros(1 << n, dtype=np.complex128)
+    want[0] = 1
+    W.run_on_cpu(gates, want, port)
+    assert np.max(np.abs(s.get_vector() - want)) <= AMP_TOL
+
+
+@pytest.mark.parametrize("n", [26])
+def test_large_circuit_properties(n):
+    """At sizes beyond the oracle: norm is preserved, and circuit followed by its inverse returns |0>."""
+    gates = W.layered_rotation_circuit(n, 2, seed=77)
+    inv = []
+    for g in reversed(gates):
+        if g[0] in ("RX", "RY", "RZ"):
+            inv.append((g[0], g[1], -g[2]))
+        else:
+            inv.append(g)
+    for mode in MODES:
+        s = QuantumState(n)
+        W.to_circuit(gates, n).update_quantum_state(s, mode=mode)
+        assert abs(s.get_squared_norm() - 1.0) <= 1e-12
+        W.to_circuit(inv, n).update_quantum_state(s, mode=mode)
+        assert abs(s.get_zero_probability(0) - 1.0) <= 1e-12
+        assert abs(s.get_marginal_probability([0] * n) - 1.0) <= 1e-12

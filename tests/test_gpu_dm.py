@@ -1,0 +1,70 @@
+"""Density-matrix kernels on the B200 against the oracle and the reference golden fixture."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import AMP_TOL, EV_TOL, GOLDEN, random_density_matrix, random_unitary
+from qulacs_b200 import DensityMatrix, QuantumState, gate as G
+from qulacs_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def dev(rho):
+    d = DensityMatrix(int(np.log2(rho.shape[0])))
+    d.load(rho)
+    return d
+
+
+def test_dm_gates_and_channels(port):
+    rng = np.random.default_rng(1100)
+    n = 5
+    rho0 = random_density_matrix(n, rng)
+    cases = [
+        (G.DenseMatrix(3, random_unitary(1, rng)), lambda r, g: port.dm_single_qubit_dense_matrix_gate(3, g.get_matrix(), r)),
+        (G.DenseMatrix([4, 1], random_unitary(2, rng)), lambda r, g: port.dm_multi_qubit_dense_matrix_gate([4, 1], g.get_matrix(), r)),
+        (G.DenseMatrix([0, 2, 4], random_unitary(3, rng)), lambda r, g: port.dm_multi_qubit_dense_matrix_gate([0, 2, 4], g.get_matrix(), r)),
+        (G.DenseMatrix([0, 1, 2, 4], random_unitary(4, rng)), lambda r, g: port.dm_multi_qubit_dense_matrix_gate([0, 1, 2, 4], g.get_matrix(), r)),
+        (G.CNOT(4, 0), lambda r, g: port.dm_CNOT_gate(4, 0, r)),
+        (G.CZ(1, 3), lambda r, g: port.dm_CZ_gate(1, 3, r)),
+        (G.RX(2, 0.4), lambda r, g: port.dm_single_qubit_dense_matrix_gate(2, W.rotation_matrix("RX", 0.4), r)),
+        (G.DepolarizingNoise(1, 0.05), lambda r, g: port.dm_depolarizing_noise(1, 0.05, r)),
+        (G.TwoQubitDepolarizingNoise(3, 0, 0.07), lambda r, g: port.dm_two_qubit_depolarizing_noise(3, 0, 0.07, r)),
+    ]
+    for gate, oracle_fn in cases:
+        want = rho0.copy()
+        oracle_fn(want, gate)
+        d = dev(rho0)
+        gate.update_quantum_state(d)
+        assert np.max(np.abs(d.get_matrix() - want)) <= AMP_TOL, gate
+
+
+def test_noisy_circuit_golden_and_stats(port):
+    g = np.load(os.path.join(GOLDEN, "noisy_dm_n5.npz"))
+    n = int(g["n"])
+    gates = W.noisy_circuit(W.hea_circuit(n, int(g["depth"]), int(g["gate_seed"])), float(g["p"]))
+    d = DensityMatrix(n)
+    W.to_circuit(gates, n).update_quantum_state(d)
+    rho = d.get_matrix()
+    assert np.max(np.abs(rho - g["rho"])) <= AMP_TOL
+    terms = W.random_pauli_terms(n, 16, 1, 3, int(g["term_seed"]))
+    obs = W.to_observable(terms, n)
+    assert np.max(np.abs(obs.term_values(d) - g["term_values"])) <= EV_TOL
+    assert abs(d.get_squared_norm() - 1.0) <= 1e-12
+    u = np.random.default_rng(5).random(512)
+    assert np.array_equal(d.sampling_with_uniforms(u), port.dm_sampling_with_uniforms(rho, u))
+
+
+def test_pure_state_density_matrix_matches_state_vector(port):
+    n = 6
+    s = QuantumState(n)
+    circ = W.to_circuit(W.hea_circuit(n, 3, seed=9), n)
+    circ.update_quantum_state(s)
+    d = DensityMatrix(n)
+    W.to_circuit(W.hea_circuit(n, 3, seed=9), n).update_quantum_state(d)
+    v = s.get_vector()
+    assert np.max(np.abs(d.get_matrix() - np.outer(v, v.conj()))) <= AMP_TOL
+    d2 = DensityMatrix(n)
+    d2.load(s)
+    assert np.max(np.abs(d2.get_matrix() - np.outer(v, v.conj()))) <= AMP_TOL
