@@ -68,7 +68,7 @@ struct OpZero {
 // One amplitude per item: index = expand(item) | fixed.
 template <class OP, int ITEMS>
 __global__ void __launch_bounds__(kThreads) k_single(
-    double2* __restrict__ s, ITYPE items, Positions pos, ITYPE fixed, OP op) {
+    double2* __restrict__ s, ITYPE items, const __grid_constant__ Positions pos, ITYPE fixed, OP op) {
     const ITYPE base = (ITYPE)blockIdx.x * (kThreads * ITEMS) + threadIdx.x;
     ITYPE idx[ITEMS];
     double2 v[ITEMS];
@@ -90,7 +90,7 @@ __global__ void __launch_bounds__(kThreads) k_single(
 // Two amplitudes per item: b = expand(item); (b | off0, b | off1).
 template <class OP, int ITEMS>
 __global__ void __launch_bounds__(kThreads) k_pair(
-    double2* __restrict__ s, ITYPE items, Positions pos, ITYPE off0, ITYPE off1, OP op) {
+    double2* __restrict__ s, ITYPE items, const __grid_constant__ Positions pos, ITYPE off0, ITYPE off1, OP op) {
     const ITYPE base = (ITYPE)blockIdx.x * (kThreads * ITEMS) + threadIdx.x;
     ITYPE b[ITEMS];
     double2 v0[ITEMS], v1[ITEMS];
@@ -155,7 +155,7 @@ __global__ void __launch_bounds__(kThreads) k_diag1(double2* __restrict__ s, ITY
 }
 
 // Elementwise diagonal on k qubits: a[i] *= diag[bits of i at targets].
-__global__ void __launch_bounds__(kThreads) k_diagK(double2* __restrict__ s, ITYPE dim, Positions tl,
+__global__ void __launch_bounds__(kThreads) k_diagK(double2* __restrict__ s, ITYPE dim, const __grid_constant__ Positions tl,
     const double2* __restrict__ diag) {
     const ITYPE stride = (ITYPE)gridDim.x * kThreads;
     for (ITYPE i = (ITYPE)blockIdx.x * kThreads + threadIdx.x; i < dim; i += stride) {
@@ -167,7 +167,7 @@ __global__ void __launch_bounds__(kThreads) k_diagK(double2* __restrict__ s, ITY
 
 // Two-qubit dense on quads: b = expand(item) | fixed, amplitudes b | off[j], j in 0..3.
 template <int ITEMS>
-__global__ void __launch_bounds__(kThreads) k_dense2(double2* __restrict__ s, ITYPE items, Positions pos,
+__global__ void __launch_bounds__(kThreads) k_dense2(double2* __restrict__ s, ITYPE items, const __grid_constant__ Positions pos,
     ITYPE fixed, ITYPE m1, ITYPE m2, Mat4 m) {
     const ITYPE base = (ITYPE)blockIdx.x * (kThreads * ITEMS) + threadIdx.x;
     const ITYPE off[4] = {0, m1, m2, m1 | m2};
@@ -193,7 +193,7 @@ __global__ void __launch_bounds__(kThreads) k_dense2(double2* __restrict__ s, IT
 // (2048 amplitudes, 32 KiB) in shared memory, then every thread computes outputs (y, c) with the
 // warp sharing the matrix row y (a broadcast read) and reading consecutive cosets c.
 constexpr int kDenseTile = 2048;
-__global__ void __launch_bounds__(kThreads) k_denseK(double2* __restrict__ s, ITYPE cosets, Positions pos,
+__global__ void __launch_bounds__(kThreads) k_denseK(double2* __restrict__ s, ITYPE cosets, const __grid_constant__ Positions pos,
     ITYPE fixed, int k, const UINT* __restrict__ tgt, const double2* __restrict__ mat) {
     extern __shared__ double2 tile[];
     __shared__ ITYPE masks[64];

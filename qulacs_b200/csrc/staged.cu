@@ -1,0 +1,612 @@
+// Staged executor: several gates per HBM pass, each gate applied with its own (unfused) arithmetic.
+//
+// A pass owns a set Q of m "tile qubits" (always including qubits 0..3, so every HBM access is a
+// run of >= 16 contiguous amplitudes = 256 B).  Each CTA loads one tile -- the 2^m amplitudes that
+// share the values of the other n - m qubits -- into shared memory, applies every gate of the pass
+// (all of whose qubits lie in Q), and writes the tile back: one read and one write of the state per
+// pass instead of one per gate.  Inside the tile, gates are grouped into "phases" of at most 4 tile
+// qubits: each thread gathers the 16 amplitudes of its 4-qubit coset into registers, applies all the
+// phase's gates there, and scatters them back, so shared memory is touched once per phase, not once
+// per gate.  The host scheduler (below) builds passes and phases greedily from the gate list; a gate
+// is only moved past gates on disjoint qubits, so the result equals gate-by-gate application up to
+// rounding order (~1e-16).  Gates the pass kernel does not cover (more than 2 targets, controls,
+// Pauli strings, multi-qubit diagonals) run between passes with the gate-by-gate kernels.
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <vector>
+
+#include "circuit.hpp"
+#include "qs_internal.cuh"
+
+namespace qs {
+
+constexpr int kLowFixed = 4;      // qubits 0..3 always belong to a tile
+constexpr int kTileBits = 11;     // 2^11 amplitudes = 32 KiB of shared memory per CTA
+constexpr int kStThreads = 128;   // 2^11 / 16 amplitudes per thread
+constexpr int kPhaseBits = 4;     // 16 amplitudes in registers per thread
+
+enum StKind : uint8_t { ST_DENSE1 = 0, ST_DIAG1, ST_RX, ST_RY, ST_CNOT, ST_CZ, ST_SWAP, ST_DENSE2 };
+
+struct StOp {
+    uint8_t kind, a, b, pad;  // a, b: register-bit indices 0..3 within the phase
+    uint32_t param;           // index into the parameter pool (double2)
+};
+struct StPhase {
+    uint8_t bits[4];  // tile-local bit positions, ascending
+    uint32_t op_begin, op_count;
+};
+struct StPassArgs {
+    int m;                 // tile bits (<= kTileBits)
+    int nphases;
+    UINT q[kTileBits];     // global qubit of tile bit j, ascending, q[j] = j for j < kLowFixed
+    const StPhase* phases;
+    const StOp* ops;
+    const double2* pool;
+};
+
+// ---------------------------------------------------------------- register ops
+template <int B>
+__device__ __forceinline__ void r_dense1(double2 (&r)[16], const double2* __restrict__ p) {
+    const double2 m0 = p[0], m1 = p[1], m2 = p[2], m3 = p[3];
+#pragma unroll
+    for (int j = 0; j < 16; ++j)
+        if (!(j & (1 << B))) {
+            const double2 x = r[j], y = r[j | (1 << B)];
+            r[j] = cfma(m1, y, cmul(m0, x));
+            r[j | (1 << B)] = cfma(m3, y, cmul(m2, x));
+        }
+}
+template <int B>
+__device__ __forceinline__ void r_diag1(double2 (&r)[16], const double2* __restrict__ p) {
+    const double2 d0 = p[0], d1 = p[1];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) r[j] = cmul((j & (1 << B)) ? d1 : d0, r[j]);
+}
+// RX: {c, i s; i s, c}
+template <int B>
+__device__ __forceinline__ void r_rx(double2 (&r)[16], const double2* __restrict__ p) {
+    const double c = p[0].x, s = p[0].y;
+#pragma unroll
+    for (int j = 0; j < 16; ++j)
+        if (!(j & (1 << B))) {
+            const double2 x = r[j], y = r[j | (1 << B)];
+            r[j] = make_double2(fma(c, x.x, -s * y.y), fma(c, x.y, s * y.x));
+            r[j | (1 << B)] = make_double2(fma(c, y.x, -s * x.y), fma(c, y.y, s * x.x));
+        }
+}
+// RY: {c, s; -s, c}
+template <int B>
+__device__ __forceinline__ void r_ry(double2 (&r)[16], const double2* __restrict__ p) {
+    const double c = p[0].x, s = p[0].y;
+#pragma unroll
+    for (int j = 0; j < 16; ++j)
+        if (!(j & (1 << B))) {
+            const double2 x = r[j], y = r[j | (1 << B)];
+            r[j] = make_double2(fma(c, x.x, s * y.x), fma(c, x.y, s * y.y));
+            r[j | (1 << B)] = make_double2(fma(c, y.x, -s * x.x), fma(c, y.y, -s * x.y));
+        }
+}
+template <int C, int T>
+__device__ __forceinline__ void r_cnot(double2 (&r)[16]) {
+#pragma unroll
+    for (int j = 0; j < 16; ++j)
+        if ((j & (1 << C)) && !(j & (1 << T))) {
+            const double2 t = r[j];
+            r[j] = r[j | (1 << T)];
+            r[j | (1 << T)] = t;
+        }
+}
+template <int A, int B>
+__device__ __forceinline__ void r_cz(double2 (&r)[16]) {
+#pragma unroll
+    for (int j = 0; j < 16; ++j)
+        if ((j & (1 << A)) && (j & (1 << B))) r[j] = make_double2(-r[j].x, -r[j].y);
+}
+template <int A, int B>
+__device__ __forceinline__ void r_swap(double2 (&r)[16]) {
+#pragma unroll
+    for (int j = 0; j < 16; ++j)
+        if ((j & (1 << A)) && !(j & (1 << B))) {
+            const int k = j ^ (1 << A) ^ (1 << B);
+            const double2 t = r[j];
+            r[j] = r[k];
+            r[k] = t;
+        }
+}
+// matrix-index bit 0 <-> register bit A (first target), bit 1 <-> B
+template <int A, int B>
+__device__ __forceinline__ void r_dense2(double2 (&r)[16], const double2* __restrict__ p) {
+#pragma unroll
+    for (int j = 0; j < 16; ++j)
+        if (!(j & (1 << A)) && !(j & (1 << B))) {
+            const int o[4] = {j, j | (1 << A), j | (1 << B), j | (1 << A) | (1 << B)};
+            double2 v[4];
+#pragma unroll
+            for (int x = 0; x < 4; ++x) v[x] = r[o[x]];
+#pragma unroll
+            for (int y = 0; y < 4; ++y) {
+                double2 acc = cmul(p[y * 4], v[0]);
+#pragma unroll
+                for (int x = 1; x < 4; ++x) acc = cfma(p[y * 4 + x], v[x], acc);
+                r[o[y]] = acc;
+            }
+        }
+}
+
+template <int A>
+__device__ __forceinline__ void dispatch1(uint8_t kind, double2 (&r)[16], const double2* p) {
+    switch (kind) {
+        case ST_DENSE1: r_dense1<A>(r, p); break;
+        case ST_DIAG1: r_diag1<A>(r, p); break;
+        case ST_RX: r_rx<A>(r, p); break;
+        case ST_RY: r_ry<A>(r, p); break;
+        default: break;
+    }
+}
+template <int A, int B>
+__device__ __forceinline__ void dispatch2ab(uint8_t kind, double2 (&r)[16], const double2* p) {
+    switch (kind) {
+        case ST_CNOT: r_cnot<A, B>(r); break;
+        case ST_CZ: r_cz<A, B>(r); break;
+        case ST_SWAP: r_swap<A, B>(r); break;
+        case ST_DENSE2: r_dense2<A, B>(r, p); break;
+        default: break;
+    }
+}
+template <int A>
+__device__ __forceinline__ void dispatch2a(uint8_t kind, int b, double2 (&r)[16], const double2* p) {
+    switch (b) {
+        case 0: if (A != 0) dispatch2ab<A, (A != 0 ? 0 : 1)>(kind, r, p); break;
+        case 1: if (A != 1) dispatch2ab<A, (A != 1 ? 1 : 0)>(kind, r, p); break;
+        case 2: if (A != 2) dispatch2ab<A, (A != 2 ? 2 : 0)>(kind, r, p); break;
+        default: if (A != 3) dispatch2ab<A, (A != 3 ? 3 : 0)>(kind, r, p); break;
+    }
+}
+__device__ __forceinline__ void apply_op(const StOp& op, double2 (&r)[16], const double2* pool) {
+    const double2* p = pool + op.param;
+    if (op.kind <= ST_RY) {
+        switch (op.a) {
+            case 0: dispatch1<0>(op.kind, r, p); break;
+            case 1: dispatch1<1>(op.kind, r, p); break;
+            case 2: dispatch1<2>(op.kind, r, p); break;
+            default: dispatch1<3>(op.kind, r, p); break;
+        }
+    } else {
+        switch (op.a) {
+            case 0: dispatch2a<0>(op.kind, op.b, r, p); break;
+            case 1: dispatch2a<1>(op.kind, op.b, r, p); break;
+            case 2: dispatch2a<2>(op.kind, op.b, r, p); break;
+            default: dispatch2a<3>(op.kind, op.b, r, p); break;
+        }
+    }
+}
+
+// XOR swizzle of the tile index for conflict-free 16-byte shared-memory accesses (linear over XOR,
+// so swz(a | b) = swz(a) ^ swz(b) for disjoint bit sets).
+__device__ __forceinline__ UINT swz(UINT u) { return u ^ (((u >> 4) ^ (u >> 7) ^ (u >> 10)) & 7u); }
+
+__global__ void __launch_bounds__(kStThreads, 3) k_staged_pass(double2* __restrict__ s, const __grid_constant__ StPassArgs a) {
+    __shared__ double2 tile[1 << kTileBits];
+    __shared__ ITYPE hi_off[16];
+    __shared__ UINT s_off[16];
+    const int m = a.m;
+    const UINT tsize = 1u << m;
+    const ITYPE T = blockIdx.x;
+    // base: insert zeros at the tile qubits into the tile index
+    ITYPE base = T;
+    for (int j = 0; j < m; ++j) base = insert0(base, a.q[j]);
+    // global offset of tile index u = tid + k * kStThreads: low part from tid (bits 0..6), high from k
+    const int tid = threadIdx.x;
+    if (tid < 16) {
+        ITYPE o = 0;
+        for (int j = 7; j < m; ++j)
+            if ((tid >> (j - 7)) & 1) o |= 1ULL << a.q[j];
+        hi_off[tid] = o;
+    }
+    ITYPE lo_off = 0;
+    for (int j = 0; j < 7 && j < m; ++j)
+        if ((tid >> j) & 1) lo_off |= 1ULL << a.q[j];
+    __syncthreads();
+    // tile index u = tid + k * kStThreads (16 per thread when m = 11; fewer threads busy when m < 7)
+    {
+        double2 v[16];
+#pragma unroll
+        for (int k = 0; k < 16; ++k)
+            if ((UINT)tid + (UINT)k * kStThreads < tsize) v[k] = ld_stream(s + (base | lo_off | hi_off[k]));
+#pragma unroll
+        for (int k = 0; k < 16; ++k)
+            if ((UINT)tid + (UINT)k * kStThreads < tsize) tile[swz((UINT)tid + (UINT)k * kStThreads)] = v[k];
+    }
+    __syncthreads();
+    const UINT ncos = tsize >> kPhaseBits;  // cosets per phase
+    for (int ph = 0; ph < a.nphases; ++ph) {
+        const StPhase P = a.phases[ph];
+        if (tid < 16) {
+            UINT o = 0;
+#pragma unroll
+            for (int p = 0; p < 4; ++p)
+                if ((tid >> p) & 1) o |= 1u << P.bits[p];
+            s_off[tid] = swz(o);
+        }
+        __syncthreads();
+        for (UINT c = tid; c < ncos; c += kStThreads) {
+            UINT u0 = c;
+#pragma unroll
+            for (int p = 0; p < 4; ++p) u0 = (UINT)insert0(u0, P.bits[p]);
+            const UINT u0s = swz(u0);
+            double2 r[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j) r[j] = tile[u0s ^ s_off[j]];
+            for (UINT o = 0; o < P.op_count; ++o) apply_op(a.ops[P.op_begin + o], r, a.pool);
+#pragma unroll
+            for (int j = 0; j < 16; ++j) tile[u0s ^ s_off[j]] = r[j];
+        }
+        __syncthreads();
+    }
+    {
+        double2 v[16];
+#pragma unroll
+        for (int k = 0; k < 16; ++k)
+            if ((UINT)tid + (UINT)k * kStThreads < tsize) v[k] = tile[swz((UINT)tid + (UINT)k * kStThreads)];
+#pragma unroll
+        for (int k = 0; k < 16; ++k)
+            if ((UINT)tid + (UINT)k * kStThreads < tsize) st_stream(s + (base | lo_off | hi_off[k]), v[k]);
+    }
+}
+
+// ---------------------------------------------------------------- host scheduler
+using cd = std::complex<double>;
+
+static bool stageable(const GateRec& g) {
+    if (!g.controls.empty()) return false;
+    switch (g.kind) {
+        case QS_GATE_RX:
+        case QS_GATE_RY:
+        case QS_GATE_RZ:
+        case QS_GATE_CNOT:
+        case QS_GATE_CZ:
+        case QS_GATE_SWAP: return true;
+        case QS_GATE_DENSE: return g.targets.size() <= 2;
+        case QS_GATE_DIAGONAL: return g.targets.size() == 1;
+        default: return false;
+    }
+}
+
+static ITYPE qmask(const std::vector<UINT>& qs) {
+    ITYPE m = 0;
+    for (UINT q : qs) m |= 1ULL << q;
+    return m;
+}
+
+struct PassPlan {
+    bool single = false;  // a gate run by the gate-by-gate kernels
+    int gate = -1;
+    std::vector<UINT> q;  // tile qubits (ascending)
+    std::vector<int> gates;
+};
+
+// Absorb greedily in program order with a fixed tile set; returns the absorbed gate indices.
+static std::vector<int> absorb(const std::vector<GateRec>& G, const std::vector<int>& pending, ITYPE Q, UINT n) {
+    std::vector<int> out;
+    ITYPE blocked = 0;
+    const ITYPE all = (n >= 64) ? ~0ULL : ((1ULL << n) - 1);
+    for (int gi : pending) {
+        const ITYPE gm = qmask(G[gi].qubits());
+        if ((gm & blocked) || !stageable(G[gi]) || (gm & ~Q)) {
+            blocked |= gm;
+            if ((blocked & all) == all) break;
+            continue;
+        }
+        out.push_back(gi);
+    }
+    return out;
+}
+
+// Grow Q greedily in program order (capacity m), absorbing as we go.
+static ITYPE greedy_q(const std::vector<GateRec>& G, const std::vector<int>& pending, ITYPE Q, int m) {
+    ITYPE blocked = 0;
+    for (int gi : pending) {
+        const ITYPE gm = qmask(G[gi].qubits());
+        if ((gm & blocked) || !stageable(G[gi])) {
+            blocked |= gm;
+            continue;
+        }
+        if ((gm & ~Q) == 0) continue;
+        if (__builtin_popcountll(Q | gm) <= m) Q |= gm;
+        else blocked |= gm;
+    }
+    return Q;
+}
+
+static std::vector<PassPlan> plan_passes(const std::vector<GateRec>& G, UINT n) {
+    std::vector<PassPlan> plan;
+    std::vector<int> pending(G.size());
+    for (size_t i = 0; i < G.size(); ++i) pending[i] = (int)i;
+    const int m = (int)std::min<UINT>(kTileBits, n);
+    const int low = std::min(kLowFixed, m);
+    const ITYPE lowmask = (1ULL << low) - 1;
+    while (!pending.empty()) {
+        if (!stageable(G[pending[0]])) {
+            PassPlan p;
+            p.single = true;
+            p.gate = pending[0];
+            plan.push_back(p);
+            pending.erase(pending.begin());
+            continue;
+        }
+        // candidate tile sets: greedy in program order, and windows of consecutive high qubits
+        std::vector<ITYPE> cands;
+        cands.push_back(greedy_q(G, pending, lowmask, m));
+        for (int a = low; a + (m - low) <= (int)n; ++a) {
+            ITYPE Q = lowmask;
+            for (int j = 0; j < m - low; ++j) Q |= 1ULL << (a + j);
+            cands.push_back(Q);
+        }
+        std::vector<int> best;
+        ITYPE bestQ = 0;
+        for (ITYPE Q : cands) {
+            std::vector<int> got = absorb(G, pending, Q, n);
+            if (got.size() > best.size()) {
+                best = got;
+                bestQ = Q;
+            }
+        }
+        if (best.empty()) {  // cannot happen for a stageable front gate; keep progress anyway
+            PassPlan p;
+            p.single = true;
+            p.gate = pending[0];
+            plan.push_back(p);
+            pending.erase(pending.begin());
+            continue;
+        }
+        // pad Q to m qubits with the lowest unused ones
+        for (UINT q = 0; q < n && __builtin_popcountll(bestQ) < m; ++q) bestQ |= 1ULL << q;
+        PassPlan p;
+        for (UINT q = 0; q < n; ++q)
+            if (bestQ >> q & 1ULL) p.q.push_back(q);
+        p.gates = best;
+        plan.push_back(p);
+        std::vector<char> taken(G.size(), 0);
+        for (int gi : best) taken[gi] = 1;
+        std::vector<int> rest;
+        for (int gi : pending)
+            if (!taken[gi]) rest.push_back(gi);
+        pending.swap(rest);
+    }
+    return plan;
+}
+
+struct DevPass {
+    bool single;
+    int gate;
+    StPassArgs args;
+};
+
+struct StagedPlan {
+    ITYPE dim = 0;
+    std::vector<DevPass> passes;
+    void* dev = nullptr;  // phases | ops | pool
+    ~StagedPlan() {
+        if (dev) cudaFree(dev);
+    }
+};
+
+// Tile-local bit of a global qubit.
+static int local_bit(const std::vector<UINT>& q, UINT g) {
+    for (size_t j = 0; j < q.size(); ++j)
+        if (q[j] == g) return (int)j;
+    return -1;
+}
+
+static int build_plan(Circuit& c, ITYPE dim, std::shared_ptr<StagedPlan>* out) {
+    const UINT n = c.n;
+    auto P = std::make_shared<StagedPlan>();
+    P->dim = dim;
+    std::vector<PassPlan> passes = plan_passes(c.gates, n);
+    std::vector<StPhase> phases;
+    std::vector<StOp> ops;
+    std::vector<double2> pool;
+    struct Pending {
+        size_t phase_begin, nphases;
+    };
+    std::vector<Pending> pp;
+    for (const PassPlan& p : passes) {
+        if (p.single) {
+            pp.push_back({0, 0});
+            continue;
+        }
+        const size_t ph0 = phases.size();
+        // phases: greedy over the pass's gates (program order) with 4 register bits each
+        std::vector<int> todo = p.gates;
+        const int m = (int)p.q.size();
+        while (!todo.empty()) {
+            std::vector<int> lb;  // per gate: its tile-local bits
+            // candidates: greedy in order, and windows of 4 consecutive tile bits
+            auto bits_of = [&](int gi) {
+                ITYPE bm = 0;
+                for (UINT g : c.gates[gi].qubits()) bm |= 1ULL << local_bit(p.q, g);
+                return bm;
+            };
+            auto take = [&](ITYPE R, std::vector<int>* got) {
+                ITYPE blocked = 0;
+                for (int gi : todo) {
+                    const ITYPE bm = bits_of(gi);
+                    if ((bm & blocked) || (bm & ~R)) {
+                        blocked |= bm;
+                        continue;
+                    }
+                    got->push_back(gi);
+                }
+            };
+            std::vector<ITYPE> cands;
+            {
+                ITYPE R = 0, blocked = 0;
+                for (int gi : todo) {
+                    const ITYPE bm = bits_of(gi);
+                    if (bm & blocked) {
+                        blocked |= bm;
+                        continue;
+                    }
+                    if (__builtin_popcountll(R | bm) <= kPhaseBits) R |= bm;
+                    else blocked |= bm;
+                }
+                cands.push_back(R);
+            }
+            for (int a0 = 0; a0 + kPhaseBits <= m; ++a0) cands.push_back(((1ULL << kPhaseBits) - 1) << a0);
+            std::vector<int> best;
+            ITYPE bestR = 0;
+            for (ITYPE R : cands) {
+                std::vector<int> got;
+                take(R, &got);
+                if (got.size() > best.size()) {
+                    best = got;
+                    bestR = R;
+                }
+            }
+            for (int b = 0; b < m && __builtin_popcountll(bestR) < kPhaseBits; ++b) bestR |= 1ULL << b;
+            StPhase ph;
+            int nb = 0;
+            int regbit[64];
+            for (int b = 0; b < m; ++b)
+                if (bestR >> b & 1ULL) {
+                    regbit[b] = nb;
+                    ph.bits[nb++] = (uint8_t)b;
+                }
+            ph.op_begin = (uint32_t)ops.size();
+            for (int gi : best) {
+                const GateRec& g = c.gates[gi];
+                StOp op{};
+                auto rb = [&](UINT gq) { return (uint8_t)regbit[local_bit(p.q, gq)]; };
+                op.param = (uint32_t)pool.size();
+                const double ang = g.angle;
+                switch (g.kind) {
+                    case QS_GATE_RX:
+                        op.kind = ST_RX;
+                        op.a = rb(g.targets[0]);
+                        pool.push_back(make_double2(std::cos(ang / 2), std::sin(ang / 2)));
+                        break;
+                    case QS_GATE_RY:
+                        op.kind = ST_RY;
+                        op.a = rb(g.targets[0]);
+                        pool.push_back(make_double2(std::cos(ang / 2), std::sin(ang / 2)));
+                        break;
+                    case QS_GATE_RZ:
+                        op.kind = ST_DIAG1;
+                        op.a = rb(g.targets[0]);
+                        pool.push_back(make_double2(std::cos(ang / 2), std::sin(ang / 2)));
+                        pool.push_back(make_double2(std::cos(ang / 2), -std::sin(ang / 2)));
+                        break;
+                    case QS_GATE_CNOT:
+                        op.kind = ST_CNOT;
+                        op.a = rb(g.targets[0]);
+                        op.b = rb(g.targets[1]);
+                        break;
+                    case QS_GATE_CZ:
+                        op.kind = ST_CZ;
+                        op.a = rb(g.targets[0]);
+                        op.b = rb(g.targets[1]);
+                        break;
+                    case QS_GATE_SWAP:
+                        op.kind = ST_SWAP;
+                        op.a = rb(g.targets[0]);
+                        op.b = rb(g.targets[1]);
+                        break;
+                    case QS_GATE_DIAGONAL:
+                        op.kind = ST_DIAG1;
+                        op.a = rb(g.targets[0]);
+                        for (int i = 0; i < 2; ++i) pool.push_back(make_double2(g.matrix[i].real(), g.matrix[i].imag()));
+                        break;
+                    default:  // dense 1 or 2 targets
+                        if (g.targets.size() == 1) {
+                            op.kind = ST_DENSE1;
+                            op.a = rb(g.targets[0]);
+                            for (int i = 0; i < 4; ++i) pool.push_back(make_double2(g.matrix[i].real(), g.matrix[i].imag()));
+                        } else {
+                            op.kind = ST_DENSE2;
+                            op.a = rb(g.targets[0]);
+                            op.b = rb(g.targets[1]);
+                            for (int i = 0; i < 16; ++i) pool.push_back(make_double2(g.matrix[i].real(), g.matrix[i].imag()));
+                        }
+                        break;
+                }
+                ops.push_back(op);
+            }
+            ph.op_count = (uint32_t)(ops.size() - ph.op_begin);
+            phases.push_back(ph);
+            std::vector<char> taken(c.gates.size(), 0);
+            for (int gi : best) taken[gi] = 1;
+            std::vector<int> rest;
+            for (int gi : todo)
+                if (!taken[gi]) rest.push_back(gi);
+            todo.swap(rest);
+        }
+        pp.push_back({ph0, phases.size() - ph0});
+    }
+    // upload
+    const size_t bph = sizeof(StPhase) * phases.size(), bop = sizeof(StOp) * ops.size(),
+                 bpo = sizeof(double2) * pool.size();
+    const size_t o_ops = (bph + 255) / 256 * 256, o_pool = o_ops + (bop + 255) / 256 * 256;
+    const size_t total = o_pool + bpo + 256;
+    QS_CUDA_CHECK(cudaMalloc(&P->dev, total));
+    std::vector<char> host(total, 0);
+    if (bph) memcpy(host.data(), phases.data(), bph);
+    if (bop) memcpy(host.data() + o_ops, ops.data(), bop);
+    if (bpo) memcpy(host.data() + o_pool, pool.data(), bpo);
+    QS_CUDA_CHECK(cudaMemcpy(P->dev, host.data(), total, cudaMemcpyHostToDevice));
+    const StPhase* dph = (const StPhase*)P->dev;
+    const StOp* dop = (const StOp*)((char*)P->dev + o_ops);
+    const double2* dpo = (const double2*)((char*)P->dev + o_pool);
+    for (size_t i = 0; i < passes.size(); ++i) {
+        DevPass d{};
+        d.single = passes[i].single;
+        d.gate = passes[i].gate;
+        if (!d.single) {
+            d.args.m = (int)passes[i].q.size();
+            for (int j = 0; j < d.args.m; ++j) d.args.q[j] = passes[i].q[j];
+            d.args.nphases = (int)pp[i].nphases;
+            d.args.phases = dph + pp[i].phase_begin;
+            d.args.ops = dop;
+            d.args.pool = dpo;
+        }
+        P->passes.push_back(d);
+    }
+    *out = P;
+    return QS_OK;
+}
+
+static int ensure_plan(Circuit& c, ITYPE dim) {
+    if (!c.plan || c.plan->dim != dim) QS_TRY(build_plan(c, dim, &c.plan));
+    return QS_OK;
+}
+
+int run_staged(Circuit& c, void* state, ITYPE dim, cudaStream_t st) {
+    if (c.n < kPhaseBits) {  // too small for a 4-qubit register phase
+        for (const GateRec& g : c.gates) QS_TRY(apply_gate_by_gate(g, state, dim, st));
+        return QS_OK;
+    }
+    QS_TRY(ensure_plan(c, dim));
+    for (const DevPass& d : c.plan->passes) {
+        if (d.single) {
+            QS_TRY(apply_gate_by_gate(c.gates[d.gate], state, dim, st));
+            continue;
+        }
+        const ITYPE tiles = dim >> d.args.m;
+        k_staged_pass<<<(unsigned)tiles, kStThreads, 0, st>>>((double2*)state, d.args);
+        QS_TRY(check_launch("k_staged_pass"));
+    }
+    return QS_OK;
+}
+
+int staged_pass_count(Circuit& c, ITYPE dim, UINT* out) {
+    if (c.n < kPhaseBits) {
+        *out = (UINT)c.gates.size();
+        return QS_OK;
+    }
+    QS_TRY(ensure_plan(c, dim));
+    *out = (UINT)c.plan->passes.size();
+    return QS_OK;
+}
+
+}  // namespace qs
