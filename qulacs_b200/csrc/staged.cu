@@ -400,18 +400,26 @@ static int local_bit(const std::vector<UINT>& q, UINT g) {
     return -1;
 }
 
-static int build_plan(Circuit& c, ITYPE dim, std::shared_ptr<StagedPlan>* out) {
-    const UINT n = c.n;
-    auto P = std::make_shared<StagedPlan>();
-    P->dim = dim;
-    std::vector<PassPlan> passes = plan_passes(c.gates, n);
+struct HostPlan {
+    std::vector<PassPlan> passes;
     std::vector<StPhase> phases;
     std::vector<StOp> ops;
     std::vector<double2> pool;
-    struct Pending {
+    struct Range {
         size_t phase_begin, nphases;
     };
-    std::vector<Pending> pp;
+    std::vector<Range> pp;
+};
+
+// Host-only part of planning: passes, phases and encoded ops (no device calls).
+static void make_host_plan(const Circuit& c, HostPlan* H) {
+    const UINT n = c.n;
+    H->passes = plan_passes(c.gates, n);
+    const std::vector<PassPlan>& passes = H->passes;
+    std::vector<StPhase>& phases = H->phases;
+    std::vector<StOp>& ops = H->ops;
+    std::vector<double2>& pool = H->pool;
+    std::vector<HostPlan::Range>& pp = H->pp;
     for (const PassPlan& p : passes) {
         if (p.single) {
             pp.push_back({0, 0});
@@ -544,6 +552,18 @@ static int build_plan(Circuit& c, ITYPE dim, std::shared_ptr<StagedPlan>* out) {
         }
         pp.push_back({ph0, phases.size() - ph0});
     }
+}
+
+static int build_plan(Circuit& c, ITYPE dim, std::shared_ptr<StagedPlan>* out) {
+    auto P = std::make_shared<StagedPlan>();
+    P->dim = dim;
+    HostPlan H;
+    make_host_plan(c, &H);
+    const std::vector<PassPlan>& passes = H.passes;
+    const std::vector<StPhase>& phases = H.phases;
+    const std::vector<StOp>& ops = H.ops;
+    const std::vector<double2>& pool = H.pool;
+    const std::vector<HostPlan::Range>& pp = H.pp;
     // upload
     const size_t bph = sizeof(StPhase) * phases.size(), bop = sizeof(StOp) * ops.size(),
                  bpo = sizeof(double2) * pool.size();
@@ -604,8 +624,16 @@ int staged_pass_count(Circuit& c, ITYPE dim, UINT* out) {
         *out = (UINT)c.gates.size();
         return QS_OK;
     }
-    QS_TRY(ensure_plan(c, dim));
-    *out = (UINT)c.plan->passes.size();
+    HostPlan H;
+    make_host_plan(c, &H);
+    *out = (UINT)H.passes.size();
+    return QS_OK;
+}
+
+int staged_phase_count(Circuit& c, UINT* out) {
+    HostPlan H;
+    make_host_plan(c, &H);
+    *out = (UINT)H.phases.size();
     return QS_OK;
 }
 

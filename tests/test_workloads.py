@@ -56,3 +56,12 @@ def test_library_rng_matches_restatement(lib):
     out = np.zeros(500)
     assert lib.qs_reference_uniforms(1234, 500, out.ctypes.data_as(C.c_void_p)) == 0
     assert np.array_equal(out, mt19937_64_uniforms(1234, 500))
+
+
+def test_staged_planner_pass_counts():
+    """Host-only scheduler: passes needed by the staged executor (one HBM read+write each)."""
+    c = W.to_circuit(W.layered_rotation_circuit(30, 10, 1), 30)
+    p = c.pass_count()
+    assert 1 <= p <= 40  # vs 1190 gate-by-gate passes
+    c = W.to_circuit(W.layered_rotation_circuit(3, 2, 1), 3)
+    assert c.pass_count() == c.get_gate_count()  # below 4 qubits: gate by gate
