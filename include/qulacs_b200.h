@@ -176,6 +176,19 @@ QS_API int qs_state_sampling_with_uniforms(const void* state, QS_ITYPE dim, cons
  * std::mt19937_64 seeded with `random_seed`, std::uniform_real_distribution<double>(0, 1). */
 QS_API int qs_state_sampling(const void* state, QS_ITYPE dim, QS_UINT sampling_count,
     QS_UINT random_seed, QS_ITYPE* out, void* stream);
+/*
+ * qs_state_sampling_with_uniforms without any device allocation.  No counterpart in the reference:
+ * it exists for callers that cannot call cudaMalloc -- a host framework that owns all device memory
+ * through its own pool and forbids foreign allocations, or a latency-bound loop where cudaMalloc /
+ * cudaFree would stall (they can synchronise the whole device).  Its scratch is a statically
+ * reserved 2.25 MiB array in the library's device image, held by every GPU that loads the library
+ * until the process exits.  Limits: dim <= 2^28 and sampling_count <= 16384, else
+ * QS_ERR_NOT_SUPPORTED.  Same results as qs_state_sampling_with_uniforms.  The first call on a
+ * device looks up the array's device address, so make it before any stream capture.  All calls
+ * share the array: calls that overlap on the GPU race.
+ */
+QS_API int qs_state_sampling_with_uniforms_noalloc(const void* state, QS_ITYPE dim, const double* uniforms,
+    QS_UINT sampling_count, QS_ITYPE* out, void* stream);
 /* The uniforms qs_state_sampling draws for a seed (host only; cppsim/utility.hpp:54-80). */
 QS_API int qs_reference_uniforms(QS_UINT random_seed, QS_UINT count, double* out);
 

@@ -63,6 +63,7 @@ SIGNATURES = {
     "qs_state_sampling_with_uniforms": [P, IT, P, U, P, P],
     "qs_state_sampling": [P, IT, U, U, P, P],
     "qs_reference_uniforms": [U, U, P],
+    "qs_state_sampling_with_uniforms_noalloc": [P, IT, P, U, P, P],
     "qs_dm_allocate": [IT, C.POINTER(P)],
     "qs_dm_initialize_quantum_state": _STATE,
     "qs_dm_initialize_with_pure_state": [P, P, IT, P],

@@ -3,6 +3,7 @@
 // one partial per CTA written to scratch, then one CTA folds the partials in index order (no
 // floating-point atomics).
 #include <algorithm>
+#include <mutex>
 #include <random>
 #include <vector>
 
@@ -340,6 +341,39 @@ int sample_with_uniforms(const double2* s, ITYPE dim, ITYPE diag_stride, const d
     return QS_OK;
 }
 
+// ---------------------------------------------------------------- sampling without allocation
+// Scratch for qs_state_sampling_with_uniforms_noalloc, reserved statically in this module so that
+// the call never allocates: chunk sums | inclusive scan | uniforms | sampled indices.  Every GPU
+// that loads the library holds it (2.25 MiB) until the process exits.  Nothing in it has to start
+// at zero: each element a call reads was written earlier in the same call.  Calls share it, so
+// calls that overlap on the GPU (other streams, other host threads) race.
+constexpr ITYPE kNoAllocMaxDim = 1ULL << 28;   // states of up to 28 qubits
+constexpr UINT kNoAllocMaxShots = 16384;
+constexpr size_t kNoAllocChunks = kNoAllocMaxDim / kChunk;
+constexpr size_t kNoAllocDoubles = 2 * kNoAllocChunks + 2 * (size_t)kNoAllocMaxShots;
+static __device__ __align__(256) double g_noalloc_sampling_scratch[kNoAllocDoubles];
+
+static std::mutex g_noalloc_mu;
+static double* g_noalloc_ptr[64] = {nullptr};
+
+// Device address of the static scratch on the current device.  In host code the array's name is
+// only a host-side stand-in, so the address is looked up once per device (with that device
+// current) and cached.
+static int noalloc_scratch(double** out) {
+    int dev = 0;
+    QS_CUDA_CHECK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return set_error(QS_ERR_NOT_SUPPORTED, "device ordinal beyond 63");
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_sampling_scratch);
+        if (e != cudaSuccess) return check_cuda(e, "cudaGetSymbolAddress(g_noalloc_sampling_scratch)");
+        g_noalloc_ptr[dev] = (double*)p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return QS_OK;
+}
+
 // Reference RNG (cppsim/utility.hpp:54-80): mt19937_64 seeded with the seed, uniform_real_distribution(0, 1).
 void reference_uniforms(UINT seed, UINT count, std::vector<double>* u) {
     std::mt19937_64 mt;
@@ -450,6 +484,44 @@ QS_API int qs_state_sampling(const void* state, QS_ITYPE dim, QS_UINT count, QS_
     std::vector<double> u;
     reference_uniforms(seed, count, &u);
     return qs_state_sampling_with_uniforms(state, dim, u.data(), count, out, stream);
+}
+
+// Same result as qs_state_sampling_with_uniforms (same kernels, same order of summation), with all
+// scratch in g_noalloc_sampling_scratch: no cudaMalloc, cudaFree or allocating library call.  The
+// first call on a device looks up the array's device address; make that first call before any
+// stream capture.
+QS_API int qs_state_sampling_with_uniforms_noalloc(const void* state, QS_ITYPE dim, const double* uniforms,
+    QS_UINT count, QS_ITYPE* out, void* stream) {
+    UINT n;
+    QS_TRY(check_dim(dim, &n));
+    if (dim > kNoAllocMaxDim)
+        return set_error(QS_ERR_NOT_SUPPORTED,
+            "state_sampling_with_uniforms_noalloc: state larger than 2^28 amplitudes (static scratch limit)");
+    if (count > kNoAllocMaxShots)
+        return set_error(QS_ERR_NOT_SUPPORTED,
+            "state_sampling_with_uniforms_noalloc: more than 16384 shots (static scratch limit)");
+    if (count == 0) return QS_OK;
+    if (!state || !uniforms || !out) return set_error(QS_ERR_INVALID_ARGUMENT, "null pointer argument");
+    double* buf = nullptr;
+    QS_TRY(noalloc_scratch(&buf));
+    cudaStream_t st = (cudaStream_t)stream;
+    const ITYPE nchunks = (dim + kChunk - 1) / kChunk;
+    double* sums = buf;
+    double* incl = buf + kNoAllocChunks;
+    double* du = incl + kNoAllocChunks;
+    ITYPE* dout = (ITYPE*)(du + kNoAllocMaxShots);
+    QS_CUDA_CHECK(cudaMemcpyAsync(du, uniforms, sizeof(double) * count, cudaMemcpyHostToDevice, st));
+    k_chunk_sums<<<(unsigned)nchunks, 256, 0, st>>>((const double2*)state, dim, 0, sums);
+    QS_TRY(check_launch("k_chunk_sums"));
+    k_scan_sums<<<1, 1024, 0, st>>>(sums, nchunks, incl);
+    QS_TRY(check_launch("k_scan_sums"));
+    const unsigned threads = 256;
+    const unsigned blocks = (unsigned)(((ITYPE)count * 32 + threads - 1) / threads);
+    k_sample<<<blocks, threads, 0, st>>>((const double2*)state, dim, 0, incl, nchunks, du, count, dout);
+    QS_TRY(check_launch("k_sample"));
+    QS_CUDA_CHECK(cudaMemcpyAsync(out, dout, sizeof(ITYPE) * count, cudaMemcpyDeviceToHost, st));
+    QS_CUDA_CHECK(cudaStreamSynchronize(st));
+    return QS_OK;
 }
 
 QS_API int qs_reference_uniforms(QS_UINT seed, QS_UINT count, double* out) {
