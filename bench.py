@@ -102,6 +102,65 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+# DRAM bytes per amplitude per staged pass measured by ncu (dram__bytes_read.sum + write.sum of
+# k_staged_pass on the 26-qubit case: 2.092e9 B for 2^26 amplitudes; profiles/k_staged_pass_layered26.md),
+# scaled to the benchmark's size by the number of amplitudes.
+STAGED_TRAFFIC_PER_AMP = 2.092e9 / (1 << 26)
+
+
+def kernel_table(state, n: int, stream, reps: int = 5):
+    """Each gate-by-gate kernel alone at n qubits: ms per launch and GB/s against 2 x 16 x 2^n B
+    (and against the bytes the kernel actually has to move, for CNOT/CZ)."""
+    import ctypes as C
+
+    import torch
+
+    from qulacs_b200._lib import call
+    rng = np.random.default_rng(7)
+
+    def unitary(k):
+        a = rng.normal(size=(1 << k, 1 << k)) + 1j * rng.normal(size=(1 << k, 1 << k))
+        q, _ = np.linalg.qr(a)
+        return np.ascontiguousarray(q, dtype=np.complex128)
+
+    p = state.data_ptr()
+    dim = state.dim
+    h = stream.cuda_stream
+    m1 = unitary(1)
+    mats = {k: unitary(k) for k in range(2, 7)}
+    tls = {k: np.ascontiguousarray(np.arange(n - k, n, dtype=np.uint32)) for k in range(2, 7)}
+    mp = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+    cases = [
+        ("dense1 t=0 (k_dense1_shfl)", 1.0, lambda: call("qs_single_qubit_dense_matrix_gate", 0, mp(m1), p, dim, h)),
+        ("dense1 t=4 (k_dense1_shfl)", 1.0, lambda: call("qs_single_qubit_dense_matrix_gate", 4, mp(m1), p, dim, h)),
+        ("dense1 t=5 (k_pair)", 1.0, lambda: call("qs_single_qubit_dense_matrix_gate", 5, mp(m1), p, dim, h)),
+        (f"dense1 t={n // 2} (k_pair)", 1.0, lambda: call("qs_single_qubit_dense_matrix_gate", n // 2, mp(m1), p, dim, h)),
+        (f"dense1 t={n - 1} (k_pair)", 1.0, lambda: call("qs_single_qubit_dense_matrix_gate", n - 1, mp(m1), p, dim, h)),
+        ("RZ t=10 (k_diag1)", 1.0, lambda: call("qs_RZ_gate", 10, 0.3, p, dim, h)),
+        (f"CNOT {n - 2}->{n - 1} (k_pair swap)", 0.5, lambda: call("qs_CNOT_gate", n - 2, n - 1, p, dim, h)),
+        ("CNOT 0->1 (k_pair swap)", 0.5, lambda: call("qs_CNOT_gate", 0, 1, p, dim, h)),
+        ("CZ 3,17 (k_single negate)", 0.25, lambda: call("qs_CZ_gate", 3, 17, p, dim, h)),
+        (f"dense2 {n - 2},{n - 1} (k_dense2)", 1.0, lambda: call("qs_double_qubit_dense_matrix_gate_c", n - 2, n - 1, mp(mats[2]), p, dim, h)),
+    ]
+    for k in range(3, 7):
+        cases.append((f"dense{k} high targets (k_denseK)", 1.0,
+                      lambda k=k: call("qs_multi_qubit_dense_matrix_gate", mp(tls[k]), k, mp(mats[k]), p, dim, h)))
+    out = []
+    alg = bytes_per_gate(n)
+    for name, frac, fn in cases:
+        fn()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        out.append({"kernel": name, "ms": round(ms, 4), "gbs_vs_2x16x2^n": round(alg / 1e9 / (ms / 1e3), 1),
+                    "gbs_touched": round(frac * alg / 1e9 / (ms / 1e3), 1)})
+    return out
+
+
 def cpu_reference_gbs(n: int, gates, budget_s: float, threads: int, state=None):
     """Time the reference csim (oracle/_ref, else the oracle port) gate by gate on host cores."""
     os.environ.setdefault("OMP_NUM_THREADS", str(threads))
@@ -170,6 +229,7 @@ def main():
     ap.add_argument("--mode", default="staged", choices=["staged", "gate_by_gate"])
     ap.add_argument("--qubits", type=int, default=N_QUBITS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-kernel-table", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3  # timing rule: at least 3 untimed warm-up steps
@@ -236,6 +296,12 @@ def main():
     per_launch_ms = ms / max(1, passes)
     hbm_peak, peak_kind = peaks()
     achieved = bytes_per_gate(n) / 1e9 / (per_launch_ms / 1e3)
+    # FP64 view of the same work: specialised RX/RY/RZ code issues 4 FP64 instructions per amplitude
+    # per rotation gate (CNOTs move data only); B200 FP64 CUDA-core peak = 148 SMs x 64 FMA/clk.
+    rot = sum(1 for g in gates if g[0] in ("RX", "RY", "RZ"))
+    fp64_instr = 4.0 * rot * (1 << n)
+    fp64_peak = 148 * 64 * 1.965e9
+    kernels = kernel_table(state, n, stream) if not args.no_kernel_table else None
 
     # end to end through the public API: host gate list already built into the circuit, observable
     # masks and uniforms from host, results (term values + samples) back to the host
@@ -271,8 +337,17 @@ def main():
                        "parallelism": f"replicas x{world}"},
             "circuit_s": ms / 1e3,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                         "frac": achieved / hbm_peak, "peak_kind": peak_kind, "traffic": None,
-                         "kernel": "one HBM pass over the state (2 x 16 x 2^n B)"},
+                         "frac": achieved / hbm_peak, "peak_kind": peak_kind,
+                         "traffic": (STAGED_TRAFFIC_PER_AMP * (1 << n)) if mode == "staged" else None,
+                         "kernel": ("k_staged_pass: one HBM pass (2 x 16 x 2^n B) applying ~"
+                                    f"{len(gates) / max(1, passes):.0f} gates" if mode == "staged"
+                                    else "gate kernels: one HBM pass (2 x 16 x 2^n B) per gate"),
+                         "traffic_note": "scaled from the 26-qubit ncu capture by amplitudes" if mode == "staged" else None},
+            "roofline_fp64": {"achieved_tinstr_s": fp64_instr / (ms / 1e3) / 1e12,
+                              "peak_tinstr_s": fp64_peak / 1e12,
+                              "frac": fp64_instr / (ms / 1e3) / fp64_peak,
+                              "note": "4 FP64 instr/amplitude/rotation; nominal 64 FP64 FMA/clk/SM at 1965 MHz"},
+            "kernels": kernels,
             "e2e": {"value": world * gb_per_step / (e2e_ms / 1e3), "unit": "GB/s", "ms_per_step": e2e_ms,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "includes": "set_zero_state + circuit + <H> (256 strings) + 1024-shot sampling"},

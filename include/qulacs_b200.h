@@ -262,6 +262,32 @@ QS_API int qs_circuit_pass_count(qs_circuit_t circuit, QS_ITYPE dim, QS_UINT* ou
 QS_API int qs_circuit_update_density_matrix(
     qs_circuit_t circuit, void* rho, QS_ITYPE dim, int exec_mode, void* stream);
 
+/* ---- fused reduced-precision execution (no reference counterpart; its comparison point is the
+ * reference's gate merging, QuantumCircuitOptimizer::optimize, cppsim/circuit_optimizer.cpp:113-168,
+ * and gate::merge, cppsim/gate_merge.cpp:316-356) ----
+ * Applies the circuit to a complex64 state (dim (re, im) floats): gates are fused into 6-qubit blocks
+ * composed in FP64 and applied on the tensor cores as split-bf16 products (hi*hi + hi*lo + lo*hi)
+ * with FP32 accumulation.  Needs >= 10 qubits and gates of <= 6 qubits (no noise channels). */
+QS_API int qs_circuit_update_quantum_state_fused_c64(qs_circuit_t circuit, void* state_c64, QS_ITYPE dim, void* stream);
+/* Statistics of a complex64 state with FP64 accumulation (the fused path's reductions): norm, the
+ * inner product <bra_c128|ket_c64> (for the infidelity 1 - |<psi|psi_FP64>|^2), batched <P_k>
+ * (masks as qs_expectation_value_pauli_batch) and sampling with supplied uniforms. */
+QS_API int qs_state_norm_squared_c64(const void* state_c64, QS_ITYPE dim, void* stream, double* out);
+QS_API int qs_state_inner_product_c128_c64(const void* bra_c128, const void* ket_c64, QS_ITYPE dim,
+    void* stream, double out[2]);
+QS_API int qs_expectation_value_pauli_batch_c64(const QS_ITYPE* x_masks, const QS_ITYPE* z_masks,
+    const QS_UINT* y_counts, QS_UINT term_count, const void* state_c64, QS_ITYPE dim, void* stream,
+    double* values);
+QS_API int qs_state_sampling_with_uniforms_c64(const void* state_c64, QS_ITYPE dim, const double* uniforms,
+    QS_UINT sampling_count, QS_ITYPE* out, void* stream);
+/* Number of tile passes and fused blocks of the fused schedule (host only). */
+QS_API int qs_circuit_fused_stats(qs_circuit_t circuit, QS_UINT* passes, QS_UINT* blocks);
+/* Host-only export of fused block `index` (application order): the pass's tile qubits (<= 13),
+ * the block's 6 tile-local bits, its FP64 64x64 matrix (row-major interleaved complex, may be NULL)
+ * and its bf16 operand image (hi then lo, 2 x 128 x 128, K-major core-matrix layout; may be NULL). */
+QS_API int qs_circuit_fused_block_export(qs_circuit_t circuit, QS_UINT index, QS_UINT* tile_qubits,
+    int* tile_qubit_count, QS_UINT* block_bits, double* matrix, unsigned short* operand_image);
+
 #ifdef __cplusplus
 }
 #endif

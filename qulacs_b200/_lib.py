@@ -86,6 +86,13 @@ SIGNATURES = {
     "qs_circuit_update_quantum_state": [P, P, IT, I, P],
     "qs_circuit_pass_count": [P, IT, C.POINTER(U)],
     "qs_circuit_update_density_matrix": [P, P, IT, I, P],
+    "qs_circuit_update_quantum_state_fused_c64": [P, P, IT, P],
+    "qs_state_norm_squared_c64": [P, IT, P, P],
+    "qs_state_inner_product_c128_c64": [P, P, IT, P, P],
+    "qs_expectation_value_pauli_batch_c64": [P, P, P, U, P, IT, P, P],
+    "qs_state_sampling_with_uniforms_c64": [P, IT, P, U, P, P],
+    "qs_circuit_fused_stats": [P, C.POINTER(U), C.POINTER(U)],
+    "qs_circuit_fused_block_export": [P, U, P, C.POINTER(I), P, P, P],
 }
 for _n in ("X", "Y", "Z", "H", "S", "Sdag", "T", "Tdag", "sqrtX", "sqrtXdag", "sqrtY", "sqrtYdag", "P0", "P1"):
     SIGNATURES[f"qs_{_n}_gate"] = [U] + _STATE

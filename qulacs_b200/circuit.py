@@ -70,13 +70,23 @@ class QuantumCircuit:
             raise ValueError("depolarizing noise can be used up to 2 qubits")
 
     def update_quantum_state(self, state, mode: str = "staged") -> None:
-        m = {"gate_by_gate": _lib.EXEC_GATE_BY_GATE, "staged": _lib.EXEC_STAGED}[mode]
+        """Apply the circuit.  A QuantumStateC64 always takes the fused tensor-core path."""
         if state.get_qubit_count() != self.qubit_count:
             raise ValueError("state qubit count differs from the circuit's")
+        if type(state).__name__ == "QuantumStateC64":
+            call("qs_circuit_update_quantum_state_fused_c64", self._h, state.data_ptr(), state.dim, state.stream)
+            return
+        m = {"gate_by_gate": _lib.EXEC_GATE_BY_GATE, "staged": _lib.EXEC_STAGED}[mode]
         if state.is_state_vector():
             call("qs_circuit_update_quantum_state", self._h, state.data_ptr(), state.dim, m, state.stream)
         else:
             call("qs_circuit_update_density_matrix", self._h, state.data_ptr(), state.dim, m, state.stream)
+
+    def fused_stats(self):
+        """(tile passes, 6-qubit blocks) of the fused complex64 schedule."""
+        p, b = C.c_uint(), C.c_uint()
+        call("qs_circuit_fused_stats", self._h, C.byref(p), C.byref(b))
+        return p.value, b.value
 
     def pass_count(self) -> int:
         out = C.c_uint()

@@ -31,7 +31,14 @@ struct Circuit {
     std::vector<GateRec> gates;
     // cached staged schedule (built on first staged run for a given dim)
     std::shared_ptr<StagedPlan> plan;
-    void invalidate() { plan.reset(); }
+    // cached fused complex64 plan (fused_c64.cu)
+    std::shared_ptr<void> fused;
+    ITYPE fused_dim = 0;
+    void invalidate() {
+        plan.reset();
+        fused.reset();
+        fused_dim = 0;
+    }
 };
 
 int apply_gate_by_gate(const GateRec& g, void* state, ITYPE dim, cudaStream_t st);

@@ -12,6 +12,13 @@
 namespace qs {
 
 constexpr int kRThreads = 256;
+
+// FP64 view of one amplitude of a complex128 or complex64 state.
+__device__ __forceinline__ double2 amp(const double2* p) { return ld_stream(p); }
+__device__ __forceinline__ double2 amp(const float2* p) {
+    const float2 v = __ldcs(p);
+    return make_double2((double)v.x, (double)v.y);
+}
 constexpr int kMaxPartials = 4096;
 
 static unsigned reduce_blocks(ITYPE items) {
@@ -34,13 +41,14 @@ __global__ void k_fold_partials(const double* __restrict__ part, int count, int 
 // ---------------------------------------------------------------- norm / probabilities
 // mode 0: sum |a|^2 ; mode 1: sum over bit t == 0 ; mode 2: bit t == 1 ;
 // mode 3: marginal (mask/value pair)
+template <class T>
 __global__ void __launch_bounds__(kRThreads) k_prob_sum(
-    const double2* __restrict__ s, ITYPE dim, ITYPE mask, ITYPE value, double* __restrict__ part) {
+    const T* __restrict__ s, ITYPE dim, ITYPE mask, ITYPE value, double* __restrict__ part) {
     __shared__ double sm[32];
     double acc = 0.;
     const ITYPE stride = (ITYPE)gridDim.x * kRThreads;
     for (ITYPE i = (ITYPE)blockIdx.x * kRThreads + threadIdx.x; i < dim; i += stride)
-        if ((i & mask) == value) acc += norm2(ld_stream(s + i));
+        if ((i & mask) == value) acc += norm2(amp(s + i));
     acc = block_sum(acc, sm);
     if (threadIdx.x == 0) part[blockIdx.x] = acc;
 }
@@ -72,13 +80,36 @@ static int finish_reduce(double* part, unsigned blocks, int width, cudaStream_t 
     return QS_OK;
 }
 
-int prob_sum(const double2* s, ITYPE dim, ITYPE mask, ITYPE value, cudaStream_t st, double* out) {
+template <class T>
+int prob_sum_t(const T* s, ITYPE dim, ITYPE mask, ITYPE value, cudaStream_t st, double* out) {
     const unsigned blocks = reduce_blocks(dim);
     void* buf;
     QS_TRY(scratch(st, sizeof(double) * (blocks + 1), &buf));
-    k_prob_sum<<<blocks, kRThreads, 0, st>>>(s, dim, mask, value, (double*)buf);
+    k_prob_sum<T><<<blocks, kRThreads, 0, st>>>(s, dim, mask, value, (double*)buf);
     QS_TRY(check_launch("k_prob_sum"));
     return finish_reduce((double*)buf, blocks, 1, st, out);
+}
+int prob_sum(const double2* s, ITYPE dim, ITYPE mask, ITYPE value, cudaStream_t st, double* out) {
+    return prob_sum_t<double2>(s, dim, mask, value, st, out);
+}
+
+// sum conj(bra_i) ket_i with a complex128 bra and a complex64 ket, FP64 accumulation
+__global__ void __launch_bounds__(kRThreads) k_inner_mixed(const double2* __restrict__ a, const float2* __restrict__ b,
+    ITYPE dim, double* __restrict__ part) {
+    __shared__ double sm[32];
+    double re = 0., im = 0.;
+    const ITYPE stride = (ITYPE)gridDim.x * kRThreads;
+    for (ITYPE i = (ITYPE)blockIdx.x * kRThreads + threadIdx.x; i < dim; i += stride) {
+        const double2 x = ld_stream(a + i), y = amp(b + i);
+        re = fma(x.x, y.x, fma(x.y, y.y, re));
+        im = fma(x.x, y.y, fma(-x.y, y.x, im));
+    }
+    re = block_sum(re, sm);
+    im = block_sum(im, sm);
+    if (threadIdx.x == 0) {
+        part[2 * blockIdx.x] = re;
+        part[2 * blockIdx.x + 1] = im;
+    }
 }
 
 // ---------------------------------------------------------------- Pauli expectation values
@@ -99,14 +130,15 @@ __device__ __forceinline__ double phase_re_part(double2 v, UINT r) {
 
 // One term with a bit flip: sum over pivot-0 indices b0 of 2 Re(a[b0] conj(a[b0 ^ x]) i^{nY + 2 par}),
 // stat_ops_expectation_value.cpp:352-373.
-__global__ void __launch_bounds__(kRThreads) k_ev_xz(const double2* __restrict__ s, ITYPE half, PauliTerm t,
+template <class T>
+__global__ void __launch_bounds__(kRThreads) k_ev_xz(const T* __restrict__ s, ITYPE half, PauliTerm t,
     double* __restrict__ part) {
     __shared__ double sm[32];
     double acc = 0.;
     const ITYPE stride = (ITYPE)gridDim.x * kRThreads;
     for (ITYPE p = (ITYPE)blockIdx.x * kRThreads + threadIdx.x; p < half; p += stride) {
         const ITYPE b0 = insert0(p, t.pivot), b1 = b0 ^ t.x;
-        const double2 a0 = ld_stream(s + b0), a1 = ld_stream(s + b1);
+        const double2 a0 = amp(s + b0), a1 = amp(s + b1);
         const double2 v = cmul(a0, cconj(a1));
         const UINT r = t.nrot + 2u * (UINT)(__popcll(b0 & t.z) & 1);
         acc += 2.0 * phase_re_part(v, r);
@@ -117,8 +149,8 @@ __global__ void __launch_bounds__(kRThreads) k_ev_xz(const double2* __restrict__
 
 // All Z-only terms in one pass: values[w] = sum |a_i|^2 (-1)^{popcount(i & z_w)}
 // (stat_ops_expectation_value.cpp:467-482).  Partial p of term w at part[p * nz + w].
-template <int MAXZ>
-__global__ void __launch_bounds__(kRThreads) k_ev_z_batch(const double2* __restrict__ s, ITYPE dim,
+template <int MAXZ, class T>
+__global__ void __launch_bounds__(kRThreads) k_ev_z_batch(const T* __restrict__ s, ITYPE dim,
     const ITYPE* __restrict__ zmasks, int nz, double* __restrict__ part) {
     __shared__ double sm[32];
     __shared__ ITYPE zs[MAXZ];
@@ -129,7 +161,7 @@ __global__ void __launch_bounds__(kRThreads) k_ev_z_batch(const double2* __restr
     for (int w = 0; w < MAXZ; ++w) acc[w] = 0.;
     const ITYPE stride = (ITYPE)gridDim.x * kRThreads;
     for (ITYPE i = (ITYPE)blockIdx.x * kRThreads + threadIdx.x; i < dim; i += stride) {
-        const double p = norm2(ld_stream(s + i));
+        const double p = norm2(amp(s + i));
 #pragma unroll
         for (int w = 0; w < MAXZ; ++w)
             if (w < nz) acc[w] += (__popcll(i & zs[w]) & 1) ? -p : p;
@@ -181,7 +213,8 @@ static int pauli_term(const UINT* tl, const UINT* ids, UINT cnt, UINT n, PauliTe
     return QS_OK;
 }
 
-int ev_batch(const PauliTerm* terms, UINT count, const double2* s, ITYPE dim, cudaStream_t st, double* values) {
+template <class T>
+int ev_batch(const PauliTerm* terms, UINT count, const T* s, ITYPE dim, cudaStream_t st, double* values) {
     std::vector<int> zidx, xidx;
     for (UINT k = 0; k < count; ++k) (terms[k].x == 0 ? zidx : xidx).push_back((int)k);
     const unsigned blocks = reduce_blocks(dim);
@@ -197,7 +230,7 @@ int ev_batch(const PauliTerm* terms, UINT count, const double2* s, ITYPE dim, cu
         ITYPE hz[kZChunk];
         for (int w = 0; w < nz; ++w) hz[w] = terms[zidx[c0 + w]].z;
         QS_CUDA_CHECK(cudaMemcpyAsync(dz, hz, sizeof(ITYPE) * nz, cudaMemcpyHostToDevice, st));
-        k_ev_z_batch<kZChunk><<<blocks, kRThreads, 0, st>>>(s, dim, dz, nz, part);
+        k_ev_z_batch<kZChunk, T><<<blocks, kRThreads, 0, st>>>(s, dim, dz, nz, part);
         QS_TRY(check_launch("k_ev_z_batch"));
         double out[kZChunk];
         QS_TRY(finish_reduce(part, blocks, nz, st, out));
@@ -205,7 +238,7 @@ int ev_batch(const PauliTerm* terms, UINT count, const double2* s, ITYPE dim, cu
     }
     const unsigned xblocks = reduce_blocks(dim / 2);
     for (int k : xidx) {
-        k_ev_xz<<<xblocks, kRThreads, 0, st>>>(s, dim / 2, terms[k], part);
+        k_ev_xz<T><<<xblocks, kRThreads, 0, st>>>(s, dim / 2, terms[k], part);
         QS_TRY(check_launch("k_ev_xz"));
         QS_TRY(finish_reduce(part, xblocks, 1, st, &values[k]));
     }
@@ -225,8 +258,13 @@ __device__ __forceinline__ double prob_at(const double2* s, ITYPE i, ITYPE diag_
     const double2 v = s[i * diag_stride];
     return sqrt(norm2(v));
 }
+__device__ __forceinline__ double prob_at(const float2* s, ITYPE i, ITYPE) {
+    const float2 v = s[i];
+    return norm2(make_double2((double)v.x, (double)v.y));
+}
 
-__global__ void __launch_bounds__(256) k_chunk_sums(const double2* __restrict__ s, ITYPE dim, ITYPE diag_stride,
+template <class T>
+__global__ void __launch_bounds__(256) k_chunk_sums(const T* __restrict__ s, ITYPE dim, ITYPE diag_stride,
     double* __restrict__ sums) {
     __shared__ double sm[32];
     const ITYPE c0 = (ITYPE)blockIdx.x * kChunk;
@@ -263,7 +301,8 @@ __global__ void __launch_bounds__(1024) k_scan_sums(const double* __restrict__ s
 }
 
 // One warp per shot.
-__global__ void k_sample(const double2* __restrict__ s, ITYPE dim, ITYPE diag_stride, const double* __restrict__ incl,
+template <class T>
+__global__ void k_sample(const T* __restrict__ s, ITYPE dim, ITYPE diag_stride, const double* __restrict__ incl,
     ITYPE nchunks, const double* __restrict__ uniforms, UINT count, ITYPE* __restrict__ out) {
     const int lane = threadIdx.x & 31;
     const UINT shot = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -316,7 +355,8 @@ __global__ void k_sample(const double2* __restrict__ s, ITYPE dim, ITYPE diag_st
     }
 }
 
-int sample_with_uniforms(const double2* s, ITYPE dim, ITYPE diag_stride, const double* uniforms, UINT count,
+template <class T>
+int sample_with_uniforms_t(const T* s, ITYPE dim, ITYPE diag_stride, const double* uniforms, UINT count,
     ITYPE* out, cudaStream_t st) {
     if (count == 0) return QS_OK;
     const ITYPE nchunks = (dim + kChunk - 1) / kChunk;
@@ -328,17 +368,21 @@ int sample_with_uniforms(const double2* s, ITYPE dim, ITYPE diag_stride, const d
     double* du = incl + nchunks;
     ITYPE* dout = (ITYPE*)(du + count);
     QS_CUDA_CHECK(cudaMemcpyAsync(du, uniforms, sizeof(double) * count, cudaMemcpyHostToDevice, st));
-    k_chunk_sums<<<(unsigned)nchunks, 256, 0, st>>>(s, dim, diag_stride, sums);
+    k_chunk_sums<T><<<(unsigned)nchunks, 256, 0, st>>>(s, dim, diag_stride, sums);
     QS_TRY(check_launch("k_chunk_sums"));
     k_scan_sums<<<1, 1024, 0, st>>>(sums, nchunks, incl);
     QS_TRY(check_launch("k_scan_sums"));
     const unsigned threads = 256;
     const unsigned blocks = (unsigned)(((ITYPE)count * 32 + threads - 1) / threads);
-    k_sample<<<blocks, threads, 0, st>>>(s, dim, diag_stride, incl, nchunks, du, count, dout);
+    k_sample<T><<<blocks, threads, 0, st>>>(s, dim, diag_stride, incl, nchunks, du, count, dout);
     QS_TRY(check_launch("k_sample"));
     QS_CUDA_CHECK(cudaMemcpyAsync(out, dout, sizeof(ITYPE) * count, cudaMemcpyDeviceToHost, st));
     QS_CUDA_CHECK(cudaStreamSynchronize(st));
     return QS_OK;
+}
+int sample_with_uniforms(const double2* s, ITYPE dim, ITYPE diag_stride, const double* uniforms, UINT count,
+    ITYPE* out, cudaStream_t st) {
+    return sample_with_uniforms_t<double2>(s, dim, diag_stride, uniforms, count, out, st);
 }
 
 // ---------------------------------------------------------------- sampling without allocation
@@ -438,7 +482,7 @@ QS_API int qs_expectation_value_multi_qubit_Pauli_operator_partial_list(const QS
     QS_TRY(check_dim(dim, &n));
     PauliTerm t;
     QS_TRY(pauli_term(tl, ids, cnt, n, &t));
-    return ev_batch(&t, 1, (const double2*)state, dim, (cudaStream_t)stream, out);
+    return ev_batch<double2>(&t, 1, (const double2*)state, dim, (cudaStream_t)stream, out);
 }
 
 QS_API int qs_expectation_value_pauli_batch(const QS_ITYPE* x_masks, const QS_ITYPE* z_masks, const QS_UINT* y_counts,
@@ -454,7 +498,7 @@ QS_API int qs_expectation_value_pauli_batch(const QS_ITYPE* x_masks, const QS_IT
         terms[k].nrot = y_counts[k];
         terms[k].pivot = x_masks[k] ? (UINT)(63 - __builtin_clzll(x_masks[k])) : 0;
     }
-    return ev_batch(terms.data(), term_count, (const double2*)state, dim, (cudaStream_t)stream, values);
+    return ev_batch<double2>(terms.data(), term_count, (const double2*)state, dim, (cudaStream_t)stream, values);
 }
 
 QS_API int qs_transition_amplitude_multi_qubit_Pauli_operator_partial_list(const QS_UINT* tl, const QS_UINT* ids,
@@ -511,17 +555,57 @@ QS_API int qs_state_sampling_with_uniforms_noalloc(const void* state, QS_ITYPE d
     double* du = incl + kNoAllocChunks;
     ITYPE* dout = (ITYPE*)(du + kNoAllocMaxShots);
     QS_CUDA_CHECK(cudaMemcpyAsync(du, uniforms, sizeof(double) * count, cudaMemcpyHostToDevice, st));
-    k_chunk_sums<<<(unsigned)nchunks, 256, 0, st>>>((const double2*)state, dim, 0, sums);
+    k_chunk_sums<double2><<<(unsigned)nchunks, 256, 0, st>>>((const double2*)state, dim, 0, sums);
     QS_TRY(check_launch("k_chunk_sums"));
     k_scan_sums<<<1, 1024, 0, st>>>(sums, nchunks, incl);
     QS_TRY(check_launch("k_scan_sums"));
     const unsigned threads = 256;
     const unsigned blocks = (unsigned)(((ITYPE)count * 32 + threads - 1) / threads);
-    k_sample<<<blocks, threads, 0, st>>>((const double2*)state, dim, 0, incl, nchunks, du, count, dout);
+    k_sample<double2><<<blocks, threads, 0, st>>>((const double2*)state, dim, 0, incl, nchunks, du, count, dout);
     QS_TRY(check_launch("k_sample"));
     QS_CUDA_CHECK(cudaMemcpyAsync(out, dout, sizeof(ITYPE) * count, cudaMemcpyDeviceToHost, st));
     QS_CUDA_CHECK(cudaStreamSynchronize(st));
     return QS_OK;
+}
+
+// ---- complex64 states: FP64 accumulation over single-precision amplitudes ----
+QS_API int qs_state_norm_squared_c64(const void* state, QS_ITYPE dim, void* stream, double* out) {
+    UINT n;
+    QS_TRY(check_dim(dim, &n));
+    return prob_sum_t<float2>((const float2*)state, dim, 0, 0, (cudaStream_t)stream, out);
+}
+QS_API int qs_state_inner_product_c128_c64(const void* bra_c128, const void* ket_c64, QS_ITYPE dim, void* stream,
+    double out[2]) {
+    UINT n;
+    QS_TRY(check_dim(dim, &n));
+    cudaStream_t st = (cudaStream_t)stream;
+    const unsigned blocks = reduce_blocks(dim);
+    void* buf;
+    QS_TRY(scratch(st, sizeof(double) * (2 * blocks + 2), &buf));
+    k_inner_mixed<<<blocks, kRThreads, 0, st>>>((const double2*)bra_c128, (const float2*)ket_c64, dim, (double*)buf);
+    QS_TRY(check_launch("k_inner_mixed"));
+    return finish_reduce((double*)buf, blocks, 2, st, out);
+}
+QS_API int qs_expectation_value_pauli_batch_c64(const QS_ITYPE* x_masks, const QS_ITYPE* z_masks,
+    const QS_UINT* y_counts, QS_UINT term_count, const void* state, QS_ITYPE dim, void* stream, double* values) {
+    UINT n;
+    QS_TRY(check_dim(dim, &n));
+    std::vector<PauliTerm> terms(term_count);
+    for (UINT k = 0; k < term_count; ++k) {
+        if ((x_masks[k] | z_masks[k]) >> n)
+            return set_error(QS_ERR_INVALID_ARGUMENT, "expectation_value_pauli_batch_c64: mask beyond qubit count");
+        terms[k].x = x_masks[k];
+        terms[k].z = z_masks[k];
+        terms[k].nrot = y_counts[k];
+        terms[k].pivot = x_masks[k] ? (UINT)(63 - __builtin_clzll(x_masks[k])) : 0;
+    }
+    return ev_batch<float2>(terms.data(), term_count, (const float2*)state, dim, (cudaStream_t)stream, values);
+}
+QS_API int qs_state_sampling_with_uniforms_c64(const void* state, QS_ITYPE dim, const double* uniforms,
+    QS_UINT count, QS_ITYPE* out, void* stream) {
+    UINT n;
+    QS_TRY(check_dim(dim, &n));
+    return sample_with_uniforms_t<float2>((const float2*)state, dim, 0, uniforms, count, out, (cudaStream_t)stream);
 }
 
 QS_API int qs_reference_uniforms(QS_UINT seed, QS_UINT count, double* out) {

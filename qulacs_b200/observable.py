@@ -111,7 +111,9 @@ class Observable:
         ny = np.zeros(k, dtype=np.uint32)
         for i, t in enumerate(self.terms):
             xm[i], zm[i], ny[i] = masks(t.targets, t.ids)
-        call("qs_expectation_value_pauli_batch", xm.ctypes.data_as(C.c_void_p), zm.ctypes.data_as(C.c_void_p),
+        fn = "qs_expectation_value_pauli_batch_c64" if type(state).__name__ == "QuantumStateC64" else \
+            "qs_expectation_value_pauli_batch"
+        call(fn, xm.ctypes.data_as(C.c_void_p), zm.ctypes.data_as(C.c_void_p),
              ny.ctypes.data_as(C.c_void_p), k, state.data_ptr(), state.dim, state.stream,
              vals.ctypes.data_as(C.c_void_p))
         return vals

@@ -131,6 +131,89 @@ class QuantumState:
             self._ptr = None
 
 
+class QuantumStateC64:
+    """n-qubit complex64 state vector in HBM for the fused reduced-precision path.
+
+    Reductions on it (norm, <P>, inner product with a complex128 state, sampling prefix sums) read
+    the single-precision amplitudes and accumulate in FP64.
+    """
+
+    def __init__(self, qubit_count: int, stream: int | None = None):
+        _lib.load()
+        self.qubit_count = int(qubit_count)
+        self.dim = 1 << self.qubit_count
+        self.stream = _default_stream if stream is None else stream
+        p = C.c_void_p()
+        call("qs_allocate_quantum_state_c64", self.dim, C.byref(p))
+        self._ptr = p.value
+        self.set_zero_state()
+
+    def get_qubit_count(self) -> int:
+        return self.qubit_count
+
+    def get_device_name(self) -> str:
+        return "gpu"
+
+    def is_state_vector(self) -> bool:
+        return True
+
+    def data_ptr(self) -> int:
+        return self._ptr
+
+    def set_zero_state(self) -> None:
+        call("qs_initialize_quantum_state_c64", self._ptr, self.dim, self.stream)
+
+    def load(self, src) -> None:
+        """From a complex128 QuantumState (rounded on the device) or a host vector."""
+        if isinstance(src, QuantumState):
+            call("qs_state_to_c64", src.data_ptr(), self._ptr, self.dim, self.stream)
+            return
+        v = np.ascontiguousarray(np.asarray(src, dtype=np.complex128))
+        tmp = QuantumState(self.qubit_count, self.stream)
+        tmp.load(v)
+        call("qs_state_to_c64", tmp.data_ptr(), self._ptr, self.dim, self.stream)
+        call("qs_stream_synchronize", self.stream)
+
+    def to_c128(self, out: QuantumState | None = None) -> QuantumState:
+        out = out or QuantumState(self.qubit_count, self.stream)
+        call("qs_state_to_c128", self._ptr, out.data_ptr(), self.dim, self.stream)
+        return out
+
+    def get_vector(self) -> np.ndarray:
+        return self.to_c128().get_vector()
+
+    def get_squared_norm(self) -> float:
+        out = C.c_double()
+        call("qs_state_norm_squared_c64", self._ptr, self.dim, self.stream, C.byref(out))
+        return out.value
+
+    def inner_product_with(self, bra: QuantumState) -> complex:
+        """<bra|self> with a complex128 bra, FP64 accumulation."""
+        out = np.zeros(2)
+        call("qs_state_inner_product_c128_c64", bra.data_ptr(), self._ptr, self.dim, self.stream, _ptr(out))
+        return complex(out[0], out[1])
+
+    def infidelity(self, reference: QuantumState) -> float:
+        """1 - |<reference|self>|^2 / (<self|self> <reference|reference>)."""
+        ip = self.inner_product_with(reference)
+        return 1.0 - abs(ip) ** 2 / (self.get_squared_norm() * reference.get_squared_norm())
+
+    def sampling_with_uniforms(self, uniforms) -> np.ndarray:
+        u = np.ascontiguousarray(np.asarray(uniforms, dtype=np.float64))
+        out = np.empty(u.size, dtype=np.uint64)
+        call("qs_state_sampling_with_uniforms_c64", self._ptr, self.dim, _ptr(u), u.size, _ptr(out), self.stream)
+        return out
+
+    def __del__(self):
+        p = getattr(self, "_ptr", None)
+        if p:
+            try:
+                _lib.load().qs_release_quantum_state(p)
+            except Exception:
+                pass
+            self._ptr = None
+
+
 def inner_product(bra: QuantumState, ket: QuantumState) -> complex:
     """csim state_inner_product (stat_ops.cpp:65-86): sum conj(bra_i) ket_i."""
     if bra.dim != ket.dim:
