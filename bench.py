@@ -220,6 +220,58 @@ def run_reference(args, rank: int, world: int):
     print(json.dumps(line), flush=True)
 
 
+def fused_comparison(n: int, layers: int, stream, with_gate_by_gate: bool, reps: int = 2):
+    """Config 3: U3 + CZ(random matching) circuit; fused complex64 (tensor cores) vs plain complex128.
+
+    Returns times (CUDA events), the infidelity 1 - |<psi_c128|psi_c64>|^2 and |d<H>| for 256 strings of
+    weight <= 4 (coefficients N(0, 1)), both sides evaluated on the device with FP64 accumulation."""
+    import torch
+
+    import qulacs_b200 as Q
+    from qulacs_b200 import workloads as W
+    gates = W.u3_cz_circuit(n, layers, seed=3003)
+    terms = W.random_pauli_terms(n, 256, 1, 4, seed=3004)
+    circ = W.to_circuit(gates, n)
+    obs = W.to_observable(terms, n)
+
+    def timed(fn):
+        fn()  # warm-up (plan build, first touch)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps / 1e3
+
+    plain = Q.QuantumState(n)
+    t_staged = timed(lambda: (plain.set_zero_state(), circ.update_quantum_state(plain, mode="staged")))
+    t_gbg = None
+    if with_gate_by_gate:
+        t_gbg = timed(lambda: (plain.set_zero_state(), circ.update_quantum_state(plain, mode="gate_by_gate")))
+    plain.set_zero_state()
+    circ.update_quantum_state(plain, mode="staged")
+    fused = Q.QuantumStateC64(n)
+    t_fused = timed(lambda: (fused.set_zero_state(), circ.update_quantum_state(fused)))
+    fused.set_zero_state()
+    circ.update_quantum_state(fused)
+    inf = fused.infidelity(plain)
+    coefs = np.array([c for c, _, _ in terms])
+    ev_plain = obs.term_values(plain)
+    ev_fused = obs.term_values(fused)
+    passes, blocks = circ.fused_stats()
+    out = {"workload": f"U3 + CZ(random matching) n={n} layers={layers} ({len(gates)} gates)",
+           "plain_c128_staged_s": t_staged, "plain_c128_gate_by_gate_s": t_gbg, "fused_c64_tc_s": t_fused,
+           "speedup_vs_staged": t_staged / t_fused,
+           "speedup_vs_gate_by_gate": (t_gbg / t_fused) if t_gbg else None,
+           "infidelity": inf, "abs_dH": abs(float(np.dot(coefs, ev_plain - ev_fused))),
+           "max_abs_dP": float(np.max(np.abs(ev_plain - ev_fused))),
+           "fused_passes": passes, "fused_blocks": blocks, "staged_passes": circ.pass_count()}
+    del plain, fused
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -230,6 +282,11 @@ def main():
     ap.add_argument("--qubits", type=int, default=N_QUBITS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-kernel-table", action="store_true")
+    ap.add_argument("--workload", default="plain", choices=["plain", "fused"],
+                    help="fused: only the fused-vs-plain comparison (config 3)")
+    ap.add_argument("--fused-qubits", type=int, default=32)
+    ap.add_argument("--fused-layers", type=int, default=20)
+    ap.add_argument("--with-gate-by-gate", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3  # timing rule: at least 3 untimed warm-up steps
@@ -257,6 +314,11 @@ def main():
     stream = torch.cuda.current_stream()
     Q.set_default_stream(stream.cuda_stream)
     lib = _lib.load()
+    if args.workload == "fused":
+        r = fused_comparison(args.fused_qubits, args.fused_layers, stream, args.with_gate_by_gate)
+        if rank == 0:
+            print(json.dumps({"metric": "fused vs plain at infidelity<=1e-6", **r}), flush=True)
+        return
     gates = W.layered_rotation_circuit(n, DEPTH, GATE_SEED)
     terms = W.random_pauli_terms(n, N_TERMS, 1, 6, TERM_SEED)
     circ = W.to_circuit(gates, n)

@@ -54,6 +54,15 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return (uint32_t)__cvta_generic_to_shared(p);
 }
 
+// Tile layout swizzle: XOR tile bits 5..12 into bits 1..4 (bit 0 untouched, so amplitude pairs stay
+// adjacent for 16-byte copies), spreading block-bit strides over the shared-memory banks.
+__device__ __forceinline__ uint32_t tswz(uint32_t u) { return u ^ ((((u >> 5) ^ (u >> 9)) & 15u) << 1); }
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem_dst)), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // UMMA shared-memory descriptor: start >> 4 [0,14), LBO >> 4 [16,30), SBO >> 4 [32,46),
 // version 1 [46,48), layout SWIZZLE_NONE (0) [61,64).
 __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
@@ -143,27 +152,34 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused_pass(const __grid_consta
     const uint32_t idesc = idesc_bf16(kARows, (int)N);
     const uint32_t aaddr = smem_u32(sA), baddr = smem_u32(sB);
 
-    // global offset of tile index u: bits 0..7 from tid, bits 8.. from the iteration k
+    // Tile loads/stores move amplitude pairs (tile bit 0 = qubit 0), 16 B each: pair p = tid + 256 k
+    // holds tile bits 1..8 from tid and bits 9.. from k.
     ITYPE lo_off = 0;
-    for (int j = 0; j < 8 && j < m; ++j)
-        if ((tid >> j) & 1) lo_off |= 1ULL << a.q[j];
+    for (int j = 1; j <= 8 && j < m; ++j)
+        if ((tid >> (j - 1)) & 1) lo_off |= 1ULL << a.q[j];
+    const uint32_t npairs = tsize >> 1;
 
     for (ITYPE T = blockIdx.x; T < a.tiles; T += gridDim.x) {
         ITYPE base = T;
         for (int j = 0; j < m; ++j) base = insert0(base, a.q[j]);
-        // load tile
-        for (uint32_t k = 0; k * kFThreads < tsize; ++k) {
-            const uint32_t u = tid + k * kFThreads;
-            if (u < tsize) {
+        // load tile: all pairs in flight at once (cp.async, 16 B)
+#pragma unroll 4
+        for (uint32_t k = 0; k * kFThreads < npairs; ++k) {
+            const uint32_t pidx = tid + k * kFThreads;
+            if (pidx < npairs) {
                 ITYPE off = lo_off;
-                for (int j = 8; j < m; ++j)
-                    if ((k >> (j - 8)) & 1) off |= 1ULL << a.q[j];
-                tile[u] = a.state[base | off];
+                for (int j = 9; j < m; ++j)
+                    if ((k >> (j - 9)) & 1) off |= 1ULL << a.q[j];
+                cp_async16(tile + tswz(2 * pidx), a.state + (base | off));
             }
         }
+        cp_async_wait_all();
         __syncthreads();
         for (int b = 0; b < a.nblocks; ++b) {
             const uint8_t* bb = a.block_bits + b * kFBlock;
+            // A images for this block: asynchronous copy, overlapped with the B gather below
+            const uint4* img = a.images + (size_t)b * (2 * kAImageBytes / 16);
+            for (int i = tid; i < 2 * kAImageBytes / 16; i += kFThreads) cp_async16((uint4*)sA + i, img + i);
             // deposit tables: x (6 block bits) and c (the other m - 6 tile bits)
             if (tid < 64) {
                 uint32_t d = 0;
@@ -183,23 +199,28 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused_pass(const __grid_consta
                 }
                 dep_c[tid] = d;
             }
-            // A images for this block (both CTAs' copies come from L2)
-            const uint4* img = a.images + (size_t)b * (2 * kAImageBytes / 16);
-            uint4* sa4 = (uint4*)sA;
-            for (int i = tid; i < 2 * kAImageBytes / 16; i += kFThreads) sa4[i] = __ldg(img + i);
             __syncthreads();
-            // gather B: row c (coset), K = x (real part) and 64 + x (imaginary part), hi and lo
-            for (uint32_t i = tid; i < N * 64; i += kFThreads) {
-                const uint32_t x = i & 63u, c = i >> 6;
-                const float2 v = tile[dep_c[c] | dep_x[x]];
-                __nv_bfloat16_raw rh, rl, ih, il;
-                split_bf16(v.x, &rh, &rl);
-                split_bf16(v.y, &ih, &il);
-                *(__nv_bfloat16_raw*)(sB + kmajor_off(c, x)) = rh;
-                *(__nv_bfloat16_raw*)(sB + kmajor_off(c, 64 + x)) = ih;
-                *(__nv_bfloat16_raw*)(sB + bimg + kmajor_off(c, x)) = rl;
-                *(__nv_bfloat16_raw*)(sB + bimg + kmajor_off(c, 64 + x)) = il;
+            // gather B: row c (coset), K = x (real part) and 64 + x (imaginary part), hi and lo;
+            // one item = amplitudes x = 2j, 2j + 1 of coset c, stored as bf16 pairs (4 B).  Within a
+            // warp, c varies fastest over 8 rows and j over 4, so the 32 stores cover 128 distinct bytes.
+            for (uint32_t i = tid; i < N * 32; i += kFThreads) {
+                const uint32_t c = (i & 7u) | ((i >> 8) << 3);
+                const uint32_t j = ((i >> 3) & 3u) | (((i >> 5) & 7u) << 2);
+                const uint32_t x0 = 2 * j;
+                const uint32_t cb = dep_c[c];
+                const float2 v0 = tile[tswz(cb | dep_x[x0])];
+                const float2 v1 = tile[tswz(cb | dep_x[x0 + 1])];
+                __nv_bfloat16_raw h0, l0, h1, l1;
+                split_bf16(v0.x, &h0, &l0);
+                split_bf16(v1.x, &h1, &l1);
+                *(uint32_t*)(sB + kmajor_off(c, x0)) = (uint32_t)h0.x | ((uint32_t)h1.x << 16);
+                *(uint32_t*)(sB + bimg + kmajor_off(c, x0)) = (uint32_t)l0.x | ((uint32_t)l1.x << 16);
+                split_bf16(v0.y, &h0, &l0);
+                split_bf16(v1.y, &h1, &l1);
+                *(uint32_t*)(sB + kmajor_off(c, 64 + x0)) = (uint32_t)h0.x | ((uint32_t)h1.x << 16);
+                *(uint32_t*)(sB + bimg + kmajor_off(c, 64 + x0)) = (uint32_t)l0.x | ((uint32_t)l1.x << 16);
             }
+            cp_async_wait_all();
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             asm volatile("tcgen05.fence::before_thread_sync;");
             __syncthreads();
@@ -235,7 +256,7 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused_pass(const __grid_consta
                 tmem_ld16(tmem + ((32u * (warp & 3)) << 16) + c0, v);
 #pragma unroll
                 for (int i = 0; i < 16; ++i) {
-                    float* dst = (float*)&tile[dep_c[c0 + i] | xo];
+                    float* dst = (float*)&tile[tswz(dep_c[c0 + i] | xo)];
                     dst[y >> 6] = v[i];
                 }
             }
@@ -244,14 +265,15 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused_pass(const __grid_consta
             if (*s_err) break;
         }
         if (*s_err) break;
-        // store tile
-        for (uint32_t k = 0; k * kFThreads < tsize; ++k) {
-            const uint32_t u = tid + k * kFThreads;
-            if (u < tsize) {
+        // store tile (16-byte pairs)
+        for (uint32_t k = 0; k * kFThreads < npairs; ++k) {
+            const uint32_t pidx = tid + k * kFThreads;
+            if (pidx < npairs) {
                 ITYPE off = lo_off;
-                for (int j = 8; j < m; ++j)
-                    if ((k >> (j - 8)) & 1) off |= 1ULL << a.q[j];
-                a.state[base | off] = tile[u];
+                for (int j = 9; j < m; ++j)
+                    if ((k >> (j - 9)) & 1) off |= 1ULL << a.q[j];
+                const float4 v = *(const float4*)(tile + tswz(2 * pidx));
+                __stcs((float4*)(a.state + (base | off)), v);
             }
         }
         __syncthreads();
