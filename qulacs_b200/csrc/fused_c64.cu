@@ -63,6 +63,17 @@ __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
+// Two floats -> packed bf16 pairs (a in the low half): hi = RN(v), lo = RN(v - hi).
+__device__ __forceinline__ void split2_bf16(float a, float b, uint32_t* hi, uint32_t* lo) {
+    uint32_t h;
+    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(h) : "f"(b), "f"(a));
+    const float ha = __uint_as_float(h << 16), hb = __uint_as_float(h & 0xFFFF0000u);
+    uint32_t l;
+    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(l) : "f"(b - hb), "f"(a - ha));
+    *hi = h;
+    *lo = l;
+}
+
 // UMMA shared-memory descriptor: start >> 4 [0,14), LBO >> 4 [16,30), SBO >> 4 [32,46),
 // version 1 [46,48), layout SWIZZLE_NONE (0) [61,64).
 __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
@@ -180,12 +191,13 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused_pass(const __grid_consta
             // A images for this block: asynchronous copy, overlapped with the B gather below
             const uint4* img = a.images + (size_t)b * (2 * kAImageBytes / 16);
             for (int i = tid; i < 2 * kAImageBytes / 16; i += kFThreads) cp_async16((uint4*)sA + i, img + i);
-            // deposit tables: x (6 block bits) and c (the other m - 6 tile bits)
+            // deposit tables, pre-swizzled (tswz is XOR-linear, so the swizzled index of coset c and
+            // block index x is sdep_c[c] ^ sdep_x[x]): x over the 6 block bits, c over the other bits
             if (tid < 64) {
                 uint32_t d = 0;
                 for (int j = 0; j < kFBlock; ++j)
                     if ((tid >> j) & 1) d |= 1u << bb[j];
-                dep_x[tid] = d;
+                dep_x[tid] = tswz(d);
             }
             if ((uint32_t)tid < N) {
                 uint32_t d = 0, bit = 0;
@@ -197,28 +209,31 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused_pass(const __grid_consta
                         ++bit;
                     }
                 }
-                dep_c[tid] = d;
+                dep_c[tid] = tswz(d);
             }
             __syncthreads();
-            // gather B: row c (coset), K = x (real part) and 64 + x (imaginary part), hi and lo;
-            // one item = amplitudes x = 2j, 2j + 1 of coset c, stored as bf16 pairs (4 B).  Within a
-            // warp, c varies fastest over 8 rows and j over 4, so the 32 stores cover 128 distinct bytes.
-            for (uint32_t i = tid; i < N * 32; i += kFThreads) {
-                const uint32_t c = (i & 7u) | ((i >> 8) << 3);
-                const uint32_t j = ((i >> 3) & 3u) | (((i >> 5) & 7u) << 2);
-                const uint32_t x0 = 2 * j;
-                const uint32_t cb = dep_c[c];
-                const float2 v0 = tile[tswz(cb | dep_x[x0])];
-                const float2 v1 = tile[tswz(cb | dep_x[x0 + 1])];
-                __nv_bfloat16_raw h0, l0, h1, l1;
-                split_bf16(v0.x, &h0, &l0);
-                split_bf16(v1.x, &h1, &l1);
-                *(uint32_t*)(sB + kmajor_off(c, x0)) = (uint32_t)h0.x | ((uint32_t)h1.x << 16);
-                *(uint32_t*)(sB + bimg + kmajor_off(c, x0)) = (uint32_t)l0.x | ((uint32_t)l1.x << 16);
-                split_bf16(v0.y, &h0, &l0);
-                split_bf16(v1.y, &h1, &l1);
-                *(uint32_t*)(sB + kmajor_off(c, 64 + x0)) = (uint32_t)h0.x | ((uint32_t)h1.x << 16);
-                *(uint32_t*)(sB + bimg + kmajor_off(c, 64 + x0)) = (uint32_t)l0.x | ((uint32_t)l1.x << 16);
+            // gather B: row c (coset), K = x (real part) and 64 + x (imaginary part), hi and lo.
+            // Thread t owns block indices x = 2j, 2j + 1 with j = bits 3..7 of t, and cosets
+            // c = (t & 7) + 8 i: its B offsets are fixed up to i * 2048, and within a warp the 32
+            // 4-byte stores cover 128 distinct bytes.
+            {
+                const uint32_t j = ((tid >> 3) & 3u) | (((tid >> 5) & 7u) << 2);
+                const uint32_t c0 = tid & 7u;
+                const uint32_t sx0 = dep_x[2 * j], sx1 = dep_x[2 * j + 1];
+                unsigned char* ore = sB + kmajor_off(c0, 2 * j);
+                unsigned char* oim = sB + kmajor_off(c0, 64 + 2 * j);
+                for (uint32_t i = 0; c0 + 8 * i < N; ++i) {
+                    const uint32_t cb = dep_c[c0 + 8 * i];
+                    const float2 v0 = tile[cb ^ sx0];
+                    const float2 v1 = tile[cb ^ sx1];
+                    uint32_t hi, lo;
+                    split2_bf16(v0.x, v1.x, &hi, &lo);
+                    *(uint32_t*)(ore + i * 2048) = hi;
+                    *(uint32_t*)(ore + bimg + i * 2048) = lo;
+                    split2_bf16(v0.y, v1.y, &hi, &lo);
+                    *(uint32_t*)(oim + i * 2048) = hi;
+                    *(uint32_t*)(oim + bimg + i * 2048) = lo;
+                }
             }
             cp_async_wait_all();
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -256,7 +271,7 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused_pass(const __grid_consta
                 tmem_ld16(tmem + ((32u * (warp & 3)) << 16) + c0, v);
 #pragma unroll
                 for (int i = 0; i < 16; ++i) {
-                    float* dst = (float*)&tile[tswz(dep_c[c0 + i] | xo)];
+                    float* dst = (float*)&tile[dep_c[c0 + i] ^ xo];
                     dst[y >> 6] = v[i];
                 }
             }
