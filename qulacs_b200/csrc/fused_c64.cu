@@ -29,7 +29,8 @@ namespace qs {
 constexpr int kFTileMax = 13;      // tile qubits (2^13 c64 amplitudes = 64 KiB)
 constexpr int kFLow = 5;            // qubits 0..4 always in a tile
 constexpr int kFBlock = 6;          // qubits per fused block
-constexpr int kFThreads = 256;
+constexpr int kFThreads = 512;
+constexpr int kFTidBits = 9;      // log2(kFThreads)
 constexpr int kARows = 128, kAK = 128;           // real-ified block matrix
 constexpr int kAImageBytes = kARows * kAK * 2;   // one bf16 image (hi or lo): 32 KiB
 constexpr long long kWaitLimit = 4000000000LL;   // ~2 s of clock64 at 2 GHz
@@ -163,10 +164,10 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused_pass(const __grid_consta
     const uint32_t idesc = idesc_bf16(kARows, (int)N);
     const uint32_t aaddr = smem_u32(sA), baddr = smem_u32(sB);
 
-    // Tile loads/stores move amplitude pairs (tile bit 0 = qubit 0), 16 B each: pair p = tid + 256 k
-    // holds tile bits 1..8 from tid and bits 9.. from k.
+    // Tile loads/stores move amplitude pairs (tile bit 0 = qubit 0), 16 B each: pair p = tid + 512 k
+    // holds tile bits 1..9 from tid and bits 10.. from k.
     ITYPE lo_off = 0;
-    for (int j = 1; j <= 8 && j < m; ++j)
+    for (int j = 1; j <= kFTidBits && j < m; ++j)
         if ((tid >> (j - 1)) & 1) lo_off |= 1ULL << a.q[j];
     const uint32_t npairs = tsize >> 1;
 
@@ -179,8 +180,8 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused_pass(const __grid_consta
             const uint32_t pidx = tid + k * kFThreads;
             if (pidx < npairs) {
                 ITYPE off = lo_off;
-                for (int j = 9; j < m; ++j)
-                    if ((k >> (j - 9)) & 1) off |= 1ULL << a.q[j];
+                for (int j = kFTidBits + 1; j < m; ++j)
+                    if ((k >> (j - kFTidBits - 1)) & 1) off |= 1ULL << a.q[j];
                 cp_async16(tile + tswz(2 * pidx), a.state + (base | off));
             }
         }
@@ -214,25 +215,26 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused_pass(const __grid_consta
             __syncthreads();
             // gather B: row c (coset), K = x (real part) and 64 + x (imaginary part), hi and lo.
             // Thread t owns block indices x = 2j, 2j + 1 with j = bits 3..7 of t, and cosets
-            // c = (t & 7) + 8 i: its B offsets are fixed up to i * 2048, and within a warp the 32
-            // 4-byte stores cover 128 distinct bytes.
+            // c = (t & 7) + 8 (t >> 8) + 16 i: its B offsets are fixed up to i * 4096, and within a warp
+            // the 32 4-byte stores cover 128 distinct bytes.
             {
                 const uint32_t j = ((tid >> 3) & 3u) | (((tid >> 5) & 7u) << 2);
-                const uint32_t c0 = tid & 7u;
+                const uint32_t c0 = (tid & 7u) | ((uint32_t)(tid >> 8) << 3);
                 const uint32_t sx0 = dep_x[2 * j], sx1 = dep_x[2 * j + 1];
                 unsigned char* ore = sB + kmajor_off(c0, 2 * j);
                 unsigned char* oim = sB + kmajor_off(c0, 64 + 2 * j);
-                for (uint32_t i = 0; c0 + 8 * i < N; ++i) {
-                    const uint32_t cb = dep_c[c0 + 8 * i];
+#pragma unroll 2
+                for (uint32_t i = 0; c0 + 16 * i < N; ++i) {
+                    const uint32_t cb = dep_c[c0 + 16 * i];
                     const float2 v0 = tile[cb ^ sx0];
                     const float2 v1 = tile[cb ^ sx1];
                     uint32_t hi, lo;
                     split2_bf16(v0.x, v1.x, &hi, &lo);
-                    *(uint32_t*)(ore + i * 2048) = hi;
-                    *(uint32_t*)(ore + bimg + i * 2048) = lo;
+                    *(uint32_t*)(ore + i * 4096) = hi;
+                    *(uint32_t*)(ore + bimg + i * 4096) = lo;
                     split2_bf16(v0.y, v1.y, &hi, &lo);
-                    *(uint32_t*)(oim + i * 2048) = hi;
-                    *(uint32_t*)(oim + bimg + i * 2048) = lo;
+                    *(uint32_t*)(oim + i * 4096) = hi;
+                    *(uint32_t*)(oim + bimg + i * 4096) = lo;
                 }
             }
             cp_async_wait_all();
@@ -260,11 +262,12 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused_pass(const __grid_consta
             phase ^= 1u;
             if (!ok) *s_err = 1;
             asm volatile("tcgen05.fence::after_thread_sync;");
-            // read D: warp w reads TMEM lanes 32 (w % 4) .. +31 (rows y), column half w / 4
+            // warp w reads TMEM lanes 32 (w % 4) .. +31 (rows y) and column part w / 4
             const uint32_t y = 32u * (warp & 3) + lane;
-            const uint32_t half = N / 2 >= 16 ? N / 2 : N;
-            const uint32_t c_begin = (warp >> 2) * half;
-            const uint32_t c_end = (N / 2 >= 16) ? c_begin + half : ((warp >> 2) ? 0 : N);
+            const uint32_t parts = N >= 64 ? 4u : N / 16;
+            const uint32_t cw = N / parts;
+            const uint32_t c_begin = (uint32_t)(warp >> 2) < parts ? (warp >> 2) * cw : 0;
+            const uint32_t c_end = (uint32_t)(warp >> 2) < parts ? c_begin + cw : 0;
             const uint32_t xo = dep_x[y & 63u];
             for (uint32_t c0 = c_begin; c0 < c_end; c0 += 16) {
                 float v[16];
@@ -285,8 +288,8 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused_pass(const __grid_consta
             const uint32_t pidx = tid + k * kFThreads;
             if (pidx < npairs) {
                 ITYPE off = lo_off;
-                for (int j = 9; j < m; ++j)
-                    if ((k >> (j - 9)) & 1) off |= 1ULL << a.q[j];
+                for (int j = kFTidBits + 1; j < m; ++j)
+                    if ((k >> (j - kFTidBits - 1)) & 1) off |= 1ULL << a.q[j];
                 const float4 v = *(const float4*)(tile + tswz(2 * pidx));
                 __stcs((float4*)(a.state + (base | off)), v);
             }
