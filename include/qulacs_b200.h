@@ -262,6 +262,20 @@ QS_API int qs_circuit_pass_count(qs_circuit_t circuit, QS_ITYPE dim, QS_UINT* ou
 QS_API int qs_circuit_update_density_matrix(
     qs_circuit_t circuit, void* rho, QS_ITYPE dim, int exec_mode, void* stream);
 
+/* ---- batched execution of many circuits (no reference counterpart: the reference runs one
+ * QuantumCircuit::update_quantum_state at a time) ----
+ * Applies circuits[i] to states[i] (complex128, 2^n_i amplitudes, n_i >= 4, every gate stageable:
+ * <= 2 targets, no controls) for all i in ONE persistent kernel launch; each state's result is the
+ * same as running its circuit alone with QS_EXEC_STAGED.  Synchronises `stream`. */
+QS_API int qs_batch_update_quantum_states(const qs_circuit_t* circuits, void* const* states, QS_UINT count,
+    void* stream);
+/* <P_k> for the Pauli terms of many complex128 states in one launch.  Terms of state i are
+ * term_offsets[i] .. term_offsets[i+1]-1 (masks as qs_expectation_value_pauli_batch); values[k]
+ * receives <P_k>.  Synchronises `stream`. */
+QS_API int qs_batch_expectation_values(void* const* states, const QS_UINT* qubit_counts, QS_UINT count,
+    const QS_UINT* term_offsets, const QS_ITYPE* x_masks, const QS_ITYPE* z_masks, const QS_UINT* y_counts,
+    double* values, void* stream);
+
 /* ---- fused reduced-precision execution (no reference counterpart; its comparison point is the
  * reference's gate merging, QuantumCircuitOptimizer::optimize, cppsim/circuit_optimizer.cpp:113-168,
  * and gate::merge, cppsim/gate_merge.cpp:316-356) ----

@@ -187,13 +187,21 @@ __device__ __forceinline__ void apply_op(const StOp& op, double2 (&r)[16], const
 // so swz(a | b) = swz(a) ^ swz(b) for disjoint bit sets).
 __device__ __forceinline__ UINT swz(UINT u) { return u ^ (((u >> 4) ^ (u >> 7) ^ (u >> 10)) & 7u); }
 
-__global__ void __launch_bounds__(kStThreads, 3) k_staged_pass(double2* __restrict__ s, const __grid_constant__ StPassArgs a) {
-    __shared__ double2 tile[1 << kTileBits];
-    __shared__ ITYPE hi_off[16];
-    __shared__ UINT s_off[16];
+struct StSmem {
+    double2 tile[1 << kTileBits];
+    ITYPE hi_off[16];
+    UINT s_off[16];
+};
+
+// One tile of one pass: load, apply every phase, store.  Shared by the per-pass kernel and the
+// persistent multi-circuit kernel (batch.cu).  Ends with a CTA barrier so the shared buffers can be
+// reused immediately.
+__device__ __forceinline__ void staged_tile(double2* __restrict__ s, const StPassArgs& a, ITYPE T, StSmem& sm) {
+    double2* tile = sm.tile;
+    ITYPE* hi_off = sm.hi_off;
+    UINT* s_off = sm.s_off;
     const int m = a.m;
     const UINT tsize = 1u << m;
-    const ITYPE T = blockIdx.x;
     // base: insert zeros at the tile qubits into the tile index
     ITYPE base = T;
     for (int j = 0; j < m; ++j) base = insert0(base, a.q[j]);
@@ -254,6 +262,12 @@ __global__ void __launch_bounds__(kStThreads, 3) k_staged_pass(double2* __restri
         for (int k = 0; k < 16; ++k)
             if ((UINT)tid + (UINT)k * kStThreads < tsize) st_stream(s + (base | lo_off | hi_off[k]), v[k]);
     }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kStThreads, 3) k_staged_pass(double2* __restrict__ s, const __grid_constant__ StPassArgs a) {
+    __shared__ StSmem sm;
+    staged_tile(s, a, blockIdx.x, sm);
 }
 
 // ---------------------------------------------------------------- host scheduler
@@ -638,3 +652,147 @@ int staged_phase_count(Circuit& c, UINT* out) {
 }
 
 }  // namespace qs
+
+// ---------------------------------------------------------------- batched execution
+// Many circuits (each on its own state, of any size >= 4 qubits) in ONE persistent launch.  Work
+// items are (circuit, pass, tile); the queue lists every circuit's pass 0, then every circuit's
+// pass 1, and so on.  A CTA takes the next item with an atomic counter and, for pass p > 0, waits
+// until all tiles of pass p - 1 of the same circuit are done (acquire load of a per-pass counter).
+// Dependencies only point to earlier queue items, which resident CTAs already hold, so the wait
+// always ends; it is still bounded (about 2 s) and reports QS_ERR_TIMEOUT through an error flag.
+namespace qs {
+
+struct BatchRec {
+    StPassArgs args;
+    double2* state;
+    ITYPE tiles;
+    ITYPE prefix;  // first work item of this record
+    int dep;       // record of the previous pass of the same circuit, -1 for pass 0
+};
+
+constexpr unsigned kBatchSpinLimit = 1u << 25;  // x ~64 ns sleeps
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__global__ void __launch_bounds__(kStThreads, 3) k_batch_staged(const BatchRec* __restrict__ recs, int nrec,
+    ITYPE total, unsigned long long* head, unsigned* done, int* err) {
+    __shared__ StSmem sm;
+    __shared__ ITYPE s_item;
+    __shared__ int s_rec, s_abort;
+    __shared__ StPassArgs s_args;  // the record's pass, copied so the tile code indexes shared memory
+    __shared__ double2* s_state;
+    const int tid = threadIdx.x;
+    while (true) {
+        if (tid == 0) {
+            s_abort = 0;
+            s_item = atomicAdd(head, 1ULL);
+            if (s_item < total) {
+                int lo = 0, hi = nrec - 1;  // last record with prefix <= item
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) / 2;
+                    if (recs[mid].prefix <= s_item) lo = mid;
+                    else hi = mid - 1;
+                }
+                s_rec = lo;
+                const int dep = recs[lo].dep;
+                if (dep >= 0) {
+                    const unsigned need = (unsigned)recs[dep].tiles;
+                    unsigned it = 0;
+                    while (ld_acquire_u32(done + dep) < need) {
+                        if (++it > kBatchSpinLimit) {
+                            atomicExch(err, 1);
+                            s_abort = 1;
+                            break;
+                        }
+                        __nanosleep(64);
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        if (s_item >= total || s_abort) break;
+        if (tid == 0) {
+            s_args = recs[s_rec].args;
+            s_state = recs[s_rec].state;
+        }
+        __syncthreads();
+        staged_tile(s_state, s_args, s_item - recs[s_rec].prefix, sm);
+        if (tid == 0) {
+            __threadfence();
+            atomicAdd(done + s_rec, 1u);
+        }
+    }
+}
+
+int batch_update(Circuit* const* cs, void* const* states, UINT count, cudaStream_t st) {
+    if (count == 0) return QS_OK;
+    std::vector<std::vector<const DevPass*>> passes(count);
+    size_t maxp = 0;
+    for (UINT i = 0; i < count; ++i) {
+        Circuit& c = *cs[i];
+        if (c.n < kPhaseBits) return set_error(QS_ERR_NOT_SUPPORTED, "batch: circuits need at least 4 qubits");
+        QS_TRY(ensure_plan(c, 1ULL << c.n));
+        for (const DevPass& d : c.plan->passes) {
+            if (d.single)
+                return set_error(QS_ERR_NOT_SUPPORTED,
+                    "batch: every gate must be stageable (<= 2 targets, no controls, no Pauli strings)");
+            passes[i].push_back(&d);
+        }
+        maxp = std::max(maxp, passes[i].size());
+    }
+    std::vector<BatchRec> recs;
+    std::vector<int> last(count, -1);
+    ITYPE total = 0;
+    for (size_t p = 0; p < maxp; ++p)
+        for (UINT i = 0; i < count; ++i) {
+            if (p >= passes[i].size()) continue;
+            BatchRec r{};
+            r.args = passes[i][p]->args;
+            r.state = (double2*)states[i];
+            r.tiles = (1ULL << cs[i]->n) >> r.args.m;
+            r.prefix = total;
+            r.dep = last[i];
+            last[i] = (int)recs.size();
+            total += r.tiles;
+            recs.push_back(r);
+        }
+    if (recs.empty()) return QS_OK;
+    const size_t brec = sizeof(BatchRec) * recs.size();
+    const size_t bdone = sizeof(unsigned) * recs.size();
+    void* buf = nullptr;
+    QS_TRY(scratch(st, brec + bdone + 256, &buf));
+    BatchRec* drec = (BatchRec*)buf;
+    unsigned* ddone = (unsigned*)((char*)buf + brec);
+    unsigned long long* dhead = (unsigned long long*)((char*)buf + ((brec + bdone + 15) / 16 * 16));
+    int* derr = (int*)(dhead + 1);
+    QS_CUDA_CHECK(cudaMemcpyAsync(drec, recs.data(), brec, cudaMemcpyHostToDevice, st));
+    QS_CUDA_CHECK(cudaMemsetAsync(ddone, 0, (brec + bdone + 256) - brec, st));
+    int per_sm = 0;
+    QS_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_staged, kStThreads, 0));
+    const ITYPE resident = (ITYPE)std::max(1, per_sm) * sm_count();
+    const unsigned grid = (unsigned)std::min<ITYPE>(resident, total);
+    k_batch_staged<<<grid, kStThreads, 0, st>>>(drec, (int)recs.size(), total, dhead, ddone, derr);
+    QS_TRY(check_launch("k_batch_staged"));
+    int err = 0;
+    QS_CUDA_CHECK(cudaMemcpyAsync(&err, derr, sizeof(int), cudaMemcpyDeviceToHost, st));
+    QS_CUDA_CHECK(cudaStreamSynchronize(st));
+    if (err) return set_error(QS_ERR_TIMEOUT, "batch: dependency wait expired");
+    return QS_OK;
+}
+
+}  // namespace qs
+
+extern "C" QS_API int qs_batch_update_quantum_states(const qs_circuit_t* circuits, void* const* states, QS_UINT count,
+    void* stream) {
+    if (!circuits || !states) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "null argument");
+    std::vector<qs::Circuit*> cs(count);
+    for (QS_UINT i = 0; i < count; ++i) {
+        cs[i] = reinterpret_cast<qs::Circuit*>(circuits[i]);
+        if (!cs[i] || !states[i]) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "null circuit or state");
+    }
+    return qs::batch_update(cs.data(), states, count, (cudaStream_t)stream);
+}

@@ -617,3 +617,176 @@ QS_API int qs_reference_uniforms(QS_UINT seed, QS_UINT count, double* out) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- batched expectation values
+// <P_k> for the terms of MANY states in one persistent launch.  A job is either up to 16 Z-only terms
+// of one state (one pass over its amplitudes) or one term with a bit flip (one pass over its pairs);
+// jobs are cut into chunks of kEvChunk items, one CTA per chunk at a time; every chunk writes FP64
+// partial sums, which a second kernel folds per job in chunk order (deterministic).
+namespace qs {
+
+constexpr ITYPE kEvChunk = 1 << 14;
+constexpr int kEvZ = 16;
+
+struct EvJob {
+    const double2* s;
+    ITYPE items;   // amplitudes (Z job) or pairs (X job)
+    ITYPE prefix;  // first work item (chunk) of this job
+    ITYPE x, z;
+    UINT nrot, pivot;
+    int kind;      // 0: Z batch, 1: single term with bit flip
+    int nz;        // Z batch: number of terms
+    UINT zoff;     // Z batch: first index into zmasks / zout
+    UINT out;      // X job: output index
+};
+
+__global__ void __launch_bounds__(256) k_batch_ev(const EvJob* __restrict__ jobs, int njobs, ITYPE total,
+    const ITYPE* __restrict__ zmasks, double* __restrict__ partials) {
+    __shared__ double sm[32];
+    __shared__ int s_job;
+    for (ITYPE item = blockIdx.x; item < total; item += gridDim.x) {
+        if (threadIdx.x == 0) {
+            int lo = 0, hi = njobs - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) / 2;
+                if (jobs[mid].prefix <= item) lo = mid;
+                else hi = mid - 1;
+            }
+            s_job = lo;
+        }
+        __syncthreads();
+        const EvJob& J = jobs[s_job];
+        const ITYPE c0 = (item - J.prefix) * kEvChunk;
+        const ITYPE c1 = min(J.items, c0 + kEvChunk);
+        if (J.kind == 1) {
+            double acc = 0.;
+            for (ITYPE p = c0 + threadIdx.x; p < c1; p += blockDim.x) {
+                const ITYPE b0 = insert0(p, J.pivot), b1 = b0 ^ J.x;
+                const double2 v = cmul(ld_stream(J.s + b0), cconj(ld_stream(J.s + b1)));
+                const UINT r = J.nrot + 2u * (UINT)(__popcll(b0 & J.z) & 1);
+                acc += 2.0 * phase_re_part(v, r);
+            }
+            acc = block_sum(acc, sm);
+            if (threadIdx.x == 0) partials[item * kEvZ] = acc;
+        } else {
+            double acc[kEvZ];
+            ITYPE zs[kEvZ];
+#pragma unroll
+            for (int w = 0; w < kEvZ; ++w) {
+                acc[w] = 0.;
+                zs[w] = w < J.nz ? zmasks[J.zoff + w] : 0;
+            }
+            for (ITYPE i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
+                const double pr = norm2(ld_stream(J.s + i));
+#pragma unroll
+                for (int w = 0; w < kEvZ; ++w)
+                    if (w < J.nz) acc[w] += (__popcll(i & zs[w]) & 1) ? -pr : pr;
+            }
+#pragma unroll
+            for (int w = 0; w < kEvZ; ++w) {
+                if (w < J.nz) {  // uniform over the CTA
+                    const double v = block_sum(acc[w], sm);
+                    if (threadIdx.x == 0) partials[item * kEvZ + w] = v;
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void k_batch_ev_fold(const EvJob* __restrict__ jobs, const double* __restrict__ partials,
+    const UINT* __restrict__ zout, double* __restrict__ values) {
+    __shared__ double sm[32];
+    const EvJob& J = jobs[blockIdx.x];
+    const ITYPE nchunks = (J.items + kEvChunk - 1) / kEvChunk;
+    const int width = J.kind == 1 ? 1 : J.nz;
+    for (int w = 0; w < width; ++w) {
+        double v = 0.;
+        for (ITYPE c = threadIdx.x; c < nchunks; c += blockDim.x) v += partials[(J.prefix + c) * kEvZ + w];
+        v = block_sum(v, sm);
+        if (threadIdx.x == 0) values[J.kind == 1 ? J.out : zout[J.zoff + w]] = v;
+    }
+}
+
+}  // namespace qs
+
+extern "C" QS_API int qs_batch_expectation_values(void* const* states, const QS_UINT* qubit_counts, QS_UINT count,
+    const QS_UINT* term_offsets, const QS_ITYPE* x_masks, const QS_ITYPE* z_masks, const QS_UINT* y_counts,
+    double* values, void* stream) {
+    using namespace qs;
+    if (!states || !qubit_counts || !term_offsets || !values) return set_error(QS_ERR_INVALID_ARGUMENT, "null argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    std::vector<EvJob> jobs;
+    std::vector<ITYPE> zm;
+    std::vector<UINT> zout;
+    ITYPE total = 0;
+    const UINT nterms = term_offsets[count];
+    for (UINT i = 0; i < count; ++i) {
+        const UINT n = qubit_counts[i];
+        if (n < 1 || n > 40) return set_error(QS_ERR_INVALID_ARGUMENT, "batch expectation: bad qubit count");
+        const ITYPE dim = 1ULL << n;
+        std::vector<UINT> zlist;
+        for (UINT k = term_offsets[i]; k < term_offsets[i + 1]; ++k) {
+            if ((x_masks[k] | z_masks[k]) >> n)
+                return set_error(QS_ERR_INVALID_ARGUMENT, "batch expectation: mask beyond qubit count");
+            if (x_masks[k] == 0) {
+                zlist.push_back(k);
+                continue;
+            }
+            EvJob J{};
+            J.s = (const double2*)states[i];
+            J.items = dim / 2;
+            J.prefix = total;
+            J.x = x_masks[k];
+            J.z = z_masks[k];
+            J.nrot = y_counts[k];
+            J.pivot = (UINT)(63 - __builtin_clzll(x_masks[k]));
+            J.kind = 1;
+            J.out = k;
+            total += (J.items + kEvChunk - 1) / kEvChunk;
+            jobs.push_back(J);
+        }
+        for (size_t z0 = 0; z0 < zlist.size(); z0 += kEvZ) {
+            EvJob J{};
+            J.s = (const double2*)states[i];
+            J.items = dim;
+            J.prefix = total;
+            J.kind = 0;
+            J.nz = (int)std::min<size_t>(kEvZ, zlist.size() - z0);
+            J.zoff = (UINT)zm.size();
+            for (int w = 0; w < J.nz; ++w) {
+                zm.push_back(z_masks[zlist[z0 + w]]);
+                zout.push_back(zlist[z0 + w]);
+            }
+            total += (J.items + kEvChunk - 1) / kEvChunk;
+            jobs.push_back(J);
+        }
+    }
+    if (jobs.empty()) return QS_OK;
+    const size_t bj = sizeof(EvJob) * jobs.size(), bz = sizeof(ITYPE) * (zm.size() + 1),
+                 bo = sizeof(UINT) * (zout.size() + 1), bp = sizeof(double) * kEvZ * total,
+                 bv = sizeof(double) * nterms;
+    auto up = [](size_t b) { return (b + 255) / 256 * 256; };
+    void* buf;
+    QS_TRY(scratch(st, up(bj) + up(bz) + up(bo) + up(bp) + up(bv), &buf));
+    char* p = (char*)buf;
+    EvJob* dj = (EvJob*)p;
+    ITYPE* dz = (ITYPE*)(p + up(bj));
+    UINT* dzo = (UINT*)(p + up(bj) + up(bz));
+    double* dpart = (double*)(p + up(bj) + up(bz) + up(bo));
+    double* dval = (double*)(p + up(bj) + up(bz) + up(bo) + up(bp));
+    QS_CUDA_CHECK(cudaMemcpyAsync(dj, jobs.data(), bj, cudaMemcpyHostToDevice, st));
+    if (!zm.empty()) {
+        QS_CUDA_CHECK(cudaMemcpyAsync(dz, zm.data(), sizeof(ITYPE) * zm.size(), cudaMemcpyHostToDevice, st));
+        QS_CUDA_CHECK(cudaMemcpyAsync(dzo, zout.data(), sizeof(UINT) * zout.size(), cudaMemcpyHostToDevice, st));
+    }
+    QS_CUDA_CHECK(cudaMemsetAsync(dval, 0, bv, st));
+    const unsigned grid = (unsigned)std::min<ITYPE>(total, (ITYPE)sm_count() * 8);
+    k_batch_ev<<<grid, 256, 0, st>>>(dj, (int)jobs.size(), total, dz, dpart);
+    QS_TRY(check_launch("k_batch_ev"));
+    k_batch_ev_fold<<<(unsigned)jobs.size(), 256, 0, st>>>(dj, dpart, dzo, dval);
+    QS_TRY(check_launch("k_batch_ev_fold"));
+    QS_CUDA_CHECK(cudaMemcpyAsync(values, dval, bv, cudaMemcpyDeviceToHost, st));
+    QS_CUDA_CHECK(cudaStreamSynchronize(st));
+    return QS_OK;
+}
