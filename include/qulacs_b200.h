@@ -49,6 +49,9 @@ QS_API int qs_stream_synchronize(void* stream);
 QS_API int qs_allocate_quantum_state(QS_ITYPE dim, void** state_out);
 /* complex64 variant for the reduced-precision (fused) path: dim (re, im) floats. */
 QS_API int qs_allocate_quantum_state_c64(QS_ITYPE dim, void** state_out);
+/* Device buffer of `bytes` bytes (e.g. an arena that several states are carved from); release with
+ * qs_release_quantum_state.  No reference counterpart. */
+QS_API int qs_allocate_bytes(QS_ITYPE bytes, void** out);
 /* release_quantum_state (memory_ops.cpp:29-31). */
 QS_API int qs_release_quantum_state(void* state);
 /* initialize_quantum_state (init_ops_fill.cpp:10-23): |0...0>. */

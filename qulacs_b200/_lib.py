@@ -28,6 +28,7 @@ SIGNATURES = {
     "qs_allocate_quantum_state": [IT, C.POINTER(P)],
     "qs_allocate_quantum_state_c64": [IT, C.POINTER(P)],
     "qs_release_quantum_state": [P],
+    "qs_allocate_bytes": [IT, C.POINTER(P)],
     "qs_initialize_quantum_state": _STATE,
     "qs_initialize_quantum_state_c64": _STATE,
     "qs_set_computational_basis": [IT] + _STATE,

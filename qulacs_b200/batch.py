@@ -75,7 +75,7 @@ class BatchRunner:
     def _run_wave_c128(self, jobs, wave, out):
         total = sum((footprint(jobs[i][0].qubit_count) + ALIGN - 1) // ALIGN * ALIGN for i in wave)
         arena = C.c_void_p()
-        call("qs_allocate_quantum_state", max(2, total // 16), C.byref(arena))
+        call("qs_allocate_bytes", total, C.byref(arena))
         try:
             ptrs, off = [], 0
             for i in wave:

@@ -184,6 +184,16 @@ QS_API int qs_allocate_quantum_state(QS_ITYPE dim, void** state_out) {
 QS_API int qs_allocate_quantum_state_c64(QS_ITYPE dim, void** state_out) {
     return allocate_bytes(dim, 8, state_out);
 }
+QS_API int qs_allocate_bytes(QS_ITYPE bytes, void** out) {
+    if (!out) return set_error(QS_ERR_INVALID_ARGUMENT, "null output pointer");
+    *out = nullptr;
+    if (bytes == 0) return set_error(QS_ERR_INVALID_ARGUMENT, "zero-byte allocation");
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, (size_t)bytes);
+    if (e != cudaSuccess) return check_cuda(e, "cudaMalloc(bytes)");
+    *out = p;
+    return QS_OK;
+}
 QS_API int qs_release_quantum_state(void* state) {
     if (state) QS_CUDA_CHECK(cudaFree(state));
     return QS_OK;
