@@ -31,7 +31,7 @@ def test_batch_matches_alone_and_oracle(port):
     assert runner.stats.waves >= 2
     for (circ, obs), (n, gates, terms), e in zip(jobs, specs, got):
         alone = run_alone(circ, obs)
-        assert e == alone  # identical kernels and summation order
+        assert abs(e - alone) <= 1e-12  # same states; the reductions chunk the sums differently
         psi = np.zeros(1 << n, dtype=np.complex128)
         psi[0] = 1
         W.run_on_cpu(gates, psi, port)
@@ -49,11 +49,15 @@ def test_batch_states_match_gate_by_gate(port):
     circs = (C.c_void_p * len(jobs))(*[j[0]._h for j in jobs])
     ptrs = (C.c_void_p * len(jobs))(*[s.data_ptr() for s in states])
     call("qs_batch_update_quantum_states", circs, ptrs, len(jobs), None)
-    for s, (n, gates, _) in zip(states, specs):
+    for (circ, _), s, (n, gates, _) in zip(jobs, states, specs):
         psi = np.zeros(1 << n, dtype=np.complex128)
         psi[0] = 1
         W.run_on_cpu(gates, psi, port)
-        assert np.max(np.abs(s.get_vector() - psi)) <= 1e-12
+        v = s.get_vector()
+        assert np.max(np.abs(v - psi)) <= 1e-12
+        alone = QuantumState(n)
+        circ.update_quantum_state(alone, mode="staged")
+        assert np.array_equal(v, alone.get_vector())  # bit-identical alone and in the batch
 
 
 def test_batch_fused_c64(port):
