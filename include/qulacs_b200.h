@@ -43,6 +43,9 @@ QS_API const char* qs_version(void);
 QS_API unsigned long long qs_launch_count(void);
 QS_API int qs_device_synchronize(void);
 QS_API int qs_stream_synchronize(void* stream);
+/* Non-blocking CUDA stream for concurrent work (serving workers); no reference counterpart. */
+QS_API int qs_stream_create(void** stream_out);
+QS_API int qs_stream_destroy(void* stream);
 
 /* ---- memory and initialisation (src/csim/memory_ops.hpp, src/csim/init_ops.hpp) ---- */
 /* allocate_quantum_state (memory_ops.cpp:17-27): device buffer of dim complex128 amplitudes. */

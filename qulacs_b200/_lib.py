@@ -25,6 +25,8 @@ SIGNATURES = {
     "qs_launch_count": [],
     "qs_device_synchronize": [],
     "qs_stream_synchronize": [P],
+    "qs_stream_create": [C.POINTER(P)],
+    "qs_stream_destroy": [P],
     "qs_allocate_quantum_state": [IT, C.POINTER(P)],
     "qs_allocate_quantum_state_c64": [IT, C.POINTER(P)],
     "qs_release_quantum_state": [P],

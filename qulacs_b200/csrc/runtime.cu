@@ -160,6 +160,17 @@ QS_API int qs_stream_synchronize(void* stream) {
     QS_CUDA_CHECK(cudaStreamSynchronize((cudaStream_t)stream));
     return QS_OK;
 }
+QS_API int qs_stream_create(void** stream_out) {
+    if (!stream_out) return set_error(QS_ERR_INVALID_ARGUMENT, "null output pointer");
+    cudaStream_t s = nullptr;
+    QS_CUDA_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    *stream_out = (void*)s;
+    return QS_OK;
+}
+QS_API int qs_stream_destroy(void* stream) {
+    if (stream) QS_CUDA_CHECK(cudaStreamDestroy((cudaStream_t)stream));
+    return QS_OK;
+}
 
 static int allocate_bytes(ITYPE dim, size_t elem, void** out) {
     if (!out) return set_error(QS_ERR_INVALID_ARGUMENT, "null output pointer");
