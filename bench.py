@@ -272,6 +272,52 @@ def fused_comparison(n: int, layers: int, stream, with_gate_by_gate: bool, reps:
     return out
 
 
+def batched_throughput(instances: int, budget_gb: float, seed: int = 4004, precisions=("c128", "c64")):
+    """Config 4: hardware-efficient-ansatz instances, n ~ U{10..24}, depth ~ U{4..16}, RY RZ + CZ ring,
+    200 strings of weight <= 4 each.  Circuits are built once (outside the timed region, as a variational
+    loop reuses them); the timed region is admission + circuit application + <H> for all instances."""
+    from qulacs_b200 import workloads as W
+    from qulacs_b200.batch import BatchRunner
+    rng = np.random.default_rng(seed)
+    jobs = []
+    t_build = time.perf_counter()
+    for i in range(instances):
+        n = int(rng.integers(10, 25))
+        d = int(rng.integers(4, 17))
+        jobs.append((W.to_circuit(W.hea_circuit(n, d, seed * 10000 + i), n),
+                     W.to_observable(W.random_pauli_terms(n, 200, 1, 4, seed * 10000 + 5000 + i), n)))
+    t_build = time.perf_counter() - t_build
+    out = {"workload": f"{instances} HEA instances, n~U{{10..24}}, depth~U{{4..16}}, 200 strings each",
+           "host_build_s": t_build, "memory_budget_gb": budget_gb}
+    for prec in precisions:
+        runner = BatchRunner(int(budget_gb * (1 << 30)), precision=prec)
+        runner.run(jobs[: min(len(jobs), 64)])  # warm-up: plan building and first launches
+        runner = BatchRunner(int(budget_gb * (1 << 30)), precision=prec)
+        t0 = time.perf_counter()
+        e = runner.run(jobs)
+        dt = time.perf_counter() - t0
+        out[prec] = {"circuits_per_s": instances / dt, "seconds": dt, "waves": runner.stats.waves,
+                     "kernel_launches": runner.stats.kernel_launches, "energy_checksum": float(np.sum(e))}
+    return out
+
+
+def serving_latency(requests: int, rate: float, budget_gb: float, workers: int, seed: int = 5005,
+                    precisions=("c128", "c64")):
+    """Config 5: Poisson arrivals of the request mix; p50/p99 latency and jobs/s per precision."""
+    from qulacs_b200.serving import ServingLoop, make_request_mix
+    out = {"workload": f"{requests} requests, Poisson rate {rate}/s, mix 70% <H> (n 12-28) / 20% sampling "
+                       f"(n 16-30, 1024 shots) / 10% noisy DM (n 8-13)", "workers": workers,
+           "memory_budget_gb": budget_gb}
+    for prec in precisions:
+        reqs = make_request_mix(requests, rate, seed)
+        loop = ServingLoop(int(budget_gb * (1 << 30)), workers=workers, precision=prec)
+        try:
+            out[prec] = loop.run(reqs)
+        finally:
+            loop.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -282,8 +328,13 @@ def main():
     ap.add_argument("--qubits", type=int, default=N_QUBITS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-kernel-table", action="store_true")
-    ap.add_argument("--workload", default="plain", choices=["plain", "fused"],
-                    help="fused: only the fused-vs-plain comparison (config 3)")
+    ap.add_argument("--workload", default="plain", choices=["plain", "fused", "batched", "serving"],
+                    help="fused / batched / serving: only that comparison (configs 3 / 4 / 5)")
+    ap.add_argument("--instances", type=int, default=4096)
+    ap.add_argument("--budget-gb", type=float, default=96.0)
+    ap.add_argument("--requests", type=int, default=120)
+    ap.add_argument("--rate", type=float, default=8.0)
+    ap.add_argument("--workers", type=int, default=4)
     ap.add_argument("--fused-qubits", type=int, default=32)
     ap.add_argument("--fused-layers", type=int, default=20)
     ap.add_argument("--with-gate-by-gate", action="store_true")
@@ -318,6 +369,16 @@ def main():
         r = fused_comparison(args.fused_qubits, args.fused_layers, stream, args.with_gate_by_gate)
         if rank == 0:
             print(json.dumps({"metric": "fused vs plain at infidelity<=1e-6", **r}), flush=True)
+        return
+    if args.workload == "batched":
+        r = batched_throughput(args.instances, args.budget_gb)
+        if rank == 0:
+            print(json.dumps({"metric": "batched uneven circuits: circuits/s", **r}), flush=True)
+        return
+    if args.workload == "serving":
+        r = serving_latency(args.requests, args.rate, args.budget_gb, args.workers)
+        if rank == 0:
+            print(json.dumps({"metric": "serve p99 ms", **r}), flush=True)
         return
     gates = W.layered_rotation_circuit(n, DEPTH, GATE_SEED)
     terms = W.random_pauli_terms(n, N_TERMS, 1, 6, TERM_SEED)
