@@ -281,6 +281,10 @@ QS_API int qs_batch_update_quantum_states(const qs_circuit_t* circuits, void* co
 QS_API int qs_batch_expectation_values(void* const* states, const QS_UINT* qubit_counts, QS_UINT count,
     const QS_UINT* term_offsets, const QS_ITYPE* x_masks, const QS_ITYPE* z_masks, const QS_UINT* y_counts,
     double* values, void* stream);
+/* Same for complex64 states (FP64 accumulation). */
+QS_API int qs_batch_expectation_values_c64(void* const* states, const QS_UINT* qubit_counts, QS_UINT count,
+    const QS_UINT* term_offsets, const QS_ITYPE* x_masks, const QS_ITYPE* z_masks, const QS_UINT* y_counts,
+    double* values, void* stream);
 
 /* ---- fused reduced-precision execution (no reference counterpart; its comparison point is the
  * reference's gate merging, QuantumCircuitOptimizer::optimize, cppsim/circuit_optimizer.cpp:113-168,

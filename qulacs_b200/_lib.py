@@ -92,6 +92,7 @@ SIGNATURES = {
     "qs_circuit_update_quantum_state_fused_c64": [P, P, IT, P],
     "qs_batch_update_quantum_states": [P, P, U, P],
     "qs_batch_expectation_values": [P, P, U, P, P, P, P, P, P],
+    "qs_batch_expectation_values_c64": [P, P, U, P, P, P, P, P, P],
     "qs_state_norm_squared_c64": [P, IT, P, P],
     "qs_state_inner_product_c128_c64": [P, P, IT, P, P],
     "qs_expectation_value_pauli_batch_c64": [P, P, P, U, P, IT, P, P],

@@ -73,21 +73,34 @@ class BatchRunner:
         return out
 
     def _run_wave_c128(self, jobs, wave, out):
-        total = sum((footprint(jobs[i][0].qubit_count) + ALIGN - 1) // ALIGN * ALIGN for i in wave)
+        self._run_wave(jobs, wave, out, c64=False)
+
+    def _run_wave_c64(self, jobs, wave, out):
+        self._run_wave(jobs, wave, out, c64=True)
+
+    def _run_wave(self, jobs, wave, out, c64: bool):
+        prec = "c64" if c64 else "c128"
+        sizes = [(footprint(jobs[i][0].qubit_count, prec) + ALIGN - 1) // ALIGN * ALIGN for i in wave]
         arena = C.c_void_p()
-        call("qs_allocate_bytes", total, C.byref(arena))
+        call("qs_allocate_bytes", sum(sizes), C.byref(arena))
         try:
             ptrs, off = [], 0
-            for i in wave:
+            for i, sz in zip(wave, sizes):
                 n = jobs[i][0].qubit_count
                 p = arena.value + off
-                call("qs_initialize_quantum_state", p, 1 << n, self.stream)
+                call("qs_initialize_quantum_state_c64" if c64 else "qs_initialize_quantum_state", p, 1 << n,
+                     self.stream)
                 ptrs.append(p)
-                off += (footprint(n) + ALIGN - 1) // ALIGN * ALIGN
+                off += sz
             k = len(wave)
-            circs = (C.c_void_p * k)(*[jobs[i][0]._h for i in wave])
             states = (C.c_void_p * k)(*ptrs)
-            call("qs_batch_update_quantum_states", circs, states, k, self.stream)
+            if c64:  # fused tensor-core path, one launch sequence per circuit
+                for i, p in zip(wave, ptrs):
+                    circ = jobs[i][0]
+                    call("qs_circuit_update_quantum_state_fused_c64", circ._h, p, 1 << circ.qubit_count, self.stream)
+            else:  # every circuit in one persistent launch
+                circs = (C.c_void_p * k)(*[jobs[i][0]._h for i in wave])
+                call("qs_batch_update_quantum_states", circs, states, k, self.stream)
             # all terms of all observables in one launch
             xm, zm, ny, offs, coefs, nq = [], [], [], [0], [], []
             for i in wave:
@@ -107,22 +120,14 @@ class BatchRunner:
             oa = np.ascontiguousarray(np.array(offs, dtype=np.uint32))
             qa = np.ascontiguousarray(np.array(nq, dtype=np.uint32))
             vp = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
-            call("qs_batch_expectation_values", states, vp(qa), k, vp(oa), vp(xa), vp(za), vp(ya), vp(vals),
-                 self.stream)
+            call("qs_batch_expectation_values_c64" if c64 else "qs_batch_expectation_values", states, vp(qa), k,
+                 vp(oa), vp(xa), vp(za), vp(ya), vp(vals), self.stream)
             coefs = np.array(coefs, dtype=np.complex128)
             for j, i in enumerate(wave):
                 a, b = offs[j], offs[j + 1]
                 out[i] = float(np.real(np.sum(coefs[a:b] * vals[a:b])))
         finally:
             _lib.load().qs_release_quantum_state(arena.value)
-
-    def _run_wave_c64(self, jobs, wave, out):
-        for i in wave:
-            circ, obs = jobs[i]
-            s = QuantumStateC64(circ.qubit_count, self.stream)
-            circ.update_quantum_state(s)
-            out[i] = obs.get_expectation_value(s)
-            del s
 
 
 def run_alone(circ, obs, mode: str = "staged") -> float:

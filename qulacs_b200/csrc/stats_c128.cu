@@ -629,7 +629,8 @@ constexpr ITYPE kEvChunk = 1 << 14;
 constexpr int kEvZ = 16;
 
 struct EvJob {
-    const double2* s;
+    const void* s;
+    int c64;       // 1: complex64 amplitudes, 0: complex128
     ITYPE items;   // amplitudes (Z job) or pairs (X job)
     ITYPE prefix;  // first work item (chunk) of this job
     ITYPE x, z;
@@ -662,7 +663,9 @@ __global__ void __launch_bounds__(256) k_batch_ev(const EvJob* __restrict__ jobs
             double acc = 0.;
             for (ITYPE p = c0 + threadIdx.x; p < c1; p += blockDim.x) {
                 const ITYPE b0 = insert0(p, J.pivot), b1 = b0 ^ J.x;
-                const double2 v = cmul(ld_stream(J.s + b0), cconj(ld_stream(J.s + b1)));
+                const double2 a0 = J.c64 ? amp((const float2*)J.s + b0) : amp((const double2*)J.s + b0);
+                const double2 a1 = J.c64 ? amp((const float2*)J.s + b1) : amp((const double2*)J.s + b1);
+                const double2 v = cmul(a0, cconj(a1));
                 const UINT r = J.nrot + 2u * (UINT)(__popcll(b0 & J.z) & 1);
                 acc += 2.0 * phase_re_part(v, r);
             }
@@ -677,7 +680,7 @@ __global__ void __launch_bounds__(256) k_batch_ev(const EvJob* __restrict__ jobs
                 zs[w] = w < J.nz ? zmasks[J.zoff + w] : 0;
             }
             for (ITYPE i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
-                const double pr = norm2(ld_stream(J.s + i));
+                const double pr = norm2(J.c64 ? amp((const float2*)J.s + i) : amp((const double2*)J.s + i));
 #pragma unroll
                 for (int w = 0; w < kEvZ; ++w)
                     if (w < J.nz) acc[w] += (__popcll(i & zs[w]) & 1) ? -pr : pr;
@@ -710,12 +713,28 @@ __global__ void k_batch_ev_fold(const EvJob* __restrict__ jobs, const double* __
 
 }  // namespace qs
 
+namespace qs {
+static int batch_ev_impl(void* const* states, const QS_UINT* qubit_counts, QS_UINT count, const QS_UINT* term_offsets,
+    const QS_ITYPE* x_masks, const QS_ITYPE* z_masks, const QS_UINT* y_counts, double* values, int c64,
+    cudaStream_t st);
+}
 extern "C" QS_API int qs_batch_expectation_values(void* const* states, const QS_UINT* qubit_counts, QS_UINT count,
     const QS_UINT* term_offsets, const QS_ITYPE* x_masks, const QS_ITYPE* z_masks, const QS_UINT* y_counts,
     double* values, void* stream) {
-    using namespace qs;
+    return qs::batch_ev_impl(states, qubit_counts, count, term_offsets, x_masks, z_masks, y_counts, values, 0,
+        (cudaStream_t)stream);
+}
+extern "C" QS_API int qs_batch_expectation_values_c64(void* const* states, const QS_UINT* qubit_counts, QS_UINT count,
+    const QS_UINT* term_offsets, const QS_ITYPE* x_masks, const QS_ITYPE* z_masks, const QS_UINT* y_counts,
+    double* values, void* stream) {
+    return qs::batch_ev_impl(states, qubit_counts, count, term_offsets, x_masks, z_masks, y_counts, values, 1,
+        (cudaStream_t)stream);
+}
+namespace qs {
+static int batch_ev_impl(void* const* states, const QS_UINT* qubit_counts, QS_UINT count, const QS_UINT* term_offsets,
+    const QS_ITYPE* x_masks, const QS_ITYPE* z_masks, const QS_UINT* y_counts, double* values, int c64,
+    cudaStream_t st) {
     if (!states || !qubit_counts || !term_offsets || !values) return set_error(QS_ERR_INVALID_ARGUMENT, "null argument");
-    cudaStream_t st = (cudaStream_t)stream;
     std::vector<EvJob> jobs;
     std::vector<ITYPE> zm;
     std::vector<UINT> zout;
@@ -734,7 +753,8 @@ extern "C" QS_API int qs_batch_expectation_values(void* const* states, const QS_
                 continue;
             }
             EvJob J{};
-            J.s = (const double2*)states[i];
+            J.s = states[i];
+            J.c64 = c64;
             J.items = dim / 2;
             J.prefix = total;
             J.x = x_masks[k];
@@ -748,7 +768,8 @@ extern "C" QS_API int qs_batch_expectation_values(void* const* states, const QS_
         }
         for (size_t z0 = 0; z0 < zlist.size(); z0 += kEvZ) {
             EvJob J{};
-            J.s = (const double2*)states[i];
+            J.s = states[i];
+            J.c64 = c64;
             J.items = dim;
             J.prefix = total;
             J.kind = 0;
@@ -790,3 +811,4 @@ extern "C" QS_API int qs_batch_expectation_values(void* const* states, const QS_
     QS_CUDA_CHECK(cudaStreamSynchronize(st));
     return QS_OK;
 }
+}  // namespace qs
