@@ -338,6 +338,8 @@ def main():
     ap.add_argument("--fused-qubits", type=int, default=32)
     ap.add_argument("--fused-layers", type=int, default=20)
     ap.add_argument("--with-gate-by-gate", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the fused / batched / serving measurements of the default line")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3  # timing rule: at least 3 untimed warm-up steps
@@ -450,6 +452,19 @@ def main():
     if rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_reference_gbs(n, gates, 12.0, os.cpu_count() or 1)
 
+    # configs 3-5 beside the headline (each guarded: a failure is reported, not fatal)
+    extras = {}
+    if not args.no_extras:
+        del state
+        torch.cuda.synchronize()
+        for key, fn in (("fused", lambda: fused_comparison(args.fused_qubits, args.fused_layers, stream, False)),
+                        ("batched", lambda: batched_throughput(512, 64.0)),
+                        ("serving", lambda: serving_latency(60, 5.0, 96.0, 4))):
+            try:
+                extras[key] = fn()
+            except Exception as e:  # noqa: BLE001
+                extras[key] = {"error": f"{type(e).__name__}: {e}"}
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
@@ -478,6 +493,7 @@ def main():
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
+            **extras,
         }
         print(json.dumps(line), flush=True)
     if dist:
