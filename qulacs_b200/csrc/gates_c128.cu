@@ -311,14 +311,66 @@ int launch_dense2(UINT t1, UINT t2, const Mat4& m, double2* s, ITYPE dim, const 
     return check_launch("k_dense2");
 }
 
+// Register-resident k-qubit dense (3 <= K <= 6): one coset per thread.  The thread issues its 2^K
+// independent 128-bit loads at once, multiplies in registers, and stores; consecutive threads own
+// consecutive cosets, so accesses are coalesced whenever the lowest target is >= 5.  The matrix is
+// read with warp-uniform addresses: from the kernel parameter space (constant bank) for K <= 5, from
+// global memory through L1 for K = 6 (64 KiB exceeds the parameter limit).
+template <int K>
+struct DenseKArgs {
+    ITYPE mask[1 << K];           // offset of matrix index x (bit j <-> target j)
+    double2 m[K <= 5 ? (1 << (2 * K)) : 1];
+};
+
+template <int K>
+__global__ void __launch_bounds__(128) k_denseK_reg(double2* __restrict__ s, ITYPE cosets,
+    const __grid_constant__ Positions pos, ITYPE fixed, const __grid_constant__ DenseKArgs<K> a,
+    const double2* __restrict__ gm) {
+    constexpr int D = 1 << K;
+    const ITYPE c = (ITYPE)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= cosets) return;
+    const ITYPE base = expand(c, pos) | fixed;
+    double2 v[D];
+#pragma unroll
+    for (int x = 0; x < D; ++x) v[x] = ld_stream(s + (base | a.mask[x]));
+#pragma unroll 4
+    for (int y = 0; y < D; ++y) {
+        double2 acc = make_double2(0., 0.);
+#pragma unroll
+        for (int x = 0; x < D; ++x) {
+            const double2 mv = (K <= 5) ? a.m[(K <= 5 ? y * D + x : 0)] : __ldg(gm + y * D + x);
+            acc = cfma(mv, v[x], acc);
+        }
+        st_stream(s + (base | a.mask[y]), acc);
+    }
+}
+
+template <int K>
+static int launch_denseK_reg(const UINT* tl, const double* matrix, double2* s, ITYPE dim, const Positions& pos,
+    ITYPE fixed, ITYPE cosets, cudaStream_t st) {
+    constexpr int D = 1 << K;
+    static thread_local DenseKArgs<K> a;  // large parameter block, filled on the host
+    for (int x = 0; x < D; ++x) {
+        ITYPE mk = 0;
+        for (int j = 0; j < K; ++j)
+            if ((x >> j) & 1) mk |= 1ULL << tl[j];
+        a.mask[x] = mk;
+    }
+    const double2* gm = nullptr;
+    if (K <= 5) {
+        for (int i = 0; i < D * D; ++i) a.m[i] = make_double2(matrix[2 * i], matrix[2 * i + 1]);
+    } else {
+        void* buf = nullptr;
+        QS_TRY(scratch(st, (size_t)16 * D * D, &buf));
+        QS_CUDA_CHECK(cudaMemcpyAsync(buf, matrix, (size_t)16 * D * D, cudaMemcpyHostToDevice, st));
+        gm = (const double2*)buf;
+    }
+    k_denseK_reg<K><<<blocks_for(cosets, 128), 128, 0, st>>>(s, cosets, pos, fixed, a, gm);
+    return check_launch("k_denseK_reg");
+}
+
 int launch_denseK(const UINT* tl, UINT k, const double* matrix, double2* s, ITYPE dim,
     const UINT* ctl, const UINT* cval, UINT nc, cudaStream_t st) {
-    const size_t mbytes = (size_t)16 << (2 * k);
-    void* buf = nullptr;
-    QS_TRY(scratch(st, mbytes + 256, &buf));
-    UINT* dtl = (UINT*)((char*)buf + mbytes);
-    QS_CUDA_CHECK(cudaMemcpyAsync(buf, matrix, mbytes, cudaMemcpyHostToDevice, st));
-    QS_CUDA_CHECK(cudaMemcpyAsync(dtl, tl, sizeof(UINT) * k, cudaMemcpyHostToDevice, st));
     std::vector<UINT> p(tl, tl + k);
     ITYPE cm = 0;
     for (UINT i = 0; i < nc; ++i) {
@@ -326,10 +378,25 @@ int launch_denseK(const UINT* tl, UINT k, const double* matrix, double2* s, ITYP
         if (cval[i]) cm |= 1ULL << ctl[i];
     }
     const ITYPE cosets = dim >> (k + nc);
-    const int C = kDenseTile >> k;
-    k_denseK<<<blocks_for(cosets, C), kThreads, kDenseTile * sizeof(double2), st>>>(
-        s, cosets, make_positions(p), cm, (int)k, dtl, (const double2*)buf);
-    return check_launch("k_denseK");
+    const Positions pos = make_positions(p);
+    switch (k) {
+        case 3: return launch_denseK_reg<3>(tl, matrix, s, dim, pos, cm, cosets, st);
+        case 4: return launch_denseK_reg<4>(tl, matrix, s, dim, pos, cm, cosets, st);
+        case 5: return launch_denseK_reg<5>(tl, matrix, s, dim, pos, cm, cosets, st);
+        case 6: {  // 64 register amplitudes would spill: stage cosets in shared memory instead
+            const size_t mbytes = (size_t)16 << 12;
+            void* buf = nullptr;
+            QS_TRY(scratch(st, mbytes + 256, &buf));
+            UINT* dtl = (UINT*)((char*)buf + mbytes);
+            QS_CUDA_CHECK(cudaMemcpyAsync(buf, matrix, mbytes, cudaMemcpyHostToDevice, st));
+            QS_CUDA_CHECK(cudaMemcpyAsync(dtl, tl, sizeof(UINT) * 6, cudaMemcpyHostToDevice, st));
+            const int C = kDenseTile >> 6;
+            k_denseK<<<blocks_for(cosets, C), kThreads, kDenseTile * sizeof(double2), st>>>(
+                s, cosets, pos, cm, 6, dtl, (const double2*)buf);
+            return check_launch("k_denseK");
+        }
+        default: return set_error(QS_ERR_NOT_SUPPORTED, "dense gate: 3..6 targets expected here");
+    }
 }
 
 static Mat2 mat2_from(const double* m) {

@@ -213,6 +213,11 @@ static int pauli_term(const UINT* tl, const UINT* ids, UINT cnt, UINT n, PauliTe
     return QS_OK;
 }
 
+constexpr int kEvTileBitsDecl = 11;  // tile qubits of the many-terms-per-pass kernel below
+template <class T>
+int ev_tiled(const PauliTerm* terms, const std::vector<int>& xidx, UINT n, const T* s, ITYPE dim, cudaStream_t st,
+    double* values, std::vector<int>* rest);
+
 template <class T>
 int ev_batch(const PauliTerm* terms, UINT count, const T* s, ITYPE dim, cudaStream_t st, double* values) {
     std::vector<int> zidx, xidx;
@@ -235,6 +240,14 @@ int ev_batch(const PauliTerm* terms, UINT count, const T* s, ITYPE dim, cudaStre
         double out[kZChunk];
         QS_TRY(finish_reduce(part, blocks, nz, st, out));
         for (int w = 0; w < nz; ++w) values[zidx[c0 + w]] = out[w];
+    }
+    // many terms with a bit flip: evaluate them from shared-memory tiles, several terms per pass
+    UINT n = 0;
+    while ((1ULL << n) < dim) ++n;
+    if (n >= (UINT)kEvTileBitsDecl && xidx.size() >= 4) {
+        std::vector<int> rest;
+        QS_TRY(ev_tiled<T>(terms, xidx, n, s, dim, st, values, &rest));
+        xidx.swap(rest);
     }
     const unsigned xblocks = reduce_blocks(dim / 2);
     for (int k : xidx) {
@@ -811,4 +824,184 @@ static int batch_ev_impl(void* const* states, const QS_UINT* qubit_counts, QS_UI
     QS_CUDA_CHECK(cudaStreamSynchronize(st));
     return QS_OK;
 }
+}  // namespace qs
+
+// ---------------------------------------------------------------- many terms per HBM pass
+// For terms with a bit flip, one pass per term costs one full read of the state per term.  Here a
+// pass owns a set Q of kEvTileBits tile qubits (always including qubits 0..4) and evaluates EVERY
+// term whose bit-flip mask lies inside Q: each CTA loads a tile (the 2^11 amplitudes sharing the
+// values of the other qubits) into shared memory once, and warp w evaluates terms w, w + 4, ... over
+// the tile's pairs.  The phase parity splits into the tile part (popcount of the tile index under the
+// term's local Z mask) and the fixed part of the tile base.  Each CTA accumulates per-term FP64 sums
+// over its tiles in a fixed order; a fold kernel adds the CTAs' sums in index order.
+namespace qs {
+
+constexpr int kEvTileBits = kEvTileBitsDecl;
+constexpr int kEvLowFixed = 5;
+constexpr int kEvMaxTerms = 512;  // terms per pass (shared-memory accumulators)
+
+struct EvTileArgs {
+    int m;
+    UINT q[kEvTileBits];
+    int nterms;
+};
+struct EvTileTerm {
+    UINT xloc, zloc;  // masks over tile bits
+    ITYPE zglob;      // full phase-flip mask (for the base parity)
+    UINT nrot, pivot; // pivot: a tile bit of xloc
+};
+
+template <class T>
+__device__ __forceinline__ double2 tile_amp(const T* p);
+template <>
+__device__ __forceinline__ double2 tile_amp<double2>(const double2* p) { return ld_stream(p); }
+template <>
+__device__ __forceinline__ double2 tile_amp<float2>(const float2* p) {
+    const float2 v = __ldcs(p);
+    return make_double2(v.x, v.y);
+}
+
+template <class T>
+__global__ void __launch_bounds__(128) k_ev_tile(const T* __restrict__ s, ITYPE tiles, const __grid_constant__ EvTileArgs a,
+    const EvTileTerm* __restrict__ terms, double* __restrict__ partials) {
+    __shared__ double2 tile[1 << kEvTileBits];
+    __shared__ double acc[kEvMaxTerms];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m = a.m;
+    const UINT tsize = 1u << m;
+    for (int k = tid; k < a.nterms; k += 128) acc[k] = 0.;
+    ITYPE lo_off = 0;
+    for (int j = 0; j < 7 && j < m; ++j)
+        if ((tid >> j) & 1) lo_off |= 1ULL << a.q[j];
+    for (ITYPE ti = blockIdx.x; ti < tiles; ti += gridDim.x) {
+        ITYPE base = ti;
+        for (int j = 0; j < m; ++j) base = insert0(base, a.q[j]);
+        __syncthreads();
+        for (UINT k = 0; (UINT)tid + k * 128 < tsize; ++k) {
+            ITYPE off = lo_off;
+            for (int j = 7; j < m; ++j)
+                if ((k >> (j - 7)) & 1) off |= 1ULL << a.q[j];
+            tile[tid + k * 128] = tile_amp<T>(s + (base | off));
+        }
+        __syncthreads();
+        for (int t = warp; t < a.nterms; t += 4) {
+            const EvTileTerm tm = terms[t];
+            const UINT par0 = (UINT)(__popcll(base & tm.zglob) & 1);
+            double sum = 0.;
+            for (UINT p = lane; p < (tsize >> 1); p += 32) {
+                const UINT u0 = (UINT)insert0(p, tm.pivot), u1 = u0 ^ tm.xloc;
+                const double2 v = cmul(tile[u0], cconj(tile[u1]));
+                const UINT r = tm.nrot + 2u * (((UINT)__popc(u0 & tm.zloc) & 1u) ^ par0);
+                sum += 2.0 * phase_re_part(v, r);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+            if (lane == 0) acc[t] += sum;
+        }
+    }
+    __syncthreads();
+    for (int k = tid; k < a.nterms; k += 128) partials[(size_t)blockIdx.x * a.nterms + k] = acc[k];
+}
+
+__global__ void k_fold_cols(const double* __restrict__ part, int rows, int cols, double* __restrict__ out,
+    const UINT* __restrict__ out_index) {
+    __shared__ double sm[32];
+    const int c = blockIdx.x;
+    double v = 0.;
+    for (int r = threadIdx.x; r < rows; r += blockDim.x) v += part[(size_t)r * cols + c];
+    v = block_sum(v, sm);
+    if (threadIdx.x == 0) out[out_index[c]] = v;
+}
+
+// Host: cover the terms' bit-flip masks with tile sets (qubits 0..4 plus the most frequent remaining
+// flipped qubits), one pass per set.  Returns the number of passes; terms whose flipped qubits
+// outside 0..4 exceed the free tile bits stay in `rest` for the one-pass-per-term kernel.
+template <class T>
+int ev_tiled(const PauliTerm* terms, const std::vector<int>& xidx, UINT n, const T* s, ITYPE dim, cudaStream_t st,
+    double* values, std::vector<int>* rest) {
+    const int m = kEvTileBits;
+    const ITYPE low = (1ULL << kEvLowFixed) - 1;
+    const int free_bits = m - kEvLowFixed;
+    std::vector<int> todo;
+    for (int k : xidx) {
+        if (__builtin_popcountll(terms[k].x & ~low) <= free_bits) todo.push_back(k);
+        else rest->push_back(k);
+    }
+    const unsigned grid = (unsigned)std::min<ITYPE>(dim >> m, (ITYPE)sm_count() * 4);
+    std::vector<double> hvals;
+    while (!todo.empty()) {
+        // pick the free tile qubits: most frequent flipped qubits among the remaining terms,
+        // but first make sure the first remaining term fits
+        ITYPE Q = low | (terms[todo[0]].x & ~low);
+        std::vector<int> freq(64, 0);
+        for (int k : todo)
+            for (int b = 0; b < (int)n; ++b)
+                if (((terms[k].x & ~low) >> b) & 1) freq[b]++;
+        while (__builtin_popcountll(Q) < m) {
+            int best = -1;
+            for (int b = 0; b < (int)n; ++b)
+                if (!((Q >> b) & 1) && (best < 0 || freq[b] > freq[best])) best = b;
+            if (best < 0) break;
+            Q |= 1ULL << best;
+        }
+        EvTileArgs a{};
+        a.m = 0;
+        int local[64];
+        for (int b = 0; b < (int)n; ++b)
+            if ((Q >> b) & 1) {
+                local[b] = a.m;
+                a.q[a.m++] = b;
+            }
+        std::vector<EvTileTerm> tt;
+        std::vector<UINT> outi;
+        std::vector<int> left;
+        for (int k : todo) {
+            if ((terms[k].x & ~Q) || (int)tt.size() >= kEvMaxTerms) {
+                left.push_back(k);
+                continue;
+            }
+            EvTileTerm e{};
+            for (int b = 0; b < (int)n; ++b) {
+                if ((terms[k].x >> b) & 1) e.xloc |= 1u << local[b];
+                if (((terms[k].z >> b) & 1) && ((Q >> b) & 1)) e.zloc |= 1u << local[b];
+            }
+            e.zglob = terms[k].z & ~Q;  // tile bits of z are handled through zloc
+            e.nrot = terms[k].nrot;
+            e.pivot = (UINT)(31 - __builtin_clz(e.xloc));
+            tt.push_back(e);
+            outi.push_back((UINT)k);
+        }
+        a.nterms = (int)tt.size();
+        const size_t bt = sizeof(EvTileTerm) * tt.size(), bo = sizeof(UINT) * outi.size(),
+                     bp = sizeof(double) * grid * tt.size(), bv = sizeof(double) * n * 0 + sizeof(double) * 1;
+        auto up = [](size_t b) { return (b + 255) / 256 * 256; };
+        void* buf;
+        QS_TRY(scratch(st, up(bt) + up(bo) + up(bp) + up(sizeof(double) * (outi.size() + 1)) + up(bv), &buf));
+        char* p = (char*)buf;
+        EvTileTerm* dt = (EvTileTerm*)p;
+        UINT* doi = (UINT*)(p + up(bt));
+        double* dpart = (double*)(p + up(bt) + up(bo));
+        double* dval = (double*)(p + up(bt) + up(bo) + up(bp));
+        std::vector<UINT> seq(outi.size());
+        for (size_t i = 0; i < seq.size(); ++i) seq[i] = (UINT)i;
+        QS_CUDA_CHECK(cudaMemcpyAsync(dt, tt.data(), bt, cudaMemcpyHostToDevice, st));
+        QS_CUDA_CHECK(cudaMemcpyAsync(doi, seq.data(), bo, cudaMemcpyHostToDevice, st));
+        k_ev_tile<T><<<grid, 128, 0, st>>>(s, dim >> m, a, dt, dpart);
+        QS_TRY(check_launch("k_ev_tile"));
+        k_fold_cols<<<(unsigned)tt.size(), 256, 0, st>>>(dpart, (int)grid, (int)tt.size(), dval, doi);
+        QS_TRY(check_launch("k_fold_cols"));
+        hvals.resize(tt.size());
+        QS_CUDA_CHECK(cudaMemcpyAsync(hvals.data(), dval, sizeof(double) * tt.size(), cudaMemcpyDeviceToHost, st));
+        QS_CUDA_CHECK(cudaStreamSynchronize(st));
+        for (size_t i = 0; i < outi.size(); ++i) values[outi[i]] = hvals[i];
+        todo.swap(left);
+    }
+    return QS_OK;
+}
+
+template int ev_tiled<double2>(const PauliTerm*, const std::vector<int>&, UINT, const double2*, ITYPE, cudaStream_t,
+    double*, std::vector<int>*);
+template int ev_tiled<float2>(const PauliTerm*, const std::vector<int>&, UINT, const float2*, ITYPE, cudaStream_t,
+    double*, std::vector<int>*);
+
 }  // namespace qs
