@@ -39,7 +39,7 @@ def _compile(src: str, verbose: bool) -> str:
     if src.endswith(".cu"):
         cmd += CUFLAGS
     else:
-        cmd += ["-x", "c++"]
+        cmd += ["-x", "c++"] + ARCH
     if verbose:
         print(" ".join(cmd), flush=True)
     r = subprocess.run(cmd, capture_output=True, text=True)

@@ -866,10 +866,18 @@ __global__ void __launch_bounds__(128) k_ev_tile(const T* __restrict__ s, ITYPE 
     const EvTileTerm* __restrict__ terms, double* __restrict__ partials) {
     __shared__ double2 tile[1 << kEvTileBits];
     __shared__ double acc[kEvMaxTerms];
+    __shared__ ITYPE hi_off[16];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int m = a.m;
     const UINT tsize = 1u << m;
     for (int k = tid; k < a.nterms; k += 128) acc[k] = 0.;
+    // tile index u = tid + 128 k: bits 0..6 from tid, bits 7.. from k
+    if (tid < 16) {
+        ITYPE o = 0;
+        for (int j = 7; j < m; ++j)
+            if ((tid >> (j - 7)) & 1) o |= 1ULL << a.q[j];
+        hi_off[tid] = o;
+    }
     ITYPE lo_off = 0;
     for (int j = 0; j < 7 && j < m; ++j)
         if ((tid >> j) & 1) lo_off |= 1ULL << a.q[j];
@@ -877,11 +885,14 @@ __global__ void __launch_bounds__(128) k_ev_tile(const T* __restrict__ s, ITYPE 
         ITYPE base = ti;
         for (int j = 0; j < m; ++j) base = insert0(base, a.q[j]);
         __syncthreads();
-        for (UINT k = 0; (UINT)tid + k * 128 < tsize; ++k) {
-            ITYPE off = lo_off;
-            for (int j = 7; j < m; ++j)
-                if ((k >> (j - 7)) & 1) off |= 1ULL << a.q[j];
-            tile[tid + k * 128] = tile_amp<T>(s + (base | off));
+        {
+            double2 v[16];  // all loads in flight before the first shared-memory store
+#pragma unroll
+            for (int k = 0; k < 16; ++k)
+                if ((UINT)tid + (UINT)k * 128 < tsize) v[k] = tile_amp<T>(s + (base | lo_off | hi_off[k]));
+#pragma unroll
+            for (int k = 0; k < 16; ++k)
+                if ((UINT)tid + (UINT)k * 128 < tsize) tile[tid + k * 128] = v[k];
         }
         __syncthreads();
         for (int t = warp; t < a.nterms; t += 4) {
@@ -927,7 +938,8 @@ int ev_tiled(const PauliTerm* terms, const std::vector<int>& xidx, UINT n, const
         if (__builtin_popcountll(terms[k].x & ~low) <= free_bits) todo.push_back(k);
         else rest->push_back(k);
     }
-    const unsigned grid = (unsigned)std::min<ITYPE>(dim >> m, (ITYPE)sm_count() * 4);
+    const unsigned grid = (unsigned)std::min<ITYPE>(dim >> m, (ITYPE)sm_count() * 4);  // 4 resident per SM
+    constexpr size_t kMinCover = 3;  // below this a shared pass is not cheaper than one pass per term
     std::vector<double> hvals;
     while (!todo.empty()) {
         // pick the free tile qubits: most frequent flipped qubits among the remaining terms,
@@ -970,6 +982,10 @@ int ev_tiled(const PauliTerm* terms, const std::vector<int>& xidx, UINT n, const
             e.pivot = (UINT)(31 - __builtin_clz(e.xloc));
             tt.push_back(e);
             outi.push_back((UINT)k);
+        }
+        if (tt.size() < kMinCover) {  // the remaining terms go one pass each
+            rest->insert(rest->end(), todo.begin(), todo.end());
+            break;
         }
         a.nterms = (int)tt.size();
         const size_t bt = sizeof(EvTileTerm) * tt.size(), bo = sizeof(UINT) * outi.size(),
