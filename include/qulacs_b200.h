@@ -264,6 +264,10 @@ QS_API int qs_circuit_update_quantum_state(
     qs_circuit_t circuit, void* state, QS_ITYPE dim, int exec_mode, void* stream);
 /* Number of HBM passes (kernel launches over the whole state) the staged schedule uses. */
 QS_API int qs_circuit_pass_count(qs_circuit_t circuit, QS_ITYPE dim, QS_UINT* out);
+/* Host-only statistics of the staged schedule (no reference counterpart): HBM passes, register
+ * phases, operations inside phases, gates run by the gate-by-gate kernels between passes. */
+QS_API int qs_circuit_staged_stats(qs_circuit_t circuit, QS_UINT* passes, QS_UINT* phases, QS_UINT* ops,
+    QS_UINT* single_gates);
 /* Apply to a density matrix (gates as U rho U^dagger, depolarizing channels exact). */
 QS_API int qs_circuit_update_density_matrix(
     qs_circuit_t circuit, void* rho, QS_ITYPE dim, int exec_mode, void* stream);

@@ -88,6 +88,7 @@ SIGNATURES = {
     "qs_circuit_gate_count": [P, C.POINTER(U)],
     "qs_circuit_update_quantum_state": [P, P, IT, I, P],
     "qs_circuit_pass_count": [P, IT, C.POINTER(U)],
+    "qs_circuit_staged_stats": [P, C.POINTER(U), C.POINTER(U), C.POINTER(U), C.POINTER(U)],
     "qs_circuit_update_density_matrix": [P, P, IT, I, P],
     "qs_circuit_update_quantum_state_fused_c64": [P, P, IT, P],
     "qs_batch_update_quantum_states": [P, P, U, P],

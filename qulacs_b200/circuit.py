@@ -88,6 +88,12 @@ class QuantumCircuit:
         call("qs_circuit_fused_stats", self._h, C.byref(p), C.byref(b))
         return p.value, b.value
 
+    def staged_stats(self):
+        """(HBM passes, register phases, ops in phases, gates run singly) of the staged schedule."""
+        v = [C.c_uint() for _ in range(4)]
+        call("qs_circuit_staged_stats", self._h, *[C.byref(x) for x in v])
+        return tuple(x.value for x in v)
+
     def pass_count(self) -> int:
         out = C.c_uint()
         call("qs_circuit_pass_count", self._h, 1 << self.qubit_count, C.byref(out))

@@ -30,7 +30,7 @@ constexpr int kPhaseBits = 4;     // 16 amplitudes in registers per thread
 enum StKind : uint8_t { ST_DENSE1 = 0, ST_DIAG1, ST_RX, ST_RY, ST_CNOT, ST_CZ, ST_SWAP, ST_DENSE2 };
 
 struct StOp {
-    uint8_t kind, a, b, pad;  // a, b: register-bit indices 0..3 within the phase
+    uint8_t kind, a, b, pad;  // a, b: register-bit indices 0..3 within the phase; pad: dispatch code
     uint32_t param;           // index into the parameter pool (double2)
 };
 struct StPhase {
@@ -135,53 +135,41 @@ __device__ __forceinline__ void r_dense2(double2 (&r)[16], const double2* __rest
         }
 }
 
-template <int A>
-__device__ __forceinline__ void dispatch1(uint8_t kind, double2 (&r)[16], const double2* p) {
-    switch (kind) {
-        case ST_DENSE1: r_dense1<A>(r, p); break;
-        case ST_DIAG1: r_diag1<A>(r, p); break;
-        case ST_RX: r_rx<A>(r, p); break;
-        case ST_RY: r_ry<A>(r, p); break;
-        default: break;
-    }
+// One indirect branch per op: the host encodes code = kind * 16 + a * 4 + b, and every code has its
+// own fully specialised register code (unused codes are empty).
+template <int CODE>
+__device__ __forceinline__ void run_code(double2 (&r)[16], const double2* p) {
+    constexpr int kind = CODE >> 4, A = (CODE >> 2) & 3, B = CODE & 3;
+    if constexpr (kind == ST_DENSE1 && B == 0) r_dense1<A>(r, p);
+    else if constexpr (kind == ST_DIAG1 && B == 0) r_diag1<A>(r, p);
+    else if constexpr (kind == ST_RX && B == 0) r_rx<A>(r, p);
+    else if constexpr (kind == ST_RY && B == 0) r_ry<A>(r, p);
+    else if constexpr (kind == ST_CNOT && A != B) r_cnot<A, B>(r);
+    else if constexpr (kind == ST_CZ && A != B) r_cz<A, B>(r);
+    else if constexpr (kind == ST_SWAP && A != B) r_swap<A, B>(r);
+    else if constexpr (kind == ST_DENSE2 && A != B) r_dense2<A, B>(r, p);
 }
-template <int A, int B>
-__device__ __forceinline__ void dispatch2ab(uint8_t kind, double2 (&r)[16], const double2* p) {
-    switch (kind) {
-        case ST_CNOT: r_cnot<A, B>(r); break;
-        case ST_CZ: r_cz<A, B>(r); break;
-        case ST_SWAP: r_swap<A, B>(r); break;
-        case ST_DENSE2: r_dense2<A, B>(r, p); break;
-        default: break;
-    }
-}
-template <int A>
-__device__ __forceinline__ void dispatch2a(uint8_t kind, int b, double2 (&r)[16], const double2* p) {
-    switch (b) {
-        case 0: if (A != 0) dispatch2ab<A, (A != 0 ? 0 : 1)>(kind, r, p); break;
-        case 1: if (A != 1) dispatch2ab<A, (A != 1 ? 1 : 0)>(kind, r, p); break;
-        case 2: if (A != 2) dispatch2ab<A, (A != 2 ? 2 : 0)>(kind, r, p); break;
-        default: if (A != 3) dispatch2ab<A, (A != 3 ? 3 : 0)>(kind, r, p); break;
-    }
-}
+#define QS_CODE1(c) \
+    case c: run_code<c>(r, p); break;
+#define QS_CODE4(c) QS_CODE1(c) QS_CODE1(c + 1) QS_CODE1(c + 2) QS_CODE1(c + 3)
+#define QS_CODE16(c) QS_CODE4(c) QS_CODE4(c + 4) QS_CODE4(c + 8) QS_CODE4(c + 12)
 __device__ __forceinline__ void apply_op(const StOp& op, double2 (&r)[16], const double2* pool) {
     const double2* p = pool + op.param;
-    if (op.kind <= ST_RY) {
-        switch (op.a) {
-            case 0: dispatch1<0>(op.kind, r, p); break;
-            case 1: dispatch1<1>(op.kind, r, p); break;
-            case 2: dispatch1<2>(op.kind, r, p); break;
-            default: dispatch1<3>(op.kind, r, p); break;
-        }
-    } else {
-        switch (op.a) {
-            case 0: dispatch2a<0>(op.kind, op.b, r, p); break;
-            case 1: dispatch2a<1>(op.kind, op.b, r, p); break;
-            case 2: dispatch2a<2>(op.kind, op.b, r, p); break;
-            default: dispatch2a<3>(op.kind, op.b, r, p); break;
-        }
+    switch (op.pad) {
+        QS_CODE16(0)
+        QS_CODE16(16)
+        QS_CODE16(32)
+        QS_CODE16(48)
+        QS_CODE16(64)
+        QS_CODE16(80)
+        QS_CODE16(96)
+        QS_CODE16(112)
+        default: break;
     }
 }
+#undef QS_CODE16
+#undef QS_CODE4
+#undef QS_CODE1
 
 // XOR swizzle of the tile index for conflict-free 16-byte shared-memory accesses (linear over XOR,
 // so swz(a | b) = swz(a) ^ swz(b) for disjoint bit sets).
@@ -553,6 +541,7 @@ static void make_host_plan(const Circuit& c, HostPlan* H) {
                         }
                         break;
                 }
+                op.pad = (uint8_t)(op.kind * 16 + op.a * 4 + op.b);  // dispatch code
                 ops.push_back(op);
             }
             ph.op_count = (uint32_t)(ops.size() - ph.op_begin);
@@ -644,12 +633,26 @@ int staged_pass_count(Circuit& c, ITYPE dim, UINT* out) {
     return QS_OK;
 }
 
-int staged_phase_count(Circuit& c, UINT* out) {
-    HostPlan H;
-    make_host_plan(c, &H);
-    *out = (UINT)H.phases.size();
+}  // namespace qs
+
+// Host-only statistics of the staged schedule: HBM passes, register phases, operations in phases,
+// and gates run by the gate-by-gate kernels between passes.
+extern "C" QS_API int qs_circuit_staged_stats(qs_circuit_t circuit, QS_UINT* passes, QS_UINT* phases, QS_UINT* ops,
+    QS_UINT* single_gates) {
+    qs::Circuit* c = reinterpret_cast<qs::Circuit*>(circuit);
+    if (!c || !passes || !phases || !ops || !single_gates) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "null argument");
+    qs::HostPlan H;
+    qs::make_host_plan(*c, &H);
+    UINT single = 0;
+    for (const qs::PassPlan& p : H.passes) single += p.single ? 1 : 0;
+    *passes = (QS_UINT)H.passes.size();
+    *phases = (QS_UINT)H.phases.size();
+    *ops = (QS_UINT)H.ops.size();
+    *single_gates = single;
     return QS_OK;
 }
+
+namespace qs {
 
 }  // namespace qs
 
