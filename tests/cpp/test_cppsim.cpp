@@ -1,0 +1,116 @@
+// C++ surface test: cppsim-style classes over libqulacs_b200 (run by tests/test_cpp_api.py).
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <random>
+
+#include "qulacs_b200/cppsim.hpp"
+
+using namespace qulacs_b200;
+
+static int failures = 0;
+#define EXPECT(cond)                                                         \
+    do {                                                                     \
+        if (!(cond)) {                                                       \
+            std::fprintf(stderr, "FAILED %s:%d %s\n", __FILE__, __LINE__, #cond); \
+            ++failures;                                                      \
+        }                                                                    \
+    } while (0)
+
+int main() {
+    // Bell state through gate objects (reference ownership: caller deletes factory gates)
+    {
+        QuantumState s(3);
+        QuantumGateBase* h = gate::H(0);
+        QuantumGateBase* cx = gate::CNOT(0, 1);
+        h->update_quantum_state(&s);
+        cx->update_quantum_state(&s);
+        delete h;
+        delete cx;
+        const ComplexVector v = s.get_vector();
+        const double r = 1.0 / std::sqrt(2.0);
+        EXPECT(std::abs(v[0] - r) < 1e-15 && std::abs(v[3] - r) < 1e-15 && std::abs(v[1]) < 1e-15);
+        Observable zz(3);
+        zz.add_operator(1.0, "Z 0 Z 1");
+        zz.add_operator(0.5, "X 0 X 1");
+        EXPECT(std::abs(zz.get_expectation_value(&s) - 1.5) < 1e-12);
+        EXPECT(std::abs(s.get_squared_norm() - 1.0) < 1e-14);
+        EXPECT(std::abs(s.get_zero_probability(0) - 0.5) < 1e-14);
+        EXPECT(s.get_device_name() == "gpu");
+    }
+    // a random 12-qubit circuit: staged == gate by gate, and circuit + inverse == identity
+    {
+        const UINT n = 12;
+        std::mt19937_64 rng(5);
+        std::uniform_real_distribution<double> ang(0, 6.283185307179586);
+        QuantumCircuit c(n), inv(n);
+        std::vector<std::pair<int, std::pair<UINT, double>>> ops;
+        for (int layer = 0; layer < 4; ++layer) {
+            for (UINT q = 0; q < n; ++q) {
+                const double a = ang(rng), b = ang(rng);
+                c.add_gate(gate::RX(q, a));
+                c.add_gate(gate::RZ(q, b));
+                ops.push_back({0, {q, a}});
+                ops.push_back({2, {q, b}});
+            }
+            for (UINT q = 0; q + 1 < n; ++q) {
+                c.add_gate(gate::CNOT(q, q + 1));
+                ops.push_back({5, {q, 0}});
+            }
+        }
+        for (auto it = ops.rbegin(); it != ops.rend(); ++it) {
+            if (it->first == 0) inv.add_gate(gate::RX(it->second.first, -it->second.second));
+            else if (it->first == 2) inv.add_gate(gate::RZ(it->second.first, -it->second.second));
+            else inv.add_gate(gate::CNOT(it->second.first, it->second.first + 1));
+        }
+        QuantumState a(n), b(n);
+        c.update_quantum_state(&a, QS_EXEC_STAGED);
+        c.update_quantum_state(&b, QS_EXEC_GATE_BY_GATE);
+        const ComplexVector va = a.get_vector(), vb = b.get_vector();
+        double err = 0;
+        for (size_t i = 0; i < va.size(); ++i) err = std::max(err, std::abs(va[i] - vb[i]));
+        EXPECT(err <= 1e-12);
+        EXPECT(std::abs(std::abs(inner_product(a, b)) - 1.0) < 1e-12);
+        inv.update_quantum_state(&a);
+        EXPECT(std::abs(a.get_zero_probability(0) - 1.0) < 1e-12);
+        std::vector<UINT> all0(n, 0);
+        EXPECT(std::abs(a.get_marginal_probability(all0) - 1.0) < 1e-12);
+    }
+    // sampling a basis state (test/cppsim/test_state.cpp:38-47)
+    {
+        QuantumState s(10);
+        s.set_computational_basis(100);
+        for (ITYPE x : s.sampling(1024, 3)) EXPECT(x == 100);
+    }
+    // depolarizing identity on a density matrix (test/cppsim/test_noise_dm.cpp:274-309)
+    {
+        DensityMatrix rho(1);
+        const double p = 0.2;
+        QuantumGateBase* g = gate::DepolarizingNoise(0, 3 * p / 4);
+        g->update_quantum_state(&rho);
+        delete g;
+        const ComplexVector m = rho.get_matrix();
+        EXPECT(std::abs(m[0] - (1 - p / 2)) < 1e-15 && std::abs(m[3] - p / 2) < 1e-15);
+        EXPECT(std::abs(rho.get_squared_norm() - 1.0) < 1e-15);
+    }
+    // errors become exceptions
+    {
+        bool threw = false;
+        try {
+            gate::CNOT(1, 1);
+        } catch (const std::invalid_argument&) {
+            threw = true;
+        }
+        EXPECT(threw);
+        threw = false;
+        try {
+            QuantumCircuit c(3);
+            c.add_gate(gate::RX(5, 0.1));
+        } catch (const std::invalid_argument&) {
+            threw = true;
+        }
+        EXPECT(threw);
+    }
+    if (failures == 0) std::printf("OK\n");
+    return failures == 0 ? 0 : 1;
+}
