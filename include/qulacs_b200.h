@@ -312,9 +312,20 @@ QS_API int qs_state_sampling_with_uniforms_c64(const void* state_c64, QS_ITYPE d
 QS_API int qs_circuit_fused_stats(qs_circuit_t circuit, QS_UINT* passes, QS_UINT* blocks);
 /* Host-only export of fused block `index` (application order): the pass's tile qubits (<= 13),
  * the block's 6 tile-local bits, its FP64 64x64 matrix (row-major interleaved complex, may be NULL)
- * and its bf16 operand image (hi then lo, 2 x 128 x 128, K-major core-matrix layout; may be NULL). */
+ * and its bf16 operand image (hi then lo, 2 x 128 x 128, K-major core-matrix layout, rows and
+ * columns in the order qs_circuit_fused_block_layout reports; may be NULL). */
 QS_API int qs_circuit_fused_block_export(qs_circuit_t circuit, QS_UINT index, QS_UINT* tile_qubits,
     int* tile_qubit_count, QS_UINT* block_bits, double* matrix, unsigned short* operand_image);
+/* Host-only export of fused block `index`'s operand orders and device index tables:
+ * row_source[7]  source of accumulator (A) row bit i: block-local bit 0..5, or 6 = real/imaginary part;
+ * k_source[6]    block-local bit at K bit 1 + i of both operands (K bit 0 = real/imaginary part);
+ * coset_bits[m-6] tile bit at bit i of the coset (MMA N) index;
+ * tables[448]    rowtab[128] | coltab[128] | gn[128] | gj[64] as the kernel reads them (may be NULL):
+ *                accumulator element (y, n) goes to byte rowtab[y] ^ coltab[n] of the next block's
+ *                B operand (float rowtab[y] ^ coltab[n] of the swizzled output tile after the last
+ *                block); the first block's B[n][2j + part] is swizzled tile float2 gn[n] ^ gj[j]. */
+QS_API int qs_circuit_fused_block_layout(qs_circuit_t circuit, QS_UINT index, int* row_source, int* k_source,
+    QS_UINT* coset_bits, unsigned int* tables);
 
 #ifdef __cplusplus
 }

@@ -100,6 +100,7 @@ SIGNATURES = {
     "qs_state_sampling_with_uniforms_c64": [P, IT, P, U, P, P],
     "qs_circuit_fused_stats": [P, C.POINTER(U), C.POINTER(U)],
     "qs_circuit_fused_block_export": [P, U, P, C.POINTER(I), P, P, P],
+    "qs_circuit_fused_block_layout": [P, U, P, P, P, P],
 }
 for _n in ("X", "Y", "Z", "H", "S", "Sdag", "T", "Tdag", "sqrtX", "sqrtXdag", "sqrtY", "sqrtYdag", "P0", "P1"):
     SIGNATURES[f"qs_{_n}_gate"] = [U] + _STATE

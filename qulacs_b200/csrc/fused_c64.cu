@@ -7,12 +7,15 @@
 // made real, [[Re U, -Im U], [Im U, Re U]] (128 x 128), and split into bf16 hi + lo parts, written
 // in the canonical K-major no-swizzle UMMA shared-memory layout (8-row x 16-byte core matrices).
 //
-// Device side: one persistent CTA per SM.  For each tile (2^13 amplitudes = 64 KiB in shared memory):
-// per block, the 128 cosets x 64 amplitudes are gathered into the B operand (bf16 hi and lo of the
-// real and imaginary parts, K-major), one thread issues 8 K-steps x 3 products
-// (A_hi B_hi + A_hi B_lo + A_lo B_hi) of tcgen05.mma M=128 N=128 K=16 into a 128 x 128 FP32 TMEM
-// accumulator, commits to an mbarrier, and all warps read the accumulator back with tcgen05.ld into
-// the tile.  Every wait is bounded; on expiry the kernel records an error, frees its TMEM and returns.
+// Device side: one persistent CTA per SM.  Each tile (2^13 amplitudes = 64 KiB) is prefetched into
+// shared memory with cp.async while the previous tile's blocks run.  Block 0 gathers the tile's
+// 128 cosets x 64 amplitudes into the B operand (bf16 hi and lo of the real and imaginary parts,
+// K-major); one thread waits for the block's A image (bulk async copy on its own mbarrier), issues
+// 8 K-steps x 3 products (A_hi B_hi + A_hi B_lo + A_lo B_hi) of tcgen05.mma M=128 N=128 K=16 into a
+// 128 x 128 FP32 TMEM accumulator and commits to an mbarrier.  All warps then move the accumulator
+// with tcgen05.ld straight into the next block's B operand; after the last block it becomes a
+// complex64 tile that is stored to HBM.  Every wait is bounded; on expiry the kernel records an
+// error, frees its TMEM and returns.
 #include <algorithm>
 #include <cmath>
 #include <complex>
@@ -34,6 +37,10 @@ constexpr int kFTidBits = 9;      // log2(kFThreads)
 constexpr int kARows = 128, kAK = 128;           // real-ified block matrix
 constexpr int kAImageBytes = kARows * kAK * 2;   // one bf16 image (hi or lo): 32 KiB
 constexpr long long kWaitLimit = 4000000000LL;   // ~2 s of clock64 at 2 GHz
+// Per-block index tables (u32 words): rowtab[128] | coltab[128] | gn[128] | gj[64]
+constexpr int kTabRow = 0, kTabCol = 128, kTabGn = 256, kTabGj = 384, kTabWords = 448;
+constexpr int kTabBytes = kTabWords * 4;
+constexpr int kRecordBytes = 2 * kAImageBytes + kTabBytes;  // one block record in global memory
 
 // canonical K-major, no swizzle: element (r, k) of a rows x 128 bf16 operand
 __host__ __device__ __forceinline__ uint32_t kmajor_off(uint32_t r, uint32_t k) {
@@ -44,8 +51,7 @@ struct FusedPassArgs {
     int m;                        // tile qubits
     int nblocks;
     UINT q[kFTileMax];            // global qubit of tile bit j (ascending)
-    const uint8_t* block_bits;    // nblocks x 6 tile-local bits (ascending)
-    const uint4* images;          // nblocks x (hi image | lo image)
+    const unsigned char* records; // nblocks x (A hi | A lo | tables), kRecordBytes each
     float2* state;
     ITYPE tiles;
     int* err;
@@ -57,7 +63,7 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
 
 // Tile layout swizzle: XOR tile bits 5..12 into bits 1..4 (bit 0 untouched, so amplitude pairs stay
 // adjacent for 16-byte copies), spreading block-bit strides over the shared-memory banks.
-__device__ __forceinline__ uint32_t tswz(uint32_t u) { return u ^ ((((u >> 5) ^ (u >> 9)) & 15u) << 1); }
+__host__ __device__ __forceinline__ uint32_t tswz(uint32_t u) { return u ^ ((((u >> 5) ^ (u >> 9)) & 15u) << 1); }
 
 __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem_dst)), "l"(gsrc) : "memory");
@@ -128,6 +134,37 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 
 __device__ __forceinline__ void split_bf16(float v, __nv_bfloat16_raw* hi, __nv_bfloat16_raw* lo);
 
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// One block record: A image (hi | lo, 64 KiB) into `dst_a` and its index tables into `dst_t`, with bulk
+// async copies completing on `mbar` (issued by one thread; the phase completes when all bytes landed).
+__device__ __forceinline__ void bulk_load_block(uint32_t dst_a, uint32_t dst_t, const unsigned char* rec,
+                                                uint32_t mbar) {
+    asm volatile(
+        "{\n.reg .b64 st;\nmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}\n" ::"r"(mbar),
+        "r"(2 * kAImageBytes + kTabBytes)
+        : "memory");
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                         dst_a + i * (kAImageBytes / 2)),
+                     "l"(rec + i * (kAImageBytes / 2)), "r"(kAImageBytes / 2), "r"(mbar)
+                     : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst_t),
+                 "l"(rec + 2 * kAImageBytes), "r"(kTabBytes), "r"(mbar)
+                 : "memory");
+}
+
+// Per tile: the input tile (prefetched one tile ahead with cp.async into `stage`) is gathered into
+// the B operand of block 0; after every block, the FP32 accumulator goes straight from TMEM into the
+// next block's B operand (split into bf16 hi/lo), so the state does not return to a complex64 tile
+// between blocks and `stage` is free for the next tile's load; after the last block the accumulator
+// is written as a complex64 tile over the B region and stored with coalesced 16-byte stores.
+// Every data movement is a table XOR: element (row y, column n) of block b's accumulator goes to
+// byte rowtab[y] ^ coltab[n] of the next B operand (float rowtab[y] ^ coltab[n] of the output tile
+// after the last block); B_0[n][2j + part] comes from stage[gn[n] ^ gj[j]].
 __global__ void __launch_bounds__(kFThreads, 1) k_fused_pass(const __grid_constant__ FusedPassArgs a) {
     extern __shared__ __align__(1024) unsigned char smem[];
     const int m = a.m;
@@ -136,11 +173,11 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused_pass(const __grid_consta
     unsigned char* sA = smem;                                  // A hi | A lo   (64 KiB)
     unsigned char* sB = sA + 2 * kAImageBytes;                 // B hi | B lo   (2 x N x 256 B)
     const uint32_t bimg = N * 256u;
-    float2* tile = (float2*)(sB + 2 * bimg);                   // c64 tile (tsize x 8 B)
-    uint32_t* dep_x = (uint32_t*)(tile + tsize);               // 64 entries
-    uint32_t* dep_c = dep_x + 64;                              // N entries
-    uint64_t* mbar = (uint64_t*)(dep_c + 256);
-    uint32_t* tmem_slot = (uint32_t*)(mbar + 1);
+    float* outt = (float*)sB;                                  // output tile over B after the last block
+    float2* stage = (float2*)(sB + 2 * bimg);                  // input tile (tsize x 8 B)
+    uint32_t* tabs = (uint32_t*)(stage + tsize);               // [2][kTabWords]
+    uint64_t* mbar = (uint64_t*)(tabs + 2 * kTabWords);        // [0] MMA completion, [1] block record landed
+    uint32_t* tmem_slot = (uint32_t*)(mbar + 2);
     int* s_err = (int*)(tmem_slot + 1);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t ncols = N < 32 ? 32u : N;
@@ -152,6 +189,7 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused_pass(const __grid_consta
     }
     if (tid == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar)));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar + 1)));
         asm volatile("fence.mbarrier_init.release.cluster;");
         *s_err = 0;
     }
@@ -159,10 +197,11 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused_pass(const __grid_consta
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = *tmem_slot;
-    const uint32_t mb = smem_u32(mbar);
-    uint32_t phase = 0;
+    const uint32_t mb = smem_u32(mbar), mba = smem_u32(mbar + 1);
+    uint32_t phase = 0, phase_a = 0;
+    bool a_pending = false;  // a block record copy is in flight on mba (same value in every thread)
     const uint32_t idesc = idesc_bf16(kARows, (int)N);
-    const uint32_t aaddr = smem_u32(sA), baddr = smem_u32(sB);
+    const uint32_t aaddr = smem_u32(sA), baddr = smem_u32(sB), taddr = smem_u32(tabs);
 
     // Tile loads/stores move amplitude pairs (tile bit 0 = qubit 0), 16 B each: pair p = tid + 512 k
     // holds tile bits 1..9 from tid and bits 10.. from k.
@@ -170,78 +209,80 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused_pass(const __grid_consta
     for (int j = 1; j <= kFTidBits && j < m; ++j)
         if ((tid >> (j - 1)) & 1) lo_off |= 1ULL << a.q[j];
     const uint32_t npairs = tsize >> 1;
-
-    for (ITYPE T = blockIdx.x; T < a.tiles; T += gridDim.x) {
+    auto tile_base = [&](ITYPE T) {
         ITYPE base = T;
         for (int j = 0; j < m; ++j) base = insert0(base, a.q[j]);
-        // load tile: all pairs in flight at once (cp.async, 16 B)
+        return base;
+    };
+    auto pair_off = [&](uint32_t k) {
+        ITYPE off = lo_off;
+        for (int j = kFTidBits + 1; j < m; ++j)
+            if ((k >> (j - kFTidBits - 1)) & 1) off |= 1ULL << a.q[j];
+        return off;
+    };
+    auto load_tile = [&](ITYPE T) {
+        const ITYPE base = tile_base(T);
 #pragma unroll 4
         for (uint32_t k = 0; k * kFThreads < npairs; ++k) {
             const uint32_t pidx = tid + k * kFThreads;
-            if (pidx < npairs) {
-                ITYPE off = lo_off;
-                for (int j = kFTidBits + 1; j < m; ++j)
-                    if ((k >> (j - kFTidBits - 1)) & 1) off |= 1ULL << a.q[j];
-                cp_async16(tile + tswz(2 * pidx), a.state + (base | off));
+            if (pidx < npairs) cp_async16(stage + tswz(2 * pidx), a.state + (base | pair_off(k)));
+        }
+        cp_async_commit();
+    };
+    auto record = [&](int b) { return a.records + (size_t)b * kRecordBytes; };
+
+    // warp w reads TMEM lanes 32 (w % 4) .. +31 (rows y) and column part w / 4
+    const uint32_t y = 32u * (warp & 3) + lane;
+    const uint32_t parts = N >= 64 ? 4u : N / 16;
+    const uint32_t cw = N / parts;
+    const uint32_t c_begin = (uint32_t)(warp >> 2) < parts ? (warp >> 2) * cw : 0;
+    const uint32_t c_end = (uint32_t)(warp >> 2) < parts ? c_begin + cw : 0;
+    // gather: thread t owns B rows n = (t & 7) + 8 i and K pair j = bits 3..8 of t
+    const uint32_t g_n0 = tid & 7u, g_j = (uint32_t)tid >> 3;
+    const uint32_t g_off = kmajor_off(g_n0, 2 * g_j);
+
+    int slot = 0, loads = 0;  // table slot of the current block; records issued so far
+    if ((ITYPE)blockIdx.x < a.tiles) {
+        load_tile(blockIdx.x);
+        if (tid == 0) bulk_load_block(aaddr, taddr, record(0), mba);
+        a_pending = true;
+        loads = 1;
+    }
+    for (ITYPE T = blockIdx.x; T < a.tiles; T += gridDim.x) {
+        const ITYPE base = tile_base(T);
+        const bool has_next = T + gridDim.x < a.tiles;
+        cp_async_wait_group<0>();  // stage holds tile T
+        if (a_pending) {  // block 0's record (gather tables)
+            if (!mbar_wait(mba, phase_a)) *s_err = 1;
+            phase_a ^= 1u;
+            a_pending = false;
+        }
+        __syncthreads();
+        if (*s_err) break;
+        {
+            const uint32_t* gn = tabs + slot * kTabWords + kTabGn;
+            const uint32_t sj = tabs[slot * kTabWords + kTabGj + g_j];
+#pragma unroll 4
+            for (uint32_t i = 0; g_n0 + 8 * i < N; ++i) {
+                const float2 v = stage[gn[g_n0 + 8 * i] ^ sj];
+                uint32_t hi, lo;
+                split2_bf16(v.x, v.y, &hi, &lo);
+                *(uint32_t*)(sB + g_off + i * 2048) = hi;
+                *(uint32_t*)(sB + bimg + g_off + i * 2048) = lo;
             }
         }
-        cp_async_wait_all();
-        __syncthreads();
+        __syncthreads();  // every thread is done with stage
+        if (has_next) load_tile(T + gridDim.x);
         for (int b = 0; b < a.nblocks; ++b) {
-            const uint8_t* bb = a.block_bits + b * kFBlock;
-            // A images for this block: asynchronous copy, overlapped with the B gather below
-            const uint4* img = a.images + (size_t)b * (2 * kAImageBytes / 16);
-            for (int i = tid; i < 2 * kAImageBytes / 16; i += kFThreads) cp_async16((uint4*)sA + i, img + i);
-            // deposit tables, pre-swizzled (tswz is XOR-linear, so the swizzled index of coset c and
-            // block index x is sdep_c[c] ^ sdep_x[x]): x over the 6 block bits, c over the other bits
-            if (tid < 64) {
-                uint32_t d = 0;
-                for (int j = 0; j < kFBlock; ++j)
-                    if ((tid >> j) & 1) d |= 1u << bb[j];
-                dep_x[tid] = tswz(d);
-            }
-            if ((uint32_t)tid < N) {
-                uint32_t d = 0, bit = 0;
-                for (int j = 0; j < m; ++j) {
-                    bool inb = false;
-                    for (int q = 0; q < kFBlock; ++q) inb |= (bb[q] == j);
-                    if (!inb) {
-                        if ((tid >> bit) & 1) d |= 1u << j;
-                        ++bit;
-                    }
-                }
-                dep_c[tid] = tswz(d);
-            }
-            __syncthreads();
-            // gather B: row c (coset), K = x (real part) and 64 + x (imaginary part), hi and lo.
-            // Thread t owns block indices x = 2j, 2j + 1 with j = bits 3..7 of t, and cosets
-            // c = (t & 7) + 8 (t >> 8) + 16 i: its B offsets are fixed up to i * 4096, and within a warp
-            // the 32 4-byte stores cover 128 distinct bytes.
-            {
-                const uint32_t j = ((tid >> 3) & 3u) | (((tid >> 5) & 7u) << 2);
-                const uint32_t c0 = (tid & 7u) | ((uint32_t)(tid >> 8) << 3);
-                const uint32_t sx0 = dep_x[2 * j], sx1 = dep_x[2 * j + 1];
-                unsigned char* ore = sB + kmajor_off(c0, 2 * j);
-                unsigned char* oim = sB + kmajor_off(c0, 64 + 2 * j);
-#pragma unroll 2
-                for (uint32_t i = 0; c0 + 16 * i < N; ++i) {
-                    const uint32_t cb = dep_c[c0 + 16 * i];
-                    const float2 v0 = tile[cb ^ sx0];
-                    const float2 v1 = tile[cb ^ sx1];
-                    uint32_t hi, lo;
-                    split2_bf16(v0.x, v1.x, &hi, &lo);
-                    *(uint32_t*)(ore + i * 4096) = hi;
-                    *(uint32_t*)(ore + bimg + i * 4096) = lo;
-                    split2_bf16(v0.y, v1.y, &hi, &lo);
-                    *(uint32_t*)(oim + i * 4096) = hi;
-                    *(uint32_t*)(oim + bimg + i * 4096) = lo;
-                }
-            }
-            cp_async_wait_all();
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             asm volatile("tcgen05.fence::before_thread_sync;");
             __syncthreads();
-            if (tid == 0) {
+            if (a_pending) {
+                if (!mbar_wait(mba, phase_a)) *s_err = 1;
+                phase_a ^= 1u;
+                a_pending = false;
+            }
+            if (tid == 0 && !*s_err) {
                 asm volatile("tcgen05.fence::after_thread_sync;");
                 // K-step s covers K = 16 s .. 16 s + 15: two 16-byte core-matrix columns, LBO = 128 B,
                 // SBO = 2048 B (16 core matrices of one 8-row group along K)
@@ -262,40 +303,65 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused_pass(const __grid_consta
             phase ^= 1u;
             if (!ok) *s_err = 1;
             asm volatile("tcgen05.fence::after_thread_sync;");
-            // warp w reads TMEM lanes 32 (w % 4) .. +31 (rows y) and column part w / 4
-            const uint32_t y = 32u * (warp & 3) + lane;
-            const uint32_t parts = N >= 64 ? 4u : N / 16;
-            const uint32_t cw = N / parts;
-            const uint32_t c_begin = (uint32_t)(warp >> 2) < parts ? (warp >> 2) * cw : 0;
-            const uint32_t c_end = (uint32_t)(warp >> 2) < parts ? c_begin + cw : 0;
-            const uint32_t xo = dep_x[y & 63u];
-            for (uint32_t c0 = c_begin; c0 < c_end; c0 += 16) {
-                float v[16];
-                tmem_ld16(tmem + ((32u * (warp & 3)) << 16) + c0, v);
-#pragma unroll
-                for (int i = 0; i < 16; ++i) {
-                    float* dst = (float*)&tile[dep_c[c0 + i] ^ xo];
-                    dst[y >> 6] = v[i];
-                }
-            }
-            asm volatile("tcgen05.fence::before_thread_sync;");
             __syncthreads();
             if (*s_err) break;
+            // A and the other table slot are free: start the next record (the next tile's first block
+            // after the last one; a single-block pass keeps its record resident)
+            const int nxt = b + 1 < a.nblocks ? b + 1 : (has_next ? 0 : -1);
+            const int nslot = loads & 1;
+            if (nxt >= 0 && nxt != b) {
+                if (tid == 0) bulk_load_block(aaddr, taddr + nslot * kTabBytes, record(nxt), mba);
+                a_pending = true;
+                ++loads;
+            }
+            // accumulator -> next B operand (2-byte hi / lo stores), or -> output tile after the last block
+            const uint32_t* rt = tabs + slot * kTabWords + kTabRow;
+            const uint32_t* ct = tabs + slot * kTabWords + kTabCol;
+            const uint32_t ybase = rt[y];
+            const bool last = b + 1 == a.nblocks;
+            for (uint32_t cc = c_begin; cc < c_end; cc += 16) {
+                float v[16];
+                tmem_ld16(tmem + ((32u * (warp & 3)) << 16) + cc, v);
+                uint32_t o[16];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const uint4 t4 = *(const uint4*)(ct + cc + 4 * q);
+                    o[4 * q] = t4.x ^ ybase;
+                    o[4 * q + 1] = t4.y ^ ybase;
+                    o[4 * q + 2] = t4.z ^ ybase;
+                    o[4 * q + 3] = t4.w ^ ybase;
+                }
+                if (last) {
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) outt[o[i]] = v[i];
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) {
+                        uint32_t hl;
+                        asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(hl) : "f"(0.f), "f"(v[i]));
+                        const float hf = __uint_as_float(hl << 16);
+                        uint32_t ll;
+                        asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(ll) : "f"(0.f), "f"(v[i] - hf));
+                        *(uint16_t*)(sB + o[i]) = (uint16_t)hl;
+                        *(uint16_t*)(sB + bimg + o[i]) = (uint16_t)ll;
+                    }
+                }
+            }
+            if (nxt >= 0 && nxt != b) slot = nslot;
         }
         if (*s_err) break;
-        // store tile (16-byte pairs)
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        __syncthreads();
         for (uint32_t k = 0; k * kFThreads < npairs; ++k) {
             const uint32_t pidx = tid + k * kFThreads;
             if (pidx < npairs) {
-                ITYPE off = lo_off;
-                for (int j = kFTidBits + 1; j < m; ++j)
-                    if ((k >> (j - kFTidBits - 1)) & 1) off |= 1ULL << a.q[j];
-                const float4 v = *(const float4*)(tile + tswz(2 * pidx));
-                __stcs((float4*)(a.state + (base | off)), v);
+                const float4 v = *(const float4*)(outt + 2 * tswz(2 * pidx));
+                __stcs((float4*)(a.state + (base | pair_off(k))), v);
             }
         }
-        __syncthreads();
     }
+    cp_async_wait_group<0>();  // no copy in flight at exit
+    if (a_pending && !mbar_wait(mba, phase_a)) *s_err = 1;
     if (tid == 0 && *s_err) atomicExch(a.err, 1);
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
@@ -382,9 +448,22 @@ static bool fusable(const GateRec& g) {
     return g.qubits().size() <= (size_t)kFBlock;
 }
 
+// Operand orders of one block.  All are bit placements, so every index map between the tile, the
+// B operand and the accumulator is an XOR of per-bit terms (two table lookups on the device).
+//   row_src[i]    : source of accumulator row bit i (block-local bit 0..5, or 6 = real/imaginary part)
+//   k_src[i]      : block-local bit at K bit 1 + i of the operands (K bit 0 = real/imaginary part)
+//   coset_bits[i] : tile bit at bit i of the coset index (the MMA N index)
+struct BlockLayout {
+    int row_src[7];
+    int k_src[kFBlock];
+    std::vector<int> coset_bits;
+};
+
 struct FusedBlock {
-    uint8_t bits[kFBlock];
-    std::vector<uint16_t> image;  // hi image then lo image (kAImageBytes / 2 each)
+    uint8_t bits[kFBlock];        // tile-local bits (ascending); block-local bit j <-> bits[j]
+    BlockLayout lay;
+    std::vector<uint16_t> image;  // hi image then lo image (kAImageBytes / 2 each), in `lay` order
+    std::vector<uint32_t> tabs;   // kTabWords: rowtab | coltab | gn | gj
     std::vector<cd> U;            // FP64 block matrix, row-major, bit j <-> bits[j]
     int ngates;
 };
@@ -428,22 +507,208 @@ static ITYPE greedy_set(const std::vector<GateRec>& G, const std::vector<int>& t
     return S;
 }
 
-static void build_image(const std::vector<cd>& U, std::vector<uint16_t>* img) {
+// A operand of a block: row y = (real/imaginary part, output index) by lay.row_src, column K =
+// (part, input index) by lay.k_src; entries of [[Re U, -Im U], [Im U, Re U]].
+static void build_image(const std::vector<cd>& U, const BlockLayout& lay, std::vector<uint16_t>* img) {
     img->assign(kAImageBytes, 0);  // 2 images x kAImageBytes / 2 uint16
     uint16_t* hi = img->data();
     uint16_t* lo = img->data() + kAImageBytes / 2;
     for (int r = 0; r < 128; ++r)
         for (int k = 0; k < 128; ++k) {
-            const cd u = U[(r & 63) * 64 + (k & 63)];
+            int xo = 0, po = 0, xi = 0;
+            for (int i = 0; i < 7; ++i) {
+                const int bit = (r >> i) & 1;
+                if (lay.row_src[i] == 6) po = bit;
+                else xo |= bit << lay.row_src[i];
+            }
+            const int pi = k & 1;
+            for (int i = 0; i < kFBlock; ++i) xi |= ((k >> (1 + i)) & 1) << lay.k_src[i];
+            const cd u = U[xo * 64 + xi];
             double v;
-            if (r < 64) v = (k < 64) ? u.real() : -u.imag();
-            else v = (k < 64) ? u.imag() : u.real();
+            if (po == 0) v = (pi == 0) ? u.real() : -u.imag();
+            else v = (pi == 0) ? u.imag() : u.real();
             const float f = (float)v;
             const uint16_t h = host_bf16(f);
             const uint16_t l = host_bf16((float)(v - (double)host_bf16_to_float(h)));
             hi[kmajor_off(r, k) / 2] = h;
             lo[kmajor_off(r, k) / 2] = l;
         }
+}
+
+// ---- operand layouts: chosen per block so that the warp-wide shared-memory accesses of the gather,
+// the accumulator -> next-operand moves and the output scatter hit distinct banks.
+
+// Largest number of distinct 4-byte words any bank receives (accesses to one word do not conflict).
+static int bank_degree(const uint32_t* word, int count) {
+    int worst = 0;
+    for (uint32_t bank = 0; bank < 32; ++bank) {
+        uint32_t seen[64];
+        int cnt = 0;
+        for (int l = 0; l < count; ++l) {
+            if ((word[l] & 31u) != bank) continue;
+            bool dup = false;
+            for (int q = 0; q < cnt; ++q) dup |= seen[q] == word[l];
+            if (!dup) seen[cnt++] = word[l];
+        }
+        worst = std::max(worst, cnt);
+    }
+    return worst;
+}
+
+static std::vector<int> coset_bits_of(const FusedBlock& b, int m) {
+    std::vector<int> v;
+    for (int j = 0; j < m; ++j)
+        if (std::find(b.bits, b.bits + kFBlock, (uint8_t)j) == b.bits + kFBlock) v.push_back(j);
+    return v;
+}
+// `first` in the given order, then the rest of `all` ascending
+static std::vector<int> order_with_prefix(const std::vector<int>& first, const std::vector<int>& all) {
+    std::vector<int> v = first;
+    for (int x : all)
+        if (std::find(first.begin(), first.end(), x) == first.end()) v.push_back(x);
+    return v;
+}
+// tile index and part of accumulator row y
+static uint32_t row_tile_index(const uint8_t* bits, const BlockLayout& L, uint32_t y, uint32_t* part) {
+    uint32_t u = 0;
+    *part = 0;
+    for (int i = 0; i < 7; ++i) {
+        const uint32_t bit = (y >> i) & 1u;
+        if (L.row_src[i] == 6) *part = bit;
+        else u |= bit << bits[L.row_src[i]];
+    }
+    return u;
+}
+static uint32_t coset_tile_index(const BlockLayout& L, uint32_t n) {
+    uint32_t u = 0;
+    for (size_t i = 0; i < L.coset_bits.size(); ++i) u |= ((n >> i) & 1u) << L.coset_bits[i];
+    return u;
+}
+static uint32_t k_tile_index(const FusedBlock& b, uint32_t j) {  // j = K >> 1
+    uint32_t u = 0;
+    for (int i = 0; i < kFBlock; ++i) u |= ((j >> i) & 1u) << b.bits[b.lay.k_src[i]];
+    return u;
+}
+// byte offset of (tile index u, part) in the B operand of a block on `bits` with layout L
+static uint32_t b_operand_off(const uint8_t* bits, const BlockLayout& L, uint32_t u, uint32_t part) {
+    uint32_t n = 0, k = part;
+    for (size_t i = 0; i < L.coset_bits.size(); ++i) n |= ((u >> L.coset_bits[i]) & 1u) << i;
+    for (int i = 0; i < kFBlock; ++i) k |= ((u >> bits[L.k_src[i]]) & 1u) << (1 + i);
+    return kmajor_off(n, k);
+}
+
+static void choose_layouts(FusedPass& fp) {
+    const int m = (int)fp.q.size();
+    std::vector<int> locals(kFBlock);
+    for (int j = 0; j < kFBlock; ++j) locals[j] = j;
+    // block 0's gather: lanes 0..2 = coset index bits 0..2, lanes 3..4 = K pair bits 0..1; 8-byte loads
+    // of the swizzled tile, two half-warp wavefronts at best
+    {
+        FusedBlock& b0 = fp.blocks[0];
+        const std::vector<int> cos = coset_bits_of(b0, m);
+        int best = 1 << 30;
+        std::vector<int> bc, bk;
+        const int nc = (int)cos.size();
+        for (int c0 = 0; c0 < nc; ++c0)
+            for (int c1 = c0 + 1; c1 < nc; ++c1)
+                for (int c2 = c1 + 1; c2 < nc; ++c2)
+                    for (int k0 = 0; k0 < kFBlock; ++k0)
+                        for (int k1 = k0 + 1; k1 < kFBlock; ++k1) {
+                            const int lb[5] = {cos[c0], cos[c1], cos[c2], b0.bits[k0], b0.bits[k1]};
+                            int cost = 0;
+                            for (int h = 0; h < 2; ++h) {
+                                uint32_t words[32];
+                                for (int l = 0; l < 16; ++l) {
+                                    const int lane = 16 * h + l;
+                                    uint32_t u = 0;
+                                    for (int i = 0; i < 5; ++i) u |= (uint32_t)((lane >> i) & 1) << lb[i];
+                                    words[2 * l] = 2 * tswz(u);
+                                    words[2 * l + 1] = 2 * tswz(u) + 1;
+                                }
+                                cost += bank_degree(words, 32);
+                            }
+                            if (cost < best) {
+                                best = cost;
+                                bc = {cos[c0], cos[c1], cos[c2]};
+                                bk = {k0, k1};
+                            }
+                        }
+        b0.lay.coset_bits = order_with_prefix(bc, cos);
+        const std::vector<int> ks = order_with_prefix(bk, locals);
+        std::copy(ks.begin(), ks.end(), b0.lay.k_src);
+    }
+    // accumulator rows of block b: lanes 0..4 of a warp are rows y bits 0..4.  Pick the 5 row sources
+    // (of 6 block bits + part) and the next block's K / coset orders that minimise bank conflicts.
+    for (size_t b = 0; b < fp.blocks.size(); ++b) {
+        FusedBlock& cb = fp.blocks[b];
+        const bool last = b + 1 == fp.blocks.size();
+        FusedBlock* nb = last ? nullptr : &fp.blocks[b + 1];
+        const std::vector<int> ncos = last ? std::vector<int>() : coset_bits_of(*nb, m);
+        int best = 1 << 30;
+        BlockLayout best_next;
+        int best_rows[7] = {0, 1, 2, 3, 4, 5, 6};
+        for (int e1 = 0; e1 < 7; ++e1)
+            for (int e2 = e1 + 1; e2 < 7; ++e2) {
+                int rows[7], r = 0;
+                for (int s = 0; s < 7; ++s)
+                    if (s != e1 && s != e2) rows[r++] = s;
+                rows[5] = e1;
+                rows[6] = e2;
+                BlockLayout trial_next;
+                if (!last) {
+                    std::vector<int> kpre, cpre;
+                    for (int i = 0; i < 5; ++i) {
+                        if (rows[i] == 6) continue;
+                        const uint8_t tb = cb.bits[rows[i]];
+                        const uint8_t* at = std::find(nb->bits, nb->bits + kFBlock, tb);
+                        if (at != nb->bits + kFBlock) kpre.push_back((int)(at - nb->bits));
+                        else cpre.push_back(tb);
+                    }
+                    trial_next.coset_bits = order_with_prefix(cpre, ncos);
+                    const std::vector<int> ks = order_with_prefix(kpre, locals);
+                    std::copy(ks.begin(), ks.end(), trial_next.k_src);
+                }
+                BlockLayout probe = cb.lay;
+                std::copy(rows, rows + 7, probe.row_src);
+                uint32_t words[32];
+                for (uint32_t lane = 0; lane < 32; ++lane) {
+                    uint32_t part;
+                    const uint32_t u = row_tile_index(cb.bits, probe, lane, &part);
+                    words[lane] = last ? (2 * tswz(u) | part) : (b_operand_off(nb->bits, trial_next, u, part) >> 2);
+                }
+                const int cost = bank_degree(words, 32);
+                if (cost < best) {
+                    best = cost;
+                    std::copy(rows, rows + 7, best_rows);
+                    if (!last) best_next = trial_next;
+                }
+            }
+        std::copy(best_rows, best_rows + 7, cb.lay.row_src);
+        if (!last) {
+            std::copy(best_next.k_src, best_next.k_src + kFBlock, nb->lay.k_src);
+            nb->lay.coset_bits = best_next.coset_bits;
+        }
+    }
+}
+
+// Device tables of block b (rowtab / coltab into the next block's B operand, or into the output tile
+// after the last block; gn / gj for the tile -> B gather of a pass's first block).
+static void build_tables(const FusedPass& fp, size_t b, int m, std::vector<uint32_t>* t) {
+    const FusedBlock& cb = fp.blocks[b];
+    const FusedBlock* nb = b + 1 < fp.blocks.size() ? &fp.blocks[b + 1] : nullptr;
+    const uint32_t N = 1u << (m - kFBlock);
+    t->assign(kTabWords, 0);
+    for (uint32_t y = 0; y < 128; ++y) {
+        uint32_t part;
+        const uint32_t u = row_tile_index(cb.bits, cb.lay, y, &part);
+        (*t)[kTabRow + y] = nb ? b_operand_off(nb->bits, nb->lay, u, part) : (2 * tswz(u) | part);
+    }
+    for (uint32_t n = 0; n < N; ++n) {
+        const uint32_t u = coset_tile_index(cb.lay, n);
+        (*t)[kTabCol + n] = nb ? b_operand_off(nb->bits, nb->lay, u, 0) : 2 * tswz(u);
+        (*t)[kTabGn + n] = tswz(u);
+    }
+    for (uint32_t j = 0; j < 64; ++j) (*t)[kTabGj + j] = tswz(k_tile_index(cb, j));
 }
 
 int fused_plan_host(const Circuit& c, FusedPlanHost* P) {
@@ -515,7 +780,6 @@ int fused_plan_host(const Circuit& c, FusedPlanHost* P) {
                         if (bq[j] == gq) pos.push_back(j);
                 apply_to_block(U, g, pos);
             }
-            build_image(U, &blk.image);
             blk.U = U;
             blk.ngates = (int)bg.size();
             fp.blocks.push_back(std::move(blk));
@@ -525,6 +789,11 @@ int fused_plan_host(const Circuit& c, FusedPlanHost* P) {
             for (int gi : todo)
                 if (!taken[gi]) rest.push_back(gi);
             todo.swap(rest);
+        }
+        choose_layouts(fp);
+        for (size_t b = 0; b < fp.blocks.size(); ++b) {
+            build_image(fp.blocks[b].U, fp.blocks[b].lay, &fp.blocks[b].image);
+            build_tables(fp, b, (int)fp.q.size(), &fp.blocks[b].tabs);
         }
         P->nblocks += fp.blocks.size();
         P->passes.push_back(std::move(fp));
@@ -550,7 +819,7 @@ struct FusedPlanDev {
 
 static size_t fused_smem_bytes(int m) {
     const size_t tsize = size_t(1) << m, N = tsize >> kFBlock;
-    return 2 * kAImageBytes + 2 * N * 256 + tsize * 8 + (64 + 256) * 4 + 64;
+    return 2 * kAImageBytes + 2 * N * 256 + tsize * 8 + 2 * kTabBytes + 64;  // + 2 mbarriers, TMEM slot, error flag
 }
 
 // Device plan cached on the circuit (dropped when a gate is added).
@@ -563,31 +832,28 @@ static int fused_plan_dev(Circuit& c, ITYPE dim, std::shared_ptr<FusedPlanDev>* 
     QS_TRY(fused_plan_host(c, &H));
     auto D = std::make_shared<FusedPlanDev>();
     D->dim = dim;
-    size_t bits_bytes = (H.nblocks * kFBlock + 255) / 256 * 256;
-    size_t img_bytes = H.nblocks * (size_t)(2 * kAImageBytes);
-    QS_CUDA_CHECK(cudaMalloc(&D->dev, bits_bytes + img_bytes + 256));
-    std::vector<unsigned char> host(bits_bytes + img_bytes + 256, 0);
-    size_t bi = 0, ii = 0;
-    std::vector<std::pair<size_t, size_t>> offs;
+    const size_t rec_bytes = H.nblocks * (size_t)kRecordBytes;
+    QS_CUDA_CHECK(cudaMalloc(&D->dev, rec_bytes + 256));
+    std::vector<unsigned char> host(rec_bytes + 256, 0);
+    size_t ri = 0;
+    std::vector<size_t> offs;
     for (const FusedPass& p : H.passes) {
-        offs.push_back({bi, ii});
+        offs.push_back(ri);
         for (const FusedBlock& b : p.blocks) {
-            memcpy(host.data() + bi, b.bits, kFBlock);
-            bi += kFBlock;
-            memcpy(host.data() + bits_bytes + ii, b.image.data(), 2 * kAImageBytes);
-            ii += 2 * kAImageBytes;
+            memcpy(host.data() + ri, b.image.data(), 2 * kAImageBytes);
+            memcpy(host.data() + ri + 2 * kAImageBytes, b.tabs.data(), kTabBytes);
+            ri += kRecordBytes;
         }
     }
     QS_CUDA_CHECK(cudaMemcpy(D->dev, host.data(), host.size(), cudaMemcpyHostToDevice));
-    D->err = (int*)((char*)D->dev + bits_bytes + img_bytes);
+    D->err = (int*)((char*)D->dev + rec_bytes);
     QS_CUDA_CHECK(cudaMemset(D->err, 0, sizeof(int)));
     for (size_t i = 0; i < H.passes.size(); ++i) {
         FusedPassArgs a{};
         a.m = (int)H.passes[i].q.size();
         a.nblocks = (int)H.passes[i].blocks.size();
         for (int j = 0; j < a.m; ++j) a.q[j] = H.passes[i].q[j];
-        a.block_bits = (const uint8_t*)D->dev + offs[i].first;
-        a.images = (const uint4*)((const char*)D->dev + bits_bytes + offs[i].second);
+        a.records = (const unsigned char*)D->dev + offs[i];
         a.tiles = dim >> a.m;
         a.err = D->err;
         D->passes.push_back(a);
@@ -638,6 +904,23 @@ int fused_block_export(Circuit& c, UINT index, UINT* tile_qubits, int* m_out, UI
     return set_error(QS_ERR_INVALID_ARGUMENT, "fused block index out of range");
 }
 
+// Host-only export of fused block `index`'s operand layout and device index tables.
+int fused_block_layout(Circuit& c, UINT index, int* row_source, int* k_source, UINT* coset_bits, uint32_t* tables) {
+    FusedPlanHost H;
+    QS_TRY(fused_plan_host(c, &H));
+    UINT k = 0;
+    for (const FusedPass& p : H.passes)
+        for (const FusedBlock& b : p.blocks) {
+            if (k++ != index) continue;
+            for (int i = 0; i < 7; ++i) row_source[i] = b.lay.row_src[i];
+            for (int i = 0; i < kFBlock; ++i) k_source[i] = b.lay.k_src[i];
+            for (size_t i = 0; i < b.lay.coset_bits.size(); ++i) coset_bits[i] = (UINT)b.lay.coset_bits[i];
+            if (tables) memcpy(tables, b.tabs.data(), kTabBytes);
+            return QS_OK;
+        }
+    return set_error(QS_ERR_INVALID_ARGUMENT, "fused block index out of range");
+}
+
 int fused_stats(Circuit& c, UINT* passes, UINT* blocks) {
     FusedPlanHost H;
     QS_TRY(fused_plan_host(c, &H));
@@ -663,6 +946,13 @@ QS_API int qs_circuit_fused_block_export(qs_circuit_t circuit, QS_UINT index, QS
     qs::Circuit* c = reinterpret_cast<qs::Circuit*>(circuit);
     if (!c || !tile_qubits || !tile_qubit_count || !block_bits) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "null argument");
     return qs::fused_block_export(*c, index, tile_qubits, tile_qubit_count, block_bits, matrix, operand_image);
+}
+
+QS_API int qs_circuit_fused_block_layout(qs_circuit_t circuit, QS_UINT index, int* row_source, int* k_source,
+    QS_UINT* coset_bits, unsigned int* tables) {
+    auto* c = reinterpret_cast<qs::Circuit*>(circuit);
+    if (!c || !row_source || !k_source || !coset_bits) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "null argument");
+    return qs::fused_block_layout(*c, index, row_source, k_source, coset_bits, tables);
 }
 
 QS_API int qs_circuit_fused_stats(qs_circuit_t circuit, QS_UINT* passes, QS_UINT* blocks) {
