@@ -301,6 +301,23 @@ def batched_throughput(instances: int, budget_gb: float, seed: int = 4004, preci
     return out
 
 
+def fp64_per_amplitude(qubits, m) -> int:
+    """FP64 instructions per amplitude of a gate in the staged register code: a rotation, or any 1-qubit
+    matrix whose entries are each real or imaginary, and a 1-qubit diagonal cost 4; a general 1-qubit
+    matrix 8; a k-qubit permutation or +-1 diagonal (CNOT, CZ, SWAP) 0; any other k-qubit matrix
+    4 x 2^k (2^k complex multiply-adds)."""
+    e = m.ravel()
+    if len(qubits) == 1:
+        if m[0, 1] == 0 and m[1, 0] == 0:
+            return 4
+        if all(x.real == 0 or x.imag == 0 for x in e):
+            return 4
+        return 8
+    if np.all((e == 0) | (e == 1) | (e == -1)):
+        return 0
+    return 4 * (1 << len(qubits))
+
+
 def serving_latency(requests: int, rate: float, budget_gb: float, workers: int, seed: int = 5005,
                     precisions=("c128", "c64")):
     """Config 5: Poisson arrivals of the request mix; p50/p99 latency and jobs/s per precision."""
@@ -324,7 +341,9 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--mode", default="staged", choices=["staged", "gate_by_gate"])
+    ap.add_argument("--mode", default="staged_fused", choices=["staged_fused", "staged", "gate_by_gate"])
+    ap.add_argument("--no-mode-compare", action="store_true",
+                    help="skip timing the other complex128 execution modes beside the headline one")
     ap.add_argument("--qubits", type=int, default=N_QUBITS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-kernel-table", action="store_true")
@@ -417,7 +436,15 @@ def main():
     value = world * gb_per_step / (ms / 1e3)
 
     # dominant kernel roofline: one HBM pass = 2 x 16 x 2^n algorithmic bytes
-    passes = circ.pass_count() if mode == "staged" else len(gates)
+    staged_kernel = mode in ("staged", "staged_fused")
+    fusion = None
+    if mode == "staged_fused":
+        fk, fcount, passes, fest = circ.fusion_info()
+        fusion = {"k": fk, "gates_after_fusion": fcount, "autotuner_estimates_ms": fest}
+    elif mode == "staged":
+        passes = circ.pass_count()
+    else:
+        passes = len(gates)
     per_launch_ms = ms / max(1, passes)
     hbm_peak, peak_kind = peaks()
     achieved = bytes_per_gate(n) / 1e9 / (per_launch_ms / 1e3)
@@ -425,6 +452,9 @@ def main():
     # per rotation gate (CNOTs move data only); B200 FP64 CUDA-core peak = 148 SMs x 64 FMA/clk.
     rot = sum(1 for g in gates if g[0] in ("RX", "RY", "RZ"))
     fp64_instr = 4.0 * rot * (1 << n)
+    if fusion is not None and fusion["k"] > 0:
+        fl = circ.fuse(fusion["k"])
+        fp64_instr = float(sum(fp64_per_amplitude(*fl[i]) for i in range(len(fl)))) * (1 << n)
     fp64_peak = 148 * 64 * 1.965e9
     kernels = kernel_table(state, n, stream) if not args.no_kernel_table else None
 
@@ -447,6 +477,25 @@ def main():
         e2e_ms = float(t.item())
     h2d = N_TERMS * (8 + 8 + 4) + N_SHOTS * 8 + len(gates) * 64
     d2h = N_TERMS * 8 + N_SHOTS * 8
+
+    # the other complex128 execution modes on the same circuit and state (outside the timed region)
+    modes_ms = {mode: ms}
+    if not args.no_mode_compare:
+        for other in ("staged_fused", "staged", "gate_by_gate"):
+            if other == mode:
+                continue
+            reps = 1 if other == "gate_by_gate" else 2
+            state.set_zero_state()
+            circ.update_quantum_state(state, mode=other)  # warm-up (plan build, autotuning)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(reps):
+                state.set_zero_state()
+                circ.update_quantum_state(state, mode=other)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            modes_ms[other] = e0.elapsed_time(e1) / reps
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -471,20 +520,24 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "c128 (f64)", "data": "synthetic (seeded)",
             "config": {"workload": f"layered RX/RY/RZ+CNOT n={n} depth={DEPTH} ({len(gates)} gates), c128",
-                       "exec_mode": mode, "hbm_passes": passes, "l2": "state 16 GiB > L2 (no flush needed)",
+                       "exec_mode": mode, "hbm_passes": passes,
+                       "l2": f"state {(16 << n) / 2**30:g} GiB > L2 (no flush needed)",
                        "parallelism": f"replicas x{world}"},
+            "fusion": fusion,
+            "modes_ms": modes_ms,
             "circuit_s": ms / 1e3,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                          "frac": achieved / hbm_peak, "peak_kind": peak_kind,
-                         "traffic": (STAGED_TRAFFIC_PER_AMP * (1 << n)) if mode == "staged" else None,
+                         "traffic": (STAGED_TRAFFIC_PER_AMP * (1 << n)) if staged_kernel else None,
                          "kernel": ("k_staged_pass: one HBM pass (2 x 16 x 2^n B) applying ~"
-                                    f"{len(gates) / max(1, passes):.0f} gates" if mode == "staged"
+                                    f"{len(gates) / max(1, passes):.0f} circuit gates" if staged_kernel
                                     else "gate kernels: one HBM pass (2 x 16 x 2^n B) per gate"),
-                         "traffic_note": "scaled from the 26-qubit ncu capture by amplitudes" if mode == "staged" else None},
+                         "traffic_note": "scaled from the 26-qubit ncu capture by amplitudes" if staged_kernel else None},
             "roofline_fp64": {"achieved_tinstr_s": fp64_instr / (ms / 1e3) / 1e12,
                               "peak_tinstr_s": fp64_peak / 1e12,
                               "frac": fp64_instr / (ms / 1e3) / fp64_peak,
-                              "note": "4 FP64 instr/amplitude/rotation; nominal 64 FP64 FMA/clk/SM at 1965 MHz"},
+                              "note": "FP64 instr/amplitude: rotation or 1q diagonal 4, 1q dense 8, k-qubit dense "
+                                      "4 x 2^k, CNOT/CZ/SWAP 0; nominal 64 FP64 FMA/clk/SM at 1965 MHz"},
             "kernels": kernels,
             "e2e": {"value": world * gb_per_step / (e2e_ms / 1e3), "unit": "GB/s", "ms_per_step": e2e_ms,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,

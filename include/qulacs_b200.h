@@ -253,6 +253,8 @@ typedef struct qs_circuit_s* qs_circuit_t;
 /* Execution modes of qs_circuit_update_quantum_state. */
 #define QS_EXEC_GATE_BY_GATE 0 /* one kernel per gate: the reference's method */
 #define QS_EXEC_STAGED 1       /* several gates per HBM pass, identical arithmetic per gate */
+#define QS_EXEC_STAGED_FUSED 2 /* runs of gates composed in FP64 into k-qubit dense blocks (k chosen per
+                                  circuit by measurement, or forced by qs_circuit_set_fusion), then staged */
 
 QS_API int qs_circuit_create(QS_UINT qubit_count, qs_circuit_t* out);
 QS_API int qs_circuit_destroy(qs_circuit_t circuit);
@@ -268,6 +270,24 @@ QS_API int qs_circuit_pass_count(qs_circuit_t circuit, QS_ITYPE dim, QS_UINT* ou
  * phases, operations inside phases, gates run by the gate-by-gate kernels between passes. */
 QS_API int qs_circuit_staged_stats(qs_circuit_t circuit, QS_UINT* passes, QS_UINT* phases, QS_UINT* ops,
     QS_UINT* single_gates);
+/* ---- FP64 gate fusion (the reference's counterpart: QuantumCircuitOptimizer::optimize(circuit, k),
+ * cppsim/circuit_optimizer.cpp:113-168, composing with gate::merge, cppsim/gate_merge.cpp:316-356) ----
+ * New circuit whose gates are the greedy k-qubit fusion of `circuit` (0 <= k <= 6): each run of
+ * gates whose qubits fit in k qubits becomes one dense gate on them (ascending qubit order; a
+ * one-qubit diagonal product stays diagonal; a run of one gate is kept as it is).  Host only. */
+QS_API int qs_circuit_fuse(qs_circuit_t circuit, int k, qs_circuit_t* out);
+/* Dense matrix of gate `index` over its qubits (targets then controls, controls expanded; matrix
+ * index bit j <-> qubits[j]): qubits[<=6], matrix[2 * 4^count] interleaved complex.  Host only. */
+QS_API int qs_circuit_gate_matrix(qs_circuit_t circuit, QS_UINT index, QS_UINT* qubits, QS_UINT* qubit_count,
+    double* matrix);
+/* QS_EXEC_STAGED_FUSED: force the block size k (0..6; 0 = no fusion), or -1 (default) to let the
+ * autotuner choose k in 0..4 on the next run by timing each candidate's staged passes. */
+QS_API int qs_circuit_set_fusion(qs_circuit_t circuit, int k);
+/* The schedule last built for QS_EXEC_STAGED_FUSED: block size (-1 before the first run), gate count
+ * after fusion, HBM passes, and the autotuner's estimate per k = 0..4 in ms (estimates_ms[5], may be
+ * NULL; < 0 where not tried). */
+QS_API int qs_circuit_fusion_info(qs_circuit_t circuit, int* k, QS_UINT* gate_count, QS_UINT* passes,
+    double* estimates_ms);
 /* Apply to a density matrix (gates as U rho U^dagger, depolarizing channels exact). */
 QS_API int qs_circuit_update_density_matrix(
     qs_circuit_t circuit, void* rho, QS_ITYPE dim, int exec_mode, void* stream);

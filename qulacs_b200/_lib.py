@@ -90,6 +90,10 @@ SIGNATURES = {
     "qs_circuit_pass_count": [P, IT, C.POINTER(U)],
     "qs_circuit_staged_stats": [P, C.POINTER(U), C.POINTER(U), C.POINTER(U), C.POINTER(U)],
     "qs_circuit_update_density_matrix": [P, P, IT, I, P],
+    "qs_circuit_fuse": [P, I, C.POINTER(P)],
+    "qs_circuit_gate_matrix": [P, U, P, C.POINTER(U), P],
+    "qs_circuit_set_fusion": [P, I],
+    "qs_circuit_fusion_info": [P, C.POINTER(I), C.POINTER(U), C.POINTER(U), P],
     "qs_circuit_update_quantum_state_fused_c64": [P, P, IT, P],
     "qs_batch_update_quantum_states": [P, P, U, P],
     "qs_batch_expectation_values": [P, P, U, P, P, P, P, P, P],
@@ -123,6 +127,7 @@ GATE_KINDS = {
 }
 EXEC_GATE_BY_GATE = 0
 EXEC_STAGED = 1
+EXEC_STAGED_FUSED = 2
 
 
 class QsError(RuntimeError):

@@ -12,7 +12,9 @@ class QuantumCircuit:
     """Gate list applied in order by ``update_quantum_state`` (cppsim circuit.cpp:46-57).
 
     ``mode="gate_by_gate"`` launches one kernel per gate (the reference's method);
-    ``mode="staged"`` applies several gates per HBM pass with the same per-gate arithmetic.
+    ``mode="staged"`` applies several gates per HBM pass with the same per-gate arithmetic;
+    ``mode="staged_fused"`` first composes runs of gates into k-qubit dense blocks in FP64 (k chosen
+    per circuit by timing, or forced with ``set_fusion``), then stages them.
     """
 
     def __init__(self, qubit_count: int):
@@ -76,11 +78,31 @@ class QuantumCircuit:
         if type(state).__name__ == "QuantumStateC64":
             call("qs_circuit_update_quantum_state_fused_c64", self._h, state.data_ptr(), state.dim, state.stream)
             return
-        m = {"gate_by_gate": _lib.EXEC_GATE_BY_GATE, "staged": _lib.EXEC_STAGED}[mode]
+        m = {"gate_by_gate": _lib.EXEC_GATE_BY_GATE, "staged": _lib.EXEC_STAGED,
+             "staged_fused": _lib.EXEC_STAGED_FUSED}[mode]
         if state.is_state_vector():
             call("qs_circuit_update_quantum_state", self._h, state.data_ptr(), state.dim, m, state.stream)
         else:
             call("qs_circuit_update_density_matrix", self._h, state.data_ptr(), state.dim, m, state.stream)
+
+    def set_fusion(self, k: int) -> None:
+        """Block size of mode="staged_fused": 0..6, or -1 to let the autotuner choose (default)."""
+        call("qs_circuit_set_fusion", self._h, int(k))
+
+    def fusion_info(self):
+        """(k, gates after fusion, HBM passes, autotuner estimates in ms for k = 0..4) of the last
+        "staged_fused" schedule; k = -1 before the first run."""
+        k, g, p = C.c_int(), C.c_uint(), C.c_uint()
+        est = (C.c_double * 5)()
+        call("qs_circuit_fusion_info", self._h, C.byref(k), C.byref(g), C.byref(p), est)
+        return k.value, g.value, p.value, list(est)
+
+    def fuse(self, k: int) -> "FusedGateList":
+        """The greedy k-qubit FP64 fusion of this circuit (host only; cppsim QuantumCircuitOptimizer
+        semantics): a read-only list of (qubits, dense matrix) pairs."""
+        h = C.c_void_p()
+        call("qs_circuit_fuse", self._h, int(k), C.byref(h))
+        return FusedGateList(h.value, self.qubit_count)
 
     def fused_stats(self):
         """(tile passes, 6-qubit blocks) of the fused complex64 schedule."""
@@ -98,6 +120,41 @@ class QuantumCircuit:
         out = C.c_uint()
         call("qs_circuit_pass_count", self._h, 1 << self.qubit_count, C.byref(out))
         return out.value
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            try:
+                _lib.load().qs_circuit_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+
+class FusedGateList:
+    """Gates of a fused circuit as (qubits, matrix) with matrix index bit j <-> qubits[j]."""
+
+    def __init__(self, handle, qubit_count: int):
+        self._h = handle
+        self.qubit_count = qubit_count
+        out = C.c_uint()
+        call("qs_circuit_gate_count", self._h, C.byref(out))
+        self._count = out.value
+
+    def __len__(self):
+        return self._count
+
+    def __getitem__(self, i):
+        import numpy as np
+        if not 0 <= i < self._count:
+            raise IndexError(i)
+        qs = (C.c_uint * 6)()
+        cnt = C.c_uint()
+        m = np.zeros(2 * 4096, dtype=np.float64)
+        call("qs_circuit_gate_matrix", self._h, i, qs, C.byref(cnt), m.ctypes.data_as(C.c_void_p))
+        k = cnt.value
+        mat = m[:2 * 4 ** k].view(np.complex128).reshape(1 << k, 1 << k).copy()
+        return [int(qs[j]) for j in range(k)], mat
 
     def __del__(self):
         h = getattr(self, "_h", None)

@@ -263,8 +263,45 @@ QS_API int qs_circuit_update_quantum_state(qs_circuit_t circuit, void* state, QS
     if (dim != (1ULL << c->n))
         return qs::set_error(QS_ERR_INVALID_ARGUMENT, "state dimension does not match the circuit's qubit count");
     if (mode == QS_EXEC_STAGED) return qs::run_staged(*c, state, dim, (cudaStream_t)stream);
+    if (mode == QS_EXEC_STAGED_FUSED) return qs::run_staged_fused(*c, state, dim, (cudaStream_t)stream);
     if (mode != QS_EXEC_GATE_BY_GATE) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "unknown execution mode");
     for (const GateRec& g : c->gates) QS_TRY(qs::apply_gate_by_gate(g, state, dim, (cudaStream_t)stream));
+    return QS_OK;
+}
+
+QS_API int qs_circuit_fuse(qs_circuit_t circuit, int k, qs_circuit_t* out) {
+    Circuit* c = reinterpret_cast<Circuit*>(circuit);
+    if (!c || !out) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "null argument");
+    if (k < 0 || k > 6) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "fusion block size must be 0..6");
+    Circuit* f = new (std::nothrow) Circuit();
+    if (!f) return qs::set_error(QS_ERR_OUT_OF_MEMORY, "circuit");
+    f->n = c->n;
+    f->gates = qs::fuse_gates(c->gates, k);
+    *out = reinterpret_cast<qs_circuit_t>(f);
+    return QS_OK;
+}
+
+QS_API int qs_circuit_gate_matrix(qs_circuit_t circuit, QS_UINT index, QS_UINT* qubits, QS_UINT* qubit_count,
+    double* matrix) {
+    Circuit* c = reinterpret_cast<Circuit*>(circuit);
+    if (!c || !qubits || !qubit_count || !matrix) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "null argument");
+    if (index >= c->gates.size()) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "gate index out of range");
+    const GateRec& g = c->gates[index];
+    if (g.kind == QS_GATE_DEPOLARIZING) return qs::set_error(QS_ERR_NOT_SUPPORTED, "noise channel has no unitary matrix");
+    const std::vector<UINT> q = g.qubits();
+    if (q.size() > 6) return qs::set_error(QS_ERR_NOT_SUPPORTED, "gate matrix export: at most 6 qubits");
+    const int kb = (int)q.size(), md = 1 << kb;
+    std::vector<cd> U((size_t)md * md, 0.);
+    for (int i = 0; i < md; ++i) U[(size_t)i * md + i] = 1.;
+    std::vector<int> pos(kb);
+    for (int j = 0; j < kb; ++j) pos[j] = j;
+    qs::apply_gate_to_block(U, kb, g, pos);
+    for (int j = 0; j < kb; ++j) qubits[j] = q[j];
+    *qubit_count = (QS_UINT)kb;
+    for (size_t i = 0; i < U.size(); ++i) {
+        matrix[2 * i] = U[i].real();
+        matrix[2 * i + 1] = U[i].imag();
+    }
     return QS_OK;
 }
 

@@ -34,16 +34,32 @@ struct Circuit {
     // cached fused complex64 plan (fused_c64.cu)
     std::shared_ptr<void> fused;
     ITYPE fused_dim = 0;
+    // FP64-fused gate list and its staged schedule (QS_EXEC_STAGED_FUSED, staged.cu)
+    int fusion_k = -1;              // forced block size, or -1: the autotuner chooses
+    int fused_k = -1;               // block size of fgates (valid while fplan is set)
+    std::vector<GateRec> fgates;
+    std::shared_ptr<StagedPlan> fplan;
+    std::vector<double> tune_ms;    // autotuner estimate per candidate block size (ms; < 0: not tried)
     void invalidate() {
         plan.reset();
         fused.reset();
         fused_dim = 0;
+        fplan.reset();
+        fgates.clear();
+        fused_k = -1;
+        tune_ms.clear();
     }
 };
 
 int apply_gate_by_gate(const GateRec& g, void* state, ITYPE dim, cudaStream_t st);
 int apply_gate_dm(const GateRec& g, void* rho, ITYPE dim, cudaStream_t st);
 int run_staged(Circuit& c, void* state, ITYPE dim, cudaStream_t st);
+int run_staged_fused(Circuit& c, void* state, ITYPE dim, cudaStream_t st);
 int staged_pass_count(Circuit& c, ITYPE dim, UINT* out);
+
+// fusion.cpp: U <- G U for gate g on block-local bit positions `pos` (targets then controls) of a
+// kb-qubit block matrix U (2^kb x 2^kb, row-major); and the greedy k-qubit fusion of a gate list.
+void apply_gate_to_block(std::vector<std::complex<double>>& U, int kb, const GateRec& g, const std::vector<int>& pos);
+std::vector<GateRec> fuse_gates(const std::vector<GateRec>& G, int k);
 
 }  // namespace qs

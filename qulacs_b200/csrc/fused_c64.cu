@@ -398,44 +398,6 @@ static float host_bf16_to_float(uint16_t h) {
     return f;
 }
 
-// Apply a gate (dense on `pos` = positions of its qubits within the 6-bit block index, targets first
-// then controls with their values) to every column of the 64x64 matrix U (U <- G U).
-static void apply_to_block(std::vector<cd>& U, const GateRec& g, const std::vector<int>& pos) {
-    const std::vector<cd> gm = g.dense_matrix();
-    const int nt = (int)g.targets.size();
-    const int nc = (int)g.controls.size();
-    const int md = 1 << nt;
-    std::vector<cd> tmp(md);
-    for (int col = 0; col < 64; ++col) {
-        for (int base = 0; base < 64; ++base) {
-            bool is_base = true;
-            for (int j = 0; j < nt; ++j)
-                if ((base >> pos[j]) & 1) is_base = false;
-            if (!is_base) continue;
-            bool active = true;
-            for (int j = 0; j < nc; ++j)
-                if (((base >> pos[nt + j]) & 1) != (int)g.control_values[j]) active = false;
-            if (!active) continue;
-            for (int y = 0; y < md; ++y) {
-                cd acc = 0.;
-                for (int x = 0; x < md; ++x) {
-                    int idx = base;
-                    for (int j = 0; j < nt; ++j)
-                        if ((x >> j) & 1) idx |= 1 << pos[j];
-                    acc += gm[y * md + x] * U[idx * 64 + col];
-                }
-                tmp[y] = acc;
-            }
-            for (int y = 0; y < md; ++y) {
-                int idx = base;
-                for (int j = 0; j < nt; ++j)
-                    if ((y >> j) & 1) idx |= 1 << pos[j];
-                U[idx * 64 + col] = tmp[y];
-            }
-        }
-    }
-}
-
 static ITYPE gate_mask(const GateRec& g) {
     ITYPE m = 0;
     for (UINT q : g.qubits()) m |= 1ULL << q;
@@ -778,7 +740,7 @@ int fused_plan_host(const Circuit& c, FusedPlanHost* P) {
                 for (UINT gq : g.qubits())
                     for (int j = 0; j < kFBlock; ++j)
                         if (bq[j] == gq) pos.push_back(j);
-                apply_to_block(U, g, pos);
+                apply_gate_to_block(U, kFBlock, g, pos);
             }
             blk.U = U;
             blk.ngates = (int)bg.size();

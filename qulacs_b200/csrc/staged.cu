@@ -414,9 +414,8 @@ struct HostPlan {
 };
 
 // Host-only part of planning: passes, phases and encoded ops (no device calls).
-static void make_host_plan(const Circuit& c, HostPlan* H) {
-    const UINT n = c.n;
-    H->passes = plan_passes(c.gates, n);
+static void make_host_plan(const std::vector<GateRec>& gates, UINT n, HostPlan* H) {
+    H->passes = plan_passes(gates, n);
     const std::vector<PassPlan>& passes = H->passes;
     std::vector<StPhase>& phases = H->phases;
     std::vector<StOp>& ops = H->ops;
@@ -436,7 +435,7 @@ static void make_host_plan(const Circuit& c, HostPlan* H) {
             // candidates: greedy in order, and windows of 4 consecutive tile bits
             auto bits_of = [&](int gi) {
                 ITYPE bm = 0;
-                for (UINT g : c.gates[gi].qubits()) bm |= 1ULL << local_bit(p.q, g);
+                for (UINT g : gates[gi].qubits()) bm |= 1ULL << local_bit(p.q, g);
                 return bm;
             };
             auto take = [&](ITYPE R, std::vector<int>* got) {
@@ -486,7 +485,7 @@ static void make_host_plan(const Circuit& c, HostPlan* H) {
                 }
             ph.op_begin = (uint32_t)ops.size();
             for (int gi : best) {
-                const GateRec& g = c.gates[gi];
+                const GateRec& g = gates[gi];
                 StOp op{};
                 auto rb = [&](UINT gq) { return (uint8_t)regbit[local_bit(p.q, gq)]; };
                 op.param = (uint32_t)pool.size();
@@ -546,7 +545,7 @@ static void make_host_plan(const Circuit& c, HostPlan* H) {
             }
             ph.op_count = (uint32_t)(ops.size() - ph.op_begin);
             phases.push_back(ph);
-            std::vector<char> taken(c.gates.size(), 0);
+            std::vector<char> taken(gates.size(), 0);
             for (int gi : best) taken[gi] = 1;
             std::vector<int> rest;
             for (int gi : todo)
@@ -557,11 +556,11 @@ static void make_host_plan(const Circuit& c, HostPlan* H) {
     }
 }
 
-static int build_plan(Circuit& c, ITYPE dim, std::shared_ptr<StagedPlan>* out) {
+static int build_plan(const std::vector<GateRec>& gates, UINT n, ITYPE dim, std::shared_ptr<StagedPlan>* out) {
     auto P = std::make_shared<StagedPlan>();
     P->dim = dim;
     HostPlan H;
-    make_host_plan(c, &H);
+    make_host_plan(gates, n, &H);
     const std::vector<PassPlan>& passes = H.passes;
     const std::vector<StPhase>& phases = H.phases;
     const std::vector<StOp>& ops = H.ops;
@@ -600,19 +599,14 @@ static int build_plan(Circuit& c, ITYPE dim, std::shared_ptr<StagedPlan>* out) {
 }
 
 static int ensure_plan(Circuit& c, ITYPE dim) {
-    if (!c.plan || c.plan->dim != dim) QS_TRY(build_plan(c, dim, &c.plan));
+    if (!c.plan || c.plan->dim != dim) QS_TRY(build_plan(c.gates, c.n, dim, &c.plan));
     return QS_OK;
 }
 
-int run_staged(Circuit& c, void* state, ITYPE dim, cudaStream_t st) {
-    if (c.n < kPhaseBits) {  // too small for a 4-qubit register phase
-        for (const GateRec& g : c.gates) QS_TRY(apply_gate_by_gate(g, state, dim, st));
-        return QS_OK;
-    }
-    QS_TRY(ensure_plan(c, dim));
-    for (const DevPass& d : c.plan->passes) {
+static int run_plan(const std::vector<GateRec>& gates, const StagedPlan& P, void* state, ITYPE dim, cudaStream_t st) {
+    for (const DevPass& d : P.passes) {
         if (d.single) {
-            QS_TRY(apply_gate_by_gate(c.gates[d.gate], state, dim, st));
+            QS_TRY(apply_gate_by_gate(gates[d.gate], state, dim, st));
             continue;
         }
         const ITYPE tiles = dim >> d.args.m;
@@ -622,13 +616,112 @@ int run_staged(Circuit& c, void* state, ITYPE dim, cudaStream_t st) {
     return QS_OK;
 }
 
+int run_staged(Circuit& c, void* state, ITYPE dim, cudaStream_t st) {
+    if (c.n < kPhaseBits) {  // too small for a 4-qubit register phase
+        for (const GateRec& g : c.gates) QS_TRY(apply_gate_by_gate(g, state, dim, st));
+        return QS_OK;
+    }
+    QS_TRY(ensure_plan(c, dim));
+    return run_plan(c.gates, *c.plan, state, dim, st);
+}
+
+// ---- FP64 gate fusion + staged passes, block size chosen by measurement.
+// The autotuner fuses the gate list for each candidate block size k (0 = unfused), builds its staged
+// schedule and times every pass's kernel on a scratch buffer of whole tiles (the pass's ops only see
+// tile-local bits, so its tile qubits are remapped to 0..m-1); a pass costs at least its HBM time.
+// Gates left outside passes cost one HBM pass each (dense 5- and 6-qubit kernels more).
+constexpr int kTuneMaxK = 4;
+constexpr double kTuneHbmBytesPerSec = 6.5e12;  // B200 streaming copy bandwidth
+
+static double single_gate_factor(const GateRec& g) {
+    const size_t k = g.targets.size() + g.controls.size();
+    if (g.kind == QS_GATE_DENSE && k == 5) return 2.0;
+    if (g.kind == QS_GATE_DENSE && k >= 6) return 12.0;
+    return 1.0;
+}
+
+static int estimate_plan_ms(const std::vector<GateRec>& gates, const StagedPlan& P, ITYPE dim, cudaStream_t st,
+    double* out_ms) {
+    const double hbm_ms = 2.0 * 16.0 * (double)dim / kTuneHbmBytesPerSec * 1e3;
+    double total = 0.;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    QS_CUDA_CHECK(cudaEventCreate(&e0));
+    QS_CUDA_CHECK(cudaEventCreate(&e1));
+    int rc = QS_OK;
+    for (const DevPass& d : P.passes) {
+        if (d.single) {
+            total += hbm_ms * single_gate_factor(gates[d.gate]);
+            continue;
+        }
+        const ITYPE tiles = dim >> d.args.m;
+        const ITYPE tt = std::min<ITYPE>(tiles, (ITYPE)sm_count() * 3 * 4);
+        void* buf = nullptr;
+        rc = scratch(st, (size_t)(tt << d.args.m) * sizeof(double2), &buf);
+        if (rc != QS_OK) break;
+        StPassArgs a = d.args;
+        for (int j = 0; j < a.m; ++j) a.q[j] = (UINT)j;
+        k_staged_pass<<<(unsigned)tt, kStThreads, 0, st>>>((double2*)buf, a);  // warm-up
+        cudaEventRecord(e0, st);
+        k_staged_pass<<<(unsigned)tt, kStThreads, 0, st>>>((double2*)buf, a);
+        cudaEventRecord(e1, st);
+        rc = check_launch("k_staged_pass");
+        if (rc != QS_OK) break;
+        if (cudaEventSynchronize(e1) != cudaSuccess) {
+            rc = set_error(QS_ERR_CUDA, "autotune: event synchronize failed");
+            break;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        total += std::max((double)ms * (double)tiles / (double)tt, hbm_ms);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *out_ms = total;
+    return rc;
+}
+
+static int ensure_fused_plan(Circuit& c, ITYPE dim, cudaStream_t st) {
+    if (c.fplan && c.fplan->dim == dim) return QS_OK;
+    if (c.fusion_k >= 0) {
+        c.fgates = fuse_gates(c.gates, c.fusion_k);
+        c.fused_k = c.fusion_k;
+        return build_plan(c.fgates, c.n, dim, &c.fplan);
+    }
+    c.tune_ms.assign(kTuneMaxK + 1, -1.);
+    double best = 0.;
+    for (int k = 0; k <= kTuneMaxK; ++k) {
+        std::vector<GateRec> fg = fuse_gates(c.gates, k);
+        std::shared_ptr<StagedPlan> P;
+        QS_TRY(build_plan(fg, c.n, dim, &P));
+        double ms = 0.;
+        QS_TRY(estimate_plan_ms(fg, *P, dim, st, &ms));
+        c.tune_ms[k] = ms;
+        if (!c.fplan || ms < best) {
+            best = ms;
+            c.fgates.swap(fg);
+            c.fplan = P;
+            c.fused_k = k;
+        }
+    }
+    return QS_OK;
+}
+
+int run_staged_fused(Circuit& c, void* state, ITYPE dim, cudaStream_t st) {
+    if (c.n < kPhaseBits) {
+        for (const GateRec& g : c.gates) QS_TRY(apply_gate_by_gate(g, state, dim, st));
+        return QS_OK;
+    }
+    QS_TRY(ensure_fused_plan(c, dim, st));
+    return run_plan(c.fgates, *c.fplan, state, dim, st);
+}
+
 int staged_pass_count(Circuit& c, ITYPE dim, UINT* out) {
     if (c.n < kPhaseBits) {
         *out = (UINT)c.gates.size();
         return QS_OK;
     }
     HostPlan H;
-    make_host_plan(c, &H);
+    make_host_plan(c.gates, c.n, &H);
     *out = (UINT)H.passes.size();
     return QS_OK;
 }
@@ -642,7 +735,7 @@ extern "C" QS_API int qs_circuit_staged_stats(qs_circuit_t circuit, QS_UINT* pas
     qs::Circuit* c = reinterpret_cast<qs::Circuit*>(circuit);
     if (!c || !passes || !phases || !ops || !single_gates) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "null argument");
     qs::HostPlan H;
-    qs::make_host_plan(*c, &H);
+    qs::make_host_plan(c->gates, c->n, &H);
     UINT single = 0;
     for (const qs::PassPlan& p : H.passes) single += p.single ? 1 : 0;
     *passes = (QS_UINT)H.passes.size();
@@ -652,9 +745,35 @@ extern "C" QS_API int qs_circuit_staged_stats(qs_circuit_t circuit, QS_UINT* pas
     return QS_OK;
 }
 
-namespace qs {
+// Block size, gate count and HBM passes of the FP64-fused schedule last built for QS_EXEC_STAGED_FUSED
+// (k = -1 before the first run), and the autotuner's estimate per candidate k = 0..4 (ms; < 0 when
+// not tried, e.g. with a forced k).
+extern "C" QS_API int qs_circuit_fusion_info(qs_circuit_t circuit, int* k, QS_UINT* gate_count, QS_UINT* passes,
+    double* estimates_ms) {
+    qs::Circuit* c = reinterpret_cast<qs::Circuit*>(circuit);
+    if (!c || !k || !gate_count || !passes) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "null argument");
+    *k = c->fplan ? c->fused_k : -1;
+    *gate_count = c->fplan ? (QS_UINT)c->fgates.size() : 0;
+    *passes = c->fplan ? (QS_UINT)c->fplan->passes.size() : 0;
+    if (estimates_ms)
+        for (int i = 0; i <= qs::kTuneMaxK; ++i)
+            estimates_ms[i] = i < (int)c->tune_ms.size() ? c->tune_ms[i] : -1.;
+    return QS_OK;
+}
 
-}  // namespace qs
+// Force the FP64 fusion block size of QS_EXEC_STAGED_FUSED (0..6; 0 = no fusion) or, with -1, let
+// the autotuner choose on the next run.
+extern "C" QS_API int qs_circuit_set_fusion(qs_circuit_t circuit, int k) {
+    qs::Circuit* c = reinterpret_cast<qs::Circuit*>(circuit);
+    if (!c) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "null circuit");
+    if (k < -1 || k > 6) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "fusion block size must be -1..6");
+    c->fusion_k = k;
+    c->fplan.reset();
+    c->fgates.clear();
+    c->fused_k = -1;
+    c->tune_ms.clear();
+    return QS_OK;
+}
 
 // ---------------------------------------------------------------- batched execution
 // Many circuits (each on its own state, of any size >= 4 qubits) in ONE persistent launch.  Work

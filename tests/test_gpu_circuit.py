@@ -11,7 +11,7 @@ from qulacs_b200 import workloads as W
 
 pytestmark = pytest.mark.gpu
 
-MODES = ["gate_by_gate", "staged"]
+MODES = ["gate_by_gate", "staged", "staged_fused"]
 
 
 @pytest.mark.parametrize("mode", MODES)
@@ -86,3 +86,38 @@ def test_large_circuit_properties(n):
         W.to_circuit(inv, n).update_quantum_state(s, mode=mode)
         assert abs(s.get_zero_probability(0) - 1.0) <= 1e-12
         assert abs(s.get_marginal_probability([0] * n) - 1.0) <= 1e-12
+
+
+@pytest.mark.parametrize("k", [0, 1, 2, 3, 5])
+def test_forced_fusion_sizes_against_oracle(port, k):
+    n = 17
+    gates = W.layered_rotation_circuit(n, 3, seed=91) + W.u3_cz_circuit(n, 2, seed=92) + W.hea_circuit(n, 2, 93)
+    circ = W.to_circuit(gates, n)
+    circ.set_fusion(k)
+    s = QuantumState(n)
+    circ.update_quantum_state(s, mode="staged_fused")
+    want = np.zeros(1 << n, dtype=np.complex128)
+    want[0] = 1
+    W.run_on_cpu(gates, want, port)
+    assert np.max(np.abs(s.get_vector() - want)) <= AMP_TOL
+    kk, count, passes, est = circ.fusion_info()
+    assert kk == k and count == len(circ.fuse(k)) and passes >= 1
+    assert all(e < 0 for e in est)  # forced: the autotuner did not run
+
+
+def test_autotuner_records_estimates(port):
+    n = 20
+    gates = W.layered_rotation_circuit(n, 4, seed=95)
+    circ = W.to_circuit(gates, n)
+    s = QuantumState(n)
+    circ.update_quantum_state(s, mode="staged_fused")
+    k, count, passes, est = circ.fusion_info()
+    assert 0 <= k <= 4 and all(e > 0 for e in est)
+    assert est[k] == min(est)
+    want = np.zeros(1 << n, dtype=np.complex128)
+    want[0] = 1
+    W.run_on_cpu(gates, want, port)
+    assert np.max(np.abs(s.get_vector() - want)) <= AMP_TOL
+    # a second run reuses the schedule
+    circ.update_quantum_state(s, mode="staged_fused")
+    assert circ.fusion_info()[0] == k
