@@ -342,6 +342,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mode", default="staged_fused", choices=["staged_fused", "staged", "gate_by_gate"])
+    ap.add_argument("--fusion-k", type=int, default=-1,
+                    help="staged_fused block size (-1: autotuned; pin the autotuner's choice for profiler runs, "
+                         "whose instrumented launches distort its timings)")
     ap.add_argument("--no-mode-compare", action="store_true",
                     help="skip timing the other complex128 execution modes beside the headline one")
     ap.add_argument("--qubits", type=int, default=N_QUBITS)
@@ -404,6 +407,8 @@ def main():
     gates = W.layered_rotation_circuit(n, DEPTH, GATE_SEED)
     terms = W.random_pauli_terms(n, N_TERMS, 1, 6, TERM_SEED)
     circ = W.to_circuit(gates, n)
+    if args.fusion_k >= 0:
+        circ.set_fusion(args.fusion_k)
     obs = W.to_observable(terms, n)
     state = Q.QuantumState(n)
     mode = args.mode

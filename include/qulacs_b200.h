@@ -288,7 +288,16 @@ QS_API int qs_circuit_set_fusion(qs_circuit_t circuit, int k);
  * NULL; < 0 where not tried). */
 QS_API int qs_circuit_fusion_info(qs_circuit_t circuit, int* k, QS_UINT* gate_count, QS_UINT* passes,
     double* estimates_ms);
-/* Apply to a density matrix (gates as U rho U^dagger, depolarizing channels exact). */
+/* The circuit acting on a density matrix of n qubits, as a circuit on the 2n-qubit vector
+ * rho[row * 2^n + col] (column = qubits 0..n-1, row = n..2n-1): each gate U becomes U on the row
+ * qubits and conj(U) on the column qubits, each depolarizing channel its superoperator
+ * sum_k p_k K_k (x) conj(K_k) as a dense gate on (column qubits, row qubits).  Host only; this is
+ * what the staged modes of qs_circuit_update_density_matrix execute. */
+QS_API int qs_circuit_density_matrix_as_vector(qs_circuit_t circuit, qs_circuit_t* out);
+/* Apply to a density matrix (gates as U rho U^dagger, depolarizing channels exact).
+ * QS_EXEC_GATE_BY_GATE: one density-matrix kernel per gate or channel (the reference's method);
+ * QS_EXEC_STAGED / QS_EXEC_STAGED_FUSED: the vector circuit above through the staged executors, so
+ * a gate and the noise after it share passes (and, fused, one superoperator block). */
 QS_API int qs_circuit_update_density_matrix(
     qs_circuit_t circuit, void* rho, QS_ITYPE dim, int exec_mode, void* stream);
 
@@ -332,8 +341,10 @@ QS_API int qs_state_sampling_with_uniforms_c64(const void* state_c64, QS_ITYPE d
 QS_API int qs_circuit_fused_stats(qs_circuit_t circuit, QS_UINT* passes, QS_UINT* blocks);
 /* Host-only export of fused block `index` (application order): the pass's tile qubits (<= 13),
  * the block's 6 tile-local bits, its FP64 64x64 matrix (row-major interleaved complex, may be NULL)
- * and its bf16 operand image (hi then lo, 2 x 128 x 128, K-major core-matrix layout, rows and
- * columns in the order qs_circuit_fused_block_layout reports; may be NULL). */
+ * and its bf16 A operand image (2 x 128 x 128 uint16, may be NULL; rows and K in the order
+ * qs_circuit_fused_block_layout reports) in tensor-memory load order: element (row y, K = k) of the
+ * hi (lo) image is TMEM column c = k / 2 (+ 64 for lo), half k % 2, stored at 32-bit word
+ * (w * 32 + y % 32) * 32 + c % 32 with w = y / 32 + 4 * (c / 32). */
 QS_API int qs_circuit_fused_block_export(qs_circuit_t circuit, QS_UINT index, QS_UINT* tile_qubits,
     int* tile_qubit_count, QS_UINT* block_bits, double* matrix, unsigned short* operand_image);
 /* Host-only export of fused block `index`'s operand orders and device index tables:

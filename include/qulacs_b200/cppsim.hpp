@@ -328,7 +328,8 @@ public:
     }
     UINT get_gate_count() const { return (UINT)gate_list.size(); }
     qs_circuit_t handle() const { return h_; }
-    // exec_mode: QS_EXEC_STAGED (default) or QS_EXEC_GATE_BY_GATE
+    // exec_mode: QS_EXEC_STAGED (default), QS_EXEC_STAGED_FUSED (FP64 k-qubit fusion, autotuned k) or
+    // QS_EXEC_GATE_BY_GATE
     void update_quantum_state(QuantumStateBase* state, int exec_mode = QS_EXEC_STAGED) {
         if (state->qubit_count != qubit_count)
             throw std::invalid_argument("update_quantum_state: qubit count differs");

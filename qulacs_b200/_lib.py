@@ -91,6 +91,7 @@ SIGNATURES = {
     "qs_circuit_staged_stats": [P, C.POINTER(U), C.POINTER(U), C.POINTER(U), C.POINTER(U)],
     "qs_circuit_update_density_matrix": [P, P, IT, I, P],
     "qs_circuit_fuse": [P, I, C.POINTER(P)],
+    "qs_circuit_density_matrix_as_vector": [P, C.POINTER(P)],
     "qs_circuit_gate_matrix": [P, U, P, C.POINTER(U), P],
     "qs_circuit_set_fusion": [P, I],
     "qs_circuit_fusion_info": [P, C.POINTER(I), C.POINTER(U), C.POINTER(U), P],

@@ -104,6 +104,13 @@ class QuantumCircuit:
         call("qs_circuit_fuse", self._h, int(k), C.byref(h))
         return FusedGateList(h.value, self.qubit_count)
 
+    def density_matrix_as_vector(self) -> "FusedGateList":
+        """This circuit acting on a density matrix as gates on the 2n-qubit vector rho[row * 2^n + col]
+        (host only): (qubits, matrix) pairs, noise channels as superoperators."""
+        h = C.c_void_p()
+        call("qs_circuit_density_matrix_as_vector", self._h, C.byref(h))
+        return FusedGateList(h.value, 2 * self.qubit_count)
+
     def fused_stats(self):
         """(tile passes, 6-qubit blocks) of the fused complex64 schedule."""
         p, b = C.c_uint(), C.c_uint()

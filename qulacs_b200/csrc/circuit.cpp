@@ -154,6 +154,89 @@ int apply_gate_dm(const GateRec& g, void* rho, ITYPE dim, cudaStream_t st) {
     return qs_dm_multi_qubit_dense_matrix_gate(t, nt, (const double*)u.data(), rho, dim, sp);
 }
 
+static GateRec shifted(const GateRec& g, UINT by) {
+    GateRec r = g;
+    for (UINT& t : r.targets) t += by;
+    for (UINT& c : r.controls) c += by;
+    return r;
+}
+
+// Kraus weights and operators of the reference's depolarizing channels (gate_factory.cpp:451-500):
+// one qubit {1 - p: I, p/3: X, Z, Y}; two qubits {1 - p: I, p/15: each non-identity Pauli pair}.
+static std::vector<cd> depolarizing_superoperator(UINT k, double p) {
+    static const cd P[4][4] = {{1, 0, 0, 1}, {0, 1, 1, 0}, {0, cd(0, -1), cd(0, 1), 0}, {1, 0, 0, -1}};
+    const size_t md = size_t(1) << k, sd = md * md;  // Kraus dim, superoperator dim
+    const UINT nterms = k == 1 ? 4 : 16;
+    std::vector<cd> S(sd * sd, 0.);
+    for (UINT t = 0; t < nterms; ++t) {
+        const double w = t == 0 ? 1. - p : p / (double)(nterms - 1);
+        if (w == 0.) continue;
+        std::vector<cd> K(md * md);
+        for (size_t y = 0; y < md; ++y)
+            for (size_t x = 0; x < md; ++x) {
+                cd v = 1.;
+                for (UINT j = 0; j < k; ++j) v *= P[(t >> (2 * j)) & 3][((y >> j) & 1) * 2 + ((x >> j) & 1)];
+                K[y * md + x] = v;
+            }
+        // index = col + (row << k): S[(r, c), (r', c')] += w K[r][r'] conj(K[c][c'])
+        for (size_t r = 0; r < md; ++r)
+            for (size_t c = 0; c < md; ++c)
+                for (size_t r2 = 0; r2 < md; ++r2)
+                    for (size_t c2 = 0; c2 < md; ++c2)
+                        S[(c + (r << k)) * sd + (c2 + (r2 << k))] += w * K[r * md + r2] * std::conj(K[c * md + c2]);
+    }
+    return S;
+}
+
+std::vector<GateRec> dm_vector_gates(const std::vector<GateRec>& G, UINT n) {
+    std::vector<GateRec> out;
+    for (const GateRec& g : G) {
+        if (g.kind == QS_GATE_DEPOLARIZING) {
+            const UINT k = (UINT)g.targets.size();
+            GateRec s;
+            s.kind = QS_GATE_DENSE;
+            for (UINT t : g.targets) s.targets.push_back(t);
+            for (UINT t : g.targets) s.targets.push_back(t + n);
+            s.matrix = depolarizing_superoperator(k, g.prob);
+            out.push_back(s);
+            continue;
+        }
+        GateRec row = shifted(g, n), col = g;
+        switch (g.kind) {
+            case QS_GATE_RX:
+            case QS_GATE_RZ: col.angle = -g.angle; break;  // conj(exp(i a P / 2)) = exp(-i a P / 2) for X, Z
+            case QS_GATE_RY:
+            case QS_GATE_CNOT:
+            case QS_GATE_CZ:
+            case QS_GATE_SWAP: break;  // real matrices
+            case QS_GATE_DENSE:
+            case QS_GATE_DIAGONAL:
+                for (cd& v : col.matrix) v = std::conj(v);
+                break;
+            case QS_GATE_PAULI:
+            case QS_GATE_PAULI_ROTATION: {
+                // conj(P) = (-1)^{#Y} P
+                UINT ny = 0;
+                for (UINT id : g.pauli_ids) ny += id == 2 ? 1 : 0;
+                if (g.kind == QS_GATE_PAULI_ROTATION) {
+                    col.angle = (ny & 1) ? g.angle : -g.angle;
+                } else if (ny & 1) {
+                    GateRec sign;  // the global -1 of P (x) conj(P)
+                    sign.kind = QS_GATE_DIAGONAL;
+                    sign.targets = {g.targets[0]};
+                    sign.matrix = {cd(-1.), cd(-1.)};
+                    out.push_back(sign);
+                }
+                break;
+            }
+            default: break;
+        }
+        out.push_back(row);
+        out.push_back(col);
+    }
+    return out;
+}
+
 }  // namespace qs
 
 extern "C" {
@@ -281,6 +364,18 @@ QS_API int qs_circuit_fuse(qs_circuit_t circuit, int k, qs_circuit_t* out) {
     return QS_OK;
 }
 
+QS_API int qs_circuit_density_matrix_as_vector(qs_circuit_t circuit, qs_circuit_t* out) {
+    Circuit* c = reinterpret_cast<Circuit*>(circuit);
+    if (!c || !out) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "null argument");
+    if (2 * c->n > 40) return qs::set_error(QS_ERR_NOT_SUPPORTED, "density matrix: at most 20 qubits");
+    Circuit* v = new (std::nothrow) Circuit();
+    if (!v) return qs::set_error(QS_ERR_OUT_OF_MEMORY, "circuit");
+    v->n = 2 * c->n;
+    v->gates = qs::dm_vector_gates(c->gates, c->n);
+    *out = reinterpret_cast<qs_circuit_t>(v);
+    return QS_OK;
+}
+
 QS_API int qs_circuit_gate_matrix(qs_circuit_t circuit, QS_UINT index, QS_UINT* qubits, QS_UINT* qubit_count,
     double* matrix) {
     Circuit* c = reinterpret_cast<Circuit*>(circuit);
@@ -316,9 +411,22 @@ QS_API int qs_circuit_update_density_matrix(qs_circuit_t circuit, void* rho, QS_
     if (!c) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "null circuit");
     if (dim != (1ULL << c->n))
         return qs::set_error(QS_ERR_INVALID_ARGUMENT, "density matrix dimension does not match the circuit");
-    (void)mode;
-    for (const GateRec& g : c->gates) QS_TRY(qs::apply_gate_dm(g, rho, dim, (cudaStream_t)stream));
-    return QS_OK;
+    if (mode == QS_EXEC_GATE_BY_GATE) {
+        for (const GateRec& g : c->gates) QS_TRY(qs::apply_gate_dm(g, rho, dim, (cudaStream_t)stream));
+        return QS_OK;
+    }
+    if (mode != QS_EXEC_STAGED && mode != QS_EXEC_STAGED_FUSED)
+        return qs::set_error(QS_ERR_INVALID_ARGUMENT, "unknown execution mode");
+    if (2 * c->n > 40) return qs::set_error(QS_ERR_NOT_SUPPORTED, "density matrix: at most 20 qubits");
+    if (!c->dm_vec) {
+        auto v = std::make_shared<Circuit>();
+        v->n = 2 * c->n;
+        v->gates = qs::dm_vector_gates(c->gates, c->n);
+        v->fusion_k = c->fusion_k;
+        c->dm_vec = v;
+    }
+    if (mode == QS_EXEC_STAGED) return qs::run_staged(*c->dm_vec, rho, dim * dim, (cudaStream_t)stream);
+    return qs::run_staged_fused(*c->dm_vec, rho, dim * dim, (cudaStream_t)stream);
 }
 
 }  // extern "C"

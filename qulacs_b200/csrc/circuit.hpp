@@ -40,7 +40,11 @@ struct Circuit {
     std::vector<GateRec> fgates;
     std::shared_ptr<StagedPlan> fplan;
     std::vector<double> tune_ms;    // autotuner estimate per candidate block size (ms; < 0: not tried)
+    // the circuit acting on a density matrix seen as a 2n-qubit vector (circuit.cpp), for the staged
+    // executors of qs_circuit_update_density_matrix
+    std::shared_ptr<Circuit> dm_vec;
     void invalidate() {
+        dm_vec.reset();
         plan.reset();
         fused.reset();
         fused_dim = 0;
@@ -53,6 +57,11 @@ struct Circuit {
 
 int apply_gate_by_gate(const GateRec& g, void* state, ITYPE dim, cudaStream_t st);
 int apply_gate_dm(const GateRec& g, void* rho, ITYPE dim, cudaStream_t st);
+// A density-matrix circuit on n qubits as gates on the 2n-qubit vector rho[row * 2^n + col]
+// (column = bits 0..n-1, row = bits n..2n-1): a gate U -> U on the row bits and conj(U) on the
+// column bits; a noise channel -> its superoperator sum_k p_k K_k (x) conj(K_k) on its column bits
+// then row bits.
+std::vector<GateRec> dm_vector_gates(const std::vector<GateRec>& G, UINT n);
 int run_staged(Circuit& c, void* state, ITYPE dim, cudaStream_t st);
 int run_staged_fused(Circuit& c, void* state, ITYPE dim, cudaStream_t st);
 int staged_pass_count(Circuit& c, ITYPE dim, UINT* out);

@@ -768,6 +768,7 @@ extern "C" QS_API int qs_circuit_set_fusion(qs_circuit_t circuit, int k) {
     if (!c) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "null circuit");
     if (k < -1 || k > 6) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "fusion block size must be -1..6");
     c->fusion_k = k;
+    c->dm_vec.reset();
     c->fplan.reset();
     c->fgates.clear();
     c->fused_k = -1;

@@ -40,12 +40,13 @@ def test_dm_gates_and_channels(port):
         assert np.max(np.abs(d.get_matrix() - want)) <= AMP_TOL, gate
 
 
-def test_noisy_circuit_golden_and_stats(port):
+@pytest.mark.parametrize("mode", ["gate_by_gate", "staged", "staged_fused"])
+def test_noisy_circuit_golden_and_stats(port, mode):
     g = np.load(os.path.join(GOLDEN, "noisy_dm_n5.npz"))
     n = int(g["n"])
     gates = W.noisy_circuit(W.hea_circuit(n, int(g["depth"]), int(g["gate_seed"])), float(g["p"]))
     d = DensityMatrix(n)
-    W.to_circuit(gates, n).update_quantum_state(d)
+    W.to_circuit(gates, n).update_quantum_state(d, mode=mode)
     rho = d.get_matrix()
     assert np.max(np.abs(rho - g["rho"])) <= AMP_TOL
     terms = W.random_pauli_terms(n, 16, 1, 3, int(g["term_seed"]))
@@ -68,3 +69,31 @@ def test_pure_state_density_matrix_matches_state_vector(port):
     d2 = DensityMatrix(n)
     d2.load(s)
     assert np.max(np.abs(d2.get_matrix() - np.outer(v, v.conj()))) <= AMP_TOL
+
+
+@pytest.mark.parametrize("mode", ["gate_by_gate", "staged", "staged_fused"])
+@pytest.mark.parametrize("n", [3, 7, 10])
+def test_noisy_circuits_every_mode_against_oracle(port, mode, n):
+    rng = np.random.default_rng(1200 + n)
+    gates = W.noisy_circuit(W.hea_circuit(n, 2, 50 + n), 1e-3) + W.noisy_circuit(W.u3_cz_circuit(n, 2, 60 + n), 0.02)
+    rho0 = random_density_matrix(n, rng)
+    want = rho0.copy()
+    W.run_on_cpu_dm(gates, want, port)
+    d = dev(rho0)
+    W.to_circuit(gates, n).update_quantum_state(d, mode=mode)
+    assert np.max(np.abs(d.get_matrix() - want)) <= AMP_TOL
+
+
+def test_large_noisy_density_matrix_properties():
+    """At 13 qubits (2^26 entries, beyond the oracle): the staged modes agree with the gate-by-gate
+    kernels, and the trace stays 1."""
+    n = 13
+    gates = W.noisy_circuit(W.hea_circuit(n, 2, 71), 1e-3)
+    out = {}
+    for mode in ("gate_by_gate", "staged", "staged_fused"):
+        d = DensityMatrix(n)
+        W.to_circuit(gates, n).update_quantum_state(d, mode=mode)
+        assert abs(d.get_squared_norm() - 1.0) <= 1e-12
+        out[mode] = d.get_matrix()
+    assert np.max(np.abs(out["staged"] - out["gate_by_gate"])) <= AMP_TOL
+    assert np.max(np.abs(out["staged_fused"] - out["gate_by_gate"])) <= AMP_TOL
