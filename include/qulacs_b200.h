@@ -341,10 +341,8 @@ QS_API int qs_state_sampling_with_uniforms_c64(const void* state_c64, QS_ITYPE d
 QS_API int qs_circuit_fused_stats(qs_circuit_t circuit, QS_UINT* passes, QS_UINT* blocks);
 /* Host-only export of fused block `index` (application order): the pass's tile qubits (<= 13),
  * the block's 6 tile-local bits, its FP64 64x64 matrix (row-major interleaved complex, may be NULL)
- * and its bf16 A operand image (2 x 128 x 128 uint16, may be NULL; rows and K in the order
- * qs_circuit_fused_block_layout reports) in tensor-memory load order: element (row y, K = k) of the
- * hi (lo) image is TMEM column c = k / 2 (+ 64 for lo), half k % 2, stored at 32-bit word
- * (w * 32 + y % 32) * 32 + c % 32 with w = y / 32 + 4 * (c / 32). */
+ * and its bf16 operand image (hi then lo, 2 x 128 x 128, K-major core-matrix layout, rows and
+ * columns in the order qs_circuit_fused_block_layout reports; may be NULL). */
 QS_API int qs_circuit_fused_block_export(qs_circuit_t circuit, QS_UINT index, QS_UINT* tile_qubits,
     int* tile_qubit_count, QS_UINT* block_bits, double* matrix, unsigned short* operand_image);
 /* Host-only export of fused block `index`'s operand orders and device index tables:
