@@ -304,8 +304,10 @@ QS_API int qs_circuit_update_density_matrix(
 /* ---- batched execution of many circuits (no reference counterpart: the reference runs one
  * QuantumCircuit::update_quantum_state at a time) ----
  * Applies circuits[i] to states[i] (complex128, 2^n_i amplitudes, n_i >= 4, every gate stageable:
- * <= 2 targets, no controls) for all i in ONE persistent kernel launch; each state's result is the
- * same as running its circuit alone with QS_EXEC_STAGED.  Synchronises `stream`. */
+ * <= 2 targets, no controls) for all i in ONE persistent kernel launch.  Each circuit's gates are
+ * FP64-fused at block size 2 (or its qs_circuit_set_fusion size when that is 0, 1 or 2), so each
+ * state's result is the same as running its circuit alone with QS_EXEC_STAGED_FUSED at that size.
+ * Synchronises `stream`. */
 QS_API int qs_batch_update_quantum_states(const qs_circuit_t* circuits, void* const* states, QS_UINT count,
     void* stream);
 /* <P_k> for the Pauli terms of many complex128 states in one launch.  Terms of state i are

@@ -43,8 +43,16 @@ struct Circuit {
     // the circuit acting on a density matrix seen as a 2n-qubit vector (circuit.cpp), for the staged
     // executors of qs_circuit_update_density_matrix
     std::shared_ptr<Circuit> dm_vec;
+    // batched execution (qs_batch_update_quantum_states): the gate list fused at a fixed block size
+    // (<= 2, so every block stays a pass op) and its staged schedule
+    int bk = -1;
+    std::vector<GateRec> bgates;
+    std::shared_ptr<StagedPlan> bplan;
     void invalidate() {
         dm_vec.reset();
+        bplan.reset();
+        bgates.clear();
+        bk = -1;
         plan.reset();
         fused.reset();
         fused_dim = 0;

@@ -851,6 +851,19 @@ __global__ void __launch_bounds__(kStThreads, 3) k_batch_staged(const BatchRec* 
     }
 }
 
+// Block size of batched execution: the circuit's forced QS_EXEC_STAGED_FUSED size when it is at most 2,
+// else 2 (autotuning each circuit of a batch would cost more than it saves; k <= 2 keeps every fused
+// block a pass op).
+static int batch_block_size(const Circuit& c) { return (c.fusion_k >= 0 && c.fusion_k <= 2) ? c.fusion_k : 2; }
+
+static int ensure_batch_plan(Circuit& c, ITYPE dim) {
+    const int k = batch_block_size(c);
+    if (c.bplan && c.bplan->dim == dim && c.bk == k) return QS_OK;
+    c.bgates = fuse_gates(c.gates, k);
+    c.bk = k;
+    return build_plan(c.bgates, c.n, dim, &c.bplan);
+}
+
 int batch_update(Circuit* const* cs, void* const* states, UINT count, cudaStream_t st) {
     if (count == 0) return QS_OK;
     std::vector<std::vector<const DevPass*>> passes(count);
@@ -858,8 +871,8 @@ int batch_update(Circuit* const* cs, void* const* states, UINT count, cudaStream
     for (UINT i = 0; i < count; ++i) {
         Circuit& c = *cs[i];
         if (c.n < kPhaseBits) return set_error(QS_ERR_NOT_SUPPORTED, "batch: circuits need at least 4 qubits");
-        QS_TRY(ensure_plan(c, 1ULL << c.n));
-        for (const DevPass& d : c.plan->passes) {
+        QS_TRY(ensure_batch_plan(c, 1ULL << c.n));
+        for (const DevPass& d : c.bplan->passes) {
             if (d.single)
                 return set_error(QS_ERR_NOT_SUPPORTED,
                     "batch: every gate must be stageable (<= 2 targets, no controls, no Pauli strings)");

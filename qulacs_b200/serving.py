@@ -28,7 +28,11 @@ import numpy as np
 
 from . import _lib
 from . import workloads as W
-from ._lib import EXEC_STAGED, call
+from ._lib import EXEC_STAGED_FUSED, call
+
+# FP64 fusion block size for every served circuit: fixed (not autotuned per request) so that a
+# request's result does not depend on timing noise, and equal to the batch executor's.
+SERVE_FUSION_K = 2
 from .observable import masks
 
 ALIGN = 256
@@ -214,7 +218,8 @@ class ServingLoop:
             call("qs_state_sampling_with_uniforms_c64", r.ptr, 1 << r.n, _vp(u), u.size, _vp(out), stream)
         else:
             call("qs_initialize_quantum_state", r.ptr, 1 << r.n, stream)
-            call("qs_circuit_update_quantum_state", c._h, r.ptr, 1 << r.n, EXEC_STAGED, stream)
+            c.set_fusion(SERVE_FUSION_K)
+            call("qs_circuit_update_quantum_state", c._h, r.ptr, 1 << r.n, EXEC_STAGED_FUSED, stream)
             call("qs_state_sampling_with_uniforms", r.ptr, 1 << r.n, _vp(u), u.size, _vp(out), stream)
         r.result = out
 
@@ -222,7 +227,8 @@ class ServingLoop:
         c = W.to_circuit(r.gates, r.n)
         dim = 1 << r.n
         call("qs_dm_initialize_quantum_state", r.ptr, dim, stream)
-        call("qs_circuit_update_density_matrix", c._h, r.ptr, dim, EXEC_STAGED, stream)
+        c.set_fusion(SERVE_FUSION_K)
+        call("qs_circuit_update_density_matrix", c._h, r.ptr, dim, EXEC_STAGED_FUSED, stream)
         e = 0.0
         for coef, tl, ids in r.terms:
             t = np.array(tl, dtype=np.uint32)

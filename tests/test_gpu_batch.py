@@ -56,7 +56,8 @@ def test_batch_states_match_gate_by_gate(port):
         v = s.get_vector()
         assert np.max(np.abs(v - psi)) <= 1e-12
         alone = QuantumState(n)
-        circ.update_quantum_state(alone, mode="staged")
+        circ.set_fusion(2)  # the batch's block size
+        circ.update_quantum_state(alone, mode="staged_fused")
         assert np.array_equal(v, alone.get_vector())  # bit-identical alone and in the batch
 
 
