@@ -321,6 +321,27 @@ QS_API int qs_batch_expectation_values_c64(void* const* states, const QS_UINT* q
     const QS_UINT* term_offsets, const QS_ITYPE* x_masks, const QS_ITYPE* z_masks, const QS_UINT* y_counts,
     double* values, void* stream);
 
+/* ---- noisy sampling by trajectories (cppsim NoiseSimulator, noisesimulator.cpp:18-198) ----
+ * Each of `sample_count` samples replaces every depolarizing channel of `circuit` by one Kraus operator
+ * drawn as the reference draws it: the channel's operators in descending (probability, index) order
+ * (QuantumGate_Probabilistic::optimize_ProbablisticGate, gate_general.hpp:350-372), one uniform u per
+ * channel, operator lower_bound(cumulative, u) - 1 (noisesimulator.cpp:167-185).  Identical
+ * trajectories are merged and visited in descending lexicographic order of their choices; each is
+ * simulated once (from a shared device prefix state) and sampled as many times as it was drawn.  The
+ * reference seeds its generator from std::random_device; here one mt19937_64(seed) stream gives all
+ * selection uniforms (sample-major, channels in circuit order) and then each trajectory's sampling
+ * uniforms, so a run is reproducible.
+ * Host only: the number of distinct trajectories and, if `shots` is not NULL, each one's sample count. */
+QS_API int qs_noise_simulator_trajectories(qs_circuit_t circuit, QS_UINT sample_count, QS_UINT seed,
+    QS_UINT* trajectory_count, QS_UINT* shots);
+/* Run it: `samples` (may be NULL) receives sample_count basis indices grouped by trajectory in that
+ * order (Result::sampling, noisesimulator.cpp:57-65); `trajectory_states` (may be NULL, else
+ * trajectory_count device complex128 buffers of dim amplitudes, NULL entries skipped) receives each
+ * trajectory's final state (execute_and_get_result).  `initial_state` is a device state or NULL for
+ * |0...0>.  Synchronises `stream`. */
+QS_API int qs_noise_simulator_execute(qs_circuit_t circuit, const void* initial_state, QS_ITYPE dim,
+    QS_UINT sample_count, QS_UINT seed, QS_ITYPE* samples, void* const* trajectory_states, void* stream);
+
 /* ---- fused reduced-precision execution (no reference counterpart; its comparison point is the
  * reference's gate merging, QuantumCircuitOptimizer::optimize, cppsim/circuit_optimizer.cpp:113-168,
  * and gate::merge, cppsim/gate_merge.cpp:316-356) ----

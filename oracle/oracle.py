@@ -212,3 +212,118 @@ def reference() -> CpuSim | None:
     if _ref is None and os.path.exists(REF_SO):
         _ref = CpuSim(REF_SO, "ref_")
     return _ref
+
+
+# ---------------------------------------------------------------- reference RNG and NoiseSimulator
+
+def mt19937_64_uniforms(seed, count):
+    """cppsim Random (utility.hpp:54-80): mt19937_64 (Matsumoto & Nishimura 2000, 64-bit parameters) and libstdc++'s
+    generate_canonical<double, 53> for a 64-bit engine: x / 2^64, clamped below 1."""
+    n, m = 312, 156
+    mt = [0] * n
+    mt[0] = seed & 0xFFFFFFFFFFFFFFFF
+    for i in range(1, n):
+        mt[i] = (6364136223846793005 * (mt[i - 1] ^ (mt[i - 1] >> 62)) + i) & 0xFFFFFFFFFFFFFFFF
+    idx = n
+    out = []
+    upper, lower = 0xFFFFFFFF80000000, 0x7FFFFFFF
+    for _ in range(count):
+        if idx >= n:
+            for i in range(n):
+                y = (mt[i] & upper) | (mt[(i + 1) % n] & lower)
+                v = mt[(i + m) % n] ^ (y >> 1)
+                if y & 1:
+                    v ^= 0xB5026F5AA96619E9
+                mt[i] = v
+            idx = 0
+        y = mt[idx]
+        idx += 1
+        y ^= (y >> 29) & 0x5555555555555555
+        y ^= (y << 17) & 0x71D67FFFEDA60000
+        y ^= (y << 37) & 0xFFF7EEE000000000
+        y ^= y >> 43
+        r = float(y) / 18446744073709551616.0
+        if r >= 1.0:
+            r = np.nextafter(1.0, 0.0)
+        out.append(r)
+    return np.array(out)
+
+
+def _pauli(ids):
+    """Pauli string matrix, index bit j <-> ids[j] (ids 0..3 = I X Y Z)."""
+    P = [np.eye(2), np.array([[0, 1], [1, 0]]), np.array([[0, -1j], [1j, 0]]), np.diag([1.0, -1.0])]
+    m = np.array([[1.0 + 0j]])
+    for i in ids:
+        m = np.kron(P[i], m)
+    return m
+
+
+def depolarizing_channel(targets, p):
+    """(Kraus operators, cumulative distribution) in the order NoiseSimulator samples them:
+    gate_factory.cpp:451-500 lists ({X, Z, Y, I} with {p/3, p/3, p/3, 1-p}; {I, Pauli(i%4, i//4)
+    for i = 1..15} with {1-p, p/15, ...}) reordered by descending (probability, index)
+    (QuantumGate_Probabilistic::optimize_ProbablisticGate, gate_general.hpp:350-372)."""
+    if len(targets) == 1:
+        ops = [[1], [3], [2], [0]]
+        probs = [p / 3, p / 3, p / 3, 1 - p]
+    else:
+        ops = [[i % 4, i // 4] for i in range(16)]
+        probs = [1 - p] + [p / 15] * 15
+    order = sorted(((probs[i], i) for i in range(len(ops))), reverse=True)
+    kraus = [ops[i] for _, i in order]
+    cum = [0.0]
+    for w, _ in order:
+        cum.append(cum[-1] + w)
+    return kraus, cum
+
+
+def noise_simulator_execute(gates, n, sample_count, seed, sim, apply_gate, init=None, eps=1e-12):
+    """cppsim NoiseSimulator::execute (noisesimulator.cpp:18-198) restated for small n.
+
+    `gates`: list of ("DEPOL", targets, p) channels and other gates that `apply_gate(g, state)` applies.
+    One mt19937_64(seed) stream gives the selection uniforms (sample-major, channels in circuit
+    order; operator = lower_bound(cumulative, u) - 1, noisesimulator.cpp:167-185), then each
+    distinct trajectory's sampling uniforms in the order the trajectories are visited (descending
+    lexicographic order of the choices, noisesimulator.cpp:85-120).  Each trajectory is simulated
+    from the initial state.  Returns (samples, near_boundary flags, [(choices, count), ...])."""
+    import bisect
+    chans = [(j, depolarizing_channel(list(g[1]), g[2])) for j, g in enumerate(gates) if g[0] == "DEPOL"]
+    u = mt19937_64_uniforms(seed, sample_count * len(chans) + sample_count)
+    k = 0
+    sel = []
+    for _ in range(sample_count):
+        row = []
+        for _, (kraus, cum) in chans:
+            pos = bisect.bisect_left(cum, u[k]) - 1
+            row.append(min(max(pos, 0), len(kraus) - 1))
+            k += 1
+        sel.append(tuple(row))
+    sel.sort(reverse=True)
+    requests = []
+    for s in sel:
+        if requests and requests[-1][0] == s:
+            requests[-1][1] += 1
+        else:
+            requests.append([s, 1])
+    samples, near = [], []
+    for choice, count in requests:
+        state = np.zeros(1 << n, dtype=np.complex128)
+        if init is None:
+            state[0] = 1
+        else:
+            state[:] = init
+        ci = 0
+        for g in gates:
+            if g[0] == "DEPOL":
+                kraus, _ = chans[ci][1]
+                ids = kraus[choice[ci]]
+                ci += 1
+                if any(ids):
+                    sim.multi_qubit_dense_matrix_gate(list(g[1]), _pauli(ids), state)
+            else:
+                apply_gate(g, state)
+        s, nb = sim.sampling_with_uniforms(state, u[k:k + count], eps=eps)
+        k += count
+        samples.extend(int(x) for x in s)
+        near.extend(bool(x) for x in nb)
+    return np.array(samples, dtype=np.uint64), np.array(near), [(c, m) for c, m in requests]

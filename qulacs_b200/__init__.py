@@ -7,10 +7,11 @@ does, and raises if it has not been built.
 """
 from . import gate
 from .circuit import QuantumCircuit
+from .noise import NoiseSimulator
 from .observable import Observable, PauliOperator
 from .state import DensityMatrix, QuantumState, QuantumStateC64, inner_product, set_default_stream
 
 __all__ = [
     "gate", "QuantumCircuit", "Observable", "PauliOperator", "QuantumState", "QuantumStateC64",
-    "DensityMatrix", "inner_product", "set_default_stream",
+    "DensityMatrix", "inner_product", "set_default_stream", "NoiseSimulator",
 ]

@@ -91,6 +91,8 @@ SIGNATURES = {
     "qs_circuit_staged_stats": [P, C.POINTER(U), C.POINTER(U), C.POINTER(U), C.POINTER(U)],
     "qs_circuit_update_density_matrix": [P, P, IT, I, P],
     "qs_circuit_fuse": [P, I, C.POINTER(P)],
+    "qs_noise_simulator_trajectories": [P, U, U, C.POINTER(U), P],
+    "qs_noise_simulator_execute": [P, P, IT, U, U, P, P, P],
     "qs_circuit_density_matrix_as_vector": [P, C.POINTER(P)],
     "qs_circuit_gate_matrix": [P, U, P, C.POINTER(U), P],
     "qs_circuit_set_fusion": [P, I],
