@@ -837,12 +837,17 @@ static int batch_ev_impl(void* const* states, const QS_UINT* qubit_counts, QS_UI
 namespace qs {
 
 constexpr int kEvTileBits = kEvTileBitsDecl;
-constexpr int kEvLowFixed = 5;
+constexpr int kEvLowFixed = 4;    // unit vectors of qubits 0..3 in every tile basis (256-byte runs)
 constexpr int kEvMaxTerms = 512;  // terms per pass (shared-memory accumulators)
 
+// A tile is a coset of the span of m basis masks b_j over the index bits, in reduced echelon form:
+// b_j has bit piv_j set and no other basis mask has it.  Tile element u (bit j <-> b_j) of tile T is
+// index rep(T) ^ XOR_{j in u} b_j, rep(T) = T with zeros inserted at the pivots (ascending in
+// `piv_sorted`).  With unit vectors the tile is the usual set of tile qubits.
 struct EvTileArgs {
     int m;
-    UINT q[kEvTileBits];
+    ITYPE b[kEvTileBits];
+    UINT piv_sorted[kEvTileBits];
     int nterms;
 };
 struct EvTileTerm {
@@ -875,21 +880,21 @@ __global__ void __launch_bounds__(128) k_ev_tile(const T* __restrict__ s, ITYPE 
     if (tid < 16) {
         ITYPE o = 0;
         for (int j = 7; j < m; ++j)
-            if ((tid >> (j - 7)) & 1) o |= 1ULL << a.q[j];
+            if ((tid >> (j - 7)) & 1) o ^= a.b[j];
         hi_off[tid] = o;
     }
     ITYPE lo_off = 0;
     for (int j = 0; j < 7 && j < m; ++j)
-        if ((tid >> j) & 1) lo_off |= 1ULL << a.q[j];
+        if ((tid >> j) & 1) lo_off ^= a.b[j];
     for (ITYPE ti = blockIdx.x; ti < tiles; ti += gridDim.x) {
         ITYPE base = ti;
-        for (int j = 0; j < m; ++j) base = insert0(base, a.q[j]);
+        for (int j = 0; j < m; ++j) base = insert0(base, a.piv_sorted[j]);
         __syncthreads();
         {
             double2 v[16];  // all loads in flight before the first shared-memory store
 #pragma unroll
             for (int k = 0; k < 16; ++k)
-                if ((UINT)tid + (UINT)k * 128 < tsize) v[k] = tile_amp<T>(s + (base | lo_off | hi_off[k]));
+                if ((UINT)tid + (UINT)k * 128 < tsize) v[k] = tile_amp<T>(s + (base ^ lo_off ^ hi_off[k]));
 #pragma unroll
             for (int k = 0; k < 16; ++k)
                 if ((UINT)tid + (UINT)k * 128 < tsize) tile[tid + k * 128] = v[k];
@@ -924,60 +929,72 @@ __global__ void k_fold_cols(const double* __restrict__ part, int rows, int cols,
     if (threadIdx.x == 0) out[out_index[c]] = v;
 }
 
-// Host: cover the terms' bit-flip masks with tile sets (qubits 0..4 plus the most frequent remaining
-// flipped qubits), one pass per set.  Returns the number of passes; terms whose flipped qubits
-// outside 0..4 exceed the free tile bits stay in `rest` for the one-pass-per-term kernel.
+// Host: cover the terms' bit-flip masks with tiles spanned by qubits 0..3 and up to m - 4 of the terms'
+// own masks (reduced echelon form, see EvTileArgs): a pass evaluates every term whose mask lies in
+// its span from shared memory.  Terms left when a pass would cover fewer than two stay in `rest`
+// for the one-pass-per-term kernel.
 template <class T>
 int ev_tiled(const PauliTerm* terms, const std::vector<int>& xidx, UINT n, const T* s, ITYPE dim, cudaStream_t st,
     double* values, std::vector<int>* rest) {
     const int m = kEvTileBits;
-    const ITYPE low = (1ULL << kEvLowFixed) - 1;
-    const int free_bits = m - kEvLowFixed;
-    std::vector<int> todo;
-    for (int k : xidx) {
-        if (__builtin_popcountll(terms[k].x & ~low) <= free_bits) todo.push_back(k);
-        else rest->push_back(k);
-    }
+    std::vector<int> todo = xidx;
     const unsigned grid = (unsigned)std::min<ITYPE>(dim >> m, (ITYPE)sm_count() * 4);  // 4 resident per SM
-    constexpr size_t kMinCover = 3;  // below this a shared pass is not cheaper than one pass per term
+    constexpr size_t kMinCover = 2;  // below this a shared pass is not cheaper than one pass per term
     std::vector<double> hvals;
     while (!todo.empty()) {
-        // pick the free tile qubits: most frequent flipped qubits among the remaining terms,
-        // but first make sure the first remaining term fits
-        ITYPE Q = low | (terms[todo[0]].x & ~low);
-        std::vector<int> freq(64, 0);
-        for (int k : todo)
-            for (int b = 0; b < (int)n; ++b)
-                if (((terms[k].x & ~low) >> b) & 1) freq[b]++;
-        while (__builtin_popcountll(Q) < m) {
-            int best = -1;
-            for (int b = 0; b < (int)n; ++b)
-                if (!((Q >> b) & 1) && (best < 0 || freq[b] > freq[best])) best = b;
-            if (best < 0) break;
-            Q |= 1ULL << best;
+        // basis: unit vectors of qubits 0..3, then reduced term masks (greedy in term order)
+        std::vector<ITYPE> basis;
+        std::vector<int> piv;
+        for (int q = 0; q < kEvLowFixed; ++q) {
+            basis.push_back(1ULL << q);
+            piv.push_back(q);
+        }
+        auto reduce = [&](ITYPE x) {
+            for (size_t j = 0; j < basis.size(); ++j)
+                if ((x >> piv[j]) & 1) x ^= basis[j];
+            return x;
+        };
+        for (int k : todo) {
+            if ((int)basis.size() >= m) break;
+            const ITYPE r = reduce(terms[k].x);
+            if (!r) continue;
+            const int p = 63 - __builtin_clzll(r);
+            for (ITYPE& b : basis)  // keep every pivot bit in exactly one basis mask
+                if ((b >> p) & 1) b ^= r;
+            basis.push_back(r);
+            piv.push_back(p);
+        }
+        // pad with unit vectors of the lowest free qubits (a tile always has m basis masks)
+        for (int q = 0; q < (int)n && (int)basis.size() < m; ++q) {
+            if (reduce(1ULL << q) == 0) continue;
+            const ITYPE r = reduce(1ULL << q);
+            const int p = 63 - __builtin_clzll(r);
+            for (ITYPE& b : basis)
+                if ((b >> p) & 1) b ^= r;
+            basis.push_back(r);
+            piv.push_back(p);
         }
         EvTileArgs a{};
-        a.m = 0;
-        int local[64];
-        for (int b = 0; b < (int)n; ++b)
-            if ((Q >> b) & 1) {
-                local[b] = a.m;
-                a.q[a.m++] = b;
-            }
+        a.m = (int)basis.size();
+        for (int jj = 0; jj < a.m; ++jj) {
+            a.b[jj] = basis[jj];
+            a.piv_sorted[jj] = (UINT)piv[jj];
+        }
+        std::sort(a.piv_sorted, a.piv_sorted + a.m);
         std::vector<EvTileTerm> tt;
         std::vector<UINT> outi;
         std::vector<int> left;
         for (int k : todo) {
-            if ((terms[k].x & ~Q) || (int)tt.size() >= kEvMaxTerms) {
+            if (reduce(terms[k].x) != 0 || (int)tt.size() >= kEvMaxTerms) {
                 left.push_back(k);
                 continue;
             }
             EvTileTerm e{};
-            for (int b = 0; b < (int)n; ++b) {
-                if ((terms[k].x >> b) & 1) e.xloc |= 1u << local[b];
-                if (((terms[k].z >> b) & 1) && ((Q >> b) & 1)) e.zloc |= 1u << local[b];
+            for (int jj = 0; jj < a.m; ++jj) {
+                if ((terms[k].x >> piv[jj]) & 1) e.xloc |= 1u << jj;
+                if (__builtin_popcountll(basis[jj] & terms[k].z) & 1) e.zloc |= 1u << jj;
             }
-            e.zglob = terms[k].z & ~Q;  // tile bits of z are handled through zloc
+            e.zglob = terms[k].z;  // parity of rep(T) & z; the tile-element part is zloc
             e.nrot = terms[k].nrot;
             e.pivot = (UINT)(31 - __builtin_clz(e.xloc));
             tt.push_back(e);
@@ -989,7 +1006,7 @@ int ev_tiled(const PauliTerm* terms, const std::vector<int>& xidx, UINT n, const
         }
         a.nterms = (int)tt.size();
         const size_t bt = sizeof(EvTileTerm) * tt.size(), bo = sizeof(UINT) * outi.size(),
-                     bp = sizeof(double) * grid * tt.size(), bv = sizeof(double) * n * 0 + sizeof(double) * 1;
+                     bp = sizeof(double) * grid * tt.size(), bv = sizeof(double) * 1;
         auto up = [](size_t b) { return (b + 255) / 256 * 256; };
         void* buf;
         QS_TRY(scratch(st, up(bt) + up(bo) + up(bp) + up(sizeof(double) * (outi.size() + 1)) + up(bv), &buf));
@@ -1002,7 +1019,7 @@ int ev_tiled(const PauliTerm* terms, const std::vector<int>& xidx, UINT n, const
         for (size_t i = 0; i < seq.size(); ++i) seq[i] = (UINT)i;
         QS_CUDA_CHECK(cudaMemcpyAsync(dt, tt.data(), bt, cudaMemcpyHostToDevice, st));
         QS_CUDA_CHECK(cudaMemcpyAsync(doi, seq.data(), bo, cudaMemcpyHostToDevice, st));
-        k_ev_tile<T><<<grid, 128, 0, st>>>(s, dim >> m, a, dt, dpart);
+        k_ev_tile<T><<<grid, 128, 0, st>>>(s, dim >> a.m, a, dt, dpart);
         QS_TRY(check_launch("k_ev_tile"));
         k_fold_cols<<<(unsigned)tt.size(), 256, 0, st>>>(dpart, (int)grid, (int)tt.size(), dval, doi);
         QS_TRY(check_launch("k_fold_cols"));
