@@ -301,6 +301,45 @@ def batched_throughput(instances: int, budget_gb: float, seed: int = 4004, preci
     return out
 
 
+def noise_sampling(n: int = 20, depth: int = 4, p: float = 1e-3, shots: int = 1000, seed: int = 6006):
+    """NoiseSimulator: HEA circuit with depolarizing noise after every gate (cppsim add_noise_gate rule),
+    `shots` trajectories sampled on the device; the oracle port's time for a few trajectories on the
+    host cores is the CPU comparison (extrapolated to all distinct trajectories)."""
+    import torch
+
+    import qulacs_b200 as Q
+    from qulacs_b200 import workloads as W
+    gates = W.noisy_circuit(W.hea_circuit(n, depth, seed), p)
+    circ = W.to_circuit(gates, n)
+    sim = Q.NoiseSimulator(circ, seed=seed)
+    traj = sim.trajectories(shots)
+    sim.execute(min(shots, 16))  # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    out = sim.execute(shots)
+    torch.cuda.synchronize()
+    gpu_s = time.perf_counter() - t0
+    res = {"workload": f"HEA n={n} depth={depth} + depolarizing p={p} after every gate ({len(gates)} ops), "
+                       f"{shots} shots", "distinct_trajectories": int(traj.size), "gpu_s": gpu_s,
+           "shots_per_s": shots / gpu_s, "checksum": int(out.sum() % (1 << 31))}
+    try:
+        from oracle import oracle as O
+        port = O.port()
+        sample = 1
+        t0 = time.perf_counter()
+        for _ in range(sample):
+            st = np.zeros(1 << n, dtype=np.complex128)
+            st[0] = 1
+            W.run_on_cpu([g for g in gates if g[0] != "DEPOL"], st, port)
+        cpu_per = (time.perf_counter() - t0) / sample
+        res["cpu_port_s_per_trajectory"] = cpu_per
+        res["cpu_port_s_estimate"] = cpu_per * traj.size
+        res["cpu_sample"] = f"{sample} full trajectory (noise-free gates) with the oracle port, 1 core"
+    except Exception as e:  # noqa: BLE001
+        res["cpu_port"] = f"unavailable: {type(e).__name__}: {e}"
+    return res
+
+
 def fp64_per_amplitude(qubits, m) -> int:
     """FP64 instructions per amplitude of a gate in the staged register code: a rotation, or any 1-qubit
     matrix whose entries are each real or imaginary, and a 1-qubit diagonal cost 4; a general 1-qubit
@@ -350,7 +389,7 @@ def main():
     ap.add_argument("--qubits", type=int, default=N_QUBITS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-kernel-table", action="store_true")
-    ap.add_argument("--workload", default="plain", choices=["plain", "fused", "batched", "serving"],
+    ap.add_argument("--workload", default="plain", choices=["plain", "fused", "batched", "serving", "noise"],
                     help="fused / batched / serving: only that comparison (configs 3 / 4 / 5)")
     ap.add_argument("--instances", type=int, default=4096)
     ap.add_argument("--budget-gb", type=float, default=96.0)
@@ -398,6 +437,11 @@ def main():
         r = batched_throughput(args.instances, args.budget_gb)
         if rank == 0:
             print(json.dumps({"metric": "batched uneven circuits: circuits/s", **r}), flush=True)
+        return
+    if args.workload == "noise":
+        r = noise_sampling()
+        if rank == 0:
+            print(json.dumps({"metric": "noisy trajectory sampling: shots/s", **r}), flush=True)
         return
     if args.workload == "serving":
         r = serving_latency(args.requests, args.rate, args.budget_gb, args.workers)
@@ -513,7 +557,8 @@ def main():
         torch.cuda.synchronize()
         for key, fn in (("fused", lambda: fused_comparison(args.fused_qubits, args.fused_layers, stream, False)),
                         ("batched", lambda: batched_throughput(512, 64.0)),
-                        ("serving", lambda: serving_latency(60, 5.0, 96.0, 4))):
+                        ("serving", lambda: serving_latency(60, 5.0, 96.0, 4)),
+                        ("noise", lambda: noise_sampling())):
             try:
                 extras[key] = fn()
             except Exception as e:  # noqa: BLE001

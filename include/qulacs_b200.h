@@ -45,6 +45,10 @@ QS_API int qs_device_synchronize(void);
 QS_API int qs_stream_synchronize(void* stream);
 /* Non-blocking CUDA stream for concurrent work (serving workers); no reference counterpart. */
 QS_API int qs_stream_create(void** stream_out);
+/* Same with the device's highest (high != 0) or lowest scheduling priority: pending CTAs of kernels on
+ * a higher-priority stream are scheduled before those of lower-priority streams (serving: small
+ * requests are not held behind a large one). */
+QS_API int qs_stream_create_with_priority(int high, void** stream_out);
 QS_API int qs_stream_destroy(void* stream);
 
 /* ---- memory and initialisation (src/csim/memory_ops.hpp, src/csim/init_ops.hpp) ---- */
@@ -310,9 +314,11 @@ QS_API int qs_circuit_update_density_matrix(
  * Synchronises `stream`. */
 QS_API int qs_batch_update_quantum_states(const qs_circuit_t* circuits, void* const* states, QS_UINT count,
     void* stream);
-/* <P_k> for the Pauli terms of many complex128 states in one launch.  Terms of state i are
- * term_offsets[i] .. term_offsets[i+1]-1 (masks as qs_expectation_value_pauli_batch); values[k]
- * receives <P_k>.  Synchronises `stream`. */
+/* <P_k> for the Pauli terms of many complex128 states.  Terms of state i are term_offsets[i] ..
+ * term_offsets[i+1]-1 (masks as qs_expectation_value_pauli_batch); values[k] receives <P_k>.  States
+ * of fewer than 18 qubits share one launch (jobs of 16 Z-only strings or one bit-flip string);
+ * larger states are evaluated as qs_expectation_value_pauli_batch does (bit-flip strings from
+ * shared-memory span tiles).  Synchronises `stream`. */
 QS_API int qs_batch_expectation_values(void* const* states, const QS_UINT* qubit_counts, QS_UINT count,
     const QS_UINT* term_offsets, const QS_ITYPE* x_masks, const QS_ITYPE* z_masks, const QS_UINT* y_counts,
     double* values, void* stream);

@@ -26,6 +26,7 @@ SIGNATURES = {
     "qs_device_synchronize": [],
     "qs_stream_synchronize": [P],
     "qs_stream_create": [C.POINTER(P)],
+    "qs_stream_create_with_priority": [I, C.POINTER(P)],
     "qs_stream_destroy": [P],
     "qs_allocate_quantum_state": [IT, C.POINTER(P)],
     "qs_allocate_quantum_state_c64": [IT, C.POINTER(P)],

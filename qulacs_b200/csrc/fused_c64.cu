@@ -20,6 +20,7 @@
 #include <cmath>
 #include <complex>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include <cuda_bf16.h>
@@ -784,6 +785,24 @@ static size_t fused_smem_bytes(int m) {
     return 2 * kAImageBytes + 2 * N * 256 + tsize * 8 + 2 * kTabBytes + 64;  // + 2 mbarriers, TMEM slot, error flag
 }
 
+// The kernel's dynamic shared-memory limit is a process-wide attribute: set it once per device to
+// the largest tile's need (a launch may use less), never per launch, so concurrent host threads
+// launching passes of different tile sizes cannot undo each other's setting.
+static int fused_allow_smem() {
+    static std::mutex mu;
+    static bool done[64] = {};
+    int dev = 0;
+    QS_CUDA_CHECK(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev < 0 || dev >= 64) return set_error(QS_ERR_NOT_SUPPORTED, "device index");
+    if (!done[dev]) {
+        QS_CUDA_CHECK(cudaFuncSetAttribute(k_fused_pass, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            (int)fused_smem_bytes(kFTileMax)));
+        done[dev] = true;
+    }
+    return QS_OK;
+}
+
 // Device plan cached on the circuit (dropped when a gate is added).
 static int fused_plan_dev(Circuit& c, ITYPE dim, std::shared_ptr<FusedPlanDev>* out) {
     if (c.fused && c.fused_dim == dim) {
@@ -830,11 +849,11 @@ int run_fused_c64(Circuit& c, void* state, ITYPE dim, cudaStream_t st) {
     if (c.n < 10) return set_error(QS_ERR_NOT_SUPPORTED, "fused path needs at least 10 qubits");
     std::shared_ptr<FusedPlanDev> D;
     QS_TRY(fused_plan_dev(c, dim, &D));
+    QS_TRY(fused_allow_smem());
     for (const FusedPassArgs& p0 : D->passes) {
         FusedPassArgs p = p0;
         p.state = (float2*)state;
         const size_t smem = fused_smem_bytes(p.m);
-        QS_CUDA_CHECK(cudaFuncSetAttribute(k_fused_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         const unsigned grid = (unsigned)std::min<ITYPE>(p.tiles, (ITYPE)sm_count());
         k_fused_pass<<<grid, kFThreads, smem, st>>>(p);
         QS_TRY(check_launch("k_fused_pass"));

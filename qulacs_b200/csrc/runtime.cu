@@ -167,8 +167,31 @@ QS_API int qs_stream_create(void** stream_out) {
     *stream_out = (void*)s;
     return QS_OK;
 }
+QS_API int qs_stream_create_with_priority(int high, void** stream_out) {
+    if (!stream_out) return set_error(QS_ERR_INVALID_ARGUMENT, "null output pointer");
+    int least = 0, greatest = 0;
+    QS_CUDA_CHECK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    cudaStream_t s = nullptr;
+    QS_CUDA_CHECK(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, high ? greatest : least));
+    *stream_out = (void*)s;
+    return QS_OK;
+}
 QS_API int qs_stream_destroy(void* stream) {
-    if (stream) QS_CUDA_CHECK(cudaStreamDestroy((cudaStream_t)stream));
+    if (!stream) return QS_OK;
+    QS_CUDA_CHECK(cudaStreamSynchronize((cudaStream_t)stream));
+    {
+        // this stream's scratch buffers (any device) go with it
+        std::lock_guard<std::mutex> lk(g_scratch_mu);
+        for (auto it = g_scratch.begin(); it != g_scratch.end();) {
+            if (it->first.second == (cudaStream_t)stream) {
+                if (it->second.ptr) cudaFree(it->second.ptr);
+                it = g_scratch.erase(it);
+            } else {
+                ++it;
+            }
+        }
+    }
+    QS_CUDA_CHECK(cudaStreamDestroy((cudaStream_t)stream));
     return QS_OK;
 }
 

@@ -744,6 +744,8 @@ extern "C" QS_API int qs_batch_expectation_values_c64(void* const* states, const
         (cudaStream_t)stream);
 }
 namespace qs {
+constexpr UINT kBatchEvSingleQubits = 18;  // states at least this large are evaluated on their own
+
 static int batch_ev_impl(void* const* states, const QS_UINT* qubit_counts, QS_UINT count, const QS_UINT* term_offsets,
     const QS_ITYPE* x_masks, const QS_ITYPE* z_masks, const QS_UINT* y_counts, double* values, int c64,
     cudaStream_t st) {
@@ -757,6 +759,26 @@ static int batch_ev_impl(void* const* states, const QS_UINT* qubit_counts, QS_UI
         const UINT n = qubit_counts[i];
         if (n < 1 || n > 40) return set_error(QS_ERR_INVALID_ARGUMENT, "batch expectation: bad qubit count");
         const ITYPE dim = 1ULL << n;
+        if (n >= kBatchEvSingleQubits) {
+            // a large state: its own passes (Z-only strings 16 per pass, bit-flip strings from
+            // span tiles) cost far fewer state reads than one job per bit-flip string
+            const UINT k0 = term_offsets[i], nk = term_offsets[i + 1] - k0;
+            std::vector<PauliTerm> pt(nk);
+            for (UINT j = 0; j < nk; ++j) {
+                const UINT k = k0 + j;
+                if ((x_masks[k] | z_masks[k]) >> n)
+                    return set_error(QS_ERR_INVALID_ARGUMENT, "batch expectation: mask beyond qubit count");
+                pt[j].x = x_masks[k];
+                pt[j].z = z_masks[k];
+                pt[j].nrot = y_counts[k];
+                pt[j].pivot = x_masks[k] ? (UINT)(63 - __builtin_clzll(x_masks[k])) : 0u;
+            }
+            if (nk) {
+                if (c64) QS_TRY(ev_batch<float2>(pt.data(), nk, (const float2*)states[i], dim, st, values + k0));
+                else QS_TRY(ev_batch<double2>(pt.data(), nk, (const double2*)states[i], dim, st, values + k0));
+            }
+            continue;
+        }
         std::vector<UINT> zlist;
         for (UINT k = term_offsets[i]; k < term_offsets[i + 1]; ++k) {
             if ((x_masks[k] | z_masks[k]) >> n)
@@ -820,8 +842,13 @@ static int batch_ev_impl(void* const* states, const QS_UINT* qubit_counts, QS_UI
     QS_TRY(check_launch("k_batch_ev"));
     k_batch_ev_fold<<<(unsigned)jobs.size(), 256, 0, st>>>(dj, dpart, dzo, dval);
     QS_TRY(check_launch("k_batch_ev_fold"));
-    QS_CUDA_CHECK(cudaMemcpyAsync(values, dval, bv, cudaMemcpyDeviceToHost, st));
+    // only the entries of the states evaluated here (large states' values are already in `values`)
+    std::vector<double> hv(nterms);
+    QS_CUDA_CHECK(cudaMemcpyAsync(hv.data(), dval, bv, cudaMemcpyDeviceToHost, st));
     QS_CUDA_CHECK(cudaStreamSynchronize(st));
+    for (UINT i = 0; i < count; ++i)
+        if (qubit_counts[i] < kBatchEvSingleQubits)
+            for (UINT k = term_offsets[i]; k < term_offsets[i + 1]; ++k) values[k] = hv[k];
     return QS_OK;
 }
 }  // namespace qs

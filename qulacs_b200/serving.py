@@ -33,6 +33,8 @@ from ._lib import EXEC_STAGED_FUSED, call
 # FP64 fusion block size for every served circuit: fixed (not autotuned per request) so that a
 # request's result does not depend on timing noise, and equal to the batch executor's.
 SERVE_FUSION_K = 2
+# requests whose device footprint is at most this run on high-priority streams (24-qubit complex128)
+SMALL_REQUEST_BYTES = 16 << 24
 from .observable import masks
 
 ALIGN = 256
@@ -240,9 +242,11 @@ class ServingLoop:
         r.result = e
 
     def _worker(self, t0):
-        s = C.c_void_p()
-        call("qs_stream_create", C.byref(s))
-        stream = s.value
+        # two streams: requests whose state is small run on the high-priority one, so their kernels'
+        # CTAs are scheduled ahead of a large request's remaining CTAs
+        hi, lo = C.c_void_p(), C.c_void_p()
+        call("qs_stream_create_with_priority", 1, C.byref(hi))
+        call("qs_stream_create_with_priority", 0, C.byref(lo))
         try:
             while True:
                 with self.cv:
@@ -257,6 +261,7 @@ class ServingLoop:
                         batch = [head]
                     for r in batch:
                         self.ready.remove(r)
+                stream = hi.value if max(r.fp for r in batch) <= SMALL_REQUEST_BYTES else lo.value
                 try:
                     if batch[0].kind == "expectation":
                         self._run_expectation_batch(batch, stream)
@@ -278,7 +283,8 @@ class ServingLoop:
                         self.outstanding -= 1
                     self.cv.notify_all()
         finally:
-            _lib.load().qs_stream_destroy(stream)
+            _lib.load().qs_stream_destroy(hi.value)
+            _lib.load().qs_stream_destroy(lo.value)
 
     def run(self, requests):
         """Serve `requests` (their `arrival` offsets are honoured in wall-clock time); returns stats."""

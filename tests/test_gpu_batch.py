@@ -70,3 +70,22 @@ def test_batch_fused_c64(port):
         W.run_on_cpu(gates, psi, port)
         want = sum(c * port.expectation_value(tl, ids, psi) for c, tl, ids in terms)
         assert abs(e - want) <= 1e-4
+
+
+@pytest.mark.parametrize("precision", ["c128", "c64"])
+def test_batch_mixed_sizes_across_the_single_state_threshold(port, precision):
+    """States of 12 and 19-20 qubits in one batch: the large ones take the single-state span-tile
+    evaluation, the small ones the shared job launch; every energy matches its state alone."""
+    jobs, specs = [], []
+    for i, n in enumerate([12, 19, 13, 20, 12]):
+        gates = W.hea_circuit(n, 3, seed=7700 + i)
+        terms = W.random_pauli_terms(n, 60, 1, 5, seed=7800 + i)
+        jobs.append((W.to_circuit(gates, n), W.to_observable(terms, n)))
+        specs.append((n, gates, terms))
+    got = BatchRunner(memory_budget_bytes=1 << 34, precision=precision).run(jobs)
+    for (circ, obs), (n, gates, terms), e in zip(jobs, specs, got):
+        psi = np.zeros(1 << n, dtype=np.complex128)
+        psi[0] = 1
+        W.run_on_cpu(gates, psi, port)
+        want = sum(c * port.expectation_value(tl, ids, psi) for c, tl, ids in terms)
+        assert abs(e - want) <= (EV_TOL if precision == "c128" else 1e-5), (n, e, want)
