@@ -340,6 +340,42 @@ def noise_sampling(n: int = 20, depth: int = 4, p: float = 1e-3, shots: int = 10
     return res
 
 
+def timed_region(step, steps: int, warmup: int, dist=None, sync=None, make_timer=None, device: str = "cpu") -> float:
+    """The timing contract: `warmup` untimed steps, then a barrier with a device synchronize on both
+    sides, exactly `steps` timed steps, a synchronize, and the per-step time in ms as the MAX over
+    ranks (`dist` = torch.distributed or None).  `make_timer()` returns (start, stop) where stop()
+    returns elapsed ms (CUDA events on the launching stream in the bench; a host clock in CPU tests)."""
+    import torch
+    sync = sync or (lambda: None)
+    if make_timer is None:
+        def make_timer():
+            t = [0.0]
+
+            def start():
+                t[0] = time.perf_counter()
+
+            def stop():
+                return (time.perf_counter() - t[0]) * 1e3
+            return start, stop
+    for _ in range(warmup):
+        step()
+    sync()
+    if dist:
+        dist.barrier()
+    sync()
+    start, stop = make_timer()
+    start()
+    for _ in range(steps):
+        step()
+    sync()
+    ms = stop() / steps
+    if dist:
+        t = torch.tensor([ms], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms
+
+
 def fp64_per_amplitude(qubits, m) -> int:
     """FP64 instructions per amplitude of a gate in the staged register code: a rotation, or any 1-qubit
     matrix whose entries are each real or imaginary, and a 1-qubit diagonal cost 4; a general 1-qubit
@@ -461,26 +497,24 @@ def main():
         state.set_zero_state()
         circ.update_quantum_state(state, mode=mode)
 
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    l0 = lib.qs_launch_count()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launch0 = [0]
+
+    def cuda_timer():
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+        def start():
+            launch0[0] = lib.qs_launch_count()
+            ev0.record(stream)
+
+        def stop():
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            return ev0.elapsed_time(ev1)
+        return start, stop
+
     with ClockSampler(local) as clk:
-        ev0.record(stream)
-        for _ in range(args.steps):
-            step()
-        ev1.record(stream)
-        torch.cuda.synchronize()
-    launches = lib.qs_launch_count() - l0
-    ms = ev0.elapsed_time(ev1) / args.steps
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = timed_region(step, args.steps, args.warmup, dist, torch.cuda.synchronize, cuda_timer, "cuda")
+    launches = lib.qs_launch_count() - launch0[0]
     gb_per_step = len(gates) * bytes_per_gate(n) / 1e9
     value = world * gb_per_step / (ms / 1e3)
 
