@@ -378,10 +378,11 @@ QS_API int qs_circuit_fused_block_export(qs_circuit_t circuit, QS_UINT index, QS
  * row_source[7]  source of accumulator (A) row bit i: block-local bit 0..5, or 6 = real/imaginary part;
  * k_source[6]    block-local bit at K bit 1 + i of both operands (K bit 0 = real/imaginary part);
  * coset_bits[m-6] tile bit at bit i of the coset (MMA N) index;
- * tables[448]    rowtab[128] | coltab[128] | gn[128] | gj[64] as the kernel reads them (may be NULL):
- *                accumulator element (y, n) goes to byte rowtab[y] ^ coltab[n] of the next block's
- *                B operand (float rowtab[y] ^ coltab[n] of the swizzled output tile after the last
- *                block); the first block's B[n][2j + part] is swizzled tile float2 gn[n] ^ gj[j]. */
+ * tables[640]    32-bit words rowtab[128] | coltab[128] | gn[128] (64-bit) | gj[64] (64-bit) as the
+ *                kernel reads them (may be NULL): accumulator element (y, n) goes to byte
+ *                rowtab[y] ^ coltab[n] of the next block's B operand (float rowtab[y] ^ coltab[n] of
+ *                the swizzled output tile after the last block); the first block's B[n][2j + part] is
+ *                complex64 amplitude tile_base | gn[n] | gj[j] of the state. */
 QS_API int qs_circuit_fused_block_layout(qs_circuit_t circuit, QS_UINT index, int* row_source, int* k_source,
     QS_UINT* coset_bits, unsigned int* tables);
 

@@ -38,8 +38,8 @@ constexpr int kFTidBits = 9;      // log2(kFThreads)
 constexpr int kARows = 128, kAK = 128;           // real-ified block matrix
 constexpr int kAImageBytes = kARows * kAK * 2;   // one bf16 image (hi or lo): 32 KiB
 constexpr long long kWaitLimit = 4000000000LL;   // ~2 s of clock64 at 2 GHz
-// Per-block index tables (u32 words): rowtab[128] | coltab[128] | gn[128] | gj[64]
-constexpr int kTabRow = 0, kTabCol = 128, kTabGn = 256, kTabGj = 384, kTabWords = 448;
+// Per-block index tables (u32 words): rowtab[128] | coltab[128] | gn[128] (u64) | gj[64] (u64)
+constexpr int kTabRow = 0, kTabCol = 128, kTabGn = 256, kTabGj = 512, kTabWords = 640;
 constexpr int kTabBytes = kTabWords * 4;
 constexpr int kRecordBytes = 2 * kAImageBytes + kTabBytes;  // one block record in global memory
 
@@ -158,30 +158,30 @@ __device__ __forceinline__ void bulk_load_block(uint32_t dst_a, uint32_t dst_t, 
                  : "memory");
 }
 
-// Per tile: the input tile (prefetched one tile ahead with cp.async into `stage`) is gathered into
-// the B operand of block 0; after every block, the FP32 accumulator goes straight from TMEM into the
-// next block's B operand (split into bf16 hi/lo), so the state does not return to a complex64 tile
-// between blocks and `stage` is free for the next tile's load; after the last block the accumulator
-// is written as a complex64 tile over the B region and stored with coalesced 16-byte stores.
-// Every data movement is a table XOR: element (row y, column n) of block b's accumulator goes to
-// byte rowtab[y] ^ coltab[n] of the next B operand (float rowtab[y] ^ coltab[n] of the output tile
-// after the last block); B_0[n][2j + part] comes from stage[gn[n] ^ gj[j]].
+// Two tiles in flight.  A CTA takes its tiles in pairs (X, Y) that go through the pass's blocks in
+// lockstep and share each block's A operand: X's and Y's MMAs are issued back to back into two TMEM
+// accumulators, X's accumulator moves run while Y's MMAs do, and the next block's A image (bulk copy)
+// lands while Y's accumulator moves run.  A tile is gathered straight from HBM into its B operand
+// (bf16 hi / lo) through 64-bit offset tables; after the last block its accumulator becomes a
+// complex64 tile over its own B region, stored with 16-byte streaming stores.
+// Every in-tile data movement is a table XOR: element (row y, column n) of a block's accumulator goes
+// to byte rowtab[y] ^ coltab[n] of the next B operand (float rowtab[y] ^ coltab[n] of the output
+// tile after the last block).
 __global__ void __launch_bounds__(kFThreads, 1) k_fused_pass(const __grid_constant__ FusedPassArgs a) {
     extern __shared__ __align__(1024) unsigned char smem[];
     const int m = a.m;
     const uint32_t tsize = 1u << m;
     const uint32_t N = tsize >> kFBlock;  // cosets per block = MMA N
-    unsigned char* sA = smem;                                  // A hi | A lo   (64 KiB)
-    unsigned char* sB = sA + 2 * kAImageBytes;                 // B hi | B lo   (2 x N x 256 B)
     const uint32_t bimg = N * 256u;
-    float* outt = (float*)sB;                                  // output tile over B after the last block
-    float2* stage = (float2*)(sB + 2 * bimg);                  // input tile (tsize x 8 B)
-    uint32_t* tabs = (uint32_t*)(stage + tsize);               // [2][kTabWords]
-    uint64_t* mbar = (uint64_t*)(tabs + 2 * kTabWords);        // [0] MMA completion, [1] block record landed
-    uint32_t* tmem_slot = (uint32_t*)(mbar + 2);
+    unsigned char* sA = smem;                                  // A hi | A lo   (64 KiB)
+    unsigned char* sB0 = sA + 2 * kAImageBytes;                // tile X: B hi | B lo, then its output tile
+    unsigned char* sB1 = sB0 + 2 * bimg;                       // tile Y
+    uint32_t* tabs = (uint32_t*)(sB1 + 2 * bimg);              // [2][kTabWords]
+    uint64_t* mbar = (uint64_t*)(tabs + 2 * kTabWords);        // [0] MMA X, [1] MMA Y, [2] block record
+    uint32_t* tmem_slot = (uint32_t*)(mbar + 3);
     int* s_err = (int*)(tmem_slot + 1);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const uint32_t ncols = N < 32 ? 32u : N;
+    const uint32_t ncols = 2 * N < 32 ? 32u : 2 * N;  // D_X at column 0, D_Y at column N
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
@@ -189,8 +189,7 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused_pass(const __grid_consta
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar)));
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar + 1)));
+        for (int i = 0; i < 3; ++i) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar + i)));
         asm volatile("fence.mbarrier_init.release.cluster;");
         *s_err = 0;
     }
@@ -198,14 +197,13 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused_pass(const __grid_consta
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = *tmem_slot;
-    const uint32_t mb = smem_u32(mbar), mba = smem_u32(mbar + 1);
-    uint32_t phase = 0, phase_a = 0;
-    bool a_pending = false;  // a block record copy is in flight on mba (same value in every thread)
+    const uint32_t mb0 = smem_u32(mbar), mb1 = smem_u32(mbar + 1), mba = smem_u32(mbar + 2);
+    uint32_t ph0 = 0, ph1 = 0, pha = 0;
+    bool a_pending = false;  // a block record copy is in flight on mba (same in every thread)
     const uint32_t idesc = idesc_bf16(kARows, (int)N);
-    const uint32_t aaddr = smem_u32(sA), baddr = smem_u32(sB), taddr = smem_u32(tabs);
+    const uint32_t aaddr = smem_u32(sA), taddr = smem_u32(tabs);
 
-    // Tile loads/stores move amplitude pairs (tile bit 0 = qubit 0), 16 B each: pair p = tid + 512 k
-    // holds tile bits 1..9 from tid and bits 10.. from k.
+    // output stores move amplitude pairs (tile bit 0 = qubit 0), 16 B each: pair p = tid + 512 k
     ITYPE lo_off = 0;
     for (int j = 1; j <= kFTidBits && j < m; ++j)
         if ((tid >> (j - 1)) & 1) lo_off |= 1ULL << a.q[j];
@@ -221,18 +219,9 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused_pass(const __grid_consta
             if ((k >> (j - kFTidBits - 1)) & 1) off |= 1ULL << a.q[j];
         return off;
     };
-    auto load_tile = [&](ITYPE T) {
-        const ITYPE base = tile_base(T);
-#pragma unroll 4
-        for (uint32_t k = 0; k * kFThreads < npairs; ++k) {
-            const uint32_t pidx = tid + k * kFThreads;
-            if (pidx < npairs) cp_async16(stage + tswz(2 * pidx), a.state + (base | pair_off(k)));
-        }
-        cp_async_commit();
-    };
     auto record = [&](int b) { return a.records + (size_t)b * kRecordBytes; };
 
-    // warp w reads TMEM lanes 32 (w % 4) .. +31 (rows y) and column part w / 4
+    // accumulator reads: warp w reads TMEM lanes 32 (w % 4) .. +31 (rows y) and column part w / 4
     const uint32_t y = 32u * (warp & 3) + lane;
     const uint32_t parts = N >= 64 ? 4u : N / 16;
     const uint32_t cw = N / parts;
@@ -242,117 +231,87 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused_pass(const __grid_consta
     const uint32_t g_n0 = tid & 7u, g_j = (uint32_t)tid >> 3;
     const uint32_t g_off = kmajor_off(g_n0, 2 * g_j);
 
-    int slot = 0, loads = 0;  // table slot of the current block; records issued so far
-    if ((ITYPE)blockIdx.x < a.tiles) {
-        load_tile(blockIdx.x);
-        if (tid == 0) bulk_load_block(aaddr, taddr, record(0), mba);
-        a_pending = true;
-        loads = 1;
-    }
-    for (ITYPE T = blockIdx.x; T < a.tiles; T += gridDim.x) {
+    // tiles -> B operands straight from HBM: 64-bit offsets of coset n (gn) and block index j (gj);
+    // both tiles' loads are in flight together
+    auto gather = [&](ITYPE TX, ITYPE TY, bool hasY, int slot) {
+        const uint64_t* gn = (const uint64_t*)(tabs + slot * kTabWords + kTabGn);
+        const ITYPE gj = ((const uint64_t*)(tabs + slot * kTabWords + kTabGj))[g_j];
+        const ITYPE bx = tile_base(TX) | gj, by = hasY ? (tile_base(TY) | gj) : bx;
+        float2 vx[16], vy[16];
+#pragma unroll
+        for (uint32_t i = 0; i < 16; ++i)
+            if (g_n0 + 8 * i < N) {
+                const ITYPE o = gn[g_n0 + 8 * i];
+                vx[i] = __ldcs(a.state + (bx | o));
+                if (hasY) vy[i] = __ldcs(a.state + (by | o));
+            }
+        auto put = [&](unsigned char* sB, const float2 (&v)[16]) {
+#pragma unroll
+            for (uint32_t i = 0; i < 16; ++i)
+                if (g_n0 + 8 * i < N) {
+                    uint32_t hi, lo;
+                    split2_bf16(v[i].x, v[i].y, &hi, &lo);
+                    *(uint32_t*)(sB + g_off + i * 2048) = hi;
+                    *(uint32_t*)(sB + bimg + g_off + i * 2048) = lo;
+                }
+        };
+        put(sB0, vx);
+        if (hasY) put(sB1, vy);
+    };
+    auto issue_mma = [&](unsigned char* sB, uint32_t dcol, uint32_t mbar_addr) {
+        const uint32_t baddr = smem_u32(sB);
+        // shared addresses are below 256 KiB, so the 14-bit start-address field never wraps: the
+        // descriptor of K-step s is the K-step-0 descriptor plus 256 B >> 4 = 16 per step
+        const uint64_t ahi0 = umma_desc(aaddr, 128, 2048), alo0 = umma_desc(aaddr + kAImageBytes, 128, 2048);
+        const uint64_t bhi0 = umma_desc(baddr, 128, 2048), blo0 = umma_desc(baddr + bimg, 128, 2048);
+#pragma unroll
+        for (int s = 0; s < kAK / 16; ++s) {
+            const uint64_t ds = 16u * (uint64_t)s;
+            mma_bf16(tmem + dcol, ahi0 + ds, bhi0 + ds, idesc, s > 0 ? 1u : 0u);
+            mma_bf16(tmem + dcol, ahi0 + ds, blo0 + ds, idesc, 1u);
+            mma_bf16(tmem + dcol, alo0 + ds, bhi0 + ds, idesc, 1u);
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar_addr)
+                     : "memory");
+    };
+    // accumulator (TMEM columns dcol..) -> next B operand in sB, or -> complex64 output tile over sB
+    auto move = [&](unsigned char* sB, uint32_t dcol, int slot, bool last) {
+        const uint32_t* rt = tabs + slot * kTabWords + kTabRow;
+        const uint32_t* ct = tabs + slot * kTabWords + kTabCol;
+        const uint32_t ybase = rt[y];
+        float* outt = (float*)sB;
+        for (uint32_t cc = c_begin; cc < c_end; cc += 16) {
+            float v[16];
+            tmem_ld16(tmem + ((32u * (warp & 3)) << 16) + dcol + cc, v);
+            uint32_t o[16];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const uint4 t4 = *(const uint4*)(ct + cc + 4 * q);
+                o[4 * q] = t4.x ^ ybase;
+                o[4 * q + 1] = t4.y ^ ybase;
+                o[4 * q + 2] = t4.z ^ ybase;
+                o[4 * q + 3] = t4.w ^ ybase;
+            }
+            if (last) {
+#pragma unroll
+                for (int i = 0; i < 16; ++i) outt[o[i]] = v[i];
+            } else {
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    uint32_t hl;
+                    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(hl) : "f"(0.f), "f"(v[i]));
+                    const float hf = __uint_as_float(hl << 16);
+                    uint32_t ll;
+                    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(ll) : "f"(0.f), "f"(v[i] - hf));
+                    *(uint16_t*)(sB + o[i]) = (uint16_t)hl;
+                    *(uint16_t*)(sB + bimg + o[i]) = (uint16_t)ll;
+                }
+            }
+        }
+    };
+    auto store_out = [&](ITYPE T, const unsigned char* sB) {
         const ITYPE base = tile_base(T);
-        const bool has_next = T + gridDim.x < a.tiles;
-        cp_async_wait_group<0>();  // stage holds tile T
-        if (a_pending) {  // block 0's record (gather tables)
-            if (!mbar_wait(mba, phase_a)) *s_err = 1;
-            phase_a ^= 1u;
-            a_pending = false;
-        }
-        __syncthreads();
-        if (*s_err) break;
-        {
-            const uint32_t* gn = tabs + slot * kTabWords + kTabGn;
-            const uint32_t sj = tabs[slot * kTabWords + kTabGj + g_j];
-#pragma unroll 4
-            for (uint32_t i = 0; g_n0 + 8 * i < N; ++i) {
-                const float2 v = stage[gn[g_n0 + 8 * i] ^ sj];
-                uint32_t hi, lo;
-                split2_bf16(v.x, v.y, &hi, &lo);
-                *(uint32_t*)(sB + g_off + i * 2048) = hi;
-                *(uint32_t*)(sB + bimg + g_off + i * 2048) = lo;
-            }
-        }
-        __syncthreads();  // every thread is done with stage
-        if (has_next) load_tile(T + gridDim.x);
-        for (int b = 0; b < a.nblocks; ++b) {
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            asm volatile("tcgen05.fence::before_thread_sync;");
-            __syncthreads();
-            if (a_pending) {
-                if (!mbar_wait(mba, phase_a)) *s_err = 1;
-                phase_a ^= 1u;
-                a_pending = false;
-            }
-            if (tid == 0 && !*s_err) {
-                asm volatile("tcgen05.fence::after_thread_sync;");
-                // K-step s covers K = 16 s .. 16 s + 15: two 16-byte core-matrix columns, LBO = 128 B,
-                // SBO = 2048 B (16 core matrices of one 8-row group along K)
-#pragma unroll 1
-                for (int s = 0; s < kAK / 16; ++s) {
-                    const uint64_t ahi = umma_desc(aaddr + s * 256, 128, 2048);
-                    const uint64_t alo = umma_desc(aaddr + kAImageBytes + s * 256, 128, 2048);
-                    const uint64_t bhi = umma_desc(baddr + s * 256, 128, 2048);
-                    const uint64_t blo = umma_desc(baddr + bimg + s * 256, 128, 2048);
-                    mma_bf16(tmem, ahi, bhi, idesc, s > 0 ? 1u : 0u);
-                    mma_bf16(tmem, ahi, blo, idesc, 1u);
-                    mma_bf16(tmem, alo, bhi, idesc, 1u);
-                }
-                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mb)
-                             : "memory");
-            }
-            const bool ok = mbar_wait(mb, phase);
-            phase ^= 1u;
-            if (!ok) *s_err = 1;
-            asm volatile("tcgen05.fence::after_thread_sync;");
-            __syncthreads();
-            if (*s_err) break;
-            // A and the other table slot are free: start the next record (the next tile's first block
-            // after the last one; a single-block pass keeps its record resident)
-            const int nxt = b + 1 < a.nblocks ? b + 1 : (has_next ? 0 : -1);
-            const int nslot = loads & 1;
-            if (nxt >= 0 && nxt != b) {
-                if (tid == 0) bulk_load_block(aaddr, taddr + nslot * kTabBytes, record(nxt), mba);
-                a_pending = true;
-                ++loads;
-            }
-            // accumulator -> next B operand (2-byte hi / lo stores), or -> output tile after the last block
-            const uint32_t* rt = tabs + slot * kTabWords + kTabRow;
-            const uint32_t* ct = tabs + slot * kTabWords + kTabCol;
-            const uint32_t ybase = rt[y];
-            const bool last = b + 1 == a.nblocks;
-            for (uint32_t cc = c_begin; cc < c_end; cc += 16) {
-                float v[16];
-                tmem_ld16(tmem + ((32u * (warp & 3)) << 16) + cc, v);
-                uint32_t o[16];
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const uint4 t4 = *(const uint4*)(ct + cc + 4 * q);
-                    o[4 * q] = t4.x ^ ybase;
-                    o[4 * q + 1] = t4.y ^ ybase;
-                    o[4 * q + 2] = t4.z ^ ybase;
-                    o[4 * q + 3] = t4.w ^ ybase;
-                }
-                if (last) {
-#pragma unroll
-                    for (int i = 0; i < 16; ++i) outt[o[i]] = v[i];
-                } else {
-#pragma unroll
-                    for (int i = 0; i < 16; ++i) {
-                        uint32_t hl;
-                        asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(hl) : "f"(0.f), "f"(v[i]));
-                        const float hf = __uint_as_float(hl << 16);
-                        uint32_t ll;
-                        asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(ll) : "f"(0.f), "f"(v[i] - hf));
-                        *(uint16_t*)(sB + o[i]) = (uint16_t)hl;
-                        *(uint16_t*)(sB + bimg + o[i]) = (uint16_t)ll;
-                    }
-                }
-            }
-            if (nxt >= 0 && nxt != b) slot = nslot;
-        }
-        if (*s_err) break;
-        asm volatile("tcgen05.fence::before_thread_sync;");
-        __syncthreads();
+        const float* outt = (const float*)sB;
         for (uint32_t k = 0; k * kFThreads < npairs; ++k) {
             const uint32_t pidx = tid + k * kFThreads;
             if (pidx < npairs) {
@@ -360,9 +319,71 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused_pass(const __grid_consta
                 __stcs((float4*)(a.state + (base | pair_off(k))), v);
             }
         }
+    };
+    auto wait_record = [&]() {
+        if (a_pending) {
+            if (!mbar_wait(mba, pha)) *s_err = 1;
+            pha ^= 1u;
+            a_pending = false;
+        }
+    };
+
+    int slot = 0, loads = 0;  // table slot of the current block's record; records issued so far
+    if ((ITYPE)blockIdx.x < a.tiles) {
+        if (tid == 0) bulk_load_block(aaddr, taddr, record(0), mba);
+        a_pending = true;
+        loads = 1;
     }
-    cp_async_wait_group<0>();  // no copy in flight at exit
-    if (a_pending && !mbar_wait(mba, phase_a)) *s_err = 1;
+    const ITYPE stride = 2 * (ITYPE)gridDim.x;
+    for (ITYPE TX = blockIdx.x; TX < a.tiles; TX += stride) {
+        const ITYPE TY = TX + gridDim.x;
+        const bool hasY = TY < a.tiles;
+        const bool has_next = TX + stride < a.tiles;
+        wait_record();  // block 0's record: its gather tables
+        __syncthreads();
+        if (*s_err) break;
+        gather(TX, TY, hasY, slot);
+        for (int b = 0; b < a.nblocks; ++b) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            asm volatile("tcgen05.fence::before_thread_sync;");
+            __syncthreads();
+            wait_record();  // this block's A image and tables
+            if (tid == 0 && !*s_err) {
+                asm volatile("tcgen05.fence::after_thread_sync;");
+                issue_mma(sB0, 0, mb0);
+                if (hasY) issue_mma(sB1, N, mb1);
+            }
+            const bool last = b + 1 == a.nblocks;
+            if (!mbar_wait(mb0, ph0)) *s_err = 1;
+            ph0 ^= 1u;
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            move(sB0, 0, slot, last);  // while Y's MMAs run
+            if (hasY) {
+                if (!mbar_wait(mb1, ph1)) *s_err = 1;
+                ph1 ^= 1u;
+                asm volatile("tcgen05.fence::after_thread_sync;");
+            }
+            __syncthreads();  // both MMAs done: A and the other table slot are free
+            if (*s_err) break;
+            const int nxt = b + 1 < a.nblocks ? b + 1 : (has_next ? 0 : -1);
+            const int nslot = loads & 1;
+            const bool reload = nxt >= 0 && nxt != b;  // a single-block pass keeps its record resident
+            if (reload) {
+                if (tid == 0) bulk_load_block(aaddr, taddr + nslot * kTabBytes, record(nxt), mba);
+                a_pending = true;
+                ++loads;
+            }
+            if (hasY) move(sB1, N, slot, last);  // while the next record lands
+            if (reload) slot = nslot;
+        }
+        if (*s_err) break;
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        __syncthreads();
+        store_out(TX, sB0);
+        if (hasY) store_out(TY, sB1);
+        __syncthreads();  // the next pair's gather overwrites the output tiles
+    }
+    if (a_pending && !mbar_wait(mba, pha)) *s_err = 1;  // no copy in flight at exit
     if (tid == 0 && *s_err) atomicExch(a.err, 1);
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
@@ -564,8 +585,8 @@ static void choose_layouts(FusedPass& fp) {
     const int m = (int)fp.q.size();
     std::vector<int> locals(kFBlock);
     for (int j = 0; j < kFBlock; ++j) locals[j] = j;
-    // block 0's gather: lanes 0..2 = coset index bits 0..2, lanes 3..4 = K pair bits 0..1; 8-byte loads
-    // of the swizzled tile, two half-warp wavefronts at best
+    // block 0's gather straight from HBM: lanes 0..2 = coset index bits 0..2, lanes 3..4 = K pair bits
+    // 0..1; pick them so a warp's 32 eight-byte loads touch the fewest 32-byte sectors (8 at best)
     {
         FusedBlock& b0 = fp.blocks[0];
         const std::vector<int> cos = coset_bits_of(b0, m);
@@ -578,18 +599,15 @@ static void choose_layouts(FusedPass& fp) {
                     for (int k0 = 0; k0 < kFBlock; ++k0)
                         for (int k1 = k0 + 1; k1 < kFBlock; ++k1) {
                             const int lb[5] = {cos[c0], cos[c1], cos[c2], b0.bits[k0], b0.bits[k1]};
-                            int cost = 0;
-                            for (int h = 0; h < 2; ++h) {
-                                uint32_t words[32];
-                                for (int l = 0; l < 16; ++l) {
-                                    const int lane = 16 * h + l;
-                                    uint32_t u = 0;
-                                    for (int i = 0; i < 5; ++i) u |= (uint32_t)((lane >> i) & 1) << lb[i];
-                                    words[2 * l] = 2 * tswz(u);
-                                    words[2 * l + 1] = 2 * tswz(u) + 1;
-                                }
-                                cost += bank_degree(words, 32);
+                            std::vector<ITYPE> sectors;
+                            for (int lane = 0; lane < 32; ++lane) {
+                                ITYPE g = 0;
+                                for (int i = 0; i < 5; ++i)
+                                    if ((lane >> i) & 1) g |= 1ULL << fp.q[lb[i]];
+                                sectors.push_back(g >> 2);  // 4 complex64 amplitudes per 32-byte sector
                             }
+                            std::sort(sectors.begin(), sectors.end());
+                            const int cost = (int)(std::unique(sectors.begin(), sectors.end()) - sectors.begin());
                             if (cost < best) {
                                 best = cost;
                                 bc = {cos[c0], cos[c1], cos[c2]};
@@ -666,12 +684,23 @@ static void build_tables(const FusedPass& fp, size_t b, int m, std::vector<uint3
         const uint32_t u = row_tile_index(cb.bits, cb.lay, y, &part);
         (*t)[kTabRow + y] = nb ? b_operand_off(nb->bits, nb->lay, u, part) : (2 * tswz(u) | part);
     }
+    // global amplitude offset of tile index u (tile bit j <-> qubit q[j])
+    auto global_off = [&](uint32_t u) {
+        ITYPE g = 0;
+        for (int j = 0; j < m; ++j)
+            if ((u >> j) & 1) g |= 1ULL << fp.q[j];
+        return g;
+    };
+    auto put64 = [&](int word, ITYPE v) {
+        (*t)[word] = (uint32_t)v;
+        (*t)[word + 1] = (uint32_t)(v >> 32);
+    };
     for (uint32_t n = 0; n < N; ++n) {
         const uint32_t u = coset_tile_index(cb.lay, n);
         (*t)[kTabCol + n] = nb ? b_operand_off(nb->bits, nb->lay, u, 0) : 2 * tswz(u);
-        (*t)[kTabGn + n] = tswz(u);
+        put64(kTabGn + 2 * n, global_off(u));
     }
-    for (uint32_t j = 0; j < 64; ++j) (*t)[kTabGj + j] = tswz(k_tile_index(cb, j));
+    for (uint32_t j = 0; j < 64; ++j) put64(kTabGj + 2 * j, global_off(k_tile_index(cb, j)));
 }
 
 int fused_plan_host(const Circuit& c, FusedPlanHost* P) {
@@ -782,7 +811,8 @@ struct FusedPlanDev {
 
 static size_t fused_smem_bytes(int m) {
     const size_t tsize = size_t(1) << m, N = tsize >> kFBlock;
-    return 2 * kAImageBytes + 2 * N * 256 + tsize * 8 + 2 * kTabBytes + 64;  // + 2 mbarriers, TMEM slot, error flag
+    (void)tsize;
+    return 2 * kAImageBytes + 2 * (2 * N * 256) + 2 * kTabBytes + 64;  // A, two B / output tiles, tables, 3 mbarriers, TMEM slot, flag
 }
 
 // The kernel's dynamic shared-memory limit is a process-wide attribute: set it once per device to
@@ -854,7 +884,7 @@ int run_fused_c64(Circuit& c, void* state, ITYPE dim, cudaStream_t st) {
         FusedPassArgs p = p0;
         p.state = (float2*)state;
         const size_t smem = fused_smem_bytes(p.m);
-        const unsigned grid = (unsigned)std::min<ITYPE>(p.tiles, (ITYPE)sm_count());
+        const unsigned grid = (unsigned)std::min<ITYPE>((p.tiles + 1) / 2, (ITYPE)sm_count());  // tile pairs
         k_fused_pass<<<grid, kFThreads, smem, st>>>(p);
         QS_TRY(check_launch("k_fused_pass"));
     }

@@ -59,7 +59,7 @@ def block_layout(circ, index):
     rows = np.zeros(7, dtype=np.int32)
     ks = np.zeros(6, dtype=np.int32)
     cos = np.zeros(7, dtype=np.uint32)
-    tabs = np.zeros(448, dtype=np.uint32)
+    tabs = np.zeros(640, dtype=np.uint32)
     call("qs_circuit_fused_block_layout", circ._h, index, rows.ctypes.data_as(C.c_void_p),
          ks.ctypes.data_as(C.c_void_p), cos.ctypes.data_as(C.c_void_p), tabs.ctypes.data_as(C.c_void_p))
     return rows, ks, cos, tabs
@@ -113,7 +113,7 @@ def tswz(u):
 
 def emulate_fused(circ, n, state):
     """Replays the fused kernel's data movement on the CPU from the exported operand images and index
-    tables: swizzled tile -> B gather (gn ^ gj), A (hi + lo) times B in FP64, accumulator -> next B
+    tables: state -> B gather (global offsets gn | gj), A (hi + lo) times B in FP64, accumulator -> next B
     operand or output tile through rowtab[y] ^ coltab[n]."""
     npasses, blocks = export_blocks(circ)
     groups = []
@@ -144,12 +144,10 @@ def emulate_fused(circ, n, state):
             base = 0
             for j, q in enumerate(others):
                 base |= ((T >> j) & 1) << q
-            t = state[base | local]
-            stage = np.zeros(1 << m, dtype=np.complex128)
-            stage[tswz(u)] = t
             tabs = layouts[0][3]
-            gn, gj = tabs[256:256 + N].astype(np.int64), tabs[384:448].astype(np.int64)
-            v = stage[gn[:, None] ^ gj[None, :]]                    # (N, 64)
+            gn = np.ascontiguousarray(tabs[256:512]).view(np.uint64)[:N].astype(np.int64)  # global offsets
+            gj = np.ascontiguousarray(tabs[512:640]).view(np.uint64).astype(np.int64)
+            v = state[base | gn[:, None] | gj[None, :]]             # (N, 64), read straight from the state
             B = np.empty((N, 128))
             B[:, 0::2], B[:, 1::2] = v.real, v.imag
             for b in range(len(idxs)):
