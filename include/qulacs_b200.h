@@ -370,8 +370,10 @@ QS_API int qs_state_sampling_with_uniforms_c64(const void* state_c64, QS_ITYPE d
 QS_API int qs_circuit_fused_stats(qs_circuit_t circuit, QS_UINT* passes, QS_UINT* blocks);
 /* Host-only export of fused block `index` (application order): the pass's tile qubits (<= 13),
  * the block's 6 tile-local bits, its FP64 64x64 matrix (row-major interleaved complex, may be NULL)
- * and its bf16 operand image (hi then lo, 2 x 128 x 128, K-major core-matrix layout, rows and
- * columns in the order qs_circuit_fused_block_layout reports; may be NULL). */
+ * and its bf16 operand image (hi then lo, 2 x 128 x 128, may be NULL) in the UMMA K-major layout
+ * with the 128-byte swizzle: 8-row x 64-element atoms of 1 KiB, atom (r / 8, k / 64) at
+ * ((r / 8) * 2 + k / 64) KiB, row r % 8 at 128 (r % 8) bytes, 16-byte chunk (k / 8) % 8 stored at
+ * chunk ((k / 8) % 8) ^ (r % 8); rows and columns in the order qs_circuit_fused_block_layout reports. */
 QS_API int qs_circuit_fused_block_export(qs_circuit_t circuit, QS_UINT index, QS_UINT* tile_qubits,
     int* tile_qubit_count, QS_UINT* block_bits, double* matrix, unsigned short* operand_image);
 /* Host-only export of fused block `index`'s operand orders and device index tables:

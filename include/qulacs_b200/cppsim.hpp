@@ -328,6 +328,8 @@ public:
     }
     UINT get_gate_count() const { return (UINT)gate_list.size(); }
     qs_circuit_t handle() const { return h_; }
+    // block size of QS_EXEC_STAGED_FUSED: 0..6, or -1 (default) for the autotuner's choice
+    void set_fusion(int k) { check(qs_circuit_set_fusion(h_, k), "set_fusion"); }
     // exec_mode: QS_EXEC_STAGED (default), QS_EXEC_STAGED_FUSED (FP64 k-qubit fusion, autotuned k) or
     // QS_EXEC_GATE_BY_GATE
     void update_quantum_state(QuantumStateBase* state, int exec_mode = QS_EXEC_STAGED) {
@@ -343,6 +345,71 @@ public:
 
 private:
     qs_circuit_t h_ = nullptr;
+};
+
+// ------------------------------------------------------------------ noisy sampling
+// cppsim NoiseSimulator (noisesimulator.hpp): trajectories drawn as the reference draws them, distinct
+// ones simulated once on the device.  The reference seeds from std::random_device; here the seed is
+// an argument (reproducible runs).
+class NoiseSimulator {
+public:
+    struct Result {
+        std::vector<std::pair<QuantumState*, UINT>> result;
+        Result() = default;
+        Result(const Result&) = delete;
+        Result& operator=(const Result&) = delete;
+        ~Result() {
+            for (auto& p : result) delete p.first;
+        }
+        std::vector<ITYPE> sampling(UINT seed = 0) const {
+            std::vector<ITYPE> out;
+            UINT i = 0;
+            for (const auto& p : result) {
+                const std::vector<ITYPE> s = p.first->sampling(p.second, seed + i++);
+                out.insert(out.end(), s.begin(), s.end());
+            }
+            return out;
+        }
+    };
+
+    explicit NoiseSimulator(const QuantumCircuit* circuit, const QuantumState* init_state = nullptr, UINT seed = 0)
+        : circuit_(circuit), init_(init_state), seed_(seed) {}
+
+    std::vector<ITYPE> execute(UINT sample_count) {
+        std::vector<ITYPE> out(sample_count);
+        check(qs_noise_simulator_execute(circuit_->handle(), init_ ? init_->data() : nullptr,
+                  ITYPE(1) << circuit_->qubit_count, sample_count, seed_, out.data(), nullptr, stream()),
+            "NoiseSimulator::execute");
+        return out;
+    }
+    // caller deletes the result (as the reference's execute_and_get_result)
+    Result* execute_and_get_result(UINT execution_count) {
+        UINT count = 0;
+        check(qs_noise_simulator_trajectories(circuit_->handle(), execution_count, seed_, &count, nullptr),
+            "NoiseSimulator::execute_and_get_result");
+        std::vector<UINT> shots(count);
+        check(qs_noise_simulator_trajectories(circuit_->handle(), execution_count, seed_, &count, shots.data()),
+            "NoiseSimulator::execute_and_get_result");
+        auto* r = new Result();
+        std::vector<void*> ptrs;
+        for (UINT i = 0; i < count; ++i) {
+            r->result.push_back({new QuantumState(circuit_->qubit_count, stream()), shots[i]});
+            ptrs.push_back(r->result.back().first->data());
+        }
+        const int rc = qs_noise_simulator_execute(circuit_->handle(), init_ ? init_->data() : nullptr,
+            ITYPE(1) << circuit_->qubit_count, execution_count, seed_, nullptr, ptrs.data(), stream());
+        if (rc != QS_OK) {
+            delete r;
+            check(rc, "NoiseSimulator::execute_and_get_result");
+        }
+        return r;
+    }
+
+private:
+    void* stream() const { return init_ ? init_->get_cuda_stream() : nullptr; }
+    const QuantumCircuit* circuit_;
+    const QuantumState* init_;
+    UINT seed_;
 };
 
 // ------------------------------------------------------------------ operators

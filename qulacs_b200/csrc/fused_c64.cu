@@ -5,17 +5,18 @@
 // always included so every HBM access is a >= 256-byte run); inside a pass, gates are fused greedily
 // into blocks of 6 qubits and each block's 64x64 complex matrix is composed in FP64.  The matrix is
 // made real, [[Re U, -Im U], [Im U, Re U]] (128 x 128), and split into bf16 hi + lo parts, written
-// in the canonical K-major no-swizzle UMMA shared-memory layout (8-row x 16-byte core matrices).
+// in the UMMA K-major shared-memory layout with the 128-byte swizzle.  Per block the host also picks
+// the operand orders (rows, K, cosets) that make the kernel's warp-wide shared-memory accesses
+// conflict-free, and emits them as XOR tables.
 //
-// Device side: one persistent CTA per SM.  Each tile (2^13 amplitudes = 64 KiB) is prefetched into
-// shared memory with cp.async while the previous tile's blocks run.  Block 0 gathers the tile's
-// 128 cosets x 64 amplitudes into the B operand (bf16 hi and lo of the real and imaginary parts,
-// K-major); one thread waits for the block's A image (bulk async copy on its own mbarrier), issues
-// 8 K-steps x 3 products (A_hi B_hi + A_hi B_lo + A_lo B_hi) of tcgen05.mma M=128 N=128 K=16 into a
-// 128 x 128 FP32 TMEM accumulator and commits to an mbarrier.  All warps then move the accumulator
-// with tcgen05.ld straight into the next block's B operand; after the last block it becomes a
-// complex64 tile that is stored to HBM.  Every wait is bounded; on expiry the kernel records an
-// error, frees its TMEM and returns.
+// Device side: one persistent CTA (512 threads) per SM takes its tiles in pairs that go through the
+// pass's blocks in lockstep and share each block's A image (bulk async copy).  Per block, one thread
+// issues for each tile 8 K-steps x 3 products (A_hi B_hi + A_hi B_lo + A_lo B_hi) of tcgen05.mma
+// M=128 N=128 K=16 into its 128 x 128 FP32 TMEM accumulator and commits to an mbarrier; all warps
+// move the first tile's accumulator (tcgen05.ld) into its next B operand while the second tile's
+// MMAs run.  Tiles are gathered straight from HBM; after the last block each becomes a complex64
+// tile stored to HBM.  Every wait is bounded; on expiry the kernel records an error, frees its TMEM
+// and returns.
 #include <algorithm>
 #include <cmath>
 #include <complex>
@@ -43,9 +44,13 @@ constexpr int kTabRow = 0, kTabCol = 128, kTabGn = 256, kTabGj = 512, kTabWords 
 constexpr int kTabBytes = kTabWords * 4;
 constexpr int kRecordBytes = 2 * kAImageBytes + kTabBytes;  // one block record in global memory
 
-// canonical K-major, no swizzle: element (r, k) of a rows x 128 bf16 operand
+// K-major with the 128-byte swizzle: element (r, k) of a rows x 128 bf16 operand.  Atoms of 8 rows x
+// 64 K (8 rows of 128 B = 1024 B, 1024-byte aligned); atom (r / 8, k / 64) at ((r / 8) * 2 + k / 64) KiB;
+// in an atom, row r % 8 at 128 (r % 8) and its 16-byte chunk (k / 8) % 8 at chunk ((k / 8) % 8) ^ (r % 8).
+// A bit placement with an XOR, so offsets of XORed indices XOR.
 __host__ __device__ __forceinline__ uint32_t kmajor_off(uint32_t r, uint32_t k) {
-    return (r >> 3) * 2048u + (k >> 3) * 128u + (r & 7u) * 16u + (k & 7u) * 2u;
+    return ((r >> 3) * 2u + (k >> 6)) * 1024u + (r & 7u) * 128u + ((((k >> 3) & 7u) ^ (r & 7u)) << 4) +
+           (k & 7u) * 2u;
 }
 
 struct FusedPassArgs {
@@ -82,14 +87,17 @@ __device__ __forceinline__ void split2_bf16(float a, float b, uint32_t* hi, uint
     *lo = l;
 }
 
-// UMMA shared-memory descriptor: start >> 4 [0,14), LBO >> 4 [16,30), SBO >> 4 [32,46),
-// version 1 [46,48), layout SWIZZLE_NONE (0) [61,64).
-__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+// UMMA shared-memory descriptor for the swizzled K-major operands above: start >> 4 [0,14),
+// LBO field 1 [16,30) (unused by swizzled K-major layouts), SBO >> 4 = 2048 B between 8-row groups
+// [32,46), version 1 [46,48), base offset 0 (1024-byte aligned atoms), layout SWIZZLE_128B (2) [61,64).
+// K-step s (K = 16 s .. 16 s + 15) starts at atom column s / 4 (+1 KiB) and 32 B (s % 4) into the row.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
     uint64_t d = 0;
     d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
-    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
-    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 16;
+    d |= (uint64_t)(2048u >> 4) << 32;
     d |= (uint64_t)1 << 46;
+    d |= (uint64_t)2 << 61;
     return d;
 }
 
@@ -261,12 +269,12 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused_pass(const __grid_consta
     auto issue_mma = [&](unsigned char* sB, uint32_t dcol, uint32_t mbar_addr) {
         const uint32_t baddr = smem_u32(sB);
         // shared addresses are below 256 KiB, so the 14-bit start-address field never wraps: the
-        // descriptor of K-step s is the K-step-0 descriptor plus 256 B >> 4 = 16 per step
-        const uint64_t ahi0 = umma_desc(aaddr, 128, 2048), alo0 = umma_desc(aaddr + kAImageBytes, 128, 2048);
-        const uint64_t bhi0 = umma_desc(baddr, 128, 2048), blo0 = umma_desc(baddr + bimg, 128, 2048);
+        // descriptor of K-step s is the K-step-0 descriptor plus its start offset >> 4
+        const uint64_t ahi0 = umma_desc(aaddr), alo0 = umma_desc(aaddr + kAImageBytes);
+        const uint64_t bhi0 = umma_desc(baddr), blo0 = umma_desc(baddr + bimg);
 #pragma unroll
         for (int s = 0; s < kAK / 16; ++s) {
-            const uint64_t ds = 16u * (uint64_t)s;
+            const uint64_t ds = (uint64_t)(((s >> 2) * 1024 + (s & 3) * 32) >> 4);
             mma_bf16(tmem + dcol, ahi0 + ds, bhi0 + ds, idesc, s > 0 ? 1u : 0u);
             mma_bf16(tmem + dcol, ahi0 + ds, blo0 + ds, idesc, 1u);
             mma_bf16(tmem + dcol, alo0 + ds, bhi0 + ds, idesc, 1u);

@@ -93,6 +93,40 @@ int main() {
         EXPECT(std::abs(m[0] - (1 - p / 2)) < 1e-15 && std::abs(m[3] - p / 2) < 1e-15);
         EXPECT(std::abs(rho.get_squared_norm() - 1.0) < 1e-15);
     }
+    // FP64-fused staged mode equals gate by gate; NoiseSimulator draws and merges trajectories
+    {
+        const UINT n = 10;
+        QuantumCircuit c(n);
+        for (int layer = 0; layer < 3; ++layer) {
+            for (UINT q = 0; q < n; ++q) c.add_noise_gate(gate::RY(q, 0.3 + 0.1 * q + layer), "Depolarizing", 0.01);
+            for (UINT q = 0; q + 1 < n; ++q) c.add_noise_gate(gate::CZ(q, q + 1), "Depolarizing", 0.01);
+        }
+        NoiseSimulator sim(&c, nullptr, 11);
+        const std::vector<ITYPE> s = sim.execute(200);
+        EXPECT(s.size() == 200);
+        for (ITYPE x : s) EXPECT(x < (ITYPE(1) << n));
+        NoiseSimulator::Result* r = sim.execute_and_get_result(200);
+        UINT total = 0;
+        for (const auto& p : r->result) {
+            total += p.second;
+            EXPECT(std::abs(p.first->get_squared_norm() - 1.0) < 1e-12);
+        }
+        EXPECT(total == 200 && !r->result.empty());
+        delete r;
+        QuantumCircuit u(n);
+        for (UINT q = 0; q < n; ++q) {
+            u.add_gate(gate::RX(q, 0.2 * q));
+            u.add_gate(gate::RZ(q, 0.7));
+        }
+        for (UINT q = 0; q + 1 < n; ++q) u.add_gate(gate::CNOT(q, q + 1));
+        QuantumState a(n), b(n);
+        u.update_quantum_state(&a, QS_EXEC_STAGED_FUSED);
+        u.update_quantum_state(&b, QS_EXEC_GATE_BY_GATE);
+        const ComplexVector va = a.get_vector(), vb = b.get_vector();
+        double err = 0;
+        for (size_t i = 0; i < va.size(); ++i) err = std::max(err, std::abs(va[i] - vb[i]));
+        EXPECT(err <= 1e-12);
+    }
     // errors become exceptions
     {
         bool threw = false;

@@ -12,7 +12,8 @@ from qulacs_b200._lib import call
 
 
 def kmajor_off(r, k):
-    return (r >> 3) * 2048 + (k >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2
+    """K-major, 128-byte swizzle (8-row x 128 B atoms, 16-byte chunk index XOR row % 8)."""
+    return ((r >> 3) * 2 + (k >> 6)) * 1024 + (r & 7) * 128 + ((((k >> 3) & 7) ^ (r & 7)) << 4) + (k & 7) * 2
 
 
 def bf16_to_f32(h):
