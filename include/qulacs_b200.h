@@ -73,6 +73,38 @@ QS_API int qs_get_state(const void* state, void* host_dst, QS_ITYPE dim, void* s
 QS_API int qs_state_to_c64(const void* state_c128, void* state_c64, QS_ITYPE dim, void* stream);
 QS_API int qs_state_to_c128(const void* state_c64, void* state_c128, QS_ITYPE dim, void* stream);
 
+/* ---- whole-state arithmetic (src/csim/update_ops.hpp:510, 1500-1505; update_ops_named_state.cpp) ---- */
+/* state_add (:1500): state += state_added */
+QS_API int qs_state_add(const void* state_added, void* state, QS_ITYPE dim, void* stream);
+/* state_add_with_coef (:1501): state += coef * state_added (coef interleaved complex) */
+QS_API int qs_state_add_with_coef(const double coef[2], const void* state_added, void* state, QS_ITYPE dim,
+    void* stream);
+/* state_multiply (:1505): state *= coef */
+QS_API int qs_state_multiply(const double coef[2], void* state, QS_ITYPE dim, void* stream);
+/* normalize (:510): state *= sqrt(1 / squared_norm) */
+QS_API int qs_normalize(double squared_norm, void* state, QS_ITYPE dim, void* stream);
+/* Haar-random pure state: amplitudes g1 + i g2 of independent standard normals, normalised.  The
+ * reference (init_ops_random.cpp:21-80) draws from per-OpenMP-thread xorshift streams, so its values
+ * depend on the host's thread count; this draws from a counter-based generator (splitmix64 per
+ * amplitude index and seed), the same distribution, reproducible for a seed on any device. */
+QS_API int qs_initialize_Haar_random_state_with_seed(void* state, QS_ITYPE dim, QS_UINT seed, void* stream);
+/* state[i] *= factors[i], `factors` a device array of dim complex128 (cppsim
+ * QuantumStateCpu::multiply_elementwise_function, cppsim/state.hpp:885-891, with func(i) tabulated). */
+QS_API int qs_state_multiply_elementwise(const void* factors, void* state, QS_ITYPE dim, void* stream);
+/* cppsim gate::RandomUnitary(targets, seed) (gate_factory.cpp:351-380) on the host: the same
+ * mt19937_64 / std::normal_distribution draws in the same order, and the Q of their QR factorisation
+ * with a positive real R diagonal.  `matrix_out`: 4^qubit_count complex128, row-major; 1..10 qubits. */
+QS_API int qs_random_unitary_matrix(QS_UINT qubit_count, QS_UINT seed, double* matrix_out);
+/* GeneralQuantumOperator::add_random_operator(count, seed) (general_quantum_operator.cpp:179-202) on
+ * the host: for each term t, pauli_ids_out[t * qubit_count + q] is qubit q's Pauli id (0..3) and
+ * coefs_out[t] its real coefficient in [-1, 1), from the reference's mt19937_64 draws. */
+QS_API int qs_random_operator_terms(QS_UINT qubit_count, QS_UINT operator_count, QS_UINT seed,
+    QS_UINT* pauli_ids_out, double* coefs_out);
+/* Device-to-device copy of `count` complex128 entries (cppsim QuantumStateGpu::load(state)). */
+QS_API int qs_copy_state(const void* src, void* dst, QS_ITYPE count, void* stream);
+/* One amplitude to the host (cppsim QuantumState::data_cpp()[index]).  Synchronises `stream`. */
+QS_API int qs_get_amplitude(const void* state, QS_ITYPE dim, QS_ITYPE index, double out[2], void* stream);
+
 /* ---- single-qubit gates (src/csim/update_ops.hpp) ---- */
 /* update_ops.hpp:720 single_qubit_dense_matrix_gate(UINT, const CTYPE[4], CTYPE*, ITYPE) */
 QS_API int qs_single_qubit_dense_matrix_gate(
@@ -148,6 +180,9 @@ QS_API int qs_multi_qubit_Pauli_rotation_gate_partial_list(const QS_UINT* target
 
 /* ---- statistics (src/csim/stat_ops.hpp); results to host, stream synchronised ---- */
 /* stat_ops.hpp:5 state_norm_squared */
+/* measurement_distribution_entropy (stat_ops.hpp:10, stat_ops_probability.cpp:83-99): sum of -p log p
+ * over p = |a_i|^2 clamped below at 1e-15.  Synchronises `stream`. */
+QS_API int qs_measurement_distribution_entropy(const void* state, QS_ITYPE dim, void* stream, double* out);
 QS_API int qs_state_norm_squared(const void* state, QS_ITYPE dim, void* stream, double* out);
 /* stat_ops.hpp:12 state_inner_product: sum conj(bra_i) ket_i -> out[0] + i out[1] */
 QS_API int qs_state_inner_product(const void* state_bra, const void* state_ket, QS_ITYPE dim,
@@ -233,6 +268,21 @@ QS_API int qs_dm_expectation_value_multi_qubit_Pauli_operator_partial_list(
 QS_API int qs_dm_sampling_with_uniforms(const void* rho, QS_ITYPE dim, const double* uniforms,
     QS_UINT sampling_count, QS_ITYPE* out, void* stream);
 /* stat_ops_dm.hpp dm_state_norm_squared (trace) */
+/* stat_ops_dm.hpp:6-11: dm_measurement_distribution_entropy (diagonal p = Re rho_ii, p <= 1e-15
+ * skipped), dm_state_add, dm_state_add_with_coef, dm_state_multiply (over all dim x dim entries). */
+QS_API int qs_dm_measurement_distribution_entropy(const void* rho, QS_ITYPE dim, void* stream, double* out);
+QS_API int qs_dm_state_add(const void* rho_added, void* rho, QS_ITYPE dim, void* stream);
+QS_API int qs_dm_state_add_with_coef(const double coef[2], const void* rho_added, void* rho, QS_ITYPE dim,
+    void* stream);
+QS_API int qs_dm_state_multiply(const double coef[2], void* rho, QS_ITYPE dim, void* stream);
+/* update_ops_dm.cpp:14-28 dm_normalize: rho *= 1 / squared_norm (the trace, not its square root). */
+QS_API int qs_dm_normalize(double squared_norm, void* rho, QS_ITYPE dim, void* stream);
+/* stat_ops_dm.cpp:50-120 dm_M0_prob, dm_M1_prob, dm_marginal_prob: sums of Re rho_ii over the
+ * matching diagonal indices.  Synchronise `stream`. */
+QS_API int qs_dm_M0_prob(QS_UINT target, const void* rho, QS_ITYPE dim, void* stream, double* out);
+QS_API int qs_dm_M1_prob(QS_UINT target, const void* rho, QS_ITYPE dim, void* stream, double* out);
+QS_API int qs_dm_marginal_prob(const QS_UINT* targets, const QS_UINT* values, QS_UINT count, const void* rho,
+    QS_ITYPE dim, void* stream, double* out);
 QS_API int qs_dm_state_norm_squared(const void* rho, QS_ITYPE dim, void* stream, double* out);
 
 /* ---- circuits (cppsim QuantumCircuit, src/cppsim/circuit.hpp) ----

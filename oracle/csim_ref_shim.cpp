@@ -85,6 +85,26 @@ REF_API void ref_multi_qubit_Pauli_rotation_gate_partial_list(
 }
 
 // ---- statistics (csim/stat_ops.hpp) ----
+REF_API void ref_state_add_with_coef(const double* coef, const double* added, double* s, ITYPE dim) {
+    state_add_with_coef(CTYPE(coef[0], coef[1]), CC(added), C(s), dim);
+}
+REF_API void ref_state_multiply(const double* coef, double* s, ITYPE dim) {
+    state_multiply(CTYPE(coef[0], coef[1]), C(s), dim);
+}
+REF_API void ref_normalize(double squared_norm, double* s, ITYPE dim) { normalize(squared_norm, C(s), dim); }
+REF_API double ref_measurement_distribution_entropy(const double* s, ITYPE dim) {
+    return measurement_distribution_entropy(CC(s), dim);
+}
+REF_API double ref_dm_measurement_distribution_entropy(const double* r, ITYPE dim) {
+    return dm_measurement_distribution_entropy(CC(r), dim);
+}
+REF_API double ref_dm_M0_prob(UINT t, const double* r, ITYPE dim) { return dm_M0_prob(t, CC(r), dim); }
+REF_API double ref_dm_M1_prob(UINT t, const double* r, ITYPE dim) { return dm_M1_prob(t, CC(r), dim); }
+REF_API double ref_dm_marginal_prob(
+    const UINT* sorted_tl, const UINT* vals, UINT cnt, const double* r, ITYPE dim) {
+    return dm_marginal_prob(sorted_tl, vals, cnt, CC(r), dim);
+}
+REF_API void ref_dm_normalize(double squared_norm, double* r, ITYPE dim) { dm_normalize(squared_norm, C(r), dim); }
 REF_API double ref_state_norm_squared(const double* s, ITYPE dim) {
     return state_norm_squared(CC(s), dim);
 }

@@ -11,6 +11,7 @@ Only tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py``
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 import subprocess
 import threading
@@ -127,6 +128,37 @@ class CpuSim:
         self._f("multi_qubit_Pauli_rotation_gate_partial_list")(
             _ptr(tl), _ptr(ids), _U(tl.size), _D(angle), _ptr(s), _IT(s.size))
 
+    # ---- whole-state arithmetic ----
+    def state_add_with_coef(self, coef, added, s):
+        c = np.array([complex(coef).real, complex(coef).imag])
+        self._f("state_add_with_coef")(_ptr(c), _ptr(added), _ptr(s), _IT(s.size))
+
+    def state_multiply(self, coef, s):
+        c = np.array([complex(coef).real, complex(coef).imag])
+        self._f("state_multiply")(_ptr(c), _ptr(s), _IT(s.size))
+
+    def normalize(self, squared_norm, s):
+        self._f("normalize")(_D(squared_norm), _ptr(s), _IT(s.size))
+
+    def measurement_distribution_entropy(self, s) -> float:
+        return self._f("measurement_distribution_entropy", _D)(_ptr(s), _IT(s.size))
+
+    def dm_measurement_distribution_entropy(self, r) -> float:
+        return self._f("dm_measurement_distribution_entropy", _D)(_ptr(r), _IT(r.shape[0]))
+
+    def dm_normalize(self, squared_norm, r):
+        self._f("dm_normalize")(_D(squared_norm), _ptr(r), _IT(r.shape[0]))
+
+    def dm_M0_prob(self, t, r):
+        return self._f("dm_M0_prob", _D)(_U(t), _ptr(r), _IT(r.shape[0]))
+
+    def dm_M1_prob(self, t, r):
+        return self._f("dm_M1_prob", _D)(_U(t), _ptr(r), _IT(r.shape[0]))
+
+    def dm_marginal_prob(self, tl, vals, r):
+        tl, vals = _u32(tl), _u32(vals)
+        return self._f("dm_marginal_prob", _D)(_ptr(tl), _ptr(vals), _U(tl.size), _ptr(r), _IT(r.shape[0]))
+
     # ---- statistics ----
     def state_norm_squared(self, s) -> float:
         return self._f("state_norm_squared", _D)(_ptr(s), _IT(s.size))
@@ -216,9 +248,65 @@ def reference() -> CpuSim | None:
 
 # ---------------------------------------------------------------- reference RNG and NoiseSimulator
 
+def std_normals(seed, count):
+    """cppsim Random::normal (utility.hpp:86): libstdc++ std::normal_distribution<double>(0, 1) over
+    mt19937_64(seed) -- the Marsaglia polar method: x, y = 2u - 1 until 0 < r2 = x^2 + y^2 <= 1, then
+    y * m is returned and x * m kept for the next call, m = sqrt(-2 log(r2) / r2)."""
+    u = mt19937_64_uniforms(seed, 4 * count + 64)
+    k, out = 0, []
+    while len(out) < count:
+        x = 2.0 * u[k] - 1.0
+        y = 2.0 * u[k + 1] - 1.0
+        k += 2
+        r2 = x * x + y * y
+        if r2 > 1.0 or r2 == 0.0:
+            continue
+        m = math.sqrt(-2.0 * math.log(r2) / r2)
+        out += [y * m, x * m]
+    return np.array(out[:count])
+
+
+def random_unitary(qubit_count, seed):
+    """cppsim gate::RandomUnitary(targets, seed) (gate_factory.cpp:351-380): entries (normal() + i normal())
+    / sqrt(2) row by row -- with g++ the imaginary draw comes first -- then Householder QR and column c of
+    Q times R_cc / |R_cc|."""
+    d = 1 << qubit_count
+    g = std_normals(seed, 2 * d * d)
+    a = ((g[1::2] + 1j * g[0::2]) / math.sqrt(2.0)).reshape(d, d)
+    q, r = np.linalg.qr(a)
+    ph = np.diag(r) / np.abs(np.diag(r))
+    return q * ph[None, :]
+
+
+def random_operator_terms(qubit_count, operator_count, seed):
+    """GeneralQuantumOperator::add_random_operator(count, seed) (general_quantum_operator.cpp:179-202): per
+    term, Random::int32() % 4 for qubits 0..n-1 (int32 = mt() % ULONG_MAX, utility.hpp:100), then
+    uniform() * 2 - 1.  Returns [(pauli ids per qubit, coefficient)]."""
+    raw = mt19937_64_raw(seed, operator_count * (qubit_count + 1))
+    out, k = [], 0
+    for _ in range(operator_count):
+        ids = [int(raw[k + q] % 0xFFFFFFFFFFFFFFFF % 4) for q in range(qubit_count)]
+        k += qubit_count
+        u = float(raw[k]) / 18446744073709551616.0
+        k += 1
+        out.append((ids, (u if u < 1.0 else np.nextafter(1.0, 0.0)) * 2 - 1.0))
+    return out
+
+
 def mt19937_64_uniforms(seed, count):
-    """cppsim Random (utility.hpp:54-80): mt19937_64 (Matsumoto & Nishimura 2000, 64-bit parameters) and libstdc++'s
-    generate_canonical<double, 53> for a 64-bit engine: x / 2^64, clamped below 1."""
+    """cppsim Random (utility.hpp:54-80): libstdc++'s generate_canonical<double, 53> over mt19937_64 for a
+    64-bit engine: x / 2^64, clamped below 1."""
+    out = []
+    for y in mt19937_64_raw(seed, count):
+        r = float(y) / 18446744073709551616.0
+        if r >= 1.0:
+            r = np.nextafter(1.0, 0.0)
+        out.append(r)
+    return np.array(out)
+
+
+def mt19937_64_raw(seed, count):
+    """mt19937_64 (Matsumoto & Nishimura 2000, 64-bit parameters): the first `count` outputs for `seed`."""
     n, m = 312, 156
     mt = [0] * n
     mt[0] = seed & 0xFFFFFFFFFFFFFFFF
@@ -242,11 +330,8 @@ def mt19937_64_uniforms(seed, count):
         y ^= (y << 17) & 0x71D67FFFEDA60000
         y ^= (y << 37) & 0xFFF7EEE000000000
         y ^= y >> 43
-        r = float(y) / 18446744073709551616.0
-        if r >= 1.0:
-            r = np.nextafter(1.0, 0.0)
-        out.append(r)
-    return np.array(out)
+        out.append(y)
+    return out
 
 
 def _pauli(ids):

@@ -535,3 +535,92 @@ OR_API void or_dm_sampling_with_uniforms(const double* r, ITYPE dim, const doubl
     }
     free(stacked);
 }
+
+/* ---- whole-state arithmetic and entropy ---- */
+
+/* update_ops_named_state.cpp:62-75 state_add_with_coef: state[i] += coef * added[i]
+ * (state_add, :47-60, is coef = 1). */
+OR_API void or_state_add_with_coef(const double* coef, const double* added, double* s, ITYPE dim) {
+    const cplx c = coef[0] + I * coef[1];
+    for (ITYPE i = 0; i < dim; ++i) {
+        cplx v = s[2 * i] + I * s[2 * i + 1];
+        v += c * (added[2 * i] + I * added[2 * i + 1]);
+        s[2 * i] = creal(v);
+        s[2 * i + 1] = cimag(v);
+    }
+}
+
+/* update_ops_named_state.cpp:86-95 state_multiply: state[i] *= coef. */
+OR_API void or_state_multiply(const double* coef, double* s, ITYPE dim) {
+    const cplx c = coef[0] + I * coef[1];
+    for (ITYPE i = 0; i < dim; ++i) {
+        const cplx v = c * (s[2 * i] + I * s[2 * i + 1]);
+        s[2 * i] = creal(v);
+        s[2 * i + 1] = cimag(v);
+    }
+}
+
+/* update_ops_named_state.cpp:21-30 normalize: state[i] *= sqrt(1 / squared_norm). */
+OR_API void or_normalize(double squared_norm, double* s, ITYPE dim) {
+    const double f = sqrt(1. / squared_norm);
+    for (ITYPE i = 0; i < 2 * dim; ++i) s[i] *= f;
+}
+
+/* stat_ops_probability.cpp:83-99 measurement_distribution_entropy: sum of -p log p over
+ * p = |amplitude|^2 clamped below at 1e-15. */
+OR_API double or_measurement_distribution_entropy(const double* s, ITYPE dim) {
+    const double eps = 1e-15;
+    double ent = 0;
+    for (ITYPE i = 0; i < dim; ++i) {
+        double p = pow(cabs(s[2 * i] + I * s[2 * i + 1]), 2);
+        p = (p > eps) ? p : eps;
+        ent += -1.0 * p * log(p);
+    }
+    return ent;
+}
+
+/* stat_ops_dm.cpp:29-46 dm_measurement_distribution_entropy: sum of -p log p over the diagonal
+ * p = Re rho[i][i], terms with p <= 1e-15 skipped. */
+OR_API double or_dm_measurement_distribution_entropy(const double* r, ITYPE dim) {
+    const double eps = 1e-15;
+    double ent = 0;
+    for (ITYPE i = 0; i < dim; ++i) {
+        const double p = r[2 * (i * dim + i)];
+        if (p > eps) ent += -1.0 * p * log(p);
+    }
+    return ent;
+}
+
+/* ---- density-matrix probabilities and normalisation ---- */
+
+/* stat_ops_dm.cpp:95-120 dm_marginal_prob: sum of Re rho[b][b] over the basis indices b whose
+ * bits at the (sorted) targets equal the measured values; dm_M0_prob (:50-67) and dm_M1_prob
+ * (:70-89) are the one-target cases. */
+OR_API double or_dm_marginal_prob(const UINT* sorted_targets, const UINT* values, UINT count,
+    const double* r, ITYPE dim) {
+    const ITYPE loop_dim = dim >> count;
+    double sum = 0.;
+    for (ITYPE k = 0; k < loop_dim; ++k) {
+        ITYPE b = k;
+        for (UINT c = 0; c < count; ++c) {
+            const ITYPE low = b & ((1ULL << sorted_targets[c]) - 1);
+            b = ((b - low) << 1) | low | ((ITYPE)values[c] << sorted_targets[c]);
+        }
+        sum += r[2 * (b * dim + b)];
+    }
+    return sum;
+}
+OR_API double or_dm_M0_prob(UINT t, const double* r, ITYPE dim) {
+    const UINT v = 0;
+    return or_dm_marginal_prob(&t, &v, 1, r, dim);
+}
+OR_API double or_dm_M1_prob(UINT t, const double* r, ITYPE dim) {
+    const UINT v = 1;
+    return or_dm_marginal_prob(&t, &v, 1, r, dim);
+}
+
+/* update_ops_dm.cpp:14-28 dm_normalize: rho *= 1 / squared_norm. */
+OR_API void or_dm_normalize(double squared_norm, double* r, ITYPE dim) {
+    const double f = 1. / squared_norm;
+    for (ITYPE i = 0; i < 2 * dim * dim; ++i) r[i] *= f;
+}

@@ -57,6 +57,25 @@ SIGNATURES = {
     "qs_multi_qubit_Pauli_gate_partial_list": [P, P, U] + _STATE,
     "qs_multi_qubit_Pauli_rotation_gate_partial_list": [P, P, U, D] + _STATE,
     "qs_state_norm_squared": [P, IT, P, P],
+    "qs_measurement_distribution_entropy": [P, IT, P, P],
+    "qs_dm_measurement_distribution_entropy": [P, IT, P, P],
+    "qs_state_add": [P, P, IT, P],
+    "qs_state_add_with_coef": [P, P, P, IT, P],
+    "qs_state_multiply": [P, P, IT, P],
+    "qs_normalize": [D, P, IT, P],
+    "qs_dm_state_add": [P, P, IT, P],
+    "qs_dm_state_add_with_coef": [P, P, P, IT, P],
+    "qs_dm_state_multiply": [P, P, IT, P],
+    "qs_initialize_Haar_random_state_with_seed": [P, IT, U, P],
+    "qs_get_amplitude": [P, IT, IT, P, P],
+    "qs_copy_state": [P, P, IT, P],
+    "qs_random_unitary_matrix": [U, U, P],
+    "qs_random_operator_terms": [U, U, U, P, P],
+    "qs_state_multiply_elementwise": [P, P, IT, P],
+    "qs_dm_normalize": [D, P, IT, P],
+    "qs_dm_M0_prob": [U, P, IT, P, P],
+    "qs_dm_M1_prob": [U, P, IT, P, P],
+    "qs_dm_marginal_prob": [P, P, U, P, IT, P, P],
     "qs_state_inner_product": [P, P, IT, P, P],
     "qs_M0_prob": [U, P, IT, P, P],
     "qs_M1_prob": [U, P, IT, P, P],

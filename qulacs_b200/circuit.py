@@ -24,6 +24,7 @@ class QuantumCircuit:
         call("qs_circuit_create", self.qubit_count, C.byref(h))
         self._h = h.value
         self.gate_list = []
+        self._fusion_k = None
 
     def get_qubit_count(self) -> int:
         return self.qubit_count
@@ -31,22 +32,115 @@ class QuantumCircuit:
     def get_gate_count(self) -> int:
         return len(self.gate_list)
 
-    def add_gate(self, gate: G.QuantumGateBase) -> None:
-        gate._add_to(self._h)
-        self.gate_list.append(gate)
+    def _check_qubits(self, gate: G.QuantumGateBase) -> None:
+        # cppsim check_gate_index (circuit.cpp:119-131)
+        for q in gate.get_target_index_list() + gate.get_control_index_list():
+            if not 0 <= q < self.qubit_count:
+                raise ValueError("gate must be applied to qubits of which the indices are smaller than qubit_count")
+
+    def _rebuild(self) -> None:
+        """Re-create the native circuit from gate_list (after an insertion or removal)."""
+        h = C.c_void_p()
+        call("qs_circuit_create", self.qubit_count, C.byref(h))
+        old, self._h = self._h, h.value
+        _lib.load().qs_circuit_destroy(old)
+        for g in self.gate_list:
+            g._add_to(self._h)
+        if self._fusion_k is not None:
+            call("qs_circuit_set_fusion", self._h, self._fusion_k)
+
+    def add_gate(self, gate: G.QuantumGateBase, position: int | None = None) -> None:
+        """Append (or insert before ``position``) a copy of ``gate`` (cppsim circuit.cpp:133-165)."""
+        self._check_qubits(gate)
+        g = gate.copy()
+        if position is None:
+            g._add_to(self._h)
+            self.gate_list.append(g)
+            return
+        if not 0 <= position <= len(self.gate_list):
+            raise IndexError("insert index must be smaller than or equal to gate_count")
+        self.gate_list.insert(position, g)
+        self._rebuild()
 
     add_gate_copy = add_gate
+    add_gate_consume = add_gate
 
-    # convenience adders (cppsim circuit.hpp:130-600)
+    def remove_gate(self, index: int) -> None:
+        """cppsim circuit.cpp:250-258."""
+        if not 0 <= index < len(self.gate_list):
+            raise IndexError("index must be smaller than gate_count")
+        del self.gate_list[index]
+        self._rebuild()
+
+    def get_gate(self, index: int) -> G.QuantumGateBase:
+        if not 0 <= index < len(self.gate_list):
+            raise IndexError("index must be smaller than gate_count")
+        return self.gate_list[index].copy()
+
+    def copy(self) -> "QuantumCircuit":
+        """cppsim circuit.cpp:111-117."""
+        c = QuantumCircuit(self.qubit_count)
+        c.merge_circuit(self)
+        return c
+
+    def merge_circuit(self, circuit: "QuantumCircuit") -> None:
+        """Append copies of ``circuit``'s gates (cppsim circuit.hpp:150-155)."""
+        for g in circuit.gate_list:
+            self.add_gate(g)
+
+    def get_inverse(self) -> "QuantumCircuit":
+        """The inverses of the gates in reverse order (cppsim circuit.cpp:571-578)."""
+        c = QuantumCircuit(self.qubit_count)
+        for g in reversed(self.gate_list):
+            c.add_gate(g.get_inverse())
+        return c
+
+    def calculate_depth(self) -> int:
+        """Greedy layering over each gate's targets and controls (cppsim circuit.cpp:295-322)."""
+        filled = [0] * self.qubit_count
+        depth = 0
+        for g in self.gate_list:
+            qubits = g.get_target_index_list() + g.get_control_index_list()
+            step = max((filled[q] for q in qubits), default=0) + 1
+            for q in qubits:
+                filled[q] = step
+            depth = max(depth, step)
+        return depth
+
+    def to_string(self) -> str:
+        """cppsim circuit.cpp:324-349."""
+        sizes = [len(g.get_target_index_list()) + len(g.get_control_index_list()) for g in self.gate_list]
+        top = max(sizes, default=0)
+        lines = ["*** Quantum Circuit Info ***", f"# of qubit: {self.qubit_count}",
+                 f"# of step : {self.calculate_depth()}", f"# of gate : {len(self.gate_list)}"]
+        lines += [f"# of {i + 1} qubit gate: {sizes.count(i + 1)}" for i in range(top)]
+        lines += ["Clifford  : no", "Gaussian  : no", ""]
+        return "\n".join(lines) + "\n"
+
+    def __str__(self) -> str:
+        return self.to_string()
+
+    # convenience adders (cppsim circuit.cpp:361-557)
     def add_X_gate(self, t): self.add_gate(G.X(t))
     def add_Y_gate(self, t): self.add_gate(G.Y(t))
     def add_Z_gate(self, t): self.add_gate(G.Z(t))
     def add_H_gate(self, t): self.add_gate(G.H(t))
     def add_S_gate(self, t): self.add_gate(G.S(t))
+    def add_Sdag_gate(self, t): self.add_gate(G.Sdag(t))
     def add_T_gate(self, t): self.add_gate(G.T(t))
+    def add_Tdag_gate(self, t): self.add_gate(G.Tdag(t))
+    def add_sqrtX_gate(self, t): self.add_gate(G.sqrtX(t))
+    def add_sqrtXdag_gate(self, t): self.add_gate(G.sqrtXdag(t))
+    def add_sqrtY_gate(self, t): self.add_gate(G.sqrtY(t))
+    def add_sqrtYdag_gate(self, t): self.add_gate(G.sqrtYdag(t))
+    def add_P0_gate(self, t): self.add_gate(G.P0(t))
+    def add_P1_gate(self, t): self.add_gate(G.P1(t))
     def add_RX_gate(self, t, a): self.add_gate(G.RX(t, a))
     def add_RY_gate(self, t, a): self.add_gate(G.RY(t, a))
     def add_RZ_gate(self, t, a): self.add_gate(G.RZ(t, a))
+    def add_RotInvX_gate(self, t, a): self.add_gate(G.RotInvX(t, a))
+    def add_RotInvY_gate(self, t, a): self.add_gate(G.RotInvY(t, a))
+    def add_RotInvZ_gate(self, t, a): self.add_gate(G.RotInvZ(t, a))
     def add_RotX_gate(self, t, a): self.add_gate(G.RotX(t, a))
     def add_RotY_gate(self, t, a): self.add_gate(G.RotY(t, a))
     def add_RotZ_gate(self, t, a): self.add_gate(G.RotZ(t, a))
@@ -57,6 +151,29 @@ class QuantumCircuit:
     def add_CZ_gate(self, c, t): self.add_gate(G.CZ(c, t))
     def add_SWAP_gate(self, a, b): self.add_gate(G.SWAP(a, b))
     def add_dense_matrix_gate(self, targets, m): self.add_gate(G.DenseMatrix(targets, m))
+
+    def add_random_unitary_gate(self, targets, seed: int | None = None) -> None:
+        self.add_gate(G.RandomUnitary(targets, seed))
+
+    def add_multi_Pauli_gate(self, targets_or_pauli, pauli_ids=None) -> None:
+        """(targets, pauli_ids) or a PauliOperator (cppsim circuit.cpp:454-461)."""
+        if pauli_ids is None:
+            p = targets_or_pauli
+            self.add_gate(G.Pauli(p.get_index_list(), p.get_pauli_id_list()))
+        else:
+            self.add_gate(G.Pauli(targets_or_pauli, pauli_ids))
+
+    def add_multi_Pauli_rotation_gate(self, targets_or_pauli, pauli_ids=None, angle=None) -> None:
+        """(targets, pauli_ids, angle), or a PauliOperator whose real coefficient is the angle
+        (cppsim circuit.cpp:462-480)."""
+        if pauli_ids is None:
+            p = targets_or_pauli
+            c = complex(p.get_coef())
+            if abs(c.imag) > 1e-14:
+                raise ValueError("add_multi_Pauli_rotation_gate: not implemented for non hermitian")
+            self.add_gate(G.PauliRotation(p.get_index_list(), p.get_pauli_id_list(), c.real))
+        else:
+            self.add_gate(G.PauliRotation(targets_or_pauli, pauli_ids, angle))
 
     def add_noise_gate(self, gate: G.QuantumGateBase, noise_type: str, prob: float) -> None:
         """cppsim circuit.cpp:167-190: the gate, then depolarizing noise on its targets + controls."""
@@ -88,6 +205,7 @@ class QuantumCircuit:
     def set_fusion(self, k: int) -> None:
         """Block size of mode="staged_fused": 0..6, or -1 to let the autotuner choose (default)."""
         call("qs_circuit_set_fusion", self._h, int(k))
+        self._fusion_k = int(k)
 
     def fusion_info(self):
         """(k, gates after fusion, HBM passes, autotuner estimates in ms for k = 0..4) of the last

@@ -93,6 +93,63 @@ int prob_sum(const double2* s, ITYPE dim, ITYPE mask, ITYPE value, cudaStream_t 
     return prob_sum_t<double2>(s, dim, mask, value, st, out);
 }
 
+// Shannon entropy of the measurement distribution (stat_ops_probability.cpp:83-99): sum of -p log p,
+// p = |a_i|^2 clamped below at 1e-15.  Density matrix (stat_ops_dm.cpp:29-46): p = Re rho_ii taken at
+// stride dim + 1, terms with p <= 1e-15 skipped.
+template <bool DM>
+__global__ void __launch_bounds__(kRThreads) k_entropy(const double2* __restrict__ s, ITYPE count, ITYPE stride_elems,
+    double* __restrict__ part) {
+    __shared__ double sm[32];
+    const double eps = 1e-15;
+    double acc = 0.;
+    const ITYPE stride = (ITYPE)gridDim.x * kRThreads;
+    for (ITYPE i = (ITYPE)blockIdx.x * kRThreads + threadIdx.x; i < count; i += stride) {
+        const double2 v = s[i * stride_elems];
+        if (DM) {
+            const double p = v.x;
+            if (p > eps) acc += -1.0 * p * log(p);
+        } else {
+            double p = v.x * v.x + v.y * v.y;
+            p = (p > eps) ? p : eps;
+            acc += -1.0 * p * log(p);
+        }
+    }
+    acc = block_sum(acc, sm);
+    if (threadIdx.x == 0) part[blockIdx.x] = acc;
+}
+
+// Sum of Re rho_ii over the diagonal indices i with (i & mask) == value (stat_ops_dm.cpp:50-120:
+// dm_M0_prob, dm_M1_prob, dm_marginal_prob).
+__global__ void __launch_bounds__(kRThreads) k_dm_diag_sum(const double2* __restrict__ rho, ITYPE dim, ITYPE mask,
+    ITYPE value, double* __restrict__ part) {
+    __shared__ double sm[32];
+    double acc = 0.;
+    const ITYPE stride = (ITYPE)gridDim.x * kRThreads;
+    for (ITYPE i = (ITYPE)blockIdx.x * kRThreads + threadIdx.x; i < dim; i += stride)
+        if ((i & mask) == value) acc += rho[i * (dim + 1)].x;
+    acc = block_sum(acc, sm);
+    if (threadIdx.x == 0) part[blockIdx.x] = acc;
+}
+
+static int dm_diag_sum(const double2* rho, ITYPE dim, ITYPE mask, ITYPE value, cudaStream_t st, double* out) {
+    const unsigned blocks = reduce_blocks(dim);
+    void* buf;
+    QS_TRY(scratch(st, sizeof(double) * (blocks + 1), &buf));
+    k_dm_diag_sum<<<blocks, kRThreads, 0, st>>>(rho, dim, mask, value, (double*)buf);
+    QS_TRY(check_launch("k_dm_diag_sum"));
+    return finish_reduce((double*)buf, blocks, 1, st, out);
+}
+
+template <bool DM>
+static int entropy(const double2* s, ITYPE count, ITYPE stride_elems, cudaStream_t st, double* out) {
+    const unsigned blocks = reduce_blocks(count);
+    void* buf;
+    QS_TRY(scratch(st, sizeof(double) * (blocks + 1), &buf));
+    k_entropy<DM><<<blocks, kRThreads, 0, st>>>(s, count, stride_elems, (double*)buf);
+    QS_TRY(check_launch("k_entropy"));
+    return finish_reduce((double*)buf, blocks, 1, st, out);
+}
+
 // sum conj(bra_i) ket_i with a complex128 bra and a complex64 ket, FP64 accumulation
 __global__ void __launch_bounds__(kRThreads) k_inner_mixed(const double2* __restrict__ a, const float2* __restrict__ b,
     ITYPE dim, double* __restrict__ part) {
@@ -446,6 +503,47 @@ using namespace qs;
 
 extern "C" {
 
+QS_API int qs_measurement_distribution_entropy(const void* state, QS_ITYPE dim, void* stream, double* out) {
+    UINT n;
+    QS_TRY(check_dim(dim, &n));
+    if (!out) return set_error(QS_ERR_INVALID_ARGUMENT, "null output pointer");
+    return entropy<false>((const double2*)state, dim, 1, (cudaStream_t)stream, out);
+}
+QS_API int qs_dm_measurement_distribution_entropy(const void* rho, QS_ITYPE dim, void* stream, double* out) {
+    UINT n;
+    QS_TRY(check_dim(dim, &n));
+    if (n > 20) return set_error(QS_ERR_NOT_SUPPORTED, "density matrix: at most 20 qubits");
+    if (!out) return set_error(QS_ERR_INVALID_ARGUMENT, "null output pointer");
+    return entropy<true>((const double2*)rho, dim, dim + 1, (cudaStream_t)stream, out);
+}
+QS_API int qs_dm_M0_prob(QS_UINT t, const void* rho, QS_ITYPE dim, void* stream, double* out) {
+    UINT n;
+    QS_TRY(check_dim(dim, &n));
+    QS_TRY(check_target(t, n, "dm_M0_prob"));
+    if (!out) return set_error(QS_ERR_INVALID_ARGUMENT, "null output pointer");
+    return dm_diag_sum((const double2*)rho, dim, 1ULL << t, 0, (cudaStream_t)stream, out);
+}
+QS_API int qs_dm_M1_prob(QS_UINT t, const void* rho, QS_ITYPE dim, void* stream, double* out) {
+    UINT n;
+    QS_TRY(check_dim(dim, &n));
+    QS_TRY(check_target(t, n, "dm_M1_prob"));
+    if (!out) return set_error(QS_ERR_INVALID_ARGUMENT, "null output pointer");
+    return dm_diag_sum((const double2*)rho, dim, 1ULL << t, 1ULL << t, (cudaStream_t)stream, out);
+}
+QS_API int qs_dm_marginal_prob(const QS_UINT* targets, const QS_UINT* values, QS_UINT count, const void* rho,
+    QS_ITYPE dim, void* stream, double* out) {
+    UINT n;
+    QS_TRY(check_dim(dim, &n));
+    QS_TRY(check_distinct(targets, count, n, "dm_marginal_prob"));
+    if (!out || (count && !values)) return set_error(QS_ERR_INVALID_ARGUMENT, "null argument");
+    ITYPE mask = 0, value = 0;
+    for (UINT i = 0; i < count; ++i) {
+        mask |= 1ULL << targets[i];
+        if (values[i] > 1) return set_error(QS_ERR_INVALID_ARGUMENT, "dm_marginal_prob: measured value must be 0 or 1");
+        if (values[i]) value |= 1ULL << targets[i];
+    }
+    return dm_diag_sum((const double2*)rho, dim, mask, value, (cudaStream_t)stream, out);
+}
 QS_API int qs_state_norm_squared(const void* state, QS_ITYPE dim, void* stream, double* out) {
     UINT n;
     QS_TRY(check_dim(dim, &n));

@@ -41,8 +41,24 @@ class QuantumGateBase:
     def get_control_index_list(self):
         return list(self.controls)
 
+    def get_control_value_list(self):
+        return list(self.control_values)
+
+    def get_control_index_value_list(self):
+        return [[c, v] for c, v in zip(self.controls, self.control_values)]
+
     def get_name(self) -> str:
         return self.name
+
+    def is_diagonal(self) -> bool:
+        return self.kind in ("DIAGONAL", "RZ", "CZ") or (
+            self.kind in ("PAULI", "PAULI_ROTATION") and all(int(i) in (0, 3) for i in self._pauli_ids()))
+
+    def is_Pauli(self) -> bool:
+        return self.kind == "PAULI" or self.name in ("I", "X", "Y", "Z")
+
+    def is_parametric(self) -> bool:
+        return False
 
     def copy(self) -> "QuantumGateBase":
         g = QuantumGateBase(self.kind, self.targets, self.params.copy(), self.controls, self.control_values, self.name)
@@ -51,17 +67,89 @@ class QuantumGateBase:
     def add_control_qubit(self, qubit: int, control_value: int) -> None:
         if self.kind != "DENSE":
             raise NotImplementedError("controls can be added to DenseMatrix gates")
+        if int(qubit) in self.targets or int(qubit) in self.controls:
+            raise ValueError("control qubit is already a target or control of this gate")
         self.controls.append(int(qubit))
         self.control_values.append(int(control_value))
 
+    def multiply_scalar(self, value: complex) -> None:
+        """QuantumGateMatrix::multiply_scalar: matrix *= value (DenseMatrix / DiagonalMatrix gates)."""
+        if self.kind not in ("DENSE", "DIAGONAL"):
+            raise NotImplementedError("multiply_scalar is defined for matrix gates")
+        self.params = _cplx_params((self.params[0::2] + 1j * self.params[1::2]) * complex(value))
+
+    def _pauli_ids(self):
+        n = len(self.targets)
+        return [int(x) for x in self.params[:n]]
+
     def get_matrix(self) -> np.ndarray:
+        """The gate's matrix on its targets (bit j of the index <-> targets[j]); controlled gates give
+        the target matrix, as cppsim's set_matrix does (CNOT -> X, CZ -> Z)."""
         k = len(self.targets)
         if self.kind == "DENSE":
             md = 1 << k
-            return (self.params[0::2] + 1j * self.params[1::2]).reshape(md, md)
+            return (self.params[0::2] + 1j * self.params[1::2]).reshape(md, md).copy()
         if self.kind == "DIAGONAL":
             return np.diag(self.params[0::2] + 1j * self.params[1::2])
-        raise NotImplementedError(f"get_matrix for {self.kind}")
+        if self.kind in ("RX", "RY", "RZ"):
+            c, s = math.cos(self.params[0] / 2), math.sin(self.params[0] / 2)
+            return {"RX": np.array([[c, 1j * s], [1j * s, c]]), "RY": np.array([[c, s], [-s, c]]),
+                    "RZ": np.diag([c + 1j * s, c - 1j * s])}[self.kind]
+        if self.kind == "CNOT":
+            return _PAULI[1].copy()
+        if self.kind == "CZ":
+            return _PAULI[3].copy()
+        if self.kind == "SWAP":
+            return np.eye(4, dtype=np.complex128)[[0, 2, 1, 3]]
+        if self.kind in ("PAULI", "PAULI_ROTATION"):
+            m = np.ones((1, 1), dtype=np.complex128)
+            for pid in self._pauli_ids():  # targets[j] <-> bit j: later targets are the left factors
+                m = np.kron(_PAULI[pid], m)
+            if self.kind == "PAULI":
+                return m
+            a = self.params[k]
+            return math.cos(a / 2) * np.eye(m.shape[0]) + 1j * math.sin(a / 2) * m
+        raise NotImplementedError(f"get_matrix for {self.name}")
+
+    def get_inverse(self) -> "QuantumGateBase":
+        """cppsim get_inverse: named one-qubit gates map to their named inverses (gate_named_one.cpp:3-48),
+        rotations negate the angle (:51-62, gate_named_pauli.hpp:305), matrix gates take the adjoint
+        (gate_matrix.cpp:330), CNOT/CZ/SWAP/Pauli are their own inverses; projections and noise have none."""
+        if self.name in _NAMED_INVERSE:
+            return _NAMED_INVERSE[self.name](self.targets[0])
+        if self.name in ("Projection-0", "Projection-1"):
+            raise NotImplementedError("Projection gate hasn't inverse gate")
+        if self.kind in ("RX", "RY", "RZ"):
+            return QuantumGateBase(self.kind, self.targets, [-self.params[0]], name=self.name)
+        if self.kind == "PAULI_ROTATION":
+            p = self.params.copy()
+            p[-1] = -p[-1]
+            return QuantumGateBase(self.kind, self.targets, p, name=self.name)
+        if self.kind in ("CNOT", "CZ", "SWAP", "PAULI"):
+            return self.copy()
+        if self.kind == "DENSE":
+            g = self.copy()
+            g.params = _cplx_params(self.get_matrix().conj().T)
+            return g
+        if self.kind == "DIAGONAL":
+            g = self.copy()
+            g.params = _cplx_params((self.params[0::2] + 1j * self.params[1::2]).conj())
+            return g
+        raise NotImplementedError(f"Inverse of {self.name} gate is not Implemented")
+
+    def to_string(self) -> str:
+        """Debug text in cppsim's layout (gate.cpp:101-128); commutation flags are not tracked."""
+        yn = lambda b: "yes" if b else "no"  # noqa: E731
+        lines = [" *** gate info *** ", f" * gate name : {self.name}", " * target    : "]
+        lines += [f" {t} : commute       " for t in self.targets]
+        lines.append(" * control   : ")
+        lines += [f" {c} : value {v}" for c, v in zip(self.controls, self.control_values)]
+        lines += [f" * Pauli     : {yn(self.is_Pauli())}", " * Clifford  : no", " * Gaussian  : no",
+                  f" * Parametric: {yn(self.is_parametric())}", f" * Diagonal  : {yn(self.is_diagonal())}"]
+        return "\n".join(lines) + "\n"
+
+    def __str__(self) -> str:
+        return self.to_string()
 
     def _add_to(self, circuit_handle) -> None:
         t = _arr_u(self.targets)
@@ -120,65 +208,77 @@ def DiagonalMatrix(targets, diagonal) -> QuantumGateBase:
     return QuantumGateBase("DIAGONAL", targets, _cplx_params(d), name="DiagonalMatrix")
 
 
-# csim/constant.cpp:4-30
+def _named(gate: QuantumGateBase, name: str) -> QuantumGateBase:
+    gate.name = name
+    return gate
+
+
+# csim/constant.cpp:4-30; names as cppsim gate_named_one.hpp:87-323
 def X(t):
-    return DenseMatrix(t, [[0, 1], [1, 0]])
+    return _named(DenseMatrix(t, [[0, 1], [1, 0]]), "X")
 
 
 def Y(t):
-    return DenseMatrix(t, [[0, -1j], [1j, 0]])
+    return _named(DenseMatrix(t, [[0, -1j], [1j, 0]]), "Y")
 
 
 def Z(t):
-    return DiagonalMatrix(t, [1, -1])
+    return _named(DiagonalMatrix(t, [1, -1]), "Z")
 
 
 def H(t):
-    return DenseMatrix(t, [[_SQ2, _SQ2], [_SQ2, -_SQ2]])
+    return _named(DenseMatrix(t, [[_SQ2, _SQ2], [_SQ2, -_SQ2]]), "H")
 
 
 def S(t):
-    return DiagonalMatrix(t, [1, 1j])
+    return _named(DiagonalMatrix(t, [1, 1j]), "S")
 
 
 def Sdag(t):
-    return DiagonalMatrix(t, [1, -1j])
+    return _named(DiagonalMatrix(t, [1, -1j]), "Sdag")
 
 
 def T(t):
-    return DiagonalMatrix(t, [1, (1 + 1j) * _SQ2])
+    return _named(DiagonalMatrix(t, [1, (1 + 1j) * _SQ2]), "T")
 
 
 def Tdag(t):
-    return DiagonalMatrix(t, [1, (1 - 1j) * _SQ2])
+    return _named(DiagonalMatrix(t, [1, (1 - 1j) * _SQ2]), "Tdag")
 
 
 def sqrtX(t):
-    return DenseMatrix(t, [[0.5 + 0.5j, 0.5 - 0.5j], [0.5 - 0.5j, 0.5 + 0.5j]])
+    return _named(DenseMatrix(t, [[0.5 + 0.5j, 0.5 - 0.5j], [0.5 - 0.5j, 0.5 + 0.5j]]), "sqrtX")
 
 
 def sqrtXdag(t):
-    return DenseMatrix(t, [[0.5 - 0.5j, 0.5 + 0.5j], [0.5 + 0.5j, 0.5 - 0.5j]])
+    return _named(DenseMatrix(t, [[0.5 - 0.5j, 0.5 + 0.5j], [0.5 + 0.5j, 0.5 - 0.5j]]), "sqrtXdag")
 
 
 def sqrtY(t):
-    return DenseMatrix(t, [[0.5 + 0.5j, -0.5 - 0.5j], [0.5 + 0.5j, 0.5 + 0.5j]])
+    return _named(DenseMatrix(t, [[0.5 + 0.5j, -0.5 - 0.5j], [0.5 + 0.5j, 0.5 + 0.5j]]), "sqrtY")
 
 
 def sqrtYdag(t):
-    return DenseMatrix(t, [[0.5 - 0.5j, 0.5 - 0.5j], [-0.5 + 0.5j, 0.5 - 0.5j]])
+    return _named(DenseMatrix(t, [[0.5 - 0.5j, 0.5 - 0.5j], [-0.5 + 0.5j, 0.5 - 0.5j]]), "sqrtYdag")
 
 
 def P0(t):
-    return DiagonalMatrix(t, [1, 0])
+    return _named(DiagonalMatrix(t, [1, 0]), "Projection-0")
 
 
 def P1(t):
-    return DiagonalMatrix(t, [0, 1])
+    return _named(DiagonalMatrix(t, [0, 1]), "Projection-1")
 
 
 def Identity(t):
-    return DiagonalMatrix(t, [1, 1])
+    return _named(DiagonalMatrix(t, [1, 1]), "I")
+
+
+_PAULI = [np.eye(2, dtype=np.complex128), np.array([[0, 1], [1, 0]], dtype=np.complex128),
+          np.array([[0, -1j], [1j, 0]]), np.diag([1.0 + 0j, -1.0])]
+
+_NAMED_INVERSE = {"I": Identity, "X": X, "Y": Y, "Z": Z, "H": H, "S": Sdag, "Sdag": S, "T": Tdag, "Tdag": T,
+                  "sqrtX": sqrtXdag, "sqrtXdag": sqrtX, "sqrtY": sqrtYdag, "sqrtYdag": sqrtY}
 
 
 def RX(t, angle):
@@ -245,21 +345,53 @@ def SWAP(a, b):
     return QuantumGateBase("SWAP", [a, b], name="SWAP")
 
 
+def _check_pauli(targets, pauli_ids):
+    if len(targets) != len(pauli_ids):
+        raise ValueError("target list and Pauli id list differ in length")
+    if len(set(int(t) for t in targets)) != len(targets):
+        raise ValueError("target list contains duplicated values")
+    if any(int(i) > 3 for i in pauli_ids):
+        raise ValueError("Pauli ids must be 0..3 (I, X, Y, Z)")
+
+
 def Pauli(targets, pauli_ids):
+    """cppsim gate::Pauli (gate_factory.cpp:255-266): the product of pauli_ids[j] on targets[j]."""
+    _check_pauli(targets, pauli_ids)
     return QuantumGateBase("PAULI", targets, list(pauli_ids), name="Pauli")
 
 
 def PauliRotation(targets, pauli_ids, angle):
-    return QuantumGateBase("PAULI_ROTATION", targets, list(pauli_ids) + [angle], name="PauliRotation")
+    """cppsim gate::PauliRotation (gate_factory.cpp:267-280): exp(+i angle P / 2)."""
+    _check_pauli(targets, pauli_ids)
+    return QuantumGateBase("PAULI_ROTATION", targets, list(pauli_ids) + [angle], name="Pauli-rotation")
+
+
+def RandomUnitary(targets, seed: int | None = None) -> QuantumGateBase:
+    """cppsim gate::RandomUnitary (gate_factory.cpp:322-380): a Haar-random dense matrix on ``targets``;
+    with a seed, the reference's matrix for that seed (same mt19937_64 normal draws, same QR phase
+    convention)."""
+    if isinstance(targets, (int, np.integer)):
+        targets = [int(targets)]
+    targets = [int(t) for t in targets]
+    if len(set(targets)) != len(targets):
+        raise ValueError("RandomUnitary: target list contains duplicated values")
+    if seed is None:
+        seed = int(np.random.SeedSequence().entropy & 0xFFFFFFFF)
+    k = len(targets)
+    m = np.zeros(2 * 4 ** k)
+    _lib.load()
+    call("qs_random_unitary_matrix", k, int(seed) & 0xFFFFFFFF, m.ctypes.data_as(C.c_void_p))
+    return DenseMatrix(targets, m.view(np.complex128).reshape(1 << k, 1 << k))
 
 
 def DepolarizingNoise(t, prob):
-    """cppsim gate_factory.cpp:456-466 (exact channel on a DensityMatrix)."""
-    return QuantumGateBase("DEPOLARIZING", [t], [prob], name="DepolarizingNoise")
+    """cppsim gate_factory.cpp:456-466 (exact channel on a DensityMatrix; sampled by NoiseSimulator).
+    Named "Probabilistic" like the reference's QuantumGate_Probabilistic."""
+    return QuantumGateBase("DEPOLARIZING", [t], [prob], name="Probabilistic")
 
 
 def TwoQubitDepolarizingNoise(t1, t2, prob):
-    """cppsim gate_factory.cpp:471-500 (exact channel on a DensityMatrix)."""
+    """cppsim gate_factory.cpp:471-500 (exact channel on a DensityMatrix; sampled by NoiseSimulator)."""
     if t1 == t2:
         raise ValueError("TwoQubitDepolarizingNoise: duplicated qubit")
-    return QuantumGateBase("DEPOLARIZING", [t1, t2], [prob], name="TwoQubitDepolarizingNoise")
+    return QuantumGateBase("DEPOLARIZING", [t1, t2], [prob], name="Probabilistic")

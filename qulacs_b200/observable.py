@@ -16,17 +16,23 @@ _PAULI = {"I": 0, "X": 1, "Y": 2, "Z": 3}
 
 
 def _parse(pauli_string: str):
+    """"X 0 Y 3 ..." -> (targets, ids); identity factors are dropped, as pauli_operator.cpp:17-47 does."""
     toks = pauli_string.split()
     if len(toks) % 2:
-        raise ValueError(f"bad Pauli string {pauli_string!r}")
+        raise ValueError(f"Detected pauli_str without indices: {pauli_string!r}")
     tl, ids = [], []
     for i in range(0, len(toks), 2):
         p = toks[i].upper()
         if p not in _PAULI:
-            raise ValueError(f"bad Pauli symbol {toks[i]!r}")
-        tl.append(int(toks[i + 1]))
-        ids.append(_PAULI[p])
+            raise ValueError(f"invalid Pauli string is given : {toks[i]!r}")
+        if _PAULI[p]:
+            tl.append(int(toks[i + 1]))
+            ids.append(_PAULI[p])
     return tl, ids
+
+
+def _u32(seq) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(seq, dtype=np.uint32))
 
 
 def masks(targets, ids):
@@ -61,11 +67,46 @@ class PauliOperator:
     def get_coef(self) -> complex:
         return self.coef
 
+    def change_coef(self, coef: complex) -> None:
+        self.coef = complex(coef)
+
     def get_index_list(self):
         return list(self.targets)
 
     def get_pauli_id_list(self):
         return list(self.ids)
+
+    def get_qubit_count(self) -> int:
+        return max(self.targets, default=-1) + 1
+
+    def add_single_Pauli(self, index: int, pauli_id: int) -> None:
+        """pauli_operator.cpp:116-130."""
+        if not 0 <= int(pauli_id) <= 3:
+            raise ValueError("Pauli id must be 0..3")
+        if int(index) in self.targets:
+            raise ValueError("duplicated qubit in Pauli operator")
+        self.targets.append(int(index))
+        self.ids.append(int(pauli_id))
+
+    def get_pauli_string(self) -> str:
+        """"X 0 Y 3" (pauli_operator.cpp:264-286); identity factors are left out."""
+        return " ".join(f"{'IXYZ'[p]} {t}" for t, p in zip(self.targets, self.ids) if p)
+
+    def copy(self) -> "PauliOperator":
+        return PauliOperator(coef=self.coef, targets=self.targets, pauli_ids=self.ids)
+
+    def get_transition_amplitude(self, state_bra, state_ket) -> complex:
+        """coef * <bra|P|ket> (pauli_operator.cpp:225-262)."""
+        if not (state_bra.is_state_vector() and state_ket.is_state_vector()):
+            raise NotImplementedError("get_transition_amplitude for density matrix is not implemented")
+        if state_bra.dim != state_ket.dim:
+            raise ValueError("bra and ket differ in qubit count")
+        tl, ids = _u32(self.targets), _u32(self.ids)
+        out = np.zeros(2)
+        call("qs_transition_amplitude_multi_qubit_Pauli_operator_partial_list", tl.ctypes.data_as(C.c_void_p),
+             ids.ctypes.data_as(C.c_void_p), tl.size, state_bra.data_ptr(), state_ket.data_ptr(), state_ket.dim,
+             state_ket.stream, out.ctypes.data_as(C.c_void_p))
+        return self.coef * complex(out[0], out[1])
 
     def get_expectation_value(self, state) -> complex:
         """coef * <P> (pauli_operator.cpp:132-183)."""
@@ -90,11 +131,57 @@ class Observable:
             raise ValueError("Pauli operator acts on a qubit beyond the observable's qubit count")
         self.terms.append(op)
 
+    add_operator_copy = add_operator
+    add_operator_move = add_operator
+
+    def add_random_operator(self, operator_count: int, seed: int | None = None) -> None:
+        """general_quantum_operator.cpp:179-202: terms with a Pauli on every qubit and a real coefficient
+        in [-1, 1); with a seed, the reference's terms for that seed."""
+        if seed is None:
+            seed = int(np.random.SeedSequence().entropy & 0xFFFFFFFF)
+        n, k = self.qubit_count, int(operator_count)
+        ids = np.zeros(max(n * k, 1), dtype=np.uint32)
+        coefs = np.zeros(max(k, 1))
+        call("qs_random_operator_terms", n, k, int(seed) & 0xFFFFFFFF, ids.ctypes.data_as(C.c_void_p),
+             coefs.ctypes.data_as(C.c_void_p))
+        for t in range(k):
+            row = [int(x) for x in ids[t * n:(t + 1) * n]]
+            self.terms.append(PauliOperator(coef=coefs[t], targets=[q for q in range(n) if row[q]],
+                                            pauli_ids=[p for p in row if p]))
+
     def get_term_count(self) -> int:
         return len(self.terms)
 
+    def get_term(self, index: int) -> PauliOperator:
+        if not 0 <= index < len(self.terms):
+            raise IndexError("index out of range")
+        return self.terms[index].copy()
+
     def get_qubit_count(self) -> int:
         return self.qubit_count
+
+    def get_state_dim(self) -> int:
+        return 1 << self.qubit_count
+
+    def get_transition_amplitude(self, state_bra, state_ket) -> complex:
+        """sum_k coef_k <bra|P_k|ket> (general_quantum_operator.cpp:160-177)."""
+        if self.qubit_count > state_bra.get_qubit_count() or state_bra.dim != state_ket.dim:
+            raise ValueError("invalid qubit count")
+        return sum((t.get_transition_amplitude(state_bra, state_ket) for t in self.terms), 0j)
+
+    def apply_to_state(self, work_state, state_to_be_multiplied, dst_state) -> None:
+        """dst = sum_k coef_k P_k |state> (general_quantum_operator.cpp:330-348), through a work state."""
+        if state_to_be_multiplied.get_qubit_count() != dst_state.get_qubit_count():
+            raise ValueError("Qubit count of state_to_be_multiplied and dst_state must be the same")
+        dst_state.set_zero_norm_state()
+        for t in self.terms:
+            work_state.load(state_to_be_multiplied)
+            if t.targets:
+                tl, ids = _u32(t.targets), _u32(t.ids)
+                call("qs_multi_qubit_Pauli_gate_partial_list", tl.ctypes.data_as(C.c_void_p),
+                     ids.ctypes.data_as(C.c_void_p), tl.size, work_state.data_ptr(), work_state.dim,
+                     work_state.stream)
+            dst_state.add_state_with_coef(t.coef, work_state)
 
     def term_values(self, state) -> np.ndarray:
         """<P_k> for every term (real), one batched device call for a state vector."""
@@ -122,3 +209,5 @@ class Observable:
         vals = self.term_values(state)
         coefs = np.array([t.coef for t in self.terms], dtype=np.complex128)
         return float(np.real(np.sum(coefs * vals)))
+
+    get_expectation_value_single_thread = get_expectation_value

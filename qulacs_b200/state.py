@@ -30,6 +30,24 @@ def _ptr(a: np.ndarray):
     return a.ctypes.data_as(C.c_void_p)
 
 
+def _coef(c) -> np.ndarray:
+    c = complex(c)
+    return np.array([c.real, c.imag])
+
+
+def _random_seed() -> int:
+    """A fresh 32-bit seed, for calls that take an optional one (the reference draws it from its Random)."""
+    return int(np.random.SeedSequence().entropy & 0xFFFFFFFF)
+
+
+def _marginal_lists(measured_values, qubit_count: int):
+    """Qulacs convention: a list of length n with 0, 1 or 2 (2 = not measured)."""
+    if len(measured_values) != qubit_count:
+        raise ValueError("the length of measured_values must be equal to qubit_count")
+    tl = [i for i, v in enumerate(measured_values) if v in (0, 1)]
+    return _u(tl), _u([measured_values[i] for i in tl])
+
+
 class QuantumState:
     """n-qubit complex128 state vector in HBM (cppsim QuantumStateGpu semantics)."""
 
@@ -37,6 +55,7 @@ class QuantumState:
         _lib.load()
         if qubit_count < 1:
             raise ValueError("qubit_count must be >= 1")
+        self.classical_register: list = []
         self.qubit_count = int(qubit_count)
         self.dim = 1 << self.qubit_count
         self.stream = _default_stream if stream is None else stream
@@ -65,11 +84,30 @@ class QuantumState:
     def set_computational_basis(self, basis: int) -> None:
         call("qs_set_computational_basis", int(basis), self._ptr, self.dim, self.stream)
 
+    def set_zero_norm_state(self) -> None:
+        """All amplitudes 0 (cppsim/state.hpp:484-487)."""
+        self.set_zero_state()
+        self.multiply_coef(0.0)
+
+    def set_Haar_random_state(self, seed: int | None = None) -> None:
+        """Haar-random pure state (cppsim/state.hpp:520-540): independent complex Gaussian amplitudes,
+        normalised.  A seed gives the same state on every run; the values are not the reference's (its
+        Gaussians come from its own Random), only the distribution is."""
+        if seed is None:
+            seed = _random_seed()
+        call("qs_initialize_Haar_random_state_with_seed", self._ptr, self.dim, int(seed) & 0xFFFFFFFF, self.stream)
+
     def load(self, src) -> None:
+        """From another state vector (device copy, classical register included) or host amplitudes
+        (cppsim/state.hpp:700-760)."""
+        if isinstance(src, DensityMatrix):
+            raise TypeError("cannot load DensityMatrix to StateVector")
         if isinstance(src, QuantumState):
-            if src.dim != self.dim:
-                raise ValueError("dimension mismatch")
-            src = src.get_vector()
+            if src.qubit_count != self.qubit_count:
+                raise ValueError("invalid qubit count")
+            call("qs_copy_state", src._ptr, self._ptr, self.dim, self.stream)
+            self.classical_register = list(src.classical_register)
+            return
         v = np.ascontiguousarray(np.asarray(src, dtype=np.complex128))
         if v.size != self.dim:
             raise ValueError(f"expected {self.dim} amplitudes, got {v.size}")
@@ -81,10 +119,78 @@ class QuantumState:
         call("qs_get_state", self._ptr, _ptr(out), self.dim, self.stream)
         return out
 
+    def get_amplitude(self, index: int) -> complex:
+        out = np.zeros(2)
+        call("qs_get_amplitude", self._ptr, self.dim, int(index), _ptr(out), self.stream)
+        return complex(out[0], out[1])
+
+    def allocate_buffer(self) -> "QuantumState":
+        """A new |0...0> state of the same size (cppsim/state.hpp:670-682)."""
+        return QuantumState(self.qubit_count, self.stream)
+
     def copy(self) -> "QuantumState":
-        s = QuantumState(self.qubit_count, self.stream)
+        """Deep copy on the device, classical register included (cppsim/state.hpp:688-697)."""
+        s = self.allocate_buffer()
         s.load(self)
         return s
+
+    # --- whole-state arithmetic (csim update_ops_named_state.cpp) ---
+    def _other(self, state, what) -> "QuantumState":
+        if not isinstance(state, QuantumState):
+            raise TypeError(f"{what}: cannot add DensityMatrix to StateVector")
+        if state.dim != self.dim:
+            raise ValueError(f"{what}: invalid qubit count")
+        return state
+
+    def add_state(self, state: "QuantumState") -> None:
+        """self += state (cppsim/state.hpp:825-836)."""
+        call("qs_state_add", self._other(state, "add_state")._ptr, self._ptr, self.dim, self.stream)
+
+    def add_state_with_coef(self, coef: complex, state: "QuantumState") -> None:
+        """self += coef * state (cppsim/state.hpp:841-856)."""
+        c = _coef(coef)
+        call("qs_state_add_with_coef", _ptr(c), self._other(state, "add_state_with_coef")._ptr, self._ptr,
+             self.dim, self.stream)
+
+    def multiply_coef(self, coef: complex) -> None:
+        c = _coef(coef)
+        call("qs_state_multiply", _ptr(c), self._ptr, self.dim, self.stream)
+
+    def normalize(self, squared_norm: float) -> None:
+        """Amplitudes *= 1 / sqrt(squared_norm) (csim update_ops_named_state.cpp:21-30)."""
+        call("qs_normalize", float(squared_norm), self._ptr, self.dim, self.stream)
+
+    def multiply_elementwise_function(self, func) -> None:
+        """amplitude[i] *= func(i): the values are tabulated on the host, then multiplied in on the
+        device (cppsim/state.hpp:885-891)."""
+        f = np.fromiter((complex(func(i)) for i in range(self.dim)), dtype=np.complex128, count=self.dim)
+        tmp = QuantumState(self.qubit_count, self.stream)
+        tmp.load(f)
+        call("qs_state_multiply_elementwise", tmp._ptr, self._ptr, self.dim, self.stream)
+        call("qs_stream_synchronize", self.stream)
+
+    # --- classical register (cppsim/state.hpp:313-340) ---
+    def get_classical_value(self, index: int) -> int:
+        if len(self.classical_register) <= index:
+            self.classical_register.extend([0] * (index + 1 - len(self.classical_register)))
+        return self.classical_register[index]
+
+    def set_classical_value(self, index: int, value: int) -> None:
+        if len(self.classical_register) <= index:
+            self.classical_register.extend([0] * (index + 1 - len(self.classical_register)))
+        self.classical_register[index] = int(value)
+
+    def get_classical_register(self) -> list:
+        return list(self.classical_register)
+
+    def to_string(self) -> str:
+        """Debug text in cppsim's layout (cppsim/state.hpp:365-392)."""
+        body = "\n".join(f"({a.real:g},{a.imag:g})" for a in self.get_vector())
+        return (f" *** Quantum State ***\n * Qubit Count : {self.qubit_count}\n * Dimension   : {self.dim}\n"
+                f" * State vector : \n{body}\n")
+
+    def __str__(self) -> str:
+        return self.to_string()
 
     # --- statistics (csim stat_ops) ---
     def get_squared_norm(self) -> float:
@@ -97,19 +203,23 @@ class QuantumState:
         call("qs_M0_prob", int(target), self._ptr, self.dim, self.stream, C.byref(out))
         return out.value
 
+    def get_entropy(self) -> float:
+        """Shannon entropy of the computational-basis distribution (csim stat_ops_probability.cpp:83-99)."""
+        out = C.c_double()
+        call("qs_measurement_distribution_entropy", self._ptr, self.dim, self.stream, C.byref(out))
+        return out.value
+
     def get_marginal_probability(self, measured_values) -> float:
         """Qulacs convention: a list of length n with 0, 1 or 2 (2 = not measured)."""
-        tl = [i for i, v in enumerate(measured_values) if v in (0, 1)]
-        vals = [measured_values[i] for i in tl]
+        t, v = _marginal_lists(measured_values, self.qubit_count)
         out = C.c_double()
-        t, v = _u(tl), _u(vals)
-        call("qs_marginal_prob", _ptr(t), _ptr(v), len(tl), self._ptr, self.dim, self.stream, C.byref(out))
+        call("qs_marginal_prob", _ptr(t), _ptr(v), t.size, self._ptr, self.dim, self.stream, C.byref(out))
         return out.value
 
     def sampling(self, sampling_count: int, random_seed: int | None = None) -> list:
         """cppsim QuantumStateCpu::sampling (cppsim/state.hpp:899-992): mt19937_64 draws."""
         if random_seed is None:
-            random_seed = int(np.random.SeedSequence().entropy & 0xFFFFFFFF)
+            random_seed = _random_seed()
         out = np.empty(sampling_count, dtype=np.uint64)
         call("qs_state_sampling", self._ptr, self.dim, int(sampling_count), int(random_seed) & 0xFFFFFFFF,
              _ptr(out), self.stream)
@@ -231,6 +341,7 @@ class DensityMatrix:
         self.qubit_count = int(qubit_count)
         self.dim = 1 << self.qubit_count
         self.stream = _default_stream if stream is None else stream
+        self.classical_register: list = []
         p = C.c_void_p()
         call("qs_dm_allocate", self.dim, C.byref(p))
         self._ptr = p.value
@@ -251,9 +362,47 @@ class DensityMatrix:
     def set_zero_state(self) -> None:
         call("qs_dm_initialize_quantum_state", self._ptr, self.dim, self.stream)
 
+    def set_zero_norm_state(self) -> None:
+        """The zero matrix (cppsim/state_dm.hpp:41-44)."""
+        self.set_zero_state()
+        self.multiply_coef(0.0)
+
+    def set_computational_basis(self, basis: int) -> None:
+        """|basis><basis| (cppsim/state_dm.hpp:51-61): entry basis * dim + basis of the dim^2 vector."""
+        if not 0 <= int(basis) < self.dim:
+            raise IndexError("index of computational basis must be smaller than 2^qubit_count")
+        b = int(basis)
+        call("qs_set_computational_basis", b * self.dim + b, self._ptr, self.dim * self.dim, self.stream)
+
+    def set_Haar_random_state(self, seed: int | None = None) -> None:
+        """|psi><psi| of a Haar-random pure state (cppsim/state_dm.hpp:66-80)."""
+        pure = QuantumState(self.qubit_count, self.stream)
+        pure.set_Haar_random_state(seed)
+        call("qs_dm_initialize_with_pure_state", self._ptr, pure.data_ptr(), self.dim, self.stream)
+        call("qs_stream_synchronize", self.stream)
+
+    def allocate_buffer(self) -> "DensityMatrix":
+        return DensityMatrix(self.qubit_count, self.stream)
+
+    def copy(self) -> "DensityMatrix":
+        d = self.allocate_buffer()
+        d.load(self)
+        return d
+
     def load(self, src) -> None:
+        """From a state vector (|psi><psi|), another density matrix (device copy), a host vector or a
+        host dim x dim matrix (cppsim/state_dm.hpp:199-281)."""
+        if isinstance(src, DensityMatrix):
+            if src.qubit_count != self.qubit_count:
+                raise ValueError("invalid qubit count")
+            call("qs_copy_state", src._ptr, self._ptr, self.dim * self.dim, self.stream)
+            self.classical_register = list(src.classical_register)
+            return
         if isinstance(src, QuantumState):
+            if src.qubit_count != self.qubit_count:
+                raise ValueError("invalid qubit count")
             call("qs_dm_initialize_with_pure_state", self._ptr, src.data_ptr(), self.dim, self.stream)
+            self.classical_register = list(src.classical_register)
             return
         m = np.ascontiguousarray(np.asarray(src, dtype=np.complex128))
         if m.ndim == 1:
@@ -273,11 +422,83 @@ class DensityMatrix:
         call("qs_dm_state_norm_squared", self._ptr, self.dim, self.stream, C.byref(out))
         return out.value
 
+    def get_zero_probability(self, target: int) -> float:
+        if not 0 <= int(target) < self.qubit_count:
+            raise IndexError("index of target qubit must be smaller than qubit_count")
+        out = C.c_double()
+        call("qs_dm_M0_prob", int(target), self._ptr, self.dim, self.stream, C.byref(out))
+        return out.value
+
+    def get_marginal_probability(self, measured_values) -> float:
+        t, v = _marginal_lists(measured_values, self.qubit_count)
+        out = C.c_double()
+        call("qs_dm_marginal_prob", _ptr(t), _ptr(v), t.size, self._ptr, self.dim, self.stream, C.byref(out))
+        return out.value
+
+    def get_entropy(self) -> float:
+        out = C.c_double()
+        call("qs_dm_measurement_distribution_entropy", self._ptr, self.dim, self.stream, C.byref(out))
+        return out.value
+
+    def normalize(self, squared_norm: float) -> None:
+        """rho *= 1 / squared_norm (csim update_ops_dm.cpp:14-28)."""
+        call("qs_dm_normalize", float(squared_norm), self._ptr, self.dim, self.stream)
+
+    def _other(self, state, what) -> "DensityMatrix":
+        if not isinstance(state, DensityMatrix):
+            raise TypeError(f"{what}: a state vector cannot be added to a DensityMatrix")
+        if state.dim != self.dim:
+            raise ValueError(f"{what}: invalid qubit count")
+        return state
+
+    def add_state(self, state: "DensityMatrix") -> None:
+        call("qs_dm_state_add", self._other(state, "add_state")._ptr, self._ptr, self.dim, self.stream)
+
+    def add_state_with_coef(self, coef: complex, state: "DensityMatrix") -> None:
+        c = _coef(coef)
+        call("qs_dm_state_add_with_coef", _ptr(c), self._other(state, "add_state_with_coef")._ptr, self._ptr,
+             self.dim, self.stream)
+
+    def multiply_coef(self, coef: complex) -> None:
+        c = _coef(coef)
+        call("qs_dm_state_multiply", _ptr(c), self._ptr, self.dim, self.stream)
+
+    def multiply_elementwise_function(self, func) -> None:
+        raise NotImplementedError("multiply_elementwise_function is not defined for DensityMatrix")
+
+    def sampling(self, sampling_count: int, random_seed: int | None = None) -> list:
+        """DensityMatrixCpu::sampling (cppsim/state_dm.hpp:383-407): mt19937_64(seed) uniforms over the
+        diagonal's prefix sums."""
+        if random_seed is None:
+            random_seed = _random_seed()
+        u = np.empty(int(sampling_count), dtype=np.float64)
+        call("qs_reference_uniforms", int(random_seed) & 0xFFFFFFFF, u.size, _ptr(u))
+        return [int(x) for x in self.sampling_with_uniforms(u)]
+
     def sampling_with_uniforms(self, uniforms) -> np.ndarray:
         u = np.ascontiguousarray(np.asarray(uniforms, dtype=np.float64))
         out = np.empty(u.size, dtype=np.uint64)
         call("qs_dm_sampling_with_uniforms", self._ptr, self.dim, _ptr(u), u.size, _ptr(out), self.stream)
         return out
+
+    def get_classical_value(self, index: int) -> int:
+        return QuantumState.get_classical_value(self, index)
+
+    def set_classical_value(self, index: int, value: int) -> None:
+        QuantumState.set_classical_value(self, index, value)
+
+    def get_classical_register(self) -> list:
+        return list(self.classical_register)
+
+    def to_string(self) -> str:
+        """Debug text in cppsim's layout (cppsim/state_dm.hpp:409-422)."""
+        m = self.get_matrix()
+        body = "\n".join(" ".join(f"({a.real:g},{a.imag:g})" for a in row) for row in m)
+        return (f" *** Density Matrix ***\n * Qubit Count : {self.qubit_count}\n * Dimension   : {self.dim}\n"
+                f" * Density matrix : \n{body}\n")
+
+    def __str__(self) -> str:
+        return self.to_string()
 
     def __del__(self):
         p = getattr(self, "_ptr", None)

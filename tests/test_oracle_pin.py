@@ -135,6 +135,37 @@ def test_density_matrix_ops(port, ref):
     assert np.array_equal(port.dm_sampling_with_uniforms(rho, u), ref.dm_sampling_with_uniforms(rho, u))
 
 
+def test_state_arithmetic_and_entropy(port, ref):
+    rng = np.random.default_rng(61)
+    s, s2 = random_state(8, rng), random_state(8, rng)
+    for fn, args in [("state_add_with_coef", (0.3 - 1.1j, s2)), ("state_multiply", (-0.2 + 0.7j,)),
+                     ("normalize", (2.5,))]:
+        a, b = _both(port, ref, fn, s, *args)
+        assert np.max(np.abs(a - b)) <= PIN_TOL, fn
+    sparse = s.copy()
+    sparse[::3] = 0  # entries below the 1e-15 clamp
+    for v in (s, sparse):
+        assert abs(port.measurement_distribution_entropy(v) - ref.measurement_distribution_entropy(v)) <= 1e-13
+    rho = random_density_matrix(4, rng)
+    assert abs(port.dm_measurement_distribution_entropy(rho) - ref.dm_measurement_distribution_entropy(rho)) <= 1e-13
+    a, b = rho.copy(), rho.copy()
+    port.dm_normalize(1.7, a)
+    ref.dm_normalize(1.7, b)
+    assert np.max(np.abs(a - b)) <= PIN_TOL
+
+
+def test_dm_probabilities(port, ref):
+    rng = np.random.default_rng(71)
+    n = 5
+    rho = random_density_matrix(n, rng)
+    for t in range(n):
+        assert abs(port.dm_M0_prob(t, rho) - ref.dm_M0_prob(t, rho)) <= 1e-14
+        assert abs(port.dm_M1_prob(t, rho) - ref.dm_M1_prob(t, rho)) <= 1e-14
+        assert abs(port.dm_M0_prob(t, rho) + port.dm_M1_prob(t, rho) - 1.0) <= 1e-13
+    for tl, vals in [([0, 3], [1, 0]), ([1, 2, 4], [1, 1, 0]), ([4], [1])]:
+        assert abs(port.dm_marginal_prob(tl, vals, rho) - ref.dm_marginal_prob(tl, vals, rho)) <= 1e-14
+
+
 # ---- known-answer tests restated from the reference's own test suite ----
 
 def test_kat_sampling_computational_basis(port):
