@@ -15,6 +15,7 @@
 #include <cmath>
 #include <complex>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "circuit.hpp"
@@ -22,10 +23,12 @@
 
 namespace qs {
 
-constexpr int kLowFixed = 4;      // qubits 0..3 always belong to a tile
-constexpr int kTileBits = 11;     // 2^11 amplitudes = 32 KiB of shared memory per CTA
-constexpr int kStThreads = 128;   // 2^11 / 16 amplitudes per thread
-constexpr int kPhaseBits = 4;     // 16 amplitudes in registers per thread
+constexpr int kLowFixed = 4;        // qubits 0..3 always belong to a tile
+constexpr int kTileBits = 12;       // pass kernel: 2^12 amplitudes = 64 KiB of shared memory per CTA
+constexpr int kBatchTileBits = 11;  // multi-circuit kernel: 2^11 amplitudes = 32 KiB (its persistent loop
+                                    // spills twice as much with the 12-bit tile code)
+constexpr int kStThreads = 128;     // 16 (m = 11) or 32 (m = 12) amplitudes per thread; 1 or 2 cosets per phase
+constexpr int kPhaseBits = 4;       // 16 amplitudes in registers per thread
 
 enum StKind : uint8_t { ST_DENSE1 = 0, ST_DIAG1, ST_RX, ST_RY, ST_CNOT, ST_CZ, ST_SWAP, ST_DENSE2 };
 
@@ -175,27 +178,46 @@ __device__ __forceinline__ void apply_op(const StOp& op, double2 (&r)[16], const
 // so swz(a | b) = swz(a) ^ swz(b) for disjoint bit sets).
 __device__ __forceinline__ UINT swz(UINT u) { return u ^ (((u >> 4) ^ (u >> 7) ^ (u >> 10)) & 7u); }
 
-struct StSmem {
-    double2 tile[1 << kTileBits];
-    ITYPE hi_off[16];
-    UINT s_off[16];
-};
+// Tile index u = tid + k * kStThreads (k < 2^(m-7)) has global offset base | lo_off | hi_off[k]:
+// lo_off takes tid's bits 0..6 to the tile qubits q[0..6], hi_off[k] takes k's bits to q[7..].
+
+// Global rows of 16 amplitudes per thread between HBM and the swizzled tile (rows k0 .. k0 + 15).
+__device__ __forceinline__ void tile_rows_load(const double2* __restrict__ s, double2* tile, ITYPE off,
+    const ITYPE* hi_off, UINT tsize, int k0) {
+    const UINT tid = threadIdx.x;
+    double2 v[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k)
+        if (tid + (UINT)(k0 + k) * kStThreads < tsize) v[k] = ld_stream(s + (off | hi_off[k0 + k]));
+#pragma unroll
+    for (int k = 0; k < 16; ++k)
+        if (tid + (UINT)(k0 + k) * kStThreads < tsize) tile[swz(tid + (UINT)(k0 + k) * kStThreads)] = v[k];
+}
+__device__ __forceinline__ void tile_rows_store(double2* __restrict__ s, const double2* tile, ITYPE off,
+    const ITYPE* hi_off, UINT tsize, int k0) {
+    const UINT tid = threadIdx.x;
+    double2 v[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k)
+        if (tid + (UINT)(k0 + k) * kStThreads < tsize) v[k] = tile[swz(tid + (UINT)(k0 + k) * kStThreads)];
+#pragma unroll
+    for (int k = 0; k < 16; ++k)
+        if (tid + (UINT)(k0 + k) * kStThreads < tsize) st_stream(s + (off | hi_off[k0 + k]), v[k]);
+}
 
 // One tile of one pass: load, apply every phase, store.  Shared by the per-pass kernel and the
-// persistent multi-circuit kernel (batch.cu).  Ends with a CTA barrier so the shared buffers can be
-// reused immediately.
-__device__ __forceinline__ void staged_tile(double2* __restrict__ s, const StPassArgs& a, ITYPE T, StSmem& sm) {
-    double2* tile = sm.tile;
-    ITYPE* hi_off = sm.hi_off;
-    UINT* s_off = sm.s_off;
+// persistent multi-circuit kernel.  `tile` holds 2^m amplitudes (m <= kTileBits).  Ends with a CTA
+// barrier so the shared buffers can be reused immediately.
+template <int MAX_BITS>
+__device__ __forceinline__ void staged_tile(double2* __restrict__ s, const StPassArgs& a, ITYPE T, double2* tile,
+    ITYPE* hi_off) {
     const int m = a.m;
     const UINT tsize = 1u << m;
     // base: insert zeros at the tile qubits into the tile index
     ITYPE base = T;
     for (int j = 0; j < m; ++j) base = insert0(base, a.q[j]);
-    // global offset of tile index u = tid + k * kStThreads: low part from tid (bits 0..6), high from k
     const int tid = threadIdx.x;
-    if (tid < 16) {
+    if (tid < (1 << (MAX_BITS - 7))) {
         ITYPE o = 0;
         for (int j = 7; j < m; ++j)
             if ((tid >> (j - 7)) & 1) o |= 1ULL << a.q[j];
@@ -205,58 +227,70 @@ __device__ __forceinline__ void staged_tile(double2* __restrict__ s, const StPas
     for (int j = 0; j < 7 && j < m; ++j)
         if ((tid >> j) & 1) lo_off |= 1ULL << a.q[j];
     __syncthreads();
-    // tile index u = tid + k * kStThreads (16 per thread when m = 11; fewer threads busy when m < 7)
-    {
-        double2 v[16];
-#pragma unroll
-        for (int k = 0; k < 16; ++k)
-            if ((UINT)tid + (UINT)k * kStThreads < tsize) v[k] = ld_stream(s + (base | lo_off | hi_off[k]));
-#pragma unroll
-        for (int k = 0; k < 16; ++k)
-            if ((UINT)tid + (UINT)k * kStThreads < tsize) tile[swz((UINT)tid + (UINT)k * kStThreads)] = v[k];
-    }
+    tile_rows_load(s, tile, base | lo_off, hi_off, tsize, 0);
+    if constexpr (MAX_BITS > 11)
+        if (tsize > 16 * kStThreads) tile_rows_load(s, tile, base | lo_off, hi_off, tsize, 16);
     __syncthreads();
     const UINT ncos = tsize >> kPhaseBits;  // cosets per phase
+    char* tile_bytes = reinterpret_cast<char*>(tile);
     for (int ph = 0; ph < a.nphases; ++ph) {
         const StPhase P = a.phases[ph];
-        if (tid < 16) {
-            UINT o = 0;
+        // Byte offset of register amplitude j from the coset's first one: the XOR of sb[p] over the set
+        // bits p of j (the swizzle is XOR-linear).  The 16 amplitudes are visited in Gray-code order so
+        // that each address is the previous one with one sb[p] XORed in.
+        UINT sb[4];
 #pragma unroll
-            for (int p = 0; p < 4; ++p)
-                if ((tid >> p) & 1) o |= 1u << P.bits[p];
-            s_off[tid] = swz(o);
-        }
-        __syncthreads();
+        for (int p = 0; p < 4; ++p) sb[p] = swz(1u << P.bits[p]) << 4;
         for (UINT c = tid; c < ncos; c += kStThreads) {
             UINT u0 = c;
 #pragma unroll
             for (int p = 0; p < 4; ++p) u0 = (UINT)insert0(u0, P.bits[p]);
-            const UINT u0s = swz(u0);
             double2 r[16];
+            UINT addr = swz(u0) << 4;
 #pragma unroll
-            for (int j = 0; j < 16; ++j) r[j] = tile[u0s ^ s_off[j]];
+            for (int g = 0; g < 16; ++g) {
+                if (g) addr ^= sb[(g & 1) ? 0 : (g & 2) ? 1 : (g & 4) ? 2 : 3];
+                r[g ^ (g >> 1)] = *reinterpret_cast<const double2*>(tile_bytes + addr);
+            }
             for (UINT o = 0; o < P.op_count; ++o) apply_op(a.ops[P.op_begin + o], r, a.pool);
 #pragma unroll
-            for (int j = 0; j < 16; ++j) tile[u0s ^ s_off[j]] = r[j];
+            for (int g = 15; g >= 0; --g) {
+                *reinterpret_cast<double2*>(tile_bytes + addr) = r[g ^ (g >> 1)];
+                if (g) addr ^= sb[(g & 1) ? 0 : (g & 2) ? 1 : (g & 4) ? 2 : 3];
+            }
         }
         __syncthreads();
     }
-    {
-        double2 v[16];
-#pragma unroll
-        for (int k = 0; k < 16; ++k)
-            if ((UINT)tid + (UINT)k * kStThreads < tsize) v[k] = tile[swz((UINT)tid + (UINT)k * kStThreads)];
-#pragma unroll
-        for (int k = 0; k < 16; ++k)
-            if ((UINT)tid + (UINT)k * kStThreads < tsize) st_stream(s + (base | lo_off | hi_off[k]), v[k]);
-    }
+    tile_rows_store(s, tile, base | lo_off, hi_off, tsize, 0);
+    if constexpr (MAX_BITS > 11)
+        if (tsize > 16 * kStThreads) tile_rows_store(s, tile, base | lo_off, hi_off, tsize, 16);
     __syncthreads();
 }
 
+// One CTA per tile; the tile (2^m x 16 bytes, up to 64 KiB) is dynamic shared memory.
 __global__ void __launch_bounds__(kStThreads, 3) k_staged_pass(double2* __restrict__ s, const __grid_constant__ StPassArgs a) {
-    __shared__ StSmem sm;
-    staged_tile(s, a, blockIdx.x, sm);
+    extern __shared__ double2 st_tile[];
+    __shared__ ITYPE hi_off[1 << (kTileBits - 7)];
+    staged_tile<kTileBits>(s, a, blockIdx.x, st_tile, hi_off);
 }
+
+// Opt k_staged_pass in to 64 KiB of dynamic shared memory, once per device.
+static int staged_allow_smem() {
+    static std::mutex mu;
+    static std::vector<char> done;
+    int dev = 0;
+    QS_CUDA_CHECK(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    if ((int)done.size() <= dev) done.resize(dev + 1, 0);
+    if (!done[dev]) {
+        QS_CUDA_CHECK(cudaFuncSetAttribute(k_staged_pass, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            (int)(sizeof(double2) << kTileBits)));
+        done[dev] = 1;
+    }
+    return QS_OK;
+}
+
+static size_t staged_smem(int m) { return sizeof(double2) << m; }
 
 // ---------------------------------------------------------------- host scheduler
 using cd = std::complex<double>;
@@ -322,11 +356,11 @@ static ITYPE greedy_q(const std::vector<GateRec>& G, const std::vector<int>& pen
     return Q;
 }
 
-static std::vector<PassPlan> plan_passes(const std::vector<GateRec>& G, UINT n) {
+static std::vector<PassPlan> plan_passes(const std::vector<GateRec>& G, UINT n, int tile_bits) {
     std::vector<PassPlan> plan;
     std::vector<int> pending(G.size());
     for (size_t i = 0; i < G.size(); ++i) pending[i] = (int)i;
-    const int m = (int)std::min<UINT>(kTileBits, n);
+    const int m = (int)std::min<UINT>((UINT)tile_bits, n);
     const int low = std::min(kLowFixed, m);
     const ITYPE lowmask = (1ULL << low) - 1;
     while (!pending.empty()) {
@@ -414,8 +448,8 @@ struct HostPlan {
 };
 
 // Host-only part of planning: passes, phases and encoded ops (no device calls).
-static void make_host_plan(const std::vector<GateRec>& gates, UINT n, HostPlan* H) {
-    H->passes = plan_passes(gates, n);
+static void make_host_plan(const std::vector<GateRec>& gates, UINT n, HostPlan* H, int tile_bits = kTileBits) {
+    H->passes = plan_passes(gates, n, tile_bits);
     const std::vector<PassPlan>& passes = H->passes;
     std::vector<StPhase>& phases = H->phases;
     std::vector<StOp>& ops = H->ops;
@@ -556,11 +590,12 @@ static void make_host_plan(const std::vector<GateRec>& gates, UINT n, HostPlan* 
     }
 }
 
-static int build_plan(const std::vector<GateRec>& gates, UINT n, ITYPE dim, std::shared_ptr<StagedPlan>* out) {
+static int build_plan(const std::vector<GateRec>& gates, UINT n, ITYPE dim, std::shared_ptr<StagedPlan>* out,
+    int tile_bits = kTileBits) {
     auto P = std::make_shared<StagedPlan>();
     P->dim = dim;
     HostPlan H;
-    make_host_plan(gates, n, &H);
+    make_host_plan(gates, n, &H, tile_bits);
     const std::vector<PassPlan>& passes = H.passes;
     const std::vector<StPhase>& phases = H.phases;
     const std::vector<StOp>& ops = H.ops;
@@ -604,13 +639,14 @@ static int ensure_plan(Circuit& c, ITYPE dim) {
 }
 
 static int run_plan(const std::vector<GateRec>& gates, const StagedPlan& P, void* state, ITYPE dim, cudaStream_t st) {
+    QS_TRY(staged_allow_smem());
     for (const DevPass& d : P.passes) {
         if (d.single) {
             QS_TRY(apply_gate_by_gate(gates[d.gate], state, dim, st));
             continue;
         }
         const ITYPE tiles = dim >> d.args.m;
-        k_staged_pass<<<(unsigned)tiles, kStThreads, 0, st>>>((double2*)state, d.args);
+        k_staged_pass<<<(unsigned)tiles, kStThreads, staged_smem(d.args.m), st>>>((double2*)state, d.args);
         QS_TRY(check_launch("k_staged_pass"));
     }
     return QS_OK;
@@ -660,9 +696,9 @@ static int estimate_plan_ms(const std::vector<GateRec>& gates, const StagedPlan&
         if (rc != QS_OK) break;
         StPassArgs a = d.args;
         for (int j = 0; j < a.m; ++j) a.q[j] = (UINT)j;
-        k_staged_pass<<<(unsigned)tt, kStThreads, 0, st>>>((double2*)buf, a);  // warm-up
+        k_staged_pass<<<(unsigned)tt, kStThreads, staged_smem(a.m), st>>>((double2*)buf, a);  // warm-up
         cudaEventRecord(e0, st);
-        k_staged_pass<<<(unsigned)tt, kStThreads, 0, st>>>((double2*)buf, a);
+        k_staged_pass<<<(unsigned)tt, kStThreads, staged_smem(a.m), st>>>((double2*)buf, a);
         cudaEventRecord(e1, st);
         rc = check_launch("k_staged_pass");
         if (rc != QS_OK) break;
@@ -803,7 +839,8 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
 
 __global__ void __launch_bounds__(kStThreads, 3) k_batch_staged(const BatchRec* __restrict__ recs, int nrec,
     ITYPE total, unsigned long long* head, unsigned* done, int* err) {
-    __shared__ StSmem sm;
+    __shared__ double2 tile[1 << kBatchTileBits];
+    __shared__ ITYPE hi_off[1 << (kBatchTileBits - 7)];
     __shared__ ITYPE s_item;
     __shared__ int s_rec, s_abort;
     __shared__ StPassArgs s_args;  // the record's pass, copied so the tile code indexes shared memory
@@ -843,7 +880,7 @@ __global__ void __launch_bounds__(kStThreads, 3) k_batch_staged(const BatchRec* 
             s_state = recs[s_rec].state;
         }
         __syncthreads();
-        staged_tile(s_state, s_args, s_item - recs[s_rec].prefix, sm);
+        staged_tile<kBatchTileBits>(s_state, s_args, s_item - recs[s_rec].prefix, tile, hi_off);
         if (tid == 0) {
             __threadfence();
             atomicAdd(done + s_rec, 1u);
@@ -861,7 +898,7 @@ static int ensure_batch_plan(Circuit& c, ITYPE dim) {
     if (c.bplan && c.bplan->dim == dim && c.bk == k) return QS_OK;
     c.bgates = fuse_gates(c.gates, k);
     c.bk = k;
-    return build_plan(c.bgates, c.n, dim, &c.bplan);
+    return build_plan(c.bgates, c.n, dim, &c.bplan, kBatchTileBits);
 }
 
 int batch_update(Circuit* const* cs, void* const* states, UINT count, cudaStream_t st) {

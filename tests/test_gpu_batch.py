@@ -58,7 +58,10 @@ def test_batch_states_match_gate_by_gate(port):
         alone = QuantumState(n)
         circ.set_fusion(2)  # the batch's block size
         circ.update_quantum_state(alone, mode="staged_fused")
-        assert np.array_equal(v, alone.get_vector())  # bit-identical alone and in the batch
+        if n <= 11:  # same tiles (the multi-circuit kernel's are 2^11, the single-circuit kernel's 2^12)
+            assert np.array_equal(v, alone.get_vector())  # bit-identical alone and in the batch
+        else:  # same gates per amplitude in another pass order: rounding-level differences only
+            assert np.max(np.abs(v - alone.get_vector())) <= 1e-14
 
 
 def test_batch_fused_c64(port):
