@@ -103,9 +103,9 @@ class ClockSampler:
 
 
 # DRAM bytes per amplitude per staged pass measured by ncu (dram__bytes_read.sum + write.sum of
-# k_staged_pass on the 26-qubit case: 2.092e9 B for 2^26 amplitudes; profiles/k_staged_pass_layered26.md),
-# scaled to the benchmark's size by the number of amplitudes.
-STAGED_TRAFFIC_PER_AMP = 2.092e9 / (1 << 26)
+# k_staged_pass on the 26-qubit layered circuit: 1.074e9 + 1.014e9 B for 2^26 amplitudes), scaled to
+# the benchmark's size by the number of amplitudes.
+STAGED_TRAFFIC_PER_AMP = 2.088e9 / (1 << 26)
 
 
 def kernel_table(state, n: int, stream, reps: int = 5):

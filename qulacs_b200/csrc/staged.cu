@@ -680,6 +680,7 @@ static int estimate_plan_ms(const std::vector<GateRec>& gates, const StagedPlan&
     double* out_ms) {
     const double hbm_ms = 2.0 * 16.0 * (double)dim / kTuneHbmBytesPerSec * 1e3;
     double total = 0.;
+    QS_TRY(staged_allow_smem());
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     QS_CUDA_CHECK(cudaEventCreate(&e0));
     QS_CUDA_CHECK(cudaEventCreate(&e1));

@@ -105,6 +105,20 @@ def test_forced_fusion_sizes_against_oracle(port, k):
     assert all(e < 0 for e in est)  # forced: the autotuner did not run
 
 
+def test_autotuned_run_first_in_a_fresh_process():
+    """The autotuner's timing launches are the first kernel launches of a process (no earlier call has
+    set up any kernel attribute)."""
+    import subprocess
+    import sys
+    code = ("import qulacs_b200 as Q; from qulacs_b200 import workloads as W; n = 16; "
+            "c = W.to_circuit(W.layered_rotation_circuit(n, 3, seed=5), n); s = Q.QuantumState(n); "
+            "c.update_quantum_state(s, mode='staged_fused'); print(round(s.get_squared_norm(), 12))")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300,
+                       cwd=os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert r.stdout.strip().splitlines()[-1] == "1.0"
+
+
 def test_autotuner_records_estimates(port):
     n = 20
     gates = W.layered_rotation_circuit(n, 4, seed=95)
