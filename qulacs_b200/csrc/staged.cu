@@ -30,7 +30,10 @@ constexpr int kBatchTileBits = 11;  // multi-circuit kernel: 2^11 amplitudes = 3
 constexpr int kStThreads = 128;     // 16 (m = 11) or 32 (m = 12) amplitudes per thread; 1 or 2 cosets per phase
 constexpr int kPhaseBits = 4;       // 16 amplitudes in registers per thread
 
-enum StKind : uint8_t { ST_DENSE1 = 0, ST_DIAG1, ST_RX, ST_RY, ST_CNOT, ST_CZ, ST_SWAP, ST_DENSE2 };
+// ST_CSEL1, ST_D1_IN and ST_D1_OUT are a one-qubit dense gate with a CNOT folded in (see absorb_cnots).
+enum StKind : uint8_t {
+    ST_DENSE1 = 0, ST_DIAG1, ST_RX, ST_RY, ST_CNOT, ST_CZ, ST_SWAP, ST_DENSE2, ST_CSEL1, ST_D1_IN, ST_D1_OUT
+};
 
 struct StOp {
     uint8_t kind, a, b, pad;  // a, b: register-bit indices 0..3 within the phase; pad: dispatch code
@@ -138,24 +141,81 @@ __device__ __forceinline__ void r_dense2(double2 (&r)[16], const double2* __rest
         }
 }
 
-// One indirect branch per op: the host encodes code = kind * 16 + a * 4 + b, and every code has its
-// own fully specialised register code (unused codes are empty).
-template <int CODE>
+// Dense 2x2 along register bit A with the matrix chosen by register bit B: p[0..3] where bit B is 0,
+// p[4..7] where it is 1 (a one-qubit gate on the target of a CNOT, with the CNOT folded in).
+template <int A, int B>
+__device__ __forceinline__ void r_csel1(double2 (&r)[16], const double2* __restrict__ p) {
+    const double2 m0 = p[0], m1 = p[1], m2 = p[2], m3 = p[3];
+    const double2 n0 = p[4], n1 = p[5], n2 = p[6], n3 = p[7];
+#pragma unroll
+    for (int j = 0; j < 16; ++j)
+        if (!(j & (1 << A))) {
+            const double2 x = r[j], y = r[j | (1 << A)];
+            const bool hi = (j >> B) & 1;
+            r[j] = cfma(hi ? n1 : m1, y, cmul(hi ? n0 : m0, x));
+            r[j | (1 << A)] = cfma(hi ? n3 : m3, y, cmul(hi ? n2 : m2, x));
+        }
+}
+// A one-qubit dense gate U on the control A of CNOT(A -> B), CNOT first: for j with bits A, B clear
+// and t in {0, B}, out[j^t] = U00 in[j^t] + U01 in[j^t^A^B], out[j^t^A] = U10 in[j^t] + U11 in[j^t^A^B].
+template <int A, int B>
+__device__ __forceinline__ void r_d1_in(double2 (&r)[16], const double2* __restrict__ p) {
+    const double2 m0 = p[0], m1 = p[1], m2 = p[2], m3 = p[3];
+    double2 o[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j)
+        if (!(j & (1 << A))) {
+            const int k = j ^ (1 << A) ^ (1 << B);
+            const double2 x = r[j], y = r[k];
+            o[j] = cfma(m1, y, cmul(m0, x));
+            o[j | (1 << A)] = cfma(m3, y, cmul(m2, x));
+        }
+#pragma unroll
+    for (int j = 0; j < 16; ++j) r[j] = o[j];
+}
+// The same gate with the CNOT second: out[j^t] = U00 in[j^t] + U01 in[j^t^A],
+// out[j^t^A^B] = U10 in[j^t] + U11 in[j^t^A].
+template <int A, int B>
+__device__ __forceinline__ void r_d1_out(double2 (&r)[16], const double2* __restrict__ p) {
+    const double2 m0 = p[0], m1 = p[1], m2 = p[2], m3 = p[3];
+    double2 o[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j)
+        if (!(j & (1 << A))) {
+            const double2 x = r[j], y = r[j | (1 << A)];
+            o[j] = cfma(m1, y, cmul(m0, x));
+            o[j ^ (1 << A) ^ (1 << B)] = cfma(m3, y, cmul(m2, x));
+        }
+#pragma unroll
+    for (int j = 0; j < 16; ++j) r[j] = o[j];
+}
+
+// One indirect branch per op: the host encodes code = kind * 16 + a * 4 + b (op_code), and every code
+// has its own fully specialised register code (unused codes are empty).  One-qubit kinds use b = a;
+// their b != a codes hold the CNOT-folded ops (DENSE1: ST_CSEL1, DIAG1: ST_D1_IN, RX: ST_D1_OUT), which
+// keeps the switch at 128 codes -- more codes made every pass slower.  Passes without folded ops run
+// the FOLDS = false build, whose switch holds only the plain ops (the folded code placed among the
+// plain one-qubit cases slowed unfused schedules by 12 %).
+template <int CODE, bool FOLDS>
 __device__ __forceinline__ void run_code(double2 (&r)[16], const double2* p) {
     constexpr int kind = CODE >> 4, A = (CODE >> 2) & 3, B = CODE & 3;
-    if constexpr (kind == ST_DENSE1 && B == 0) r_dense1<A>(r, p);
-    else if constexpr (kind == ST_DIAG1 && B == 0) r_diag1<A>(r, p);
-    else if constexpr (kind == ST_RX && B == 0) r_rx<A>(r, p);
-    else if constexpr (kind == ST_RY && B == 0) r_ry<A>(r, p);
+    if constexpr (kind == ST_DENSE1 && B == A) r_dense1<A>(r, p);
+    else if constexpr (FOLDS && kind == ST_DENSE1) r_csel1<A, B>(r, p);
+    else if constexpr (kind == ST_DIAG1 && B == A) r_diag1<A>(r, p);
+    else if constexpr (FOLDS && kind == ST_DIAG1) r_d1_in<A, B>(r, p);
+    else if constexpr (kind == ST_RX && B == A) r_rx<A>(r, p);
+    else if constexpr (FOLDS && kind == ST_RX) r_d1_out<A, B>(r, p);
+    else if constexpr (kind == ST_RY && B == A) r_ry<A>(r, p);
     else if constexpr (kind == ST_CNOT && A != B) r_cnot<A, B>(r);
     else if constexpr (kind == ST_CZ && A != B) r_cz<A, B>(r);
     else if constexpr (kind == ST_SWAP && A != B) r_swap<A, B>(r);
     else if constexpr (kind == ST_DENSE2 && A != B) r_dense2<A, B>(r, p);
 }
 #define QS_CODE1(c) \
-    case c: run_code<c>(r, p); break;
+    case c: run_code<c, FOLDS>(r, p); break;
 #define QS_CODE4(c) QS_CODE1(c) QS_CODE1(c + 1) QS_CODE1(c + 2) QS_CODE1(c + 3)
 #define QS_CODE16(c) QS_CODE4(c) QS_CODE4(c + 4) QS_CODE4(c + 8) QS_CODE4(c + 12)
+template <bool FOLDS>
 __device__ __forceinline__ void apply_op(const StOp& op, double2 (&r)[16], const double2* pool) {
     const double2* p = pool + op.param;
     switch (op.pad) {
@@ -208,7 +268,7 @@ __device__ __forceinline__ void tile_rows_store(double2* __restrict__ s, const d
 // One tile of one pass: load, apply every phase, store.  Shared by the per-pass kernel and the
 // persistent multi-circuit kernel.  `tile` holds 2^m amplitudes (m <= kTileBits).  Ends with a CTA
 // barrier so the shared buffers can be reused immediately.
-template <int MAX_BITS>
+template <int MAX_BITS, bool FOLDS>
 __device__ __forceinline__ void staged_tile(double2* __restrict__ s, const StPassArgs& a, ITYPE T, double2* tile,
     ITYPE* hi_off) {
     const int m = a.m;
@@ -252,7 +312,7 @@ __device__ __forceinline__ void staged_tile(double2* __restrict__ s, const StPas
                 if (g) addr ^= sb[(g & 1) ? 0 : (g & 2) ? 1 : (g & 4) ? 2 : 3];
                 r[g ^ (g >> 1)] = *reinterpret_cast<const double2*>(tile_bytes + addr);
             }
-            for (UINT o = 0; o < P.op_count; ++o) apply_op(a.ops[P.op_begin + o], r, a.pool);
+            for (UINT o = 0; o < P.op_count; ++o) apply_op<FOLDS>(a.ops[P.op_begin + o], r, a.pool);
 #pragma unroll
             for (int g = 15; g >= 0; --g) {
                 *reinterpret_cast<double2*>(tile_bytes + addr) = r[g ^ (g >> 1)];
@@ -268,10 +328,11 @@ __device__ __forceinline__ void staged_tile(double2* __restrict__ s, const StPas
 }
 
 // One CTA per tile; the tile (2^m x 16 bytes, up to 64 KiB) is dynamic shared memory.
+template <bool FOLDS>
 __global__ void __launch_bounds__(kStThreads, 3) k_staged_pass(double2* __restrict__ s, const __grid_constant__ StPassArgs a) {
     extern __shared__ double2 st_tile[];
     __shared__ ITYPE hi_off[1 << (kTileBits - 7)];
-    staged_tile<kTileBits>(s, a, blockIdx.x, st_tile, hi_off);
+    staged_tile<kTileBits, FOLDS>(s, a, blockIdx.x, st_tile, hi_off);
 }
 
 // Opt k_staged_pass in to 64 KiB of dynamic shared memory, once per device.
@@ -283,14 +344,15 @@ static int staged_allow_smem() {
     std::lock_guard<std::mutex> lock(mu);
     if ((int)done.size() <= dev) done.resize(dev + 1, 0);
     if (!done[dev]) {
-        QS_CUDA_CHECK(cudaFuncSetAttribute(k_staged_pass, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        QS_CUDA_CHECK(cudaFuncSetAttribute(k_staged_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            (int)(sizeof(double2) << kTileBits)));
+        QS_CUDA_CHECK(cudaFuncSetAttribute(k_staged_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
             (int)(sizeof(double2) << kTileBits)));
         done[dev] = 1;
     }
     return QS_OK;
 }
 
-static size_t staged_smem(int m) { return sizeof(double2) << m; }
 
 // ---------------------------------------------------------------- host scheduler
 using cd = std::complex<double>;
@@ -416,9 +478,16 @@ static std::vector<PassPlan> plan_passes(const std::vector<GateRec>& G, UINT n, 
 
 struct DevPass {
     bool single;
+    bool folds;  // the pass has CNOT-folded ops
     int gate;
     StPassArgs args;
 };
+
+static void launch_pass(double2* state, const DevPass& d, ITYPE tiles, cudaStream_t st) {
+    const size_t smem = sizeof(double2) << d.args.m;
+    if (d.folds) k_staged_pass<true><<<(unsigned)tiles, kStThreads, smem, st>>>(state, d.args);
+    else k_staged_pass<false><<<(unsigned)tiles, kStThreads, smem, st>>>(state, d.args);
+}
 
 struct StagedPlan {
     ITYPE dim = 0;
@@ -434,6 +503,83 @@ static int local_bit(const std::vector<UINT>& q, UINT g) {
     for (size_t j = 0; j < q.size(); ++j)
         if (q[j] == g) return (int)j;
     return -1;
+}
+
+// Dispatch code of an op (see run_code).
+static uint8_t op_code(const StOp& o) {
+    int kind = o.kind;
+    if (kind == ST_CSEL1) kind = ST_DENSE1;
+    else if (kind == ST_D1_IN) kind = ST_DIAG1;
+    else if (kind == ST_D1_OUT) kind = ST_RX;
+    return (uint8_t)(kind * 16 + o.a * 4 + o.b);
+}
+
+// Fold CNOTs into a neighbouring one-qubit dense op of the same phase (ops [begin, end) of `ops`, in
+// program order), which costs the CNOT's register moves and dispatch nothing: a CNOT whose nearest
+// earlier op on its two register bits is a dense op U (on either bit) runs at U's place, after it;
+// failing that, one whose nearest later op on them is a dense op runs at that op's place, before it.
+// A folded CNOT takes its host op's place in the order, so a CNOT is not moved past an earlier folded
+// CNOT on the same bits.
+// On the target T: CNOT.U_T = U (control 0) / X U (control 1); U_T.CNOT = U / U X (ST_CSEL1).  On the
+// control C: U_C.CNOT pairs (c, t) with (c^1, t^1) on input (ST_D1_IN), CNOT.U_C on output (ST_D1_OUT).
+static void absorb_cnots(std::vector<StOp>& ops, std::vector<double2>& pool, size_t begin) {
+    auto touches = [](const StOp& o, int bit) {
+        const bool two = o.kind == ST_CNOT || o.kind == ST_CZ || o.kind == ST_SWAP || o.kind == ST_DENSE2 ||
+                         o.kind == ST_CSEL1 || o.kind == ST_D1_IN || o.kind == ST_D1_OUT;
+        return o.a == bit || (two && o.b == bit);
+    };
+    const size_t end = ops.size();
+    std::vector<char> dead(end, 0);
+    std::vector<size_t> at_op(end);  // place of each op in the order (a folded CNOT: its host op)
+    for (size_t i = begin; i < end; ++i) at_op[i] = i;
+    for (size_t i = begin; i < end; ++i) {
+        if (ops[i].kind != ST_CNOT) continue;
+        const int c = ops[i].a, t = ops[i].b;
+        // a folded CNOT on c or t placed strictly between lo and hi forbids the move
+        auto blocked = [&](size_t lo, size_t hi) {
+            for (size_t j = begin; j < end; ++j)
+                if (dead[j] && at_op[j] > lo && at_op[j] < hi && (touches(ops[j], c) || touches(ops[j], t)))
+                    return true;
+            return false;
+        };
+        auto fold = [&](size_t k, bool cnot_first) {
+            StOp& u = ops[k];
+            const double2 m0 = pool[u.param], m1 = pool[u.param + 1], m2 = pool[u.param + 2], m3 = pool[u.param + 3];
+            const uint32_t at = (uint32_t)pool.size();
+            if (u.a == t) {
+                u.kind = ST_CSEL1;
+                u.b = (uint8_t)c;
+                for (const double2& v : {m0, m1, m2, m3}) pool.push_back(v);
+                if (cnot_first) for (const double2& v : {m1, m0, m3, m2}) pool.push_back(v);  // U X
+                else for (const double2& v : {m2, m3, m0, m1}) pool.push_back(v);             // X U
+            } else {
+                u.kind = cnot_first ? ST_D1_IN : ST_D1_OUT;
+                u.b = (uint8_t)t;
+                for (const double2& v : {m0, m1, m2, m3}) pool.push_back(v);
+            }
+            u.param = at;
+            dead[i] = 1;
+            at_op[i] = k;
+        };
+        for (size_t k = i; k-- > begin;) {
+            if (dead[k] || !(touches(ops[k], c) || touches(ops[k], t))) continue;
+            if (ops[k].kind == ST_DENSE1 && !blocked(k, i)) fold(k, false);
+            break;
+        }
+        if (dead[i]) continue;
+        for (size_t k = i + 1; k < end; ++k) {
+            if (dead[k] || !(touches(ops[k], c) || touches(ops[k], t))) continue;
+            if (ops[k].kind == ST_DENSE1 && !blocked(i, k)) fold(k, true);
+            break;
+        }
+    }
+    size_t w = begin;
+    for (size_t i = begin; i < end; ++i)
+        if (!dead[i]) {
+            ops[i].pad = op_code(ops[i]);
+            ops[w++] = ops[i];
+        }
+    ops.resize(w);
 }
 
 struct HostPlan {
@@ -574,9 +720,12 @@ static void make_host_plan(const std::vector<GateRec>& gates, UINT n, HostPlan* 
                         }
                         break;
                 }
-                op.pad = (uint8_t)(op.kind * 16 + op.a * 4 + op.b);  // dispatch code
+                if (op.kind == ST_DENSE1 || op.kind == ST_DIAG1 || op.kind == ST_RX || op.kind == ST_RY)
+                    op.b = op.a;  // one-qubit ops: b = a (see run_code)
+                op.pad = op_code(op);
                 ops.push_back(op);
             }
+            absorb_cnots(ops, pool, ph.op_begin);
             ph.op_count = (uint32_t)(ops.size() - ph.op_begin);
             phases.push_back(ph);
             std::vector<char> taken(gates.size(), 0);
@@ -624,6 +773,9 @@ static int build_plan(const std::vector<GateRec>& gates, UINT n, ITYPE dim, std:
             for (int j = 0; j < d.args.m; ++j) d.args.q[j] = passes[i].q[j];
             d.args.nphases = (int)pp[i].nphases;
             d.args.phases = dph + pp[i].phase_begin;
+            for (size_t ph = pp[i].phase_begin; ph < pp[i].phase_begin + pp[i].nphases; ++ph)
+                for (uint32_t o = phases[ph].op_begin; o < phases[ph].op_begin + phases[ph].op_count; ++o)
+                    d.folds = d.folds || ops[o].kind == ST_CSEL1 || ops[o].kind == ST_D1_IN || ops[o].kind == ST_D1_OUT;
             d.args.ops = dop;
             d.args.pool = dpo;
         }
@@ -646,7 +798,7 @@ static int run_plan(const std::vector<GateRec>& gates, const StagedPlan& P, void
             continue;
         }
         const ITYPE tiles = dim >> d.args.m;
-        k_staged_pass<<<(unsigned)tiles, kStThreads, staged_smem(d.args.m), st>>>((double2*)state, d.args);
+        launch_pass((double2*)state, d, tiles, st);
         QS_TRY(check_launch("k_staged_pass"));
     }
     return QS_OK;
@@ -697,9 +849,11 @@ static int estimate_plan_ms(const std::vector<GateRec>& gates, const StagedPlan&
         if (rc != QS_OK) break;
         StPassArgs a = d.args;
         for (int j = 0; j < a.m; ++j) a.q[j] = (UINT)j;
-        k_staged_pass<<<(unsigned)tt, kStThreads, staged_smem(a.m), st>>>((double2*)buf, a);  // warm-up
+        DevPass dt = d;
+        dt.args = a;
+        launch_pass((double2*)buf, dt, tt, st);  // warm-up
         cudaEventRecord(e0, st);
-        k_staged_pass<<<(unsigned)tt, kStThreads, staged_smem(a.m), st>>>((double2*)buf, a);
+        launch_pass((double2*)buf, dt, tt, st);
         cudaEventRecord(e1, st);
         rc = check_launch("k_staged_pass");
         if (rc != QS_OK) break;
@@ -881,7 +1035,7 @@ __global__ void __launch_bounds__(kStThreads, 3) k_batch_staged(const BatchRec* 
             s_state = recs[s_rec].state;
         }
         __syncthreads();
-        staged_tile<kBatchTileBits>(s_state, s_args, s_item - recs[s_rec].prefix, tile, hi_off);
+        staged_tile<kBatchTileBits, true>(s_state, s_args, s_item - recs[s_rec].prefix, tile, hi_off);
         if (tid == 0) {
             __threadfence();
             atomicAdd(done + s_rec, 1u);

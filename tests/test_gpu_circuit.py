@@ -69,6 +69,34 @@ def test_random_circuits_against_oracle(port, n, mode):
     assert np.max(np.abs(s.get_vector() - want)) <= AMP_TOL
 
 
+@pytest.mark.parametrize("n", [5, 12, 14])
+@pytest.mark.parametrize("mode", ["staged", "staged_fused"])
+def test_cnot_chains_folded_into_dense_ops(port, n, mode):
+    """Random interleavings of one-qubit dense gates and CNOTs in both directions (and a few CZ), so
+    that CNOTs fold into dense ops before and after them, on targets and controls, next to other
+    folded CNOTs on shared qubits."""
+    rng = np.random.default_rng(4000 + n)
+    gates = []
+    for _ in range(400):
+        r = rng.random()
+        if r < 0.5:
+            a, b = (int(x) for x in rng.choice(n, size=2, replace=False))
+            gates.append(("CNOT" if r < 0.45 else "CZ", a, b))
+        else:
+            t = int(rng.integers(0, n))
+            th, ph, la = rng.uniform(0, 2 * np.pi, size=3)
+            gates.append(("U3", t, float(th), float(ph), float(la)))
+    circ = W.to_circuit(gates, n)
+    if mode == "staged_fused":
+        circ.set_fusion(1)  # runs of one-qubit gates merge, CNOTs stay separate ops to be folded
+    s = QuantumState(n)
+    circ.update_quantum_state(s, mode=mode)
+    want = np.zeros(1 << n, dtype=np.complex128)
+    want[0] = 1
+    W.run_on_cpu(gates, want, port)
+    assert np.max(np.abs(s.get_vector() - want)) <= AMP_TOL
+
+
 @pytest.mark.parametrize("n", [26])
 def test_large_circuit_properties(n):
     """At sizes beyond the oracle: norm is preserved, and circuit followed by its inverse returns |0>."""
