@@ -522,6 +522,7 @@ static uint8_t op_code(const StOp& o) {
 // CNOT on the same bits.
 // On the target T: CNOT.U_T = U (control 0) / X U (control 1); U_T.CNOT = U / U X (ST_CSEL1).  On the
 // control C: U_C.CNOT pairs (c, t) with (c^1, t^1) on input (ST_D1_IN), CNOT.U_C on output (ST_D1_OUT).
+// A CZ folds the same way into a dense op on either of its qubits: CZ.U = U / Z U, U.CZ = U / U Z.
 static void absorb_cnots(std::vector<StOp>& ops, std::vector<double2>& pool, size_t begin) {
     auto touches = [](const StOp& o, int bit) {
         const bool two = o.kind == ST_CNOT || o.kind == ST_CZ || o.kind == ST_SWAP || o.kind == ST_DENSE2 ||
@@ -533,7 +534,8 @@ static void absorb_cnots(std::vector<StOp>& ops, std::vector<double2>& pool, siz
     std::vector<size_t> at_op(end);  // place of each op in the order (a folded CNOT: its host op)
     for (size_t i = begin; i < end; ++i) at_op[i] = i;
     for (size_t i = begin; i < end; ++i) {
-        if (ops[i].kind != ST_CNOT) continue;
+        if (ops[i].kind != ST_CNOT && ops[i].kind != ST_CZ) continue;
+        const bool cz = ops[i].kind == ST_CZ;
         const int c = ops[i].a, t = ops[i].b;
         // a folded CNOT on c or t placed strictly between lo and hi forbids the move
         auto blocked = [&](size_t lo, size_t hi) {
@@ -546,7 +548,15 @@ static void absorb_cnots(std::vector<StOp>& ops, std::vector<double2>& pool, siz
             StOp& u = ops[k];
             const double2 m0 = pool[u.param], m1 = pool[u.param + 1], m2 = pool[u.param + 2], m3 = pool[u.param + 3];
             const uint32_t at = (uint32_t)pool.size();
-            if (u.a == t) {
+            const double2 n0 = make_double2(-m0.x, -m0.y), n1 = make_double2(-m1.x, -m1.y),
+                          n2 = make_double2(-m2.x, -m2.y), n3 = make_double2(-m3.x, -m3.y);
+            if (cz) {  // the other qubit selects U or its sign-flipped form
+                u.kind = ST_CSEL1;
+                u.b = (uint8_t)(u.a == t ? c : t);
+                for (const double2& v : {m0, m1, m2, m3}) pool.push_back(v);
+                if (cnot_first) for (const double2& v : {m0, n1, m2, n3}) pool.push_back(v);  // U Z
+                else for (const double2& v : {m0, m1, n2, n3}) pool.push_back(v);             // Z U
+            } else if (u.a == t) {
                 u.kind = ST_CSEL1;
                 u.b = (uint8_t)c;
                 for (const double2& v : {m0, m1, m2, m3}) pool.push_back(v);
