@@ -991,8 +991,10 @@ __device__ __forceinline__ double2 tile_amp<float2>(const float2* p) {
     return make_double2(v.x, v.y);
 }
 
+constexpr int kEvTileCtasPerSm = 6;  // 6 x 37 KiB of shared memory; the loads go 4 rows at a time to fit
+
 template <class T>
-__global__ void __launch_bounds__(128) k_ev_tile(const T* __restrict__ s, ITYPE tiles, const __grid_constant__ EvTileArgs a,
+__global__ void __launch_bounds__(128, kEvTileCtasPerSm) k_ev_tile(const T* __restrict__ s, ITYPE tiles, const __grid_constant__ EvTileArgs a,
     const EvTileTerm* __restrict__ terms, double* __restrict__ partials) {
     __shared__ double2 tile[1 << kEvTileBits];
     __shared__ double acc[kEvMaxTerms];
@@ -1015,14 +1017,15 @@ __global__ void __launch_bounds__(128) k_ev_tile(const T* __restrict__ s, ITYPE 
         ITYPE base = ti;
         for (int j = 0; j < m; ++j) base = insert0(base, a.piv_sorted[j]);
         __syncthreads();
-        {
-            double2 v[16];  // all loads in flight before the first shared-memory store
 #pragma unroll
-            for (int k = 0; k < 16; ++k)
-                if ((UINT)tid + (UINT)k * 128 < tsize) v[k] = tile_amp<T>(s + (base ^ lo_off ^ hi_off[k]));
+        for (int h = 0; h < 16; h += 4) {
+            double2 v[4];  // four loads in flight per thread before the shared-memory stores
 #pragma unroll
-            for (int k = 0; k < 16; ++k)
-                if ((UINT)tid + (UINT)k * 128 < tsize) tile[tid + k * 128] = v[k];
+            for (int k = 0; k < 4; ++k)
+                if ((UINT)tid + (UINT)(h + k) * 128 < tsize) v[k] = tile_amp<T>(s + (base ^ lo_off ^ hi_off[h + k]));
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if ((UINT)tid + (UINT)(h + k) * 128 < tsize) tile[tid + (h + k) * 128] = v[k];
         }
         __syncthreads();
         for (int t = warp; t < a.nterms; t += 4) {
@@ -1063,7 +1066,7 @@ int ev_tiled(const PauliTerm* terms, const std::vector<int>& xidx, UINT n, const
     double* values, std::vector<int>* rest) {
     const int m = kEvTileBits;
     std::vector<int> todo = xidx;
-    const unsigned grid = (unsigned)std::min<ITYPE>(dim >> m, (ITYPE)sm_count() * 4);  // 4 resident per SM
+    const unsigned grid = (unsigned)std::min<ITYPE>(dim >> m, (ITYPE)sm_count() * kEvTileCtasPerSm);
     constexpr size_t kMinCover = 2;  // below this a shared pass is not cheaper than one pass per term
     std::vector<double> hvals;
     while (!todo.empty()) {
