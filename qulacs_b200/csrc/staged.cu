@@ -46,6 +46,7 @@ struct StPhase {
 struct StPassArgs {
     int m;                 // tile bits (<= kTileBits)
     int nphases;
+    int io;                // bit 0: the first phase gathers from HBM; bit 1: the last phase scatters to HBM
     UINT q[kTileBits];     // global qubit of tile bit j, ascending, q[j] = j for j < kLowFixed
     const StPhase* phases;
     const StOp* ops;
@@ -277,53 +278,91 @@ __device__ __forceinline__ void staged_tile(double2* __restrict__ s, const StPas
     ITYPE base = T;
     for (int j = 0; j < m; ++j) base = insert0(base, a.q[j]);
     const int tid = threadIdx.x;
-    if (tid < (1 << (MAX_BITS - 7))) {
-        ITYPE o = 0;
-        for (int j = 7; j < m; ++j)
-            if ((tid >> (j - 7)) & 1) o |= 1ULL << a.q[j];
-        hi_off[tid] = o;
-    }
+    const bool hbm_first = a.io & 1, hbm_last = (a.io >> 1) & 1;
     ITYPE lo_off = 0;
-    for (int j = 0; j < 7 && j < m; ++j)
-        if ((tid >> j) & 1) lo_off |= 1ULL << a.q[j];
-    __syncthreads();
-    tile_rows_load(s, tile, base | lo_off, hi_off, tsize, 0);
-    if constexpr (MAX_BITS > 11)
-        if (tsize > 16 * kStThreads) tile_rows_load(s, tile, base | lo_off, hi_off, tsize, 16);
-    __syncthreads();
+    if (!hbm_first || !hbm_last) {
+        if (tid < (1 << (MAX_BITS - 7))) {
+            ITYPE o = 0;
+            for (int j = 7; j < m; ++j)
+                if ((tid >> (j - 7)) & 1) o |= 1ULL << a.q[j];
+            hi_off[tid] = o;
+        }
+        for (int j = 0; j < 7 && j < m; ++j)
+            if ((tid >> j) & 1) lo_off |= 1ULL << a.q[j];
+        __syncthreads();
+    }
+    if (!hbm_first) {
+        tile_rows_load(s, tile, base | lo_off, hi_off, tsize, 0);
+        if constexpr (MAX_BITS > 11)
+            if (tsize > 16 * kStThreads) tile_rows_load(s, tile, base | lo_off, hi_off, tsize, 16);
+        __syncthreads();
+    }
     const UINT ncos = tsize >> kPhaseBits;  // cosets per phase
     char* tile_bytes = reinterpret_cast<char*>(tile);
     for (int ph = 0; ph < a.nphases; ++ph) {
         const StPhase P = a.phases[ph];
+        // The first phase may gather its cosets straight from HBM and the last scatter them straight to
+        // HBM (the host sets this when the phase's bits are all >= 4, so that a coset's lanes 0..15 cover
+        // 16 consecutive amplitudes): no tile load or store round through shared memory.
+        const bool from_hbm = hbm_first && ph == 0, to_hbm = hbm_last && ph == a.nphases - 1;
         // Byte offset of register amplitude j from the coset's first one: the XOR of sb[p] over the set
-        // bits p of j (the swizzle is XOR-linear).  The 16 amplitudes are visited in Gray-code order so
-        // that each address is the previous one with one sb[p] XORed in.
+        // bits p of j (the swizzle is XOR-linear); in HBM, the XOR of gb[p].  The 16 amplitudes are
+        // visited in Gray-code order so that each address is the previous one with one offset XORed in.
         UINT sb[4];
+        ITYPE gb[4];
 #pragma unroll
-        for (int p = 0; p < 4; ++p) sb[p] = swz(1u << P.bits[p]) << 4;
+        for (int p = 0; p < 4; ++p) {
+            sb[p] = swz(1u << P.bits[p]) << 4;
+            gb[p] = 1ULL << a.q[P.bits[p]];
+        }
         for (UINT c = tid; c < ncos; c += kStThreads) {
             UINT u0 = c;
 #pragma unroll
             for (int p = 0; p < 4; ++p) u0 = (UINT)insert0(u0, P.bits[p]);
+            ITYPE g0 = base;  // global index of the coset's first amplitude (only for HBM phases)
+            if (from_hbm || to_hbm)
+                for (int j = 0; j < m; ++j)
+                    if ((u0 >> j) & 1) g0 |= 1ULL << a.q[j];
             double2 r[16];
             UINT addr = swz(u0) << 4;
+            if (from_hbm) {
+                ITYPE gi = g0;
 #pragma unroll
-            for (int g = 0; g < 16; ++g) {
-                if (g) addr ^= sb[(g & 1) ? 0 : (g & 2) ? 1 : (g & 4) ? 2 : 3];
-                r[g ^ (g >> 1)] = *reinterpret_cast<const double2*>(tile_bytes + addr);
+                for (int g = 0; g < 16; ++g) {
+                    if (g) gi ^= gb[(g & 1) ? 0 : (g & 2) ? 1 : (g & 4) ? 2 : 3];
+                    r[g ^ (g >> 1)] = ld_stream(s + gi);
+                }
+            } else {
+#pragma unroll
+                for (int g = 0; g < 16; ++g) {
+                    if (g) addr ^= sb[(g & 1) ? 0 : (g & 2) ? 1 : (g & 4) ? 2 : 3];
+                    r[g ^ (g >> 1)] = *reinterpret_cast<const double2*>(tile_bytes + addr);
+                }
+                addr = swz(u0) << 4;
             }
             for (UINT o = 0; o < P.op_count; ++o) apply_op<FOLDS>(a.ops[P.op_begin + o], r, a.pool);
+            if (to_hbm) {
+                ITYPE gi = g0;
 #pragma unroll
-            for (int g = 15; g >= 0; --g) {
-                *reinterpret_cast<double2*>(tile_bytes + addr) = r[g ^ (g >> 1)];
-                if (g) addr ^= sb[(g & 1) ? 0 : (g & 2) ? 1 : (g & 4) ? 2 : 3];
+                for (int g = 0; g < 16; ++g) {
+                    if (g) gi ^= gb[(g & 1) ? 0 : (g & 2) ? 1 : (g & 4) ? 2 : 3];
+                    st_stream(s + gi, r[g ^ (g >> 1)]);
+                }
+            } else {
+#pragma unroll
+                for (int g = 0; g < 16; ++g) {
+                    if (g) addr ^= sb[(g & 1) ? 0 : (g & 2) ? 1 : (g & 4) ? 2 : 3];
+                    *reinterpret_cast<double2*>(tile_bytes + addr) = r[g ^ (g >> 1)];
+                }
             }
         }
-        __syncthreads();
+        if (!to_hbm) __syncthreads();
     }
-    tile_rows_store(s, tile, base | lo_off, hi_off, tsize, 0);
-    if constexpr (MAX_BITS > 11)
-        if (tsize > 16 * kStThreads) tile_rows_store(s, tile, base | lo_off, hi_off, tsize, 16);
+    if (!hbm_last) {
+        tile_rows_store(s, tile, base | lo_off, hi_off, tsize, 0);
+        if constexpr (MAX_BITS > 11)
+            if (tsize > 16 * kStThreads) tile_rows_store(s, tile, base | lo_off, hi_off, tsize, 16);
+    }
     __syncthreads();
 }
 
@@ -782,6 +821,15 @@ static int build_plan(const std::vector<GateRec>& gates, UINT n, ITYPE dim, std:
             d.args.m = (int)passes[i].q.size();
             for (int j = 0; j < d.args.m; ++j) d.args.q[j] = passes[i].q[j];
             d.args.nphases = (int)pp[i].nphases;
+            auto high_bits = [&](const StPhase& ph) {  // all of the phase's tile bits >= 4
+                for (int p = 0; p < 4; ++p)
+                    if (ph.bits[p] < kLowFixed) return false;
+                return true;
+            };
+            if (pp[i].nphases) {
+                if (high_bits(phases[pp[i].phase_begin])) d.args.io |= 1;
+                if (high_bits(phases[pp[i].phase_begin + pp[i].nphases - 1])) d.args.io |= 2;
+            }
             d.args.phases = dph + pp[i].phase_begin;
             for (size_t ph = pp[i].phase_begin; ph < pp[i].phase_begin + pp[i].nphases; ++ph)
                 for (uint32_t o = phases[ph].op_begin; o < phases[ph].op_begin + phases[ph].op_count; ++o)
