@@ -364,6 +364,11 @@ QS_API int qs_circuit_update_density_matrix(
  * Synchronises `stream`. */
 QS_API int qs_batch_update_quantum_states(const qs_circuit_t* circuits, void* const* states, QS_UINT count,
     void* stream);
+/* The same on the fused complex64 tensor-core path: states_c64[i] holds circuits[i]'s 2^n complex64
+ * amplitudes (n >= 10).  Missing plans are built on host threads in parallel; the circuits run
+ * concurrently on streams forked from `stream` and joined back.  Synchronises `stream`. */
+QS_API int qs_batch_update_quantum_states_fused_c64(qs_circuit_t const* circuits, void* const* states_c64,
+    QS_UINT count, void* stream);
 /* <P_k> for the Pauli terms of many complex128 states.  Terms of state i are term_offsets[i] ..
  * term_offsets[i+1]-1 (masks as qs_expectation_value_pauli_batch); values[k] receives <P_k>.  States
  * of fewer than 18 qubits share one launch (jobs of 16 Z-only strings or one bit-flip string);

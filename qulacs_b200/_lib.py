@@ -69,6 +69,7 @@ SIGNATURES = {
     "qs_initialize_Haar_random_state_with_seed": [P, IT, U, P],
     "qs_get_amplitude": [P, IT, IT, P, P],
     "qs_copy_state": [P, P, IT, P],
+    "qs_batch_update_quantum_states_fused_c64": [P, P, U, P],
     "qs_random_unitary_matrix": [U, U, P],
     "qs_random_operator_terms": [U, U, U, P, P],
     "qs_state_multiply_elementwise": [P, P, IT, P],

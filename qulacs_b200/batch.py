@@ -4,8 +4,9 @@
 waves whose states fit an HBM budget (footprint 16 B x 2^n each, carved from one arena per wave),
 and for each wave applies every circuit in ONE persistent kernel launch
 (``qs_batch_update_quantum_states``) and evaluates every observable term in ONE more launch
-(``qs_batch_expectation_values``).  ``precision="c64"`` runs each circuit on the fused complex64
-tensor-core path instead (one fused launch sequence per circuit; reductions still FP64).
+(``qs_batch_expectation_values``).  ``precision="c64"`` runs the wave on the fused complex64
+tensor-core path instead (``qs_batch_update_quantum_states_fused_c64``: plans built on host threads in
+parallel, circuits side by side on several streams; reductions still FP64).
 """
 from __future__ import annotations
 
@@ -94,12 +95,10 @@ class BatchRunner:
                 off += sz
             k = len(wave)
             states = (C.c_void_p * k)(*ptrs)
-            if c64:  # fused tensor-core path, one launch sequence per circuit
-                for i, p in zip(wave, ptrs):
-                    circ = jobs[i][0]
-                    call("qs_circuit_update_quantum_state_fused_c64", circ._h, p, 1 << circ.qubit_count, self.stream)
+            circs = (C.c_void_p * k)(*[jobs[i][0]._h for i in wave])
+            if c64:  # fused tensor-core path: plans built in parallel, circuits side by side on streams
+                call("qs_batch_update_quantum_states_fused_c64", circs, states, k, self.stream)
             else:  # every circuit in one persistent launch
-                circs = (C.c_void_p * k)(*[jobs[i][0]._h for i in wave])
                 call("qs_batch_update_quantum_states", circs, states, k, self.stream)
             # all terms of all observables in one launch
             xm, zm, ny, offs, coefs, nq = [], [], [], [0], [], []

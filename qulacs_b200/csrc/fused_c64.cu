@@ -18,10 +18,12 @@
 // tile stored to HBM.  Every wait is bounded; on expiry the kernel records an error, frees its TMEM
 // and returns.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <complex>
 #include <cstring>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 #include <cuda_bf16.h>
@@ -841,6 +843,8 @@ static int fused_allow_smem() {
     return QS_OK;
 }
 
+static int upload_fused_plan(Circuit& c, ITYPE dim, const FusedPlanHost& H, std::shared_ptr<FusedPlanDev>* out);
+
 // Device plan cached on the circuit (dropped when a gate is added).
 static int fused_plan_dev(Circuit& c, ITYPE dim, std::shared_ptr<FusedPlanDev>* out) {
     if (c.fused && c.fused_dim == dim) {
@@ -849,6 +853,10 @@ static int fused_plan_dev(Circuit& c, ITYPE dim, std::shared_ptr<FusedPlanDev>* 
     }
     FusedPlanHost H;
     QS_TRY(fused_plan_host(c, &H));
+    return upload_fused_plan(c, dim, H, out);
+}
+
+static int upload_fused_plan(Circuit& c, ITYPE dim, const FusedPlanHost& H, std::shared_ptr<FusedPlanDev>* out) {
     auto D = std::make_shared<FusedPlanDev>();
     D->dim = dim;
     const size_t rec_bytes = H.nblocks * (size_t)kRecordBytes;
@@ -880,6 +888,97 @@ static int fused_plan_dev(Circuit& c, ITYPE dim, std::shared_ptr<FusedPlanDev>* 
     c.fused = D;
     c.fused_dim = dim;
     *out = D;
+    return QS_OK;
+}
+
+// Many circuits, each on its own complex64 state: the plans missing from the circuits' caches are
+// built on host threads in parallel (the FP64 block composition and layout search dominate a small
+// circuit's cost), then every circuit's passes are launched round-robin over kBatchStreams streams
+// forked from `st` (a small state occupies few SMs, so circuits run side by side), joined back into
+// `st`, and the completion-wait error flags are read once.
+constexpr int kBatchStreams = 8;
+
+int batch_update_fused_c64(Circuit* const* cs, void* const* states, UINT count, cudaStream_t st) {
+    for (UINT i = 0; i < count; ++i) {
+        if (!cs[i] || !states[i]) return set_error(QS_ERR_INVALID_ARGUMENT, "null circuit or state");
+        if (cs[i]->n < 10) return set_error(QS_ERR_NOT_SUPPORTED, "fused path needs at least 10 qubits");
+    }
+    // 1. host plans in parallel
+    std::vector<FusedPlanHost> H(count);
+    std::vector<int> rc(count, QS_OK), need(count, 0);
+    for (UINT i = 0; i < count; ++i) {
+        const ITYPE dim = 1ULL << cs[i]->n;
+        need[i] = !(cs[i]->fused && cs[i]->fused_dim == dim);
+        for (UINT j = 0; j < i && need[i]; ++j)  // the same circuit twice: build once
+            if (cs[j] == cs[i]) need[i] = 0;
+    }
+    {
+        std::atomic<UINT> next{0};
+        const unsigned nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+        std::vector<std::thread> pool;
+        for (unsigned t = 0; t < nt; ++t)
+            pool.emplace_back([&] {
+                for (UINT i; (i = next.fetch_add(1)) < count;)
+                    if (need[i]) rc[i] = fused_plan_host(*cs[i], &H[i]);
+            });
+        for (std::thread& t : pool) t.join();
+    }
+    for (UINT i = 0; i < count; ++i)
+        if (rc[i] != QS_OK) {  // rebuild here so that the error message is this thread's
+            FusedPlanHost again;
+            return fused_plan_host(*cs[i], &again);
+        }
+    // 2. uploads (device calls from this thread)
+    std::vector<std::shared_ptr<FusedPlanDev>> D(count);
+    for (UINT i = 0; i < count; ++i) {
+        const ITYPE dim = 1ULL << cs[i]->n;
+        if (need[i]) QS_TRY(upload_fused_plan(*cs[i], dim, H[i], &D[i]));
+        else QS_TRY(fused_plan_dev(*cs[i], dim, &D[i]));
+    }
+    QS_TRY(fused_allow_smem());
+    // 3. launches over forked streams
+    cudaEvent_t fork = nullptr;
+    cudaStream_t ss[kBatchStreams] = {};
+    cudaEvent_t joins[kBatchStreams] = {};
+    int out = QS_OK;
+    if (cudaEventCreateWithFlags(&fork, cudaEventDisableTiming) != cudaSuccess || cudaEventRecord(fork, st) != cudaSuccess)
+        out = set_error(QS_ERR_CUDA, "batch fused: event setup failed");
+    for (int k = 0; k < kBatchStreams && out == QS_OK; ++k) {
+        if (cudaStreamCreateWithFlags(&ss[k], cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&joins[k], cudaEventDisableTiming) != cudaSuccess ||
+            cudaStreamWaitEvent(ss[k], fork, 0) != cudaSuccess)
+            out = set_error(QS_ERR_CUDA, "batch fused: stream setup failed");
+    }
+    for (UINT i = 0; i < count && out == QS_OK; ++i) {
+        cudaStream_t s = ss[i % kBatchStreams];
+        for (const FusedPassArgs& p0 : D[i]->passes) {
+            FusedPassArgs p = p0;
+            p.state = (float2*)states[i];
+            const unsigned grid = (unsigned)std::min<ITYPE>((p.tiles + 1) / 2, (ITYPE)sm_count());
+            k_fused_pass<<<grid, kFThreads, fused_smem_bytes(p.m), s>>>(p);
+            out = check_launch("k_fused_pass");
+            if (out != QS_OK) break;
+        }
+    }
+    for (int k = 0; k < kBatchStreams; ++k) {
+        if (ss[k]) {
+            if (joins[k]) {
+                cudaEventRecord(joins[k], ss[k]);
+                cudaStreamWaitEvent(st, joins[k], 0);
+                cudaEventDestroy(joins[k]);
+            }
+            cudaStreamDestroy(ss[k]);  // released once its work completes
+        }
+    }
+    if (fork) cudaEventDestroy(fork);
+    QS_TRY(out);
+    // 4. completion-wait flags, read once
+    std::vector<int> errs(count, 0);
+    for (UINT i = 0; i < count; ++i)
+        QS_CUDA_CHECK(cudaMemcpyAsync(&errs[i], D[i]->err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    QS_CUDA_CHECK(cudaStreamSynchronize(st));
+    for (UINT i = 0; i < count; ++i)
+        if (errs[i]) return set_error(QS_ERR_TIMEOUT, "fused pass: tensor-core completion wait expired");
     return QS_OK;
 }
 
@@ -958,6 +1057,13 @@ QS_API int qs_circuit_update_quantum_state_fused_c64(qs_circuit_t circuit, void*
     if (dim != (1ULL << c->n))
         return qs::set_error(QS_ERR_INVALID_ARGUMENT, "state dimension does not match the circuit's qubit count");
     return qs::run_fused_c64(*c, state_c64, dim, (cudaStream_t)stream);
+}
+
+QS_API int qs_batch_update_quantum_states_fused_c64(qs_circuit_t const* circuits, void* const* states_c64,
+    QS_UINT count, void* stream) {
+    if (!circuits || !states_c64) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "null argument");
+    return qs::batch_update_fused_c64(reinterpret_cast<qs::Circuit* const*>(circuits), states_c64, count,
+        (cudaStream_t)stream);
 }
 
 QS_API int qs_circuit_fused_block_export(qs_circuit_t circuit, QS_UINT index, QS_UINT* tile_qubits, int* tile_qubit_count,
