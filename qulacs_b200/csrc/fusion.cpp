@@ -33,16 +33,23 @@ void apply_gate_to_block(std::vector<cd>& U, int kb, const GateRec& g, const std
     for (int x = 0; x < gd; ++x)
         for (int j = 0; j < nt; ++j)
             if ((x >> j) & 1) off[x] |= 1 << pos[j];
-    std::vector<cd> tmp(gd);
+    // plain real arithmetic: std::complex's operator* goes through the library's inf/nan-checking
+    // routine, which dominated the cost of composing large blocks
+    std::vector<double> tr(gd), ti(gd);
     for (int base = 0; base < md; ++base) {
         if ((base & tmask) || (base & cmask) != cval) continue;
         for (int col = 0; col < md; ++col) {
             for (int y = 0; y < gd; ++y) {
-                cd acc = 0.;
-                for (int x = 0; x < gd; ++x) acc += gm[y * gd + x] * U[(size_t)(base | off[x]) * md + col];
-                tmp[y] = acc;
+                double ar = 0., ai = 0.;
+                for (int x = 0; x < gd; ++x) {
+                    const cd m = gm[y * gd + x], u = U[(size_t)(base | off[x]) * md + col];
+                    ar += m.real() * u.real() - m.imag() * u.imag();
+                    ai += m.real() * u.imag() + m.imag() * u.real();
+                }
+                tr[y] = ar;
+                ti[y] = ai;
             }
-            for (int y = 0; y < gd; ++y) U[(size_t)(base | off[y]) * md + col] = tmp[y];
+            for (int y = 0; y < gd; ++y) U[(size_t)(base | off[y]) * md + col] = cd(tr[y], ti[y]);
         }
     }
 }

@@ -14,8 +14,10 @@
 #include <algorithm>
 #include <cmath>
 #include <complex>
+#include <atomic>
 #include <cstring>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 #include "circuit.hpp"
@@ -788,12 +790,19 @@ static void make_host_plan(const std::vector<GateRec>& gates, UINT n, HostPlan* 
     }
 }
 
+static int upload_plan(const HostPlan& H, ITYPE dim, std::shared_ptr<StagedPlan>* out);
+
 static int build_plan(const std::vector<GateRec>& gates, UINT n, ITYPE dim, std::shared_ptr<StagedPlan>* out,
     int tile_bits = kTileBits) {
-    auto P = std::make_shared<StagedPlan>();
-    P->dim = dim;
     HostPlan H;
     make_host_plan(gates, n, &H, tile_bits);
+    return upload_plan(H, dim, out);
+}
+
+// Device copy of a host plan (phases | ops | parameter pool in one allocation) and its launch args.
+static int upload_plan(const HostPlan& H, ITYPE dim, std::shared_ptr<StagedPlan>* out) {
+    auto P = std::make_shared<StagedPlan>();
+    P->dim = dim;
     const std::vector<PassPlan>& passes = H.passes;
     const std::vector<StPhase>& phases = H.phases;
     const std::vector<StOp>& ops = H.ops;
@@ -1116,11 +1125,43 @@ static int ensure_batch_plan(Circuit& c, ITYPE dim) {
 
 int batch_update(Circuit* const* cs, void* const* states, UINT count, cudaStream_t st) {
     if (count == 0) return QS_OK;
+    for (UINT i = 0; i < count; ++i)
+        if (cs[i]->n < kPhaseBits) return set_error(QS_ERR_NOT_SUPPORTED, "batch: circuits need at least 4 qubits");
+    // missing plans: FP64 fusion and host planning on host threads in parallel, uploads afterwards
+    {
+        std::vector<char> need(count, 0);
+        for (UINT i = 0; i < count; ++i) {
+            const Circuit& c = *cs[i];
+            need[i] = !(c.bplan && c.bplan->dim == (1ULL << c.n) && c.bk == batch_block_size(c));
+            for (UINT j = 0; j < i && need[i]; ++j)
+                if (cs[j] == cs[i]) need[i] = 0;
+        }
+        std::vector<std::vector<GateRec>> fg(count);
+        std::vector<HostPlan> hp(count);
+        std::atomic<UINT> next{0};
+        const unsigned nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+        std::vector<std::thread> pool;
+        for (unsigned t = 0; t < nt; ++t)
+            pool.emplace_back([&] {
+                for (UINT i; (i = next.fetch_add(1)) < count;)
+                    if (need[i]) {
+                        fg[i] = fuse_gates(cs[i]->gates, batch_block_size(*cs[i]));
+                        make_host_plan(fg[i], cs[i]->n, &hp[i], kBatchTileBits);
+                    }
+            });
+        for (std::thread& t : pool) t.join();
+        for (UINT i = 0; i < count; ++i)
+            if (need[i]) {
+                Circuit& c = *cs[i];
+                c.bgates = std::move(fg[i]);
+                c.bk = batch_block_size(c);
+                QS_TRY(upload_plan(hp[i], 1ULL << c.n, &c.bplan));
+            }
+    }
     std::vector<std::vector<const DevPass*>> passes(count);
     size_t maxp = 0;
     for (UINT i = 0; i < count; ++i) {
         Circuit& c = *cs[i];
-        if (c.n < kPhaseBits) return set_error(QS_ERR_NOT_SUPPORTED, "batch: circuits need at least 4 qubits");
         QS_TRY(ensure_batch_plan(c, 1ULL << c.n));
         for (const DevPass& d : c.bplan->passes) {
             if (d.single)
