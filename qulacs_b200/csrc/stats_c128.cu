@@ -1030,14 +1030,30 @@ __global__ void __launch_bounds__(128, kEvTileCtasPerSm) k_ev_tile(const T* __re
         __syncthreads();
         for (int t = warp; t < a.nterms; t += 4) {
             const EvTileTerm tm = terms[t];
-            const UINT par0 = (UINT)(__popcll(base & tm.zglob) & 1);
+            // Re(v i^r) with v = tile[u0] conj(tile[u0 ^ x]) and r = r0 + 2 parity(u0 & zloc): r0 picks
+            // the real or imaginary part of v and an overall sign; the parity flips the sign per pair.
+            // Only that one part of the product is computed.
+            const UINT r0 = (tm.nrot + 2u * (UINT)(__popcll(base & tm.zglob) & 1)) & 3u;
             double sum = 0.;
-            for (UINT p = lane; p < (tsize >> 1); p += 32) {
-                const UINT u0 = (UINT)insert0(p, tm.pivot), u1 = u0 ^ tm.xloc;
-                const double2 v = cmul(tile[u0], cconj(tile[u1]));
-                const UINT r = tm.nrot + 2u * (((UINT)__popc(u0 & tm.zloc) & 1u) ^ par0);
-                sum += 2.0 * phase_re_part(v, r);
+            if (r0 & 1u) {
+                for (UINT p = lane; p < (tsize >> 1); p += 32) {
+                    const UINT u0 = (UINT)insert0(p, tm.pivot);
+                    const double2 x = tile[u0], y = tile[u0 ^ tm.xloc];
+                    const double im = fma(x.y, y.x, -(x.x * y.y));
+                    const unsigned long long flip = (unsigned long long)((UINT)__popc(u0 & tm.zloc) & 1u) << 63;
+                    sum += __longlong_as_double(__double_as_longlong(im) ^ flip);
+                }
+            } else {
+                for (UINT p = lane; p < (tsize >> 1); p += 32) {
+                    const UINT u0 = (UINT)insert0(p, tm.pivot);
+                    const double2 x = tile[u0], y = tile[u0 ^ tm.xloc];
+                    const double re = fma(x.x, y.x, x.y * y.y);
+                    const unsigned long long flip = (unsigned long long)((UINT)__popc(u0 & tm.zloc) & 1u) << 63;
+                    sum += __longlong_as_double(__double_as_longlong(re) ^ flip);
+                }
             }
+            // r0 = 0: +Re, 1: -Im, 2: -Re, 3: +Im
+            sum *= (r0 == 1u || r0 == 2u) ? -2.0 : 2.0;
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
             if (lane == 0) acc[t] += sum;
