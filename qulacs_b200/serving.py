@@ -174,15 +174,24 @@ class ServingLoop:
     # ---- work execution (worker threads; each has its own stream) ----
     def _run_expectation_batch(self, reqs, stream):
         circs = [W.to_circuit(r.gates, r.n) for r in reqs]
-        c64 = self.precision == "c64"
+        if self.precision == "c64":
+            for r, c in zip(reqs, circs):
+                call("qs_initialize_quantum_state_c64", r.ptr, 1 << r.n, stream)
+                call("qs_circuit_update_quantum_state_fused_c64", c._h, r.ptr, 1 << r.n, stream)
+                xm, zm, ny = zip(*[masks(tl, ids) for _, tl, ids in r.terms])
+                vals = np.zeros(len(r.terms))
+                xa, za = np.array(xm, dtype=np.uint64), np.array(zm, dtype=np.uint64)
+                ya = np.array(ny, dtype=np.uint32)
+                call("qs_expectation_value_pauli_batch_c64", _vp(xa), _vp(za), _vp(ya), len(r.terms), r.ptr,
+                     1 << r.n, stream, _vp(vals))
+                r.result = float(np.dot([c for c, _, _ in r.terms], vals))
+            return
         k = len(reqs)
         for r in reqs:
-            call("qs_initialize_quantum_state_c64" if c64 else "qs_initialize_quantum_state", r.ptr, 1 << r.n, stream)
+            call("qs_initialize_quantum_state", r.ptr, 1 << r.n, stream)
         ch = (C.c_void_p * k)(*[c._h for c in circs])
         st = (C.c_void_p * k)(*[r.ptr for r in reqs])
-        # complex64: fused tensor-core passes, the batch's circuits side by side on forked streams
-        call("qs_batch_update_quantum_states_fused_c64" if c64 else "qs_batch_update_quantum_states", ch, st, k,
-             stream)
+        call("qs_batch_update_quantum_states", ch, st, k, stream)
         xm, zm, ny, offs, coefs = [], [], [], [0], []
         for r in reqs:
             for c, tl, ids in r.terms:
@@ -196,8 +205,7 @@ class ServingLoop:
         xa, za = np.array(xm, dtype=np.uint64), np.array(zm, dtype=np.uint64)
         ya, oa = np.array(ny, dtype=np.uint32), np.array(offs, dtype=np.uint32)
         qa = np.array([r.n for r in reqs], dtype=np.uint32)
-        call("qs_batch_expectation_values_c64" if c64 else "qs_batch_expectation_values", st, _vp(qa), k, _vp(oa),
-             _vp(xa), _vp(za), _vp(ya), _vp(vals), stream)
+        call("qs_batch_expectation_values", st, _vp(qa), k, _vp(oa), _vp(xa), _vp(za), _vp(ya), _vp(vals), stream)
         coefs = np.array(coefs)
         for j, r in enumerate(reqs):
             r.result = float(np.dot(coefs[offs[j]:offs[j + 1]], vals[offs[j]:offs[j + 1]]))
