@@ -991,11 +991,43 @@ __device__ __forceinline__ double2 tile_amp<float2>(const float2* p) {
     return make_double2(v.x, v.y);
 }
 
+// One part (C = 0: real, 1: imaginary) of x conj(y), its sign flipped when `flip` is set.
+template <int C>
+__device__ __forceinline__ double part_flipped(double2 x, double2 y, UINT flip) {
+    const double v = C ? fma(x.y, y.x, -(x.x * y.y)) : fma(x.x, y.x, x.y * y.y);
+    return __longlong_as_double(__double_as_longlong(v) ^ ((unsigned long long)flip << 63));
+}
+
+// The sums of one string (or of two strings sharing the pairing bit, which read tile[u0] once) over
+// the tile's pair bases u0 (bit `pivot` clear) of this lane.
+template <int C1>
+__device__ __forceinline__ double ev_single(const double2* tile, UINT half, UINT pivot, UINT x1, UINT z1) {
+    double s1 = 0.;
+    for (UINT p = threadIdx.x & 31; p < half; p += 32) {
+        const UINT u0 = (UINT)insert0(p, pivot);
+        s1 += part_flipped<C1>(tile[u0], tile[u0 ^ x1], (UINT)__popc(u0 & z1) & 1u);
+    }
+    return s1;
+}
+template <int C1, int C2>
+__device__ __forceinline__ void ev_pair(const double2* tile, UINT half, UINT pivot, UINT x1, UINT z1, UINT x2,
+    UINT z2, double* s1, double* s2) {
+    double a1 = 0., a2 = 0.;
+    for (UINT p = threadIdx.x & 31; p < half; p += 32) {
+        const UINT u0 = (UINT)insert0(p, pivot);
+        const double2 x = tile[u0];
+        a1 += part_flipped<C1>(x, tile[u0 ^ x1], (UINT)__popc(u0 & z1) & 1u);
+        a2 += part_flipped<C2>(x, tile[u0 ^ x2], (UINT)__popc(u0 & z2) & 1u);
+    }
+    *s1 = a1;
+    *s2 = a2;
+}
+
 constexpr int kEvTileCtasPerSm = 6;  // 6 x 37 KiB of shared memory; the loads go 4 rows at a time to fit
 
 template <class T>
 __global__ void __launch_bounds__(128, kEvTileCtasPerSm) k_ev_tile(const T* __restrict__ s, ITYPE tiles, const __grid_constant__ EvTileArgs a,
-    const EvTileTerm* __restrict__ terms, double* __restrict__ partials) {
+    const EvTileTerm* __restrict__ terms, int npairs, double* __restrict__ partials) {
     __shared__ double2 tile[1 << kEvTileBits];
     __shared__ double acc[kEvMaxTerms];
     __shared__ ITYPE hi_off[16];
@@ -1017,46 +1049,67 @@ __global__ void __launch_bounds__(128, kEvTileCtasPerSm) k_ev_tile(const T* __re
         ITYPE base = ti;
         for (int j = 0; j < m; ++j) base = insert0(base, a.piv_sorted[j]);
         __syncthreads();
+        if constexpr (sizeof(T) == sizeof(double2)) {
+            // complex128: 16-byte cp.async copies straight into shared memory, all 16 of a thread in flight
+            // without holding registers
 #pragma unroll
-        for (int h = 0; h < 16; h += 4) {
-            double2 v[4];  // four loads in flight per thread before the shared-memory stores
+            for (int k = 0; k < 16; ++k)
+                if ((UINT)tid + (UINT)k * 128 < tsize) {
+                    const unsigned dst = (unsigned)__cvta_generic_to_shared(tile + tid + k * 128);
+                    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst),
+                        "l"(s + (base ^ lo_off ^ hi_off[k])) : "memory");
+                }
+            asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
+        } else {
 #pragma unroll
-            for (int k = 0; k < 4; ++k)
-                if ((UINT)tid + (UINT)(h + k) * 128 < tsize) v[k] = tile_amp<T>(s + (base ^ lo_off ^ hi_off[h + k]));
+            for (int h = 0; h < 16; h += 4) {
+                double2 v[4];  // four loads in flight per thread before the shared-memory stores
 #pragma unroll
-            for (int k = 0; k < 4; ++k)
-                if ((UINT)tid + (UINT)(h + k) * 128 < tsize) tile[tid + (h + k) * 128] = v[k];
+                for (int k = 0; k < 4; ++k)
+                    if ((UINT)tid + (UINT)(h + k) * 128 < tsize) v[k] = tile_amp<T>(s + (base ^ lo_off ^ hi_off[h + k]));
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    if ((UINT)tid + (UINT)(h + k) * 128 < tsize) tile[tid + (h + k) * 128] = v[k];
+            }
         }
         __syncthreads();
-        for (int t = warp; t < a.nterms; t += 4) {
-            const EvTileTerm tm = terms[t];
-            // Re(v i^r) with v = tile[u0] conj(tile[u0 ^ x]) and r = r0 + 2 parity(u0 & zloc): r0 picks
-            // the real or imaginary part of v and an overall sign; the parity flips the sign per pair.
-            // Only that one part of the product is computed.
-            const UINT r0 = (tm.nrot + 2u * (UINT)(__popcll(base & tm.zglob) & 1)) & 3u;
-            double sum = 0.;
-            if (r0 & 1u) {
-                for (UINT p = lane; p < (tsize >> 1); p += 32) {
-                    const UINT u0 = (UINT)insert0(p, tm.pivot);
-                    const double2 x = tile[u0], y = tile[u0 ^ tm.xloc];
-                    const double im = fma(x.y, y.x, -(x.x * y.y));
-                    const unsigned long long flip = (unsigned long long)((UINT)__popc(u0 & tm.zloc) & 1u) << 63;
-                    sum += __longlong_as_double(__double_as_longlong(im) ^ flip);
+        // Re(v i^r) with v = tile[u0] conj(tile[u0 ^ x]) and r = r0 + 2 parity(u0 & zloc): r0 picks the
+        // real or imaginary part of v and an overall sign; the parity flips the sign per pair.  Only
+        // that one part of the product is computed.  Units: terms (2w, 2w + 1) for w < npairs share
+        // their pairing bit; the rest are single.
+        const int nunits = npairs + (a.nterms - 2 * npairs);
+        const UINT half = tsize >> 1;
+        for (int w = warp; w < nunits; w += 4) {
+            const int t1 = w < npairs ? 2 * w : npairs + w;
+            const EvTileTerm m1 = terms[t1];
+            const UINT r1 = (m1.nrot + 2u * (UINT)(__popcll(base & m1.zglob) & 1)) & 3u;
+            double s1 = 0., s2 = 0.;
+            UINT r2 = 0;
+            if (w < npairs) {
+                const EvTileTerm m2 = terms[t1 + 1];
+                r2 = (m2.nrot + 2u * (UINT)(__popcll(base & m2.zglob) & 1)) & 3u;
+                switch (((r1 & 1u) << 1) | (r2 & 1u)) {
+                    case 0: ev_pair<0, 0>(tile, half, m1.pivot, m1.xloc, m1.zloc, m2.xloc, m2.zloc, &s1, &s2); break;
+                    case 1: ev_pair<0, 1>(tile, half, m1.pivot, m1.xloc, m1.zloc, m2.xloc, m2.zloc, &s1, &s2); break;
+                    case 2: ev_pair<1, 0>(tile, half, m1.pivot, m1.xloc, m1.zloc, m2.xloc, m2.zloc, &s1, &s2); break;
+                    default: ev_pair<1, 1>(tile, half, m1.pivot, m1.xloc, m1.zloc, m2.xloc, m2.zloc, &s1, &s2); break;
                 }
             } else {
-                for (UINT p = lane; p < (tsize >> 1); p += 32) {
-                    const UINT u0 = (UINT)insert0(p, tm.pivot);
-                    const double2 x = tile[u0], y = tile[u0 ^ tm.xloc];
-                    const double re = fma(x.x, y.x, x.y * y.y);
-                    const unsigned long long flip = (unsigned long long)((UINT)__popc(u0 & tm.zloc) & 1u) << 63;
-                    sum += __longlong_as_double(__double_as_longlong(re) ^ flip);
-                }
+                s1 = (r1 & 1u) ? ev_single<1>(tile, half, m1.pivot, m1.xloc, m1.zloc)
+                               : ev_single<0>(tile, half, m1.pivot, m1.xloc, m1.zloc);
             }
             // r0 = 0: +Re, 1: -Im, 2: -Re, 3: +Im
-            sum *= (r0 == 1u || r0 == 2u) ? -2.0 : 2.0;
+            s1 *= (r1 == 1u || r1 == 2u) ? -2.0 : 2.0;
+            s2 *= (r2 == 1u || r2 == 2u) ? -2.0 : 2.0;
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
-            if (lane == 0) acc[t] += sum;
+            for (int o = 16; o > 0; o >>= 1) {
+                s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+                s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+            }
+            if (lane == 0) {
+                acc[t1] += s1;
+                if (w < npairs) acc[t1 + 1] += s2;
+            }
         }
     }
     __syncthreads();
@@ -1148,6 +1201,39 @@ int ev_tiled(const PauliTerm* terms, const std::vector<int>& xidx, UINT n, const
             rest->insert(rest->end(), todo.begin(), todo.end());
             break;
         }
+        // pair terms whose local X masks share a bit (it becomes both terms' pairing bit: the pair reads
+        // tile[u0] once); pairs first, then the single terms with their top bit
+        int npairs = 0;
+        {
+            std::vector<EvTileTerm> pt, st1;
+            std::vector<UINT> po, so;
+            std::vector<char> used(tt.size(), 0);
+            for (size_t i = 0; i < tt.size(); ++i) {
+                if (used[i]) continue;
+                used[i] = 1;
+                size_t j = i + 1;
+                for (; j < tt.size(); ++j)
+                    if (!used[j] && (tt[i].xloc & tt[j].xloc)) break;
+                if (j < tt.size()) {
+                    used[j] = 1;
+                    const UINT common = tt[i].xloc & tt[j].xloc;
+                    EvTileTerm e1 = tt[i], e2 = tt[j];
+                    e1.pivot = e2.pivot = (UINT)(31 - __builtin_clz(common));
+                    pt.push_back(e1);
+                    pt.push_back(e2);
+                    po.push_back(outi[i]);
+                    po.push_back(outi[j]);
+                    ++npairs;
+                } else {
+                    st1.push_back(tt[i]);
+                    so.push_back(outi[i]);
+                }
+            }
+            pt.insert(pt.end(), st1.begin(), st1.end());
+            po.insert(po.end(), so.begin(), so.end());
+            tt.swap(pt);
+            outi.swap(po);
+        }
         a.nterms = (int)tt.size();
         const size_t bt = sizeof(EvTileTerm) * tt.size(), bo = sizeof(UINT) * outi.size(),
                      bp = sizeof(double) * grid * tt.size(), bv = sizeof(double) * 1;
@@ -1163,7 +1249,7 @@ int ev_tiled(const PauliTerm* terms, const std::vector<int>& xidx, UINT n, const
         for (size_t i = 0; i < seq.size(); ++i) seq[i] = (UINT)i;
         QS_CUDA_CHECK(cudaMemcpyAsync(dt, tt.data(), bt, cudaMemcpyHostToDevice, st));
         QS_CUDA_CHECK(cudaMemcpyAsync(doi, seq.data(), bo, cudaMemcpyHostToDevice, st));
-        k_ev_tile<T><<<grid, 128, 0, st>>>(s, dim >> a.m, a, dt, dpart);
+        k_ev_tile<T><<<grid, 128, 0, st>>>(s, dim >> a.m, a, dt, npairs, dpart);
         QS_TRY(check_launch("k_ev_tile"));
         k_fold_cols<<<(unsigned)tt.size(), 256, 0, st>>>(dpart, (int)grid, (int)tt.size(), dval, doi);
         QS_TRY(check_launch("k_fold_cols"));
