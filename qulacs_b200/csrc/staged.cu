@@ -244,18 +244,7 @@ __device__ __forceinline__ UINT swz(UINT u) { return u ^ (((u >> 4) ^ (u >> 7) ^
 // Tile index u = tid + k * kStThreads (k < 2^(m-7)) has global offset base | lo_off | hi_off[k]:
 // lo_off takes tid's bits 0..6 to the tile qubits q[0..6], hi_off[k] takes k's bits to q[7..].
 
-// Global rows of 16 amplitudes per thread between HBM and the swizzled tile (rows k0 .. k0 + 15).
-__device__ __forceinline__ void tile_rows_load(const double2* __restrict__ s, double2* tile, ITYPE off,
-    const ITYPE* hi_off, UINT tsize, int k0) {
-    const UINT tid = threadIdx.x;
-    double2 v[16];
-#pragma unroll
-    for (int k = 0; k < 16; ++k)
-        if (tid + (UINT)(k0 + k) * kStThreads < tsize) v[k] = ld_stream(s + (off | hi_off[k0 + k]));
-#pragma unroll
-    for (int k = 0; k < 16; ++k)
-        if (tid + (UINT)(k0 + k) * kStThreads < tsize) tile[swz(tid + (UINT)(k0 + k) * kStThreads)] = v[k];
-}
+// Global rows of 16 amplitudes per thread from the swizzled tile to HBM (rows k0 .. k0 + 15).
 __device__ __forceinline__ void tile_rows_store(double2* __restrict__ s, const double2* tile, ITYPE off,
     const ITYPE* hi_off, UINT tsize, int k0) {
     const UINT tid = threadIdx.x;
@@ -294,9 +283,17 @@ __device__ __forceinline__ void staged_tile(double2* __restrict__ s, const StPas
         __syncthreads();
     }
     if (!hbm_first) {
-        tile_rows_load(s, tile, base | lo_off, hi_off, tsize, 0);
-        if constexpr (MAX_BITS > 11)
-            if (tsize > 16 * kStThreads) tile_rows_load(s, tile, base | lo_off, hi_off, tsize, 16);
+        // 16-byte cp.async copies straight into the swizzled tile: every copy of a thread in flight at
+        // once, without holding registers
+        const ITYPE off = base | lo_off;
+#pragma unroll
+        for (int k = 0; k < (1 << (MAX_BITS - 7)); ++k)
+            if ((UINT)tid + (UINT)k * kStThreads < tsize) {
+                const unsigned dst = (unsigned)__cvta_generic_to_shared(tile + swz((UINT)tid + (UINT)k * kStThreads));
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(s + (off | hi_off[k]))
+                             : "memory");
+            }
+        asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
         __syncthreads();
     }
     const UINT ncos = tsize >> kPhaseBits;  // cosets per phase
