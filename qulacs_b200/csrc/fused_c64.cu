@@ -353,6 +353,17 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused_pass(const __grid_consta
         __syncthreads();
         if (*s_err) break;
         gather(TX, TY, hasY, slot);
+        if (has_next) {  // the next pair's 256-byte runs into L2 while this pair's blocks run
+            const ITYPE T2 = TX + stride + (tid >= 256 ? (ITYPE)gridDim.x : 0);
+            const uint32_t r = (uint32_t)tid & 255u;
+            if (T2 < a.tiles && r < (tsize >> kFLow)) {
+                ITYPE off = 0;
+                for (int j = kFLow; j < m; ++j)
+                    if ((r >> (j - kFLow)) & 1u) off |= 1ULL << a.q[j];
+                asm volatile("cp.async.bulk.prefetch.L2.global [%0], 256;" ::"l"(a.state + (tile_base(T2) | off))
+                             : "memory");
+            }
+        }
         for (int b = 0; b < a.nblocks; ++b) {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             asm volatile("tcgen05.fence::before_thread_sync;");
