@@ -12,9 +12,9 @@
 // rounding order (~1e-16).  Gates the pass kernel does not cover (more than 2 targets, controls,
 // Pauli strings, multi-qubit diagonals) run between passes with the gate-by-gate kernels.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <complex>
-#include <atomic>
 #include <cstring>
 #include <mutex>
 #include <thread>
