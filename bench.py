@@ -340,6 +340,58 @@ def noise_sampling(n: int = 20, depth: int = 4, p: float = 1e-3, shots: int = 10
     return res
 
 
+def dm_noisy_circuit(n: int = 13, depth: int = 8, p: float = 1e-3, seed: int = 7007, reps: int = 3):
+    """Density matrix (rows a16-a18): HEA circuit with depolarizing noise after every gate on an n-qubit
+    density matrix (4^n entries, 1 GiB at 13 qubits), the exact channel, through the FP64-fused staged
+    executor and through the gate-by-gate DM kernels.  Effective bandwidth counts 2 x 16 x 4^n bytes per
+    gate or channel.  CPU: the reference csim's DM functions on a bounded sample of the ops."""
+    import torch
+
+    import qulacs_b200 as Q
+    from qulacs_b200 import workloads as W
+    gates = W.noisy_circuit(W.hea_circuit(n, depth, seed), p)
+    circ = W.to_circuit(gates, n)
+    rho = Q.DensityMatrix(n)
+    per_op = 2.0 * 16.0 * float(4 ** n)
+    res = {"workload": f"HEA n={n} depth={depth} + depolarizing p={p} after every gate, density matrix "
+                       f"({len(gates)} gates and channels, {16 * 4 ** n / 2 ** 30:.2f} GiB)"}
+    for mode in ("staged_fused", "gate_by_gate"):
+        for _ in range(2):
+            rho.set_zero_state()
+            circ.update_quantum_state(rho, mode=mode)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            rho.set_zero_state()
+            circ.update_quantum_state(rho, mode=mode)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        res[mode] = {"ms": ms, "effective_gbs": len(gates) * per_op / (ms / 1e3) / 1e9}
+    res["trace"] = rho.get_squared_norm()  # DensityMatrix squared norm = trace (cppsim state_dm.hpp:142)
+    try:
+        from oracle import oracle as O
+        ref = O.reference()
+        if ref is None:
+            raise RuntimeError("reference csim not built")
+        r = np.zeros((1 << n, 1 << n), dtype=np.complex128)
+        r[0, 0] = 1
+        t0 = time.perf_counter()
+        done = 0
+        for g in gates:
+            W.run_on_cpu_dm([g], r, ref)
+            done += 1
+            if time.perf_counter() - t0 > 10.0:
+                break
+        dt = time.perf_counter() - t0
+        res["cpu_reference"] = {"effective_gbs": done * per_op / dt / 1e9, "ops_timed": done, "seconds": dt,
+                                "cores": os.cpu_count() or 1}
+    except Exception as e:  # noqa: BLE001
+        res["cpu_reference"] = f"unavailable: {type(e).__name__}: {e}"
+    return res
+
+
 def timed_region(step, steps: int, warmup: int, dist=None, sync=None, make_timer=None, device: str = "cpu") -> float:
     """The timing contract: `warmup` untimed steps, then a barrier with a device synchronize on both
     sides, exactly `steps` timed steps, a synchronize, and the per-step time in ms as the MAX over
@@ -425,8 +477,9 @@ def main():
     ap.add_argument("--qubits", type=int, default=N_QUBITS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-kernel-table", action="store_true")
-    ap.add_argument("--workload", default="plain", choices=["plain", "fused", "batched", "serving", "noise"],
-                    help="fused / batched / serving: only that comparison (configs 3 / 4 / 5)")
+    ap.add_argument("--workload", default="plain", choices=["plain", "fused", "batched", "serving", "noise", "dm"],
+                    help="fused / batched / serving / noise / dm: only that measurement (configs 3 / 4 / 5, "
+                         "NoiseSimulator, noisy density matrix)")
     ap.add_argument("--instances", type=int, default=4096)
     ap.add_argument("--budget-gb", type=float, default=96.0)
     ap.add_argument("--requests", type=int, default=120)
@@ -473,6 +526,11 @@ def main():
         r = batched_throughput(args.instances, args.budget_gb)
         if rank == 0:
             print(json.dumps({"metric": "batched uneven circuits: circuits/s", **r}), flush=True)
+        return
+    if args.workload == "dm":
+        r = dm_noisy_circuit()
+        if rank == 0:
+            print(json.dumps({"metric": "noisy density matrix: effective GB/s", **r}), flush=True)
         return
     if args.workload == "noise":
         r = noise_sampling()
@@ -592,7 +650,8 @@ def main():
         for key, fn in (("fused", lambda: fused_comparison(args.fused_qubits, args.fused_layers, stream, False)),
                         ("batched", lambda: batched_throughput(512, 64.0)),
                         ("serving", lambda: serving_latency(60, 5.0, 96.0, 4)),
-                        ("noise", lambda: noise_sampling())):
+                        ("noise", lambda: noise_sampling()),
+                        ("density_matrix", lambda: dm_noisy_circuit())):
             try:
                 extras[key] = fn()
             except Exception as e:  # noqa: BLE001
