@@ -92,3 +92,15 @@ def test_batch_mixed_sizes_across_the_single_state_threshold(port, precision):
         W.run_on_cpu(gates, psi, port)
         want = sum(c * port.expectation_value(tl, ids, psi) for c, tl, ids in terms)
         assert abs(e - want) <= (EV_TOL if precision == "c128" else 1e-5), (n, e, want)
+
+
+@pytest.mark.parametrize("precision", ["c128", "c64"])
+def test_batch_repeats_a_circuit_and_reuses_plans(precision):
+    """The same circuit object twice in one batch (its plan built once), then the batch again with the
+    plans cached: every copy of a job gives the same energy."""
+    jobs, _ = make_jobs(23, 5, 10, 13)
+    jobs = jobs + [jobs[1], jobs[3]]
+    first = BatchRunner(1 << 30, precision=precision).run(jobs)
+    again = BatchRunner(1 << 30, precision=precision).run(jobs)
+    assert first[5] == first[1] and first[6] == first[3]
+    assert np.array_equal(first, again)
