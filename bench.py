@@ -638,13 +638,15 @@ def main():
             torch.cuda.synchronize()
             modes_ms[other] = e0.elapsed_time(e1) / reps
 
+    # the CPU baseline and the other configurations run at N = 1 only: with N > 1 ranks they would
+    # keep the other ranks waiting at the closing barrier
     cpu = None
-    if rank == 0 and not args.no_cpu_baseline:
+    if world == 1 and not args.no_cpu_baseline:
         cpu = cpu_reference_gbs(n, gates, 12.0, os.cpu_count() or 1)
 
     # configs 3-5 beside the headline (each guarded: a failure is reported, not fatal)
     extras = {}
-    if not args.no_extras:
+    if world == 1 and not args.no_extras:
         del state
         torch.cuda.synchronize()
         for key, fn in (("fused", lambda: fused_comparison(args.fused_qubits, args.fused_layers, stream, False)),
