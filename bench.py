@@ -143,7 +143,7 @@ def kernel_table(state, n: int, stream, reps: int = 5):
         (f"dense2 {n - 2},{n - 1} (k_dense2)", 1.0, lambda: call("qs_double_qubit_dense_matrix_gate_c", n - 2, n - 1, mp(mats[2]), p, dim, h)),
     ]
     for k in range(3, 7):
-        cases.append((f"dense{k} high targets (k_denseK)", 1.0,
+        cases.append((f"dense{k} high targets ({'k_denseK_blk' if k == 6 else 'k_denseK_reg'})", 1.0,
                       lambda k=k: call("qs_multi_qubit_dense_matrix_gate", mp(tls[k]), k, mp(mats[k]), p, dim, h)))
     out = []
     alg = bytes_per_gate(n)

@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "qs_internal.cuh"
@@ -189,39 +190,6 @@ __global__ void __launch_bounds__(kThreads) k_dense2(double2* __restrict__ s, IT
     }
 }
 
-// k-qubit dense (3 <= k <= 6), optionally controlled.  A CTA stages C cosets x 2^k amplitudes
-// (2048 amplitudes, 32 KiB) in shared memory, then every thread computes outputs (y, c) with the
-// warp sharing the matrix row y (a broadcast read) and reading consecutive cosets c.
-constexpr int kDenseTile = 2048;
-__global__ void __launch_bounds__(kThreads) k_denseK(double2* __restrict__ s, ITYPE cosets, const __grid_constant__ Positions pos,
-    ITYPE fixed, int k, const UINT* __restrict__ tgt, const double2* __restrict__ mat) {
-    extern __shared__ double2 tile[];
-    __shared__ ITYPE masks[64];
-    const int md = 1 << k;
-    const int C = kDenseTile >> k;
-    if (threadIdx.x < md) {
-        ITYPE mk = 0;
-        for (int j = 0; j < k; ++j)
-            if ((threadIdx.x >> j) & 1) mk |= 1ULL << tgt[j];
-        masks[threadIdx.x] = mk;
-    }
-    __syncthreads();
-    const ITYPE c0 = (ITYPE)blockIdx.x * C;
-    for (int idx = threadIdx.x; idx < kDenseTile; idx += kThreads) {
-        const int x = idx / C, c = idx % C;
-        if (c0 + c < cosets) tile[idx] = ld_stream(s + ((expand(c0 + c, pos) | fixed) | masks[x]));
-    }
-    __syncthreads();
-    for (int idx = threadIdx.x; idx < kDenseTile; idx += kThreads) {
-        const int y = idx / C, c = idx % C;
-        if (c0 + c >= cosets) continue;
-        const double2* row = mat + (size_t)y * md;
-        double2 acc = make_double2(0., 0.);
-        for (int x = 0; x < md; ++x) acc = cfma(__ldg(row + x), tile[x * C + c], acc);
-        st_stream(s + ((expand(c0 + c, pos) | fixed) | masks[y]), acc);
-    }
-}
-
 // Pauli string P = i^{nY} X^x Z^z (csim/utility.cpp:12-43); P|i> = ph(i) |i ^ x>.
 __device__ __forceinline__ double2 pauli_phase(ITYPE i, ITYPE zm, UINT nrot) {
     const UINT r = (nrot + 2u * (UINT)(__popcll(i & zm) & 1)) & 3u;
@@ -345,6 +313,107 @@ __global__ void __launch_bounds__(128) k_denseK_reg(double2* __restrict__ s, ITY
     }
 }
 
+// k-qubit dense, register-blocked (used for k = 6, where a coset per thread in registers would spill):
+// a persistent CTA (256 threads) keeps the matrix transposed in shared memory (UT[x][y] = U[y][x])
+// and works through tiles of 16 CP cosets: the tile's amplitudes X[x][c] arrive by cp.async, thread
+// (ty, tc) = (tid % 16, tid / 16) accumulates outputs y = ty + 16 j (j < 2^k / 16) of cosets
+// c = tc + 16 i (i < CP) -- per x it reads 2^k / 16 matrix entries (the half-warps share them) and CP
+// amplitudes for 2^k CP / 16 complex FMAs -- writes them back over X, and the tile leaves with the
+// same coalesced pattern it came in.  k = 6: CP = 2 (2 CTAs per SM) 33 ms at 30 qubits; CP = 4
+// (1 CTA per SM) 38 ms; the earlier one-output-per-thread shared-memory kernel 64 ms.
+constexpr int kBlkThreads = 256;
+
+template <int K, int CP>
+__global__ void __launch_bounds__(kBlkThreads, CP <= 2 ? 2 : 1) k_denseK_blk(double2* __restrict__ s, ITYPE cosets,
+    const __grid_constant__ Positions pos, ITYPE fixed, const double2* __restrict__ gm,
+    const ITYPE* __restrict__ gmask) {
+    constexpr int D = 1 << K, R = D / 16, C = 16 * CP;
+    extern __shared__ double2 blk_smem[];
+    double2* UT = blk_smem;       // D x D
+    double2* X = blk_smem + D * D;  // D x C, then the outputs
+    __shared__ ITYPE mask[D];
+    const int tid = threadIdx.x, ty = tid & 15, tc = tid >> 4;
+    for (int i = tid; i < D * D; i += kBlkThreads) UT[(i % D) * D + i / D] = __ldg(gm + i);
+    for (int i = tid; i < D; i += kBlkThreads) mask[i] = gmask[i];
+    __syncthreads();
+    const ITYPE ntiles = (cosets + C - 1) / C;
+    for (ITYPE T = blockIdx.x; T < ntiles; T += gridDim.x) {
+        const ITYPE c0 = T * C;
+        for (int i = tid; i < D * C; i += kBlkThreads) {  // X[x][c], c fastest: a warp reads 32 cosets
+            const int x = i / C, c = i % C;
+            if (c0 + c < cosets) {
+                const unsigned dst = (unsigned)__cvta_generic_to_shared(X + i);
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst),
+                    "l"(s + ((expand(c0 + c, pos) | fixed) | mask[x])) : "memory");
+            }
+        }
+        asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
+        __syncthreads();
+        double2 acc[R][CP];
+#pragma unroll
+        for (int j = 0; j < R; ++j)
+#pragma unroll
+            for (int i = 0; i < CP; ++i) acc[j][i] = make_double2(0., 0.);
+#pragma unroll 4
+        for (int x = 0; x < D; ++x) {
+            double2 b[CP];
+#pragma unroll
+            for (int i = 0; i < CP; ++i) b[i] = X[x * C + tc + 16 * i];
+#pragma unroll
+            for (int j = 0; j < R; ++j) {
+                const double2 aj = UT[x * D + ty + 16 * j];
+#pragma unroll
+                for (int i = 0; i < CP; ++i) acc[j][i] = cfma(aj, b[i], acc[j][i]);
+            }
+        }
+        __syncthreads();  // every X read done: the outputs go over it
+#pragma unroll
+        for (int j = 0; j < R; ++j)
+#pragma unroll
+            for (int i = 0; i < CP; ++i) X[(ty + 16 * j) * C + tc + 16 * i] = acc[j][i];
+        __syncthreads();
+        for (int i = tid; i < D * C; i += kBlkThreads) {
+            const int y = i / C, c = i % C;
+            if (c0 + c < cosets) st_stream(s + ((expand(c0 + c, pos) | fixed) | mask[y]), X[i]);
+        }
+        __syncthreads();  // the next tile's copies overwrite X
+    }
+}
+
+template <int K, int CP>
+static int launch_denseK_blk(const UINT* tl, const double* matrix, double2* s, const Positions& pos, ITYPE fixed,
+    ITYPE cosets, cudaStream_t st) {
+    constexpr int D = 1 << K, kBlkCosets = 16 * CP;
+    static std::mutex mu;
+    static std::vector<char> ready;
+    int dev = 0;
+    QS_CUDA_CHECK(cudaGetDevice(&dev));
+    const size_t smem = sizeof(double2) * ((size_t)D * D + (size_t)D * kBlkCosets);
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if ((int)ready.size() <= dev) ready.resize(dev + 1, 0);
+        if (!ready[dev]) {
+            QS_CUDA_CHECK(cudaFuncSetAttribute(k_denseK_blk<K, CP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                (int)smem));
+            ready[dev] = 1;
+        }
+    }
+    std::vector<ITYPE> mk(D, 0);
+    for (int x = 0; x < D; ++x)
+        for (int j = 0; j < K; ++j)
+            if ((x >> j) & 1) mk[x] |= 1ULL << tl[j];
+    const size_t mbytes = (size_t)16 * D * D;
+    void* buf = nullptr;
+    QS_TRY(scratch(st, mbytes + sizeof(ITYPE) * D + 256, &buf));
+    ITYPE* dmask = (ITYPE*)((char*)buf + mbytes);
+    QS_CUDA_CHECK(cudaMemcpyAsync(buf, matrix, mbytes, cudaMemcpyHostToDevice, st));
+    QS_CUDA_CHECK(cudaMemcpyAsync(dmask, mk.data(), sizeof(ITYPE) * D, cudaMemcpyHostToDevice, st));
+    const ITYPE ntiles = (cosets + kBlkCosets - 1) / kBlkCosets;
+    const unsigned grid = (unsigned)std::min<ITYPE>(ntiles, (ITYPE)sm_count() * (CP <= 2 ? 2 : 1));
+    k_denseK_blk<K, CP><<<grid, kBlkThreads, smem, st>>>(s, cosets, pos, fixed, (const double2*)buf, dmask);
+    return check_launch("k_denseK_blk");
+}
+
 template <int K>
 static int launch_denseK_reg(const UINT* tl, const double* matrix, double2* s, ITYPE dim, const Positions& pos,
     ITYPE fixed, ITYPE cosets, cudaStream_t st) {
@@ -383,18 +452,7 @@ int launch_denseK(const UINT* tl, UINT k, const double* matrix, double2* s, ITYP
         case 3: return launch_denseK_reg<3>(tl, matrix, s, dim, pos, cm, cosets, st);
         case 4: return launch_denseK_reg<4>(tl, matrix, s, dim, pos, cm, cosets, st);
         case 5: return launch_denseK_reg<5>(tl, matrix, s, dim, pos, cm, cosets, st);
-        case 6: {  // 64 register amplitudes would spill: stage cosets in shared memory instead
-            const size_t mbytes = (size_t)16 << 12;
-            void* buf = nullptr;
-            QS_TRY(scratch(st, mbytes + 256, &buf));
-            UINT* dtl = (UINT*)((char*)buf + mbytes);
-            QS_CUDA_CHECK(cudaMemcpyAsync(buf, matrix, mbytes, cudaMemcpyHostToDevice, st));
-            QS_CUDA_CHECK(cudaMemcpyAsync(dtl, tl, sizeof(UINT) * 6, cudaMemcpyHostToDevice, st));
-            const int C = kDenseTile >> 6;
-            k_denseK<<<blocks_for(cosets, C), kThreads, kDenseTile * sizeof(double2), st>>>(
-                s, cosets, pos, cm, 6, dtl, (const double2*)buf);
-            return check_launch("k_denseK");
-        }
+        case 6: return launch_denseK_blk<6, 2>(tl, matrix, s, pos, cm, cosets, st);  // 64 register amplitudes would spill
         default: return set_error(QS_ERR_NOT_SUPPORTED, "dense gate: 3..6 targets expected here");
     }
 }
