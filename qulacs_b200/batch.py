@@ -18,7 +18,7 @@ import numpy as np
 from . import _lib
 from ._lib import call
 from .observable import masks
-from .state import QuantumState, QuantumStateC64
+from .state import QuantumState
 
 ALIGN = 256
 
