@@ -273,7 +273,7 @@ static int pauli_term(const UINT* tl, const UINT* ids, UINT cnt, UINT n, PauliTe
 constexpr int kEvTileBitsDecl = 11;  // tile qubits of the many-terms-per-pass kernel below
 template <class T>
 int ev_tiled(const PauliTerm* terms, const std::vector<int>& xidx, UINT n, const T* s, ITYPE dim, cudaStream_t st,
-    double* values, std::vector<int>* rest);
+    double* values, std::vector<int>* rest, std::vector<int>* zidx);
 
 template <class T>
 int ev_batch(const PauliTerm* terms, UINT count, const T* s, ITYPE dim, cudaStream_t st, double* values) {
@@ -286,7 +286,20 @@ int ev_batch(const PauliTerm* terms, UINT count, const T* s, ITYPE dim, cudaStre
     QS_TRY(scratch(st, sizeof(double) * part_doubles + sizeof(ITYPE) * kZChunk + 1024, &buf));
     double* part = (double*)buf;
     ITYPE* dz = (ITYPE*)((char*)buf + sizeof(double) * part_doubles);
-    // Z-only terms: kZChunk per pass.
+    // many terms with a bit flip: evaluate them from shared-memory tiles, several terms per pass; the
+    // Z-only terms ride along in the first tiled pass
+    UINT n = 0;
+    while ((1ULL << n) < dim) ++n;
+    if (n >= (UINT)kEvTileBitsDecl && xidx.size() >= 4) {
+        std::vector<int> rest;
+        QS_TRY(ev_tiled<T>(terms, xidx, n, s, dim, st, values, &rest, &zidx));
+        xidx.swap(rest);
+        // the tiled passes may have grown (and so moved) this stream's scratch buffer
+        QS_TRY(scratch(st, sizeof(double) * part_doubles + sizeof(ITYPE) * kZChunk + 1024, &buf));
+        part = (double*)buf;
+        dz = (ITYPE*)((char*)buf + sizeof(double) * part_doubles);
+    }
+    // Z-only terms left: kZChunk per pass.
     for (size_t c0 = 0; c0 < zidx.size(); c0 += kZChunk) {
         const int nz = (int)std::min<size_t>(kZChunk, zidx.size() - c0);
         ITYPE hz[kZChunk];
@@ -297,14 +310,6 @@ int ev_batch(const PauliTerm* terms, UINT count, const T* s, ITYPE dim, cudaStre
         double out[kZChunk];
         QS_TRY(finish_reduce(part, blocks, nz, st, out));
         for (int w = 0; w < nz; ++w) values[zidx[c0 + w]] = out[w];
-    }
-    // many terms with a bit flip: evaluate them from shared-memory tiles, several terms per pass
-    UINT n = 0;
-    while ((1ULL << n) < dim) ++n;
-    if (n >= (UINT)kEvTileBitsDecl && xidx.size() >= 4) {
-        std::vector<int> rest;
-        QS_TRY(ev_tiled<T>(terms, xidx, n, s, dim, st, values, &rest));
-        xidx.swap(rest);
     }
     const unsigned xblocks = reduce_blocks(dim / 2);
     for (int k : xidx) {
@@ -974,6 +979,7 @@ struct EvTileArgs {
     ITYPE b[kEvTileBits];
     UINT piv_sorted[kEvTileBits];
     int nterms;
+    int nz;  // the last nz terms are Z-only strings (no bit flip)
 };
 struct EvTileTerm {
     UINT xloc, zloc;  // masks over tile bits
@@ -1006,6 +1012,16 @@ __device__ __forceinline__ double ev_single(const double2* tile, UINT half, UINT
     for (UINT p = threadIdx.x & 31; p < half; p += 32) {
         const UINT u0 = (UINT)insert0(p, pivot);
         s1 += part_flipped<C1>(tile[u0], tile[u0 ^ x1], (UINT)__popc(u0 & z1) & 1u);
+    }
+    return s1;
+}
+// The sum of one Z-only string over the tile: |tile[u]|^2 with the sign of parity(u & z1), this lane's u.
+__device__ __forceinline__ double ev_diag(const double2* tile, UINT tsize, UINT z1) {
+    double s1 = 0.;
+    for (UINT u = threadIdx.x & 31; u < tsize; u += 32) {
+        const double2 v = tile[u];
+        const double p = fma(v.x, v.x, v.y * v.y);
+        s1 += __longlong_as_double(__double_as_longlong(p) ^ ((unsigned long long)(__popc(u & z1) & 1u) << 63));
     }
     return s1;
 }
@@ -1076,8 +1092,10 @@ __global__ void __launch_bounds__(128, kEvTileCtasPerSm) k_ev_tile(const T* __re
         // Re(v i^r) with v = tile[u0] conj(tile[u0 ^ x]) and r = r0 + 2 parity(u0 & zloc): r0 picks the
         // real or imaginary part of v and an overall sign; the parity flips the sign per pair.  Only
         // that one part of the product is computed.  Units: terms (2w, 2w + 1) for w < npairs share
-        // their pairing bit; the rest are single.
+        // their pairing bit; the rest are single, the last a.nz of them Z-only strings (sum of |a|^2 with
+        // the parity sign; their r is 0 or 2, so the factor is +-1 instead of +-2).
         const int nunits = npairs + (a.nterms - 2 * npairs);
+        const int zfirst = nunits - a.nz;
         const UINT half = tsize >> 1;
         for (int w = warp; w < nunits; w += 4) {
             const int t1 = w < npairs ? 2 * w : npairs + w;
@@ -1085,6 +1103,7 @@ __global__ void __launch_bounds__(128, kEvTileCtasPerSm) k_ev_tile(const T* __re
             const UINT r1 = (m1.nrot + 2u * (UINT)(__popcll(base & m1.zglob) & 1)) & 3u;
             double s1 = 0., s2 = 0.;
             UINT r2 = 0;
+            double f1 = (r1 == 1u || r1 == 2u) ? -2.0 : 2.0;
             if (w < npairs) {
                 const EvTileTerm m2 = terms[t1 + 1];
                 r2 = (m2.nrot + 2u * (UINT)(__popcll(base & m2.zglob) & 1)) & 3u;
@@ -1094,12 +1113,15 @@ __global__ void __launch_bounds__(128, kEvTileCtasPerSm) k_ev_tile(const T* __re
                     case 2: ev_pair<1, 0>(tile, half, m1.pivot, m1.xloc, m1.zloc, m2.xloc, m2.zloc, &s1, &s2); break;
                     default: ev_pair<1, 1>(tile, half, m1.pivot, m1.xloc, m1.zloc, m2.xloc, m2.zloc, &s1, &s2); break;
                 }
-            } else {
+            } else if (w < zfirst) {
                 s1 = (r1 & 1u) ? ev_single<1>(tile, half, m1.pivot, m1.xloc, m1.zloc)
                                : ev_single<0>(tile, half, m1.pivot, m1.xloc, m1.zloc);
+            } else {
+                s1 = ev_diag(tile, tsize, m1.zloc);
+                f1 *= 0.5;
             }
             // r0 = 0: +Re, 1: -Im, 2: -Re, 3: +Im
-            s1 *= (r1 == 1u || r1 == 2u) ? -2.0 : 2.0;
+            s1 *= f1;
             s2 *= (r2 == 1u || r2 == 2u) ? -2.0 : 2.0;
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
@@ -1132,7 +1154,7 @@ __global__ void k_fold_cols(const double* __restrict__ part, int rows, int cols,
 // for the one-pass-per-term kernel.
 template <class T>
 int ev_tiled(const PauliTerm* terms, const std::vector<int>& xidx, UINT n, const T* s, ITYPE dim, cudaStream_t st,
-    double* values, std::vector<int>* rest) {
+    double* values, std::vector<int>* rest, std::vector<int>* zidx) {
     const int m = kEvTileBits;
     std::vector<int> todo = xidx;
     const unsigned grid = (unsigned)std::min<ITYPE>(dim >> m, (ITYPE)sm_count() * kEvTileCtasPerSm);
@@ -1234,6 +1256,26 @@ int ev_tiled(const PauliTerm* terms, const std::vector<int>& xidx, UINT n, const
             tt.swap(pt);
             outi.swap(po);
         }
+        // the Z-only strings join the first pass (any tile basis serves them)
+        a.nz = 0;
+        if (zidx && !zidx->empty()) {
+            std::vector<int> zleft;
+            for (int k : *zidx) {
+                if ((int)tt.size() >= kEvMaxTerms) {
+                    zleft.push_back(k);
+                    continue;
+                }
+                EvTileTerm e{};
+                for (int jj = 0; jj < a.m; ++jj)
+                    if (__builtin_popcountll(basis[jj] & terms[k].z) & 1) e.zloc |= 1u << jj;
+                e.zglob = terms[k].z;
+                e.nrot = terms[k].nrot;
+                tt.push_back(e);
+                outi.push_back((UINT)k);
+                ++a.nz;
+            }
+            zidx->swap(zleft);
+        }
         a.nterms = (int)tt.size();
         const size_t bt = sizeof(EvTileTerm) * tt.size(), bo = sizeof(UINT) * outi.size(),
                      bp = sizeof(double) * grid * tt.size(), bv = sizeof(double) * 1;
@@ -1263,8 +1305,8 @@ int ev_tiled(const PauliTerm* terms, const std::vector<int>& xidx, UINT n, const
 }
 
 template int ev_tiled<double2>(const PauliTerm*, const std::vector<int>&, UINT, const double2*, ITYPE, cudaStream_t,
-    double*, std::vector<int>*);
+    double*, std::vector<int>*, std::vector<int>*);
 template int ev_tiled<float2>(const PauliTerm*, const std::vector<int>&, UINT, const float2*, ITYPE, cudaStream_t,
-    double*, std::vector<int>*);
+    double*, std::vector<int>*, std::vector<int>*);
 
 }  // namespace qs

@@ -52,6 +52,24 @@ def test_expectation_values_single_and_batch(port, n):
     assert abs(obs.get_expectation_value(s) - float(np.dot(coefs, want))) <= EV_TOL
 
 
+def test_expectation_values_many_z_strings(port):
+    """Z-only strings share the first tiled pass with the bit-flip strings up to the per-pass term cap
+    (512); the rest go through the Z-only batch kernel."""
+    n = 14
+    rng = np.random.default_rng(870)
+    a = random_state(n, rng)
+    s = dev(a)
+    terms = W.random_pauli_terms(n, 24, 1, 4, seed=871)
+    for _ in range(600):
+        w = int(rng.integers(1, 6))
+        terms.append((float(rng.normal()), [int(x) for x in rng.choice(n, size=w, replace=False)], [3] * w))
+    obs = Observable(n)
+    for coef, tl, ids in terms:
+        obs.add_operator(PauliOperator(coef=coef, targets=tl, pauli_ids=ids))
+    want = np.array([port.expectation_value(tl, ids, a) for _, tl, ids in terms])
+    assert np.max(np.abs(obs.term_values(s) - want)) <= EV_TOL
+
+
 def test_transition_amplitude(port, ref):
     rng = np.random.default_rng(850)
     n = 8
