@@ -33,7 +33,7 @@ typedef unsigned long long QS_ITYPE; /* csim ITYPE (src/csim/type.hpp:29) */
 #define QS_ERR_OUT_OF_MEMORY 2    /* cudaMalloc failed (the reference calls exit(1), memory_ops.cpp:21-25) */
 #define QS_ERR_CUDA 3             /* any other CUDA runtime error */
 #define QS_ERR_TIMEOUT 4          /* a bounded device wait expired (persistent executor) */
-#define QS_ERR_NOT_SUPPORTED 5    /* valid request outside this build's limits */
+#define QS_ERR_NOT_SUPPORTED 5    /* valid request outside this library's limits */
 #define QS_ERR_NO_DEVICE 6        /* no CUDA device visible */
 #define QS_ERR_REJECTED 7         /* admission control refused a request (serving loop) */
 
@@ -148,7 +148,7 @@ QS_API int qs_SWAP_gate(QS_UINT target_qubit_index_0, QS_UINT target_qubit_index
 /* update_ops.hpp:1277 double_qubit_dense_matrix_gate_c (matrix bit 0 <-> t1, bit 1 <-> t2) */
 QS_API int qs_double_qubit_dense_matrix_gate_c(QS_UINT target_qubit_index1,
     QS_UINT target_qubit_index2, const double matrix[32], void* state, QS_ITYPE dim, void* stream);
-/* update_ops.hpp:1330 multi_qubit_dense_matrix_gate; this build supports 1 <= count <= 6. */
+/* update_ops.hpp:1330 multi_qubit_dense_matrix_gate; this library supports 1 <= count <= 12. */
 QS_API int qs_multi_qubit_dense_matrix_gate(const QS_UINT* target_qubit_index_list,
     QS_UINT target_qubit_index_count, const double* matrix, void* state, QS_ITYPE dim, void* stream);
 /* update_ops.hpp:1459 multi_qubit_diagonal_matrix_gate; 1 <= count <= 20. */
@@ -164,7 +164,7 @@ QS_API int qs_multi_qubit_control_single_qubit_dense_matrix_gate(
     const QS_UINT* control_qubit_index_list, const QS_UINT* control_value_list,
     QS_UINT control_qubit_index_count, QS_UINT target_qubit_index, const double matrix[8],
     void* state, QS_ITYPE dim, void* stream);
-/* update_ops.hpp:1445 multi_qubit_control_multi_qubit_dense_matrix_gate; targets <= 6. */
+/* update_ops.hpp:1445 multi_qubit_control_multi_qubit_dense_matrix_gate; targets <= 12. */
 QS_API int qs_multi_qubit_control_multi_qubit_dense_matrix_gate(
     const QS_UINT* control_qubit_index_list, const QS_UINT* control_value_list,
     QS_UINT control_qubit_index_count, const QS_UINT* target_qubit_index_list,

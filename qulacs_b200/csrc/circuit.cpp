@@ -134,7 +134,8 @@ int apply_gate_dm(const GateRec& g, void* rho, ITYPE dim, cudaStream_t st) {
         // controlled dense: expand to a matrix over targets + controls
         const std::vector<cd> u = g.dense_matrix();
         const UINT nc = (UINT)g.controls.size(), k = nt + nc;
-        if (k > 6) return set_error(QS_ERR_NOT_SUPPORTED, "density matrix: controlled gate over more than 6 qubits");
+        if (k > (UINT)kMaxDenseTargets)
+            return set_error(QS_ERR_NOT_SUPPORTED, "density matrix: controlled gate over more than 12 qubits");
         const size_t md = size_t(1) << k, mt = size_t(1) << nt;
         std::vector<cd> full(md * md, 0.);
         size_t cmask = 0;
@@ -281,7 +282,8 @@ QS_API int qs_circuit_add_gate(qs_circuit_t circuit, int kind, const QS_UINT* ta
     };
     switch (kind) {
         case QS_GATE_DENSE: {
-            if (nt < 1 || nt > 6) return qs::set_error(QS_ERR_NOT_SUPPORTED, "dense gate: 1..6 targets");
+            if (nt < 1 || nt > (QS_UINT)qs::kMaxDenseTargets)
+                return qs::set_error(QS_ERR_NOT_SUPPORTED, "dense gate: 1..12 targets");
             const size_t md = size_t(1) << nt;
             QS_TRY(need((QS_UINT)(2 * md * md)));
             g.matrix.resize(md * md);

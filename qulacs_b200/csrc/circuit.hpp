@@ -12,6 +12,9 @@ typedef unsigned int UINT;
 
 namespace qs {
 
+constexpr int kMaxQubits = 40;        // largest state (2^40 amplitudes) any entry point accepts
+constexpr int kMaxDenseTargets = 12;  // dense gates: 1..12 targets (4^12 matrix entries = 256 MiB)
+
 struct GateRec {
     int kind = 0;
     std::vector<UINT> targets, controls, control_values;

@@ -173,7 +173,8 @@ QS_API int qs_dm_single_qubit_dense_matrix_gate(QS_UINT t, const double matrix[8
 QS_API int qs_dm_multi_qubit_dense_matrix_gate(const QS_UINT* tl, QS_UINT k, const double* matrix, DM_ARGS) {
     UINT n;
     QS_TRY(dm_dims(dim, &n));
-    if (k < 1 || k > 6) return set_error(QS_ERR_NOT_SUPPORTED, "dm_multi_qubit_dense_matrix_gate: 1..6 targets");
+    if (k < 1 || k > (UINT)kMaxDenseTargets)
+        return set_error(QS_ERR_NOT_SUPPORTED, "dm_multi_qubit_dense_matrix_gate: 1..12 targets");
     QS_TRY(check_distinct(tl, k, n, "dm_multi_qubit_dense_matrix_gate"));
     return dm_apply_unitary(tl, k, (const cd*)matrix, R2, dim, n, ST);
 }

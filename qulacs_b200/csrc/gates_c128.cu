@@ -21,7 +21,7 @@ constexpr int kThreads = 256;
 
 struct Positions {
     int count;
-    UINT pos[24];  // ascending
+    UINT pos[kMaxQubits];  // ascending; every position of a state fits
 };
 
 __device__ __forceinline__ ITYPE expand(ITYPE i, const Positions& p) {
@@ -438,6 +438,92 @@ static int launch_denseK_reg(const UINT* tl, const double* matrix, double2* s, I
     return check_launch("k_denseK_reg");
 }
 
+// k-qubit dense for 7 <= k <= kMaxDenseTargets: the matrix (4^k entries, 256 KiB at k = 7, 256 MiB at
+// k = 12) does not fit on chip and streams from L2 / HBM, transposed on the host (UT[x][y] = U[y][x]) so
+// that the lanes of a warp, which hold consecutive output rows y, read consecutive entries.  A CTA
+// stages a group of kGenAmps / 2^k cosets (kGenAmps amplitudes) in shared memory as X[c][x]; thread t
+// owns the outputs o = t + kGenThreads j of the group (coset o >> k, row o & (2^k - 1)), keeps them in
+// registers until every thread has read the group, then writes them over it and the group leaves.
+// Every group re-reads the whole matrix, so this path is bound by L2 bandwidth, not by HBM.
+constexpr int kGenThreads = 256, kGenAmps = 4096, kGenOut = kGenAmps / kGenThreads;
+
+__global__ void __launch_bounds__(kGenThreads) k_denseK_gen(double2* __restrict__ s, ITYPE cosets,
+    const __grid_constant__ Positions pos, ITYPE fixed, int K, const double2* __restrict__ ut,
+    const ITYPE* __restrict__ gmask) {
+    extern __shared__ double2 gen_smem[];  // X[c * 2^K + x], kGenAmps entries
+    const int D = 1 << K, CP = kGenAmps >> K;
+    const int tid = threadIdx.x;
+    const ITYPE groups = (cosets + CP - 1) / CP;
+    for (ITYPE g = blockIdx.x; g < groups; g += gridDim.x) {
+        const ITYPE c0 = g * (ITYPE)CP;
+        for (int i = tid; i < kGenAmps; i += kGenThreads) {
+            const int c = i >> K, x = i & (D - 1);
+            if (c0 + c < cosets) {
+                const unsigned dst = (unsigned)__cvta_generic_to_shared(gen_smem + i);
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst),
+                    "l"(s + ((expand(c0 + c, pos) | fixed) | __ldg(gmask + x))) : "memory");
+            }
+        }
+        asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
+        __syncthreads();
+        double2 acc[kGenOut];
+#pragma unroll
+        for (int j = 0; j < kGenOut; ++j) acc[j] = make_double2(0., 0.);
+        for (int x = 0; x < D; ++x) {
+            const double2* row = ut + (size_t)x * D;
+#pragma unroll
+            for (int j = 0; j < kGenOut; ++j) {
+                const int o = tid + kGenThreads * j;
+                acc[j] = cfma(__ldg(row + (o & (D - 1))), gen_smem[((o >> K) << K) + x], acc[j]);
+            }
+        }
+        __syncthreads();  // every read of the group done: the outputs go over it
+#pragma unroll
+        for (int j = 0; j < kGenOut; ++j) gen_smem[tid + kGenThreads * j] = acc[j];
+        __syncthreads();
+        for (int i = tid; i < kGenAmps; i += kGenThreads) {
+            const int c = i >> K, y = i & (D - 1);
+            if (c0 + c < cosets) st_stream(s + ((expand(c0 + c, pos) | fixed) | __ldg(gmask + y)), gen_smem[i]);
+        }
+        __syncthreads();  // the next group's copies overwrite X
+    }
+}
+
+static int launch_denseK_gen(const UINT* tl, UINT k, const double* matrix, double2* s, const Positions& pos,
+    ITYPE fixed, ITYPE cosets, cudaStream_t st) {
+    const size_t D = size_t(1) << k;
+    std::vector<double2> ut(D * D);
+    for (size_t y = 0; y < D; ++y)
+        for (size_t x = 0; x < D; ++x) ut[x * D + y] = make_double2(matrix[2 * (y * D + x)], matrix[2 * (y * D + x) + 1]);
+    std::vector<ITYPE> mk(D, 0);
+    for (size_t x = 0; x < D; ++x)
+        for (UINT j = 0; j < k; ++j)
+            if ((x >> j) & 1) mk[x] |= 1ULL << tl[j];
+    const size_t ubytes = sizeof(double2) * D * D;
+    void* buf = nullptr;
+    QS_TRY(scratch(st, ubytes + sizeof(ITYPE) * D + 256, &buf));
+    ITYPE* dmask = (ITYPE*)((char*)buf + ubytes);
+    QS_CUDA_CHECK(cudaMemcpyAsync(buf, ut.data(), ubytes, cudaMemcpyHostToDevice, st));
+    QS_CUDA_CHECK(cudaMemcpyAsync(dmask, mk.data(), sizeof(ITYPE) * D, cudaMemcpyHostToDevice, st));
+    const int smem = (int)(sizeof(double2) * kGenAmps);
+    static std::mutex mu;
+    static std::vector<char> ready;
+    int dev = 0;
+    QS_CUDA_CHECK(cudaGetDevice(&dev));
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if ((int)ready.size() <= dev) ready.resize(dev + 1, 0);
+        if (!ready[dev]) {
+            QS_CUDA_CHECK(cudaFuncSetAttribute(k_denseK_gen, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+            ready[dev] = 1;
+        }
+    }
+    const ITYPE groups = (cosets + (kGenAmps >> k) - 1) / (ITYPE)(kGenAmps >> k);
+    const unsigned grid = (unsigned)std::max<ITYPE>(1, std::min<ITYPE>(groups, (ITYPE)sm_count() * 3));
+    k_denseK_gen<<<grid, kGenThreads, smem, st>>>(s, cosets, pos, fixed, (int)k, (const double2*)buf, dmask);
+    return check_launch("k_denseK_gen");
+}
+
 int launch_denseK(const UINT* tl, UINT k, const double* matrix, double2* s, ITYPE dim,
     const UINT* ctl, const UINT* cval, UINT nc, cudaStream_t st) {
     std::vector<UINT> p(tl, tl + k);
@@ -453,7 +539,9 @@ int launch_denseK(const UINT* tl, UINT k, const double* matrix, double2* s, ITYP
         case 4: return launch_denseK_reg<4>(tl, matrix, s, dim, pos, cm, cosets, st);
         case 5: return launch_denseK_reg<5>(tl, matrix, s, dim, pos, cm, cosets, st);
         case 6: return launch_denseK_blk<6, 2>(tl, matrix, s, pos, cm, cosets, st);  // 64 register amplitudes would spill
-        default: return set_error(QS_ERR_NOT_SUPPORTED, "dense gate: 3..6 targets expected here");
+        default:
+            if (k >= 7 && k <= (UINT)kMaxDenseTargets) return launch_denseK_gen(tl, k, matrix, s, pos, cm, cosets, st);
+            return set_error(QS_ERR_NOT_SUPPORTED, "dense gate: 3..12 targets expected here");
     }
 }
 
@@ -652,7 +740,8 @@ static int dense_dispatch(const UINT* tl, UINT k, const double* matrix, const UI
     UINT nc, double2* s, ITYPE dim, cudaStream_t st, const char* what) {
     UINT n;
     QS_TRY(check_dim(dim, &n));
-    if (k < 1 || k > 6) return set_error(QS_ERR_NOT_SUPPORTED, std::string(what) + ": target count must be 1..6");
+    if (k < 1 || k > (UINT)kMaxDenseTargets)
+        return set_error(QS_ERR_NOT_SUPPORTED, std::string(what) + ": target count must be 1..12");
     std::vector<UINT> all(tl, tl + k);
     for (UINT i = 0; i < nc; ++i) {
         if (cval[i] > 1) return set_error(QS_ERR_INVALID_ARGUMENT, "control value must be 0 or 1");

@@ -14,6 +14,7 @@
 #include <string>
 
 #include "../../include/qulacs_b200.h"
+#include "circuit.hpp"  // kMaxQubits, kMaxDenseTargets
 
 typedef unsigned long long ITYPE;
 typedef unsigned int UINT;
@@ -105,7 +106,7 @@ int launch_dense1(UINT t, const Mat2& m, double2* s, ITYPE dim, const UINT* ctl,
 int launch_diag1(UINT t, double2 d0, double2 d1, double2* s, ITYPE dim, cudaStream_t st);
 int launch_dense2(UINT t1, UINT t2, const Mat4& m, double2* s, ITYPE dim, const UINT* ctl,
     const UINT* cval, UINT nc, cudaStream_t st);
-// matrix: host pointer, row-major 2^k x 2^k interleaved doubles, 3 <= k <= 6
+// matrix: host pointer, row-major 2^k x 2^k interleaved doubles, 3 <= k <= kMaxDenseTargets
 int launch_denseK(const UINT* tl, UINT k, const double* matrix, double2* s, ITYPE dim,
     const UINT* ctl, const UINT* cval, UINT nc, cudaStream_t st);
 int prob_sum(const double2* s, ITYPE dim, ITYPE mask, ITYPE value, cudaStream_t st, double* out);

@@ -43,7 +43,7 @@ int check_dim(ITYPE dim, UINT* n_out) {
         return set_error(QS_ERR_INVALID_ARGUMENT, "dim must be a power of two >= 2");
     UINT n = 0;
     while ((1ULL << n) < dim) ++n;
-    if (n > 40) return set_error(QS_ERR_NOT_SUPPORTED, "more than 40 qubits");
+    if (n > (UINT)kMaxQubits) return set_error(QS_ERR_NOT_SUPPORTED, "more than 40 qubits");
     *n_out = n;
     return QS_OK;
 }

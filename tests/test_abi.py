@@ -60,10 +60,11 @@ def test_duplicate_targets_rejected(lib):
 
 
 def test_dense_k_limit(lib):
-    tl = np.arange(7, dtype=np.uint32)
-    m = np.eye(128, dtype=np.complex128)
-    rc = lib.qs_multi_qubit_dense_matrix_gate(tl.ctypes.data_as(C.c_void_p), 7, m.ctypes.data_as(C.c_void_p),
-                                              None, 1 << 8, None)
+    """Dense gates take 1..12 targets; 13 is refused before any device work (the matrix is not read)."""
+    tl = np.arange(13, dtype=np.uint32)
+    m = np.eye(2, dtype=np.complex128)
+    rc = lib.qs_multi_qubit_dense_matrix_gate(tl.ctypes.data_as(C.c_void_p), 13, m.ctypes.data_as(C.c_void_p),
+                                              None, 1 << 14, None)
     assert rc == 5  # QS_ERR_NOT_SUPPORTED
 
 

@@ -40,6 +40,20 @@ def test_dm_gates_and_channels(port):
         assert np.max(np.abs(d.get_matrix() - want)) <= AMP_TOL, gate
 
 
+def test_dm_dense_gate_over_seven_qubits(port):
+    """A 7-target unitary on an 8-qubit density matrix: two 7-qubit dense passes (rows, then columns)."""
+    rng = np.random.default_rng(1150)
+    n = 8
+    rho0 = random_density_matrix(n, rng)
+    tl = [6, 0, 3, 1, 7, 4, 2]
+    u = random_unitary(7, rng)
+    want = rho0.copy()
+    port.dm_multi_qubit_dense_matrix_gate(tl, u, want)
+    d = dev(rho0)
+    G.DenseMatrix(tl, u).update_quantum_state(d)
+    assert np.max(np.abs(d.get_matrix() - want)) <= AMP_TOL
+
+
 @pytest.mark.parametrize("mode", ["gate_by_gate", "staged", "staged_fused"])
 def test_noisy_circuit_golden_and_stats(port, mode):
     g = np.load(os.path.join(GOLDEN, "noisy_dm_n5.npz"))

@@ -104,6 +104,68 @@ def test_multi_qubit_dense(port, k):
         assert np.max(np.abs(s.get_vector() - want)) <= AMP_TOL, tl
 
 
+def _dense(k, rng):
+    """A random complex 2^k x 2^k matrix of unit-scale rows (the gate does not need a unitary)."""
+    d = 1 << k
+    return (rng.normal(size=(d, d)) + 1j * rng.normal(size=(d, d))) / np.sqrt(2 * d)
+
+
+@pytest.mark.parametrize("k,n", [(7, 10), (8, 12), (10, 13), (12, 12)])
+def test_multi_qubit_dense_beyond_six(port, k, n):
+    """7..12 targets: the matrix streams from L2 (the reference takes any target count)."""
+    rng = np.random.default_rng(450 + k)
+    s0 = random_state(n, rng)
+    for trial in range(2):
+        tl = list(range(n - k, n)) if trial == 0 else [int(x) for x in rng.choice(n, size=k, replace=False)]
+        m = _dense(k, rng)
+        want = s0.copy()
+        port.multi_qubit_dense_matrix_gate(tl, m, want)
+        s = dev(s0)
+        call("qs_multi_qubit_dense_matrix_gate", _p(np.asarray(tl, dtype=np.uint32)), k, _p(m), s.data_ptr(),
+             s.dim, None)
+        assert np.max(np.abs(s.get_vector() - want)) <= AMP_TOL, tl
+    # 7 targets under 2 controls (values 1, 0), against the full 9-qubit matrix: index bits 0..6 <-> the
+    # targets, bit 7 <-> cl[0], bit 8 <-> cl[1]; the block acts where bit 7 = 1 and bit 8 = 0
+    u = _dense(7, rng)
+    full = np.eye(512, dtype=np.complex128)
+    full[128:256, 128:256] = u
+    q = [int(x) for x in rng.permutation(n)]
+    tl, cl = q[:7], q[7:9]
+    want = s0.copy()
+    port.multi_qubit_dense_matrix_gate(tl + cl, full, want)
+    s = dev(s0)
+    call("qs_multi_qubit_control_multi_qubit_dense_matrix_gate", _p(np.asarray(cl, dtype=np.uint32)),
+         _p(np.asarray([1, 0], dtype=np.uint32)), 2, _p(np.asarray(tl, dtype=np.uint32)), 7, _p(u),
+         s.data_ptr(), s.dim, None)
+    assert np.max(np.abs(s.get_vector() - want)) <= AMP_TOL
+    with pytest.raises(NotImplementedError):
+        call("qs_multi_qubit_dense_matrix_gate", _p(np.arange(13, dtype=np.uint32)), 13,
+             _p(np.zeros(2, dtype=np.complex128)), s.data_ptr(), s.dim, None)
+
+
+@pytest.mark.parametrize("mode", ["gate_by_gate", "staged", "staged_fused"])
+def test_circuit_with_a_nine_qubit_dense_gate(port, mode):
+    from qulacs_b200 import QuantumCircuit
+    rng = np.random.default_rng(470)
+    n = 12
+    s0 = random_state(n, rng)
+    c = QuantumCircuit(n)
+    c.add_H_gate(0)
+    c.add_CNOT_gate(0, 11)
+    tl = [int(x) for x in rng.choice(n, size=9, replace=False)]
+    m = _dense(9, rng)
+    c.add_dense_matrix_gate(tl, m)
+    c.add_RX_gate(3, 0.4)
+    s = dev(s0)
+    c.update_quantum_state(s, mode=mode)
+    want = s0.copy()
+    port.single_qubit_dense_matrix_gate(0, G.H(0).get_matrix(), want)
+    port.CNOT_gate(0, 11, want)
+    port.multi_qubit_dense_matrix_gate(tl, m, want)
+    port.RX_gate(3, 0.4, want)
+    assert np.max(np.abs(s.get_vector() - want)) <= AMP_TOL
+
+
 def test_controlled_and_diagonal_and_pauli(port):
     rng = np.random.default_rng(500)
     n = 9
