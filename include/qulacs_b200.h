@@ -177,6 +177,28 @@ QS_API int qs_multi_qubit_Pauli_gate_partial_list(const QS_UINT* target_qubit_in
 QS_API int qs_multi_qubit_Pauli_rotation_gate_partial_list(const QS_UINT* target_qubit_index_list,
     const QS_UINT* Pauli_operator_type_list, QS_UINT target_qubit_index_count, double angle,
     void* state, QS_ITYPE dim, void* stream);
+/* update_ops.hpp:927 / :1097 multi_qubit_Pauli(_rotation)_gate_whole_list: id j acts on qubit j,
+ * j < qubit_count (<= the state's qubit count). */
+QS_API int qs_multi_qubit_Pauli_gate_whole_list(const QS_UINT* Pauli_operator_type_list, QS_UINT qubit_count,
+    void* state, QS_ITYPE dim, void* stream);
+QS_API int qs_multi_qubit_Pauli_rotation_gate_whole_list(const QS_UINT* Pauli_operator_type_list,
+    QS_UINT qubit_count, double angle, void* state, QS_ITYPE dim, void* stream);
+/* update_ops_pauli_single.cpp:14-52 single_qubit_Pauli_gate / single_qubit_Pauli_rotation_gate:
+ * id 0 leaves the state unchanged, 1/2/3 apply X/Y/Z or RX/RY/RZ(angle); other ids are invalid. */
+QS_API int qs_single_qubit_Pauli_gate(QS_UINT target_qubit_index, QS_UINT Pauli_operator_type, void* state,
+    QS_ITYPE dim, void* stream);
+QS_API int qs_single_qubit_Pauli_rotation_gate(QS_UINT target_qubit_index, QS_UINT Pauli_operator_index,
+    double angle, void* state, QS_ITYPE dim, void* stream);
+/* update_ops.hpp:1387 single_qubit_control_multi_qubit_dense_matrix_gate; targets <= 12. */
+QS_API int qs_single_qubit_control_multi_qubit_dense_matrix_gate(QS_UINT control_qubit_index,
+    QS_UINT control_value, const QS_UINT* target_qubit_index_list, QS_UINT target_qubit_index_count,
+    const double* matrix, void* state, QS_ITYPE dim, void* stream);
+/* update_ops.hpp:1464 multi_qubit_control_multi_qubit_diagonal_matrix_gate
+ * (update_ops_matrix_diagonal_multi.cpp:60-112): diagonal_element[y] multiplies the amplitudes whose
+ * target bits spell y and whose control bits equal the control values; targets + controls <= 20. */
+QS_API int qs_multi_qubit_control_multi_qubit_diagonal_matrix_gate(const QS_UINT* control_qubit_index_list,
+    const QS_UINT* control_value_list, QS_UINT control_qubit_index_count, const QS_UINT* target_qubit_index_list,
+    QS_UINT target_qubit_index_count, const double* diagonal_element, void* state, QS_ITYPE dim, void* stream);
 
 /* ---- statistics (src/csim/stat_ops.hpp); results to host, stream synchronised ---- */
 /* stat_ops.hpp:5 state_norm_squared */
@@ -196,6 +218,15 @@ QS_API int qs_marginal_prob(const QS_UINT* sorted_target_qubit_index_list, const
 QS_API int qs_expectation_value_multi_qubit_Pauli_operator_partial_list(
     const QS_UINT* target_qubit_index_list, const QS_UINT* Pauli_operator_type_list,
     QS_UINT target_qubit_index_count, const void* state, QS_ITYPE dim, void* stream, double* out);
+/* stat_ops.hpp:32 expectation_value_single_qubit_Pauli_operator (id 0 gives <psi|psi>) */
+QS_API int qs_expectation_value_single_qubit_Pauli_operator(QS_UINT target_qubit_index,
+    QS_UINT Pauli_operator_type, const void* state, QS_ITYPE dim, void* stream, double* out);
+/* stat_ops.hpp:35 expectation_value_multi_qubit_Pauli_operator_whole_list: id j on qubit j */
+QS_API int qs_expectation_value_multi_qubit_Pauli_operator_whole_list(const QS_UINT* Pauli_operator_type_list,
+    QS_UINT qubit_count, const void* state, QS_ITYPE dim, void* stream, double* out);
+/* stat_ops.hpp:42 transition_amplitude_multi_qubit_Pauli_operator_whole_list: <bra|P|ket> */
+QS_API int qs_transition_amplitude_multi_qubit_Pauli_operator_whole_list(const QS_UINT* Pauli_operator_type_list,
+    QS_UINT qubit_count, const void* state_bra, const void* state_ket, QS_ITYPE dim, void* stream, double out[2]);
 /* stat_ops.hpp:45 transition_amplitude_multi_qubit_Pauli_operator_partial_list: <bra|P|ket> */
 QS_API int qs_transition_amplitude_multi_qubit_Pauli_operator_partial_list(
     const QS_UINT* target_qubit_index_list, const QS_UINT* Pauli_operator_type_list,
@@ -253,6 +284,37 @@ QS_API int qs_dm_CZ_gate(QS_UINT control_qubit_index, QS_UINT target_qubit_index
 QS_API int qs_dm_RX_gate(QS_UINT target_qubit_index, double angle, void* rho, QS_ITYPE dim, void* stream);
 QS_API int qs_dm_RY_gate(QS_UINT target_qubit_index, double angle, void* rho, QS_ITYPE dim, void* stream);
 QS_API int qs_dm_RZ_gate(QS_UINT target_qubit_index, double angle, void* rho, QS_ITYPE dim, void* stream);
+/* update_ops_dm.hpp:37-58 named gates on rho (U rho U^dagger with csim's constant.cpp matrices; P0/P1
+ * project: P rho P) */
+QS_API int qs_dm_X_gate(QS_UINT target_qubit_index, void* rho, QS_ITYPE dim, void* stream);
+QS_API int qs_dm_Y_gate(QS_UINT target_qubit_index, void* rho, QS_ITYPE dim, void* stream);
+QS_API int qs_dm_Z_gate(QS_UINT target_qubit_index, void* rho, QS_ITYPE dim, void* stream);
+QS_API int qs_dm_H_gate(QS_UINT target_qubit_index, void* rho, QS_ITYPE dim, void* stream);
+QS_API int qs_dm_S_gate(QS_UINT target_qubit_index, void* rho, QS_ITYPE dim, void* stream);
+QS_API int qs_dm_Sdag_gate(QS_UINT target_qubit_index, void* rho, QS_ITYPE dim, void* stream);
+QS_API int qs_dm_T_gate(QS_UINT target_qubit_index, void* rho, QS_ITYPE dim, void* stream);
+QS_API int qs_dm_Tdag_gate(QS_UINT target_qubit_index, void* rho, QS_ITYPE dim, void* stream);
+QS_API int qs_dm_sqrtX_gate(QS_UINT target_qubit_index, void* rho, QS_ITYPE dim, void* stream);
+QS_API int qs_dm_sqrtXdag_gate(QS_UINT target_qubit_index, void* rho, QS_ITYPE dim, void* stream);
+QS_API int qs_dm_sqrtY_gate(QS_UINT target_qubit_index, void* rho, QS_ITYPE dim, void* stream);
+QS_API int qs_dm_sqrtYdag_gate(QS_UINT target_qubit_index, void* rho, QS_ITYPE dim, void* stream);
+QS_API int qs_dm_P0_gate(QS_UINT target_qubit_index, void* rho, QS_ITYPE dim, void* stream);
+QS_API int qs_dm_P1_gate(QS_UINT target_qubit_index, void* rho, QS_ITYPE dim, void* stream);
+QS_API int qs_dm_SWAP_gate(QS_UINT target_qubit_index_0, QS_UINT target_qubit_index_1, void* rho, QS_ITYPE dim,
+    void* stream);
+/* update_ops_dm.hpp:65-70 Pauli product and exp(i angle P / 2) on rho; ids 0=I 1=X 2=Y 3=Z, count <= 12 */
+QS_API int qs_dm_multi_qubit_Pauli_gate_partial_list(const QS_UINT* target_qubit_index_list,
+    const QS_UINT* Pauli_operator_type_list, QS_UINT target_qubit_index_count, void* rho, QS_ITYPE dim, void* stream);
+QS_API int qs_dm_multi_qubit_Pauli_rotation_gate_partial_list(const QS_UINT* target_qubit_index_list,
+    const QS_UINT* Pauli_operator_type_list, QS_UINT target_qubit_index_count, double angle, void* rho,
+    QS_ITYPE dim, void* stream);
+/* update_ops_dm.hpp:24-34 controlled dense gates on rho; targets + controls <= 12 */
+QS_API int qs_dm_multi_qubit_control_single_qubit_dense_matrix_gate(const QS_UINT* control_qubit_index_list,
+    const QS_UINT* control_value_list, QS_UINT control_qubit_index_count, QS_UINT target_qubit_index,
+    const double matrix[8], void* rho, QS_ITYPE dim, void* stream);
+QS_API int qs_dm_multi_qubit_control_multi_qubit_dense_matrix_gate(const QS_UINT* control_qubit_index_list,
+    const QS_UINT* control_value_list, QS_UINT control_qubit_index_count, const QS_UINT* target_qubit_index_list,
+    QS_UINT target_qubit_index_count, const double* matrix, void* rho, QS_ITYPE dim, void* stream);
 /* DepolarizingNoise(t, p) on a density matrix (cppsim/gate_factory.cpp:456-466 through the exact
  * branch of cppsim/gate_general.hpp:265-285), in one pass. */
 QS_API int qs_dm_depolarizing_noise(QS_UINT target_qubit_index, double probability, void* rho,

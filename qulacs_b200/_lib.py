@@ -56,6 +56,12 @@ SIGNATURES = {
     "qs_multi_qubit_control_multi_qubit_dense_matrix_gate": [P, P, U, P, U, P] + _STATE,
     "qs_multi_qubit_Pauli_gate_partial_list": [P, P, U] + _STATE,
     "qs_multi_qubit_Pauli_rotation_gate_partial_list": [P, P, U, D] + _STATE,
+    "qs_multi_qubit_Pauli_gate_whole_list": [P, U] + _STATE,
+    "qs_multi_qubit_Pauli_rotation_gate_whole_list": [P, U, D] + _STATE,
+    "qs_single_qubit_Pauli_gate": [U, U] + _STATE,
+    "qs_single_qubit_Pauli_rotation_gate": [U, U, D] + _STATE,
+    "qs_single_qubit_control_multi_qubit_dense_matrix_gate": [U, U, P, U, P] + _STATE,
+    "qs_multi_qubit_control_multi_qubit_diagonal_matrix_gate": [P, P, U, P, U, P] + _STATE,
     "qs_state_norm_squared": [P, IT, P, P],
     "qs_measurement_distribution_entropy": [P, IT, P, P],
     "qs_dm_measurement_distribution_entropy": [P, IT, P, P],
@@ -83,6 +89,9 @@ SIGNATURES = {
     "qs_marginal_prob": [P, P, U, P, IT, P, P],
     "qs_expectation_value_multi_qubit_Pauli_operator_partial_list": [P, P, U, P, IT, P, P],
     "qs_transition_amplitude_multi_qubit_Pauli_operator_partial_list": [P, P, U, P, P, IT, P, P],
+    "qs_expectation_value_single_qubit_Pauli_operator": [U, U, P, IT, P, P],
+    "qs_expectation_value_multi_qubit_Pauli_operator_whole_list": [P, U, P, IT, P, P],
+    "qs_transition_amplitude_multi_qubit_Pauli_operator_whole_list": [P, U, P, P, IT, P, P],
     "qs_expectation_value_pauli_batch": [P, P, P, U, P, IT, P, P],
     "qs_state_sampling_with_uniforms": [P, IT, P, U, P, P],
     "qs_state_sampling": [P, IT, U, U, P, P],
@@ -98,6 +107,13 @@ SIGNATURES = {
     "qs_dm_RX_gate": [U, D] + _STATE,
     "qs_dm_RY_gate": [U, D] + _STATE,
     "qs_dm_RZ_gate": [U, D] + _STATE,
+    **{f"qs_dm_{g}_gate": [U] + _STATE for g in ("X", "Y", "Z", "H", "S", "Sdag", "T", "Tdag", "sqrtX", "sqrtXdag",
+                                                 "sqrtY", "sqrtYdag", "P0", "P1")},
+    "qs_dm_SWAP_gate": [U, U] + _STATE,
+    "qs_dm_multi_qubit_Pauli_gate_partial_list": [P, P, U] + _STATE,
+    "qs_dm_multi_qubit_Pauli_rotation_gate_partial_list": [P, P, U, D] + _STATE,
+    "qs_dm_multi_qubit_control_single_qubit_dense_matrix_gate": [P, P, U, U, P] + _STATE,
+    "qs_dm_multi_qubit_control_multi_qubit_dense_matrix_gate": [P, P, U, P, U, P] + _STATE,
     "qs_dm_depolarizing_noise": [U, D] + _STATE,
     "qs_dm_two_qubit_depolarizing_noise": [U, U, D] + _STATE,
     "qs_dm_expectation_value_multi_qubit_Pauli_operator_partial_list": [P, P, U, P, IT, P, P],

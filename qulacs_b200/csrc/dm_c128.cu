@@ -208,6 +208,120 @@ QS_API int qs_dm_RX_gate(QS_UINT t, double a, DM_ARGS) { return dm_rot(t, a, 1, 
 QS_API int qs_dm_RY_gate(QS_UINT t, double a, DM_ARGS) { return dm_rot(t, a, 2, rho, dim, stream); }
 QS_API int qs_dm_RZ_gate(QS_UINT t, double a, DM_ARGS) { return dm_rot(t, a, 3, rho, dim, stream); }
 
+// Named gates: U rho U^dagger with csim's matrices (constant.cpp:4-30), row-major interleaved re, im.
+#define QS_DM_NAMED(NAME, ...)                                                      \
+    QS_API int qs_dm_##NAME##_gate(QS_UINT t, DM_ARGS) {                            \
+        static const double m[8] = {__VA_ARGS__};                                   \
+        return qs_dm_single_qubit_dense_matrix_gate(t, m, rho, dim, stream);        \
+    }
+#define QS_H 0.70710678118654752440
+QS_DM_NAMED(X, 0, 0, 1, 0, 1, 0, 0, 0)
+QS_DM_NAMED(Y, 0, 0, 0, -1, 0, 1, 0, 0)
+QS_DM_NAMED(Z, 1, 0, 0, 0, 0, 0, -1, 0)
+QS_DM_NAMED(H, QS_H, 0, QS_H, 0, QS_H, 0, -QS_H, 0)
+QS_DM_NAMED(S, 1, 0, 0, 0, 0, 0, 0, 1)
+QS_DM_NAMED(Sdag, 1, 0, 0, 0, 0, 0, 0, -1)
+QS_DM_NAMED(T, 1, 0, 0, 0, 0, 0, QS_H, QS_H)
+QS_DM_NAMED(Tdag, 1, 0, 0, 0, 0, 0, QS_H, -QS_H)
+QS_DM_NAMED(sqrtX, 0.5, 0.5, 0.5, -0.5, 0.5, -0.5, 0.5, 0.5)
+QS_DM_NAMED(sqrtXdag, 0.5, -0.5, 0.5, 0.5, 0.5, 0.5, 0.5, -0.5)
+QS_DM_NAMED(sqrtY, 0.5, 0.5, -0.5, -0.5, 0.5, 0.5, 0.5, 0.5)
+QS_DM_NAMED(sqrtYdag, 0.5, -0.5, 0.5, -0.5, -0.5, 0.5, 0.5, -0.5)
+QS_DM_NAMED(P0, 1, 0, 0, 0, 0, 0, 0, 0)
+QS_DM_NAMED(P1, 0, 0, 0, 0, 0, 0, 1, 0)
+#undef QS_H
+#undef QS_DM_NAMED
+
+QS_API int qs_dm_SWAP_gate(QS_UINT t0, QS_UINT t1, DM_ARGS) {
+    // matrix bit 0 <-> t0, bit 1 <-> t1: |01> <-> |10>
+    static const double m[32] = {1, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 1, 0, 0, 0,
+                                 0, 0, 1, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 1, 0};
+    const UINT tl[2] = {t0, t1};
+    return qs_dm_multi_qubit_dense_matrix_gate(tl, 2, m, rho, dim, stream);
+}
+
+static int dm_pauli_checks(const UINT* tl, const UINT* ids, UINT cnt, ITYPE dim, const char* what) {
+    UINT n;
+    QS_TRY(dm_dims(dim, &n));
+    if (cnt > (UINT)kMaxDenseTargets) return set_error(QS_ERR_NOT_SUPPORTED, std::string(what) + ": at most 12 qubits");
+    for (UINT j = 0; j < cnt; ++j)
+        if (ids[j] > 3) return set_error(QS_ERR_INVALID_ARGUMENT, std::string(what) + ": Pauli id must be 0..3");
+    return check_distinct(tl, cnt, n, what);
+}
+// P rho P^dagger for P a product over distinct qubits: one single-qubit Pauli at a time.
+QS_API int qs_dm_multi_qubit_Pauli_gate_partial_list(const QS_UINT* tl, const QS_UINT* ids, QS_UINT cnt, DM_ARGS) {
+    QS_TRY(dm_pauli_checks(tl, ids, cnt, dim, "dm_multi_qubit_Pauli_gate_partial_list"));
+    for (UINT j = 0; j < cnt; ++j) {
+        if (ids[j] == 1) QS_TRY(qs_dm_X_gate(tl[j], rho, dim, stream));
+        else if (ids[j] == 2) QS_TRY(qs_dm_Y_gate(tl[j], rho, dim, stream));
+        else if (ids[j] == 3) QS_TRY(qs_dm_Z_gate(tl[j], rho, dim, stream));
+    }
+    return QS_OK;
+}
+// exp(i angle P / 2) = cos(angle/2) I + i sin(angle/2) P as a dense matrix over the listed qubits
+// (bit j <-> tl[j]); P[x ^ xmask][x] = prod_j sigma_{id_j}[y_j][x_j].
+QS_API int qs_dm_multi_qubit_Pauli_rotation_gate_partial_list(const QS_UINT* tl, const QS_UINT* ids, QS_UINT cnt,
+    double angle, DM_ARGS) {
+    QS_TRY(dm_pauli_checks(tl, ids, cnt, dim, "dm_multi_qubit_Pauli_rotation_gate_partial_list"));
+    if (cnt == 0) return QS_OK;  // a global phase: rho is unchanged
+    const size_t md = size_t(1) << cnt;
+    size_t xmask = 0;
+    for (UINT j = 0; j < cnt; ++j)
+        if (ids[j] == 1 || ids[j] == 2) xmask |= size_t(1) << j;
+    const double c = std::cos(angle / 2), sn = std::sin(angle / 2);
+    std::vector<cd> m(md * md, 0.);
+    for (size_t x = 0; x < md; ++x) {
+        const size_t y = x ^ xmask;
+        cd v = 1.;
+        for (UINT j = 0; j < cnt; ++j) {
+            const bool xb = (x >> j) & 1;
+            if (ids[j] == 2) v *= xb ? cd(0, -1) : cd(0, 1);  // sigma_Y[y][x]: [[0, -i], [i, 0]]
+            else if (ids[j] == 3 && xb) v = -v;
+        }
+        m[y * md + x] += cd(0, sn) * v;
+        m[x * md + x] += c;
+    }
+    return qs_dm_multi_qubit_dense_matrix_gate(tl, cnt, (const double*)m.data(), rho, dim, stream);
+}
+
+// Controlled dense on rho: the matrix over (targets, controls), targets on the low bits, identity where
+// the control bits differ from the control values.
+static int dm_controlled(const UINT* ctl, const UINT* cval, UINT nc, const UINT* tl, UINT k, const cd* u,
+    void* rho, ITYPE dim, void* stream, const char* what) {
+    UINT n;
+    QS_TRY(dm_dims(dim, &n));
+    if (k < 1 || k + nc > (UINT)kMaxDenseTargets)
+        return set_error(QS_ERR_NOT_SUPPORTED, std::string(what) + ": targets + controls must be 1..12");
+    std::vector<UINT> all(tl, tl + k);
+    size_t cbits = 0;
+    for (UINT j = 0; j < nc; ++j) {
+        if (cval[j] > 1) return set_error(QS_ERR_INVALID_ARGUMENT, "control value must be 0 or 1");
+        if (cval[j]) cbits |= size_t(1) << j;
+        all.push_back(ctl[j]);
+    }
+    QS_TRY(check_distinct(all.data(), k + nc, n, what));
+    const size_t md = size_t(1) << (k + nc), mt = size_t(1) << k;
+    std::vector<cd> full(md * md, 0.);
+    for (size_t y = 0; y < md; ++y) {
+        if ((y >> k) != cbits) {
+            full[y * md + y] = 1.;
+            continue;
+        }
+        for (size_t x = 0; x < mt; ++x) full[y * md + ((y >> k) << k) + x] = u[(y & (mt - 1)) * mt + x];
+    }
+    return qs_dm_multi_qubit_dense_matrix_gate(all.data(), k + nc, (const double*)full.data(), rho, dim, stream);
+}
+QS_API int qs_dm_multi_qubit_control_single_qubit_dense_matrix_gate(const QS_UINT* ctl, const QS_UINT* cval,
+    QS_UINT nc, QS_UINT t, const double matrix[8], DM_ARGS) {
+    return dm_controlled(ctl, cval, nc, &t, 1, (const cd*)matrix, rho, dim, stream,
+        "dm_multi_qubit_control_single_qubit_dense_matrix_gate");
+}
+QS_API int qs_dm_multi_qubit_control_multi_qubit_dense_matrix_gate(const QS_UINT* ctl, const QS_UINT* cval,
+    QS_UINT nc, const QS_UINT* tl, QS_UINT k, const double* matrix, DM_ARGS) {
+    return dm_controlled(ctl, cval, nc, tl, k, (const cd*)matrix, rho, dim, stream,
+        "dm_multi_qubit_control_multi_qubit_dense_matrix_gate");
+}
+
 QS_API int qs_dm_depolarizing_noise(QS_UINT t, double p, DM_ARGS) {
     UINT n;
     QS_TRY(dm_dims(dim, &n));

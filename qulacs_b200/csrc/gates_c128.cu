@@ -802,4 +802,86 @@ QS_API int qs_multi_qubit_Pauli_rotation_gate_partial_list(
     return apply_pauli(tl, ids, cnt, true, angle, S2, dim, ST);
 }
 
+// Whole-list forms (update_ops_pauli_multi.cpp): id j acts on qubit j.
+static int whole_list_targets(QS_UINT count, ITYPE dim, const char* what, std::vector<UINT>* tl) {
+    UINT n;
+    QS_TRY(check_dim(dim, &n));
+    if (count > n) return set_error(QS_ERR_INVALID_ARGUMENT, std::string(what) + ": more Pauli ids than qubits");
+    tl->resize(count);
+    for (UINT j = 0; j < count; ++j) (*tl)[j] = j;
+    return QS_OK;
+}
+QS_API int qs_multi_qubit_Pauli_gate_whole_list(const QS_UINT* ids, QS_UINT count, STATE_ARGS) {
+    std::vector<UINT> tl;
+    QS_TRY(whole_list_targets(count, dim, "multi_qubit_Pauli_gate_whole_list", &tl));
+    return apply_pauli(tl.data(), ids, count, false, 0., S2, dim, ST);
+}
+QS_API int qs_multi_qubit_Pauli_rotation_gate_whole_list(const QS_UINT* ids, QS_UINT count, double angle,
+    STATE_ARGS) {
+    std::vector<UINT> tl;
+    QS_TRY(whole_list_targets(count, dim, "multi_qubit_Pauli_rotation_gate_whole_list", &tl));
+    return apply_pauli(tl.data(), ids, count, true, angle, S2, dim, ST);
+}
+
+QS_API int qs_single_qubit_Pauli_gate(QS_UINT t, QS_UINT id, STATE_ARGS) {
+    switch (id) {
+        case 0: {
+            UINT n;
+            QS_TRY(check_dim(dim, &n));
+            return check_target(t, n, "single_qubit_Pauli_gate");
+        }
+        case 1: return qs_X_gate(t, state, dim, stream);
+        case 2: return qs_Y_gate(t, state, dim, stream);
+        case 3: return qs_Z_gate(t, state, dim, stream);
+        default: return set_error(QS_ERR_INVALID_ARGUMENT, "single_qubit_Pauli_gate: Pauli id must be 0..3");
+    }
+}
+QS_API int qs_single_qubit_Pauli_rotation_gate(QS_UINT t, QS_UINT id, double angle, STATE_ARGS) {
+    switch (id) {
+        case 0: {
+            UINT n;
+            QS_TRY(check_dim(dim, &n));
+            return check_target(t, n, "single_qubit_Pauli_rotation_gate");
+        }
+        case 1: return qs_RX_gate(t, angle, state, dim, stream);
+        case 2: return qs_RY_gate(t, angle, state, dim, stream);
+        case 3: return qs_RZ_gate(t, angle, state, dim, stream);
+        default: return set_error(QS_ERR_INVALID_ARGUMENT, "single_qubit_Pauli_rotation_gate: Pauli id must be 0..3");
+    }
+}
+
+QS_API int qs_single_qubit_control_multi_qubit_dense_matrix_gate(QS_UINT c, QS_UINT cv, const QS_UINT* tl, QS_UINT k,
+    const double* matrix, STATE_ARGS) {
+    const UINT ctl[1] = {c}, val[1] = {cv};
+    return dense_dispatch(tl, k, matrix, ctl, val, 1, S2, dim, ST, "single_qubit_control_multi_qubit_dense_matrix_gate");
+}
+
+// The controlled diagonal as one diagonal over (targets, controls): entry y + 2^k c is diagonal[y] where the
+// control bits c spell the control values and 1 elsewhere (update_ops_matrix_diagonal_multi.cpp:60-112
+// multiplies only the amplitudes whose control bits match).
+QS_API int qs_multi_qubit_control_multi_qubit_diagonal_matrix_gate(const QS_UINT* ctl, const QS_UINT* cval, QS_UINT nc,
+    const QS_UINT* tl, QS_UINT k, const double* diag, STATE_ARGS) {
+    UINT n;
+    QS_TRY(check_dim(dim, &n));
+    const UINT total = k + nc;
+    if (k < 1 || total > 20)
+        return set_error(QS_ERR_NOT_SUPPORTED, "multi_qubit_control_multi_qubit_diagonal_matrix_gate: 1..20 qubits");
+    std::vector<UINT> all(tl, tl + k);
+    size_t cbits = 0;
+    for (UINT j = 0; j < nc; ++j) {
+        if (cval[j] > 1) return set_error(QS_ERR_INVALID_ARGUMENT, "control value must be 0 or 1");
+        if (cval[j]) cbits |= size_t(1) << j;
+        all.push_back(ctl[j]);
+    }
+    QS_TRY(check_distinct(all.data(), total, n, "multi_qubit_control_multi_qubit_diagonal_matrix_gate"));
+    const size_t full = size_t(1) << total, md = size_t(1) << k;
+    std::vector<double> d(2 * full);
+    for (size_t i = 0; i < full; ++i) {
+        const bool on = (i >> k) == cbits;
+        d[2 * i] = on ? diag[2 * (i & (md - 1))] : 1.0;
+        d[2 * i + 1] = on ? diag[2 * (i & (md - 1)) + 1] : 0.0;
+    }
+    return qs_multi_qubit_diagonal_matrix_gate(all.data(), total, d.data(), state, dim, stream);
+}
+
 }  // extern "C"

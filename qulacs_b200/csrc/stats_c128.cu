@@ -632,6 +632,34 @@ QS_API int qs_transition_amplitude_multi_qubit_Pauli_operator_partial_list(const
     return finish_reduce((double*)buf, blocks, 2, st, out);
 }
 
+QS_API int qs_expectation_value_single_qubit_Pauli_operator(QS_UINT t, QS_UINT id, const void* state, QS_ITYPE dim,
+    void* stream, double* out) {
+    return qs_expectation_value_multi_qubit_Pauli_operator_partial_list(&t, &id, 1, state, dim, stream, out);
+}
+
+// Whole-list forms (stat_ops_expectation_value.cpp, stat_ops_transition_amplitude.cpp): id j on qubit j.
+static int whole_list(QS_UINT count, QS_ITYPE dim, const char* what, std::vector<UINT>* tl) {
+    UINT n;
+    QS_TRY(check_dim(dim, &n));
+    if (count > n) return set_error(QS_ERR_INVALID_ARGUMENT, std::string(what) + ": more Pauli ids than qubits");
+    tl->resize(count);
+    for (UINT j = 0; j < count; ++j) (*tl)[j] = j;
+    return QS_OK;
+}
+QS_API int qs_expectation_value_multi_qubit_Pauli_operator_whole_list(const QS_UINT* ids, QS_UINT count,
+    const void* state, QS_ITYPE dim, void* stream, double* out) {
+    std::vector<UINT> tl;
+    QS_TRY(whole_list(count, dim, "expectation_value_multi_qubit_Pauli_operator_whole_list", &tl));
+    return qs_expectation_value_multi_qubit_Pauli_operator_partial_list(tl.data(), ids, count, state, dim, stream, out);
+}
+QS_API int qs_transition_amplitude_multi_qubit_Pauli_operator_whole_list(const QS_UINT* ids, QS_UINT count,
+    const void* bra, const void* ket, QS_ITYPE dim, void* stream, double out[2]) {
+    std::vector<UINT> tl;
+    QS_TRY(whole_list(count, dim, "transition_amplitude_multi_qubit_Pauli_operator_whole_list", &tl));
+    return qs_transition_amplitude_multi_qubit_Pauli_operator_partial_list(tl.data(), ids, count, bra, ket, dim,
+        stream, out);
+}
+
 QS_API int qs_state_sampling_with_uniforms(const void* state, QS_ITYPE dim, const double* uniforms,
     QS_UINT count, QS_ITYPE* out, void* stream) {
     UINT n;
