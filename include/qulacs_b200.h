@@ -200,6 +200,36 @@ QS_API int qs_multi_qubit_control_multi_qubit_diagonal_matrix_gate(const QS_UINT
     const QS_UINT* control_value_list, QS_UINT control_qubit_index_count, const QS_UINT* target_qubit_index_list,
     QS_UINT target_qubit_index_count, const double* diagonal_element, void* state, QS_ITYPE dim, void* stream);
 
+/* update_ops.hpp:1495 reflection_gate: state <- 2 <r|state> r - state (synchronises `stream`) */
+QS_API int qs_reflection_gate(const void* reflection_state, void* state, QS_ITYPE dim, void* stream);
+/* update_ops.hpp:435 FusedSWAP_gate: qubits [t0, t0 + block_size) swapped with [t1, t1 + block_size);
+ * the blocks must not overlap and must lie inside the state. */
+QS_API int qs_FusedSWAP_gate(QS_UINT target_qubit_index_0, QS_UINT target_qubit_index_1, QS_UINT block_size,
+    void* state, QS_ITYPE dim, void* stream);
+/* init_ops.hpp:20 initialize_Haar_random_state: the seeded form with a seed from std::random_device */
+QS_API int qs_initialize_Haar_random_state(void* state, QS_ITYPE dim, void* stream);
+
+/* ---- state manipulation (src/csim/stat_ops.hpp:17-22, stat_ops_dm.hpp:13-20); `dst` is a separate,
+ * caller-allocated device buffer of the result's size ---- */
+/* dst[l * dim_right + r] = left[l] right[r] (the right state on the low qubits) */
+QS_API int qs_state_tensor_product(const void* state_left, QS_ITYPE dim_left, const void* state_right,
+    QS_ITYPE dim_right, void* state_dst, void* stream);
+/* dst[i] = src[sum over set bits q of i of 2^qubit_order[q]]; qubit_order lists every qubit once */
+QS_API int qs_state_permutate_qubit(const QS_UINT* qubit_order, const void* state_src, void* state_dst,
+    QS_UINT qubit_count, QS_ITYPE dim, void* stream);
+/* dst (dim >> target_count amplitudes) = src restricted to target[j] = projection[j] */
+QS_API int qs_state_drop_qubits(const QS_UINT* target, const QS_UINT* projection, QS_UINT target_count,
+    const void* state_src, void* state_dst, QS_ITYPE dim, void* stream);
+QS_API int qs_dm_state_tensor_product(const void* state_left, QS_ITYPE dim_left, const void* state_right,
+    QS_ITYPE dim_right, void* state_dst, void* stream);
+QS_API int qs_dm_state_permutate_qubit(const QS_UINT* qubit_order, const void* state_src, void* state_dst,
+    QS_UINT qubit_count, QS_ITYPE dim, void* stream);
+/* partial trace over the targets; dim is the source's 2^n, dst holds (dim >> target_count)^2 entries */
+QS_API int qs_dm_state_partial_trace_from_density_matrix(const QS_UINT* target, QS_UINT target_count,
+    const void* state_src, void* state_dst, QS_ITYPE dim, void* stream);
+QS_API int qs_dm_state_partial_trace_from_state_vector(const QS_UINT* target, QS_UINT target_count,
+    const void* state_src, void* state_dst, QS_ITYPE dim, void* stream);
+
 /* ---- statistics (src/csim/stat_ops.hpp); results to host, stream synchronised ---- */
 /* stat_ops.hpp:5 state_norm_squared */
 /* measurement_distribution_entropy (stat_ops.hpp:10, stat_ops_probability.cpp:83-99): sum of -p log p

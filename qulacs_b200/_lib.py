@@ -110,6 +110,16 @@ SIGNATURES = {
     **{f"qs_dm_{g}_gate": [U] + _STATE for g in ("X", "Y", "Z", "H", "S", "Sdag", "T", "Tdag", "sqrtX", "sqrtXdag",
                                                  "sqrtY", "sqrtYdag", "P0", "P1")},
     "qs_dm_SWAP_gate": [U, U] + _STATE,
+    "qs_reflection_gate": [P, P, IT, P],
+    "qs_FusedSWAP_gate": [U, U, U] + _STATE,
+    "qs_initialize_Haar_random_state": [P, IT, P],
+    "qs_state_tensor_product": [P, IT, P, IT, P, P],
+    "qs_state_permutate_qubit": [P, P, P, U, IT, P],
+    "qs_state_drop_qubits": [P, P, U, P, P, IT, P],
+    "qs_dm_state_tensor_product": [P, IT, P, IT, P, P],
+    "qs_dm_state_permutate_qubit": [P, P, P, U, IT, P],
+    "qs_dm_state_partial_trace_from_density_matrix": [P, U, P, P, IT, P],
+    "qs_dm_state_partial_trace_from_state_vector": [P, U, P, P, IT, P],
     "qs_dm_multi_qubit_Pauli_gate_partial_list": [P, P, U] + _STATE,
     "qs_dm_multi_qubit_Pauli_rotation_gate_partial_list": [P, P, U, D] + _STATE,
     "qs_dm_multi_qubit_control_single_qubit_dense_matrix_gate": [P, P, U, U, P] + _STATE,

@@ -508,3 +508,57 @@ class DensityMatrix:
             except Exception:
                 pass
             self._ptr = None
+
+
+# ---- qulacs.state helpers (python/cppsim_wrapper.cpp:650-680; cppsim/state.cpp) ----
+def _u32(x) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(x, dtype=np.uint32))
+
+
+def tensor_product(state_left, state_right):
+    """state::tensor_product: the right state on the low qubits (stat_ops.cpp:111-121,
+    stat_ops_dm.cpp:193-211); both state vectors or both density matrices."""
+    n = state_left.qubit_count + state_right.qubit_count
+    if isinstance(state_left, DensityMatrix) and isinstance(state_right, DensityMatrix):
+        out, fn = DensityMatrix(n, state_left.stream), "qs_dm_state_tensor_product"
+    elif isinstance(state_left, QuantumState) and isinstance(state_right, QuantumState):
+        out, fn = QuantumState(n, state_left.stream), "qs_state_tensor_product"
+    else:
+        raise TypeError("tensor_product needs two QuantumStates or two DensityMatrices")
+    call(fn, state_left.data_ptr(), state_left.dim, state_right.data_ptr(), state_right.dim, out.data_ptr(),
+         out.stream)
+    return out
+
+
+def permutate_qubit(state, qubit_order):
+    """state::permutate_qubit: new qubit q is old qubit qubit_order[q] (stat_ops.cpp:122-134,
+    stat_ops_dm.cpp:213-231)."""
+    order = _u32(qubit_order)
+    if isinstance(state, DensityMatrix):
+        out, fn = DensityMatrix(state.qubit_count, state.stream), "qs_dm_state_permutate_qubit"
+    else:
+        out, fn = QuantumState(state.qubit_count, state.stream), "qs_state_permutate_qubit"
+    call(fn, _ptr(order), state.data_ptr(), out.data_ptr(), order.size, state.dim, state.stream)
+    return out
+
+
+def drop_qubit(state: QuantumState, target, projection) -> QuantumState:
+    """state::drop_qubit: the amplitudes with target[j] = projection[j], on the remaining qubits
+    (stat_ops.cpp:136-158; not renormalised)."""
+    t, p = _u32(target), _u32(projection)
+    if t.size != p.size:
+        raise ValueError("target and projection differ in length")
+    out = QuantumState(state.qubit_count - t.size, state.stream)
+    call("qs_state_drop_qubits", _ptr(t), _ptr(p), t.size, state.data_ptr(), out.data_ptr(), state.dim, state.stream)
+    return out
+
+
+def partial_trace(state, target_traceout) -> DensityMatrix:
+    """state::partial_trace: trace the listed qubits out of a state vector or a density matrix
+    (stat_ops_dm.cpp:233-296)."""
+    t = _u32(target_traceout)
+    out = DensityMatrix(state.qubit_count - t.size, state.stream)
+    fn = ("qs_dm_state_partial_trace_from_density_matrix" if isinstance(state, DensityMatrix)
+          else "qs_dm_state_partial_trace_from_state_vector")
+    call(fn, _ptr(t), t.size, state.data_ptr(), out.data_ptr(), state.dim, state.stream)
+    return out
