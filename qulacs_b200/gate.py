@@ -395,3 +395,84 @@ def TwoQubitDepolarizingNoise(t1, t2, prob):
     if t1 == t2:
         raise ValueError("TwoQubitDepolarizingNoise: duplicated qubit")
     return QuantumGateBase("DEPOLARIZING", [t1, t2], [prob], name="Probabilistic")
+
+
+# ---- matrix utilities (cppsim gate_merge.cpp:19-356, python/cppsim_wrapper.cpp gate.merge / add /
+# to_matrix_gate) and FusedSWAP (update_ops_named_FusedSWAP.cpp:19-60), composed on the host ----
+def _action(g: QuantumGateBase):
+    """(qubits, matrix): the gate's full action on its qubits, controls included (bit j <-> qubits[j])."""
+    if g.kind == "DEPOLARIZING":
+        raise NotImplementedError("a noise channel has no matrix")
+    if g.kind == "CNOT":
+        return list(g.targets), np.eye(4, dtype=np.complex128)[:, [0, 3, 2, 1]]
+    if g.kind == "CZ":
+        return list(g.targets), np.diag([1, 1, 1, -1]).astype(np.complex128)
+    m = g.get_matrix()
+    if not g.controls:
+        return list(g.targets), m
+    k, nc = len(g.targets), len(g.controls)
+    full = np.eye(1 << (k + nc), dtype=np.complex128)
+    c = sum(v << j for j, v in enumerate(g.control_values)) << k
+    full[c:c + (1 << k), c:c + (1 << k)] = m
+    return list(g.targets) + list(g.controls), full
+
+
+def _embed(qubits, m, union):
+    """m over `qubits` as a matrix over `union` (identity on the other qubits)."""
+    pos = [union.index(q) for q in qubits]
+    u, k = len(union), len(pos)
+    xs = np.arange(1 << u)
+    local = np.zeros_like(xs)
+    for j, p in enumerate(pos):
+        local |= ((xs >> p) & 1) << j
+    rest = xs & ~sum(1 << p for p in pos)
+    scat = np.array([sum(((yl >> j) & 1) << p for j, p in enumerate(pos)) for yl in range(1 << k)])
+    full = np.zeros((1 << u, 1 << u), dtype=np.complex128)
+    full[rest[None, :] | scat[:, None], xs[None, :]] = m[:, local]
+    return full
+
+
+def _union(*gates):
+    out = []
+    for g in gates:
+        for q in _action(g)[0]:
+            if q not in out:
+                out.append(q)
+    return out
+
+
+def to_matrix_gate(g: QuantumGateBase) -> QuantumGateBase:
+    """gate::to_matrix_gate: a DenseMatrix gate with the same action (controls folded in)."""
+    q, m = _action(g)
+    return DenseMatrix(q, m)
+
+
+def merge(first: QuantumGateBase, then: QuantumGateBase) -> QuantumGateBase:
+    """gate::merge(first, then): the product `then` x `first` over the union of their qubits."""
+    u = _union(first, then)
+    return DenseMatrix(u, _embed(*_action(then), u) @ _embed(*_action(first), u))
+
+
+def add(a: QuantumGateBase, b: QuantumGateBase) -> QuantumGateBase:
+    """gate::add(a, b): the sum of the two matrices over the union of their qubits."""
+    u = _union(a, b)
+    return DenseMatrix(u, _embed(*_action(a), u) + _embed(*_action(b), u))
+
+
+def FusedSWAP(t0: int, t1: int, block_size: int) -> QuantumGateBase:
+    """gate::FusedSWAP: qubits t0 + i and t1 + i exchanged for i < block_size, as one permutation
+    matrix over the 2 x block_size qubits (block_size <= 6)."""
+    lo, hi = min(t0, t1), max(t0, t1)
+    if block_size < 1 or hi <= lo + block_size - 1:
+        raise ValueError("FusedSWAP: the blocks overlap")
+    if block_size > 6:
+        raise NotImplementedError("FusedSWAP: at most 6 qubits a block")
+    b = block_size
+    qs = [t0 + i for i in range(b)] + [t1 + i for i in range(b)]
+    x = np.arange(1 << (2 * b))
+    y = (x >> b) | ((x & ((1 << b) - 1)) << b)
+    m = np.zeros((1 << (2 * b), 1 << (2 * b)), dtype=np.complex128)
+    m[y, x] = 1.0
+    g = DenseMatrix(qs, m)
+    g.name = "FusedSWAP"
+    return g

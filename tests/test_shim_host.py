@@ -177,3 +177,29 @@ def test_pauli_operator_strings():
     o.add_operator(p)
     assert o.get_term(0).get_pauli_string() == "X 0 Z 3 Y 5"
     assert o.get_state_dim() == 64
+
+
+def test_gate_merge_add_to_matrix_and_fused_swap():
+    h, x, rz = G.H(0), G.X(0), G.RZ(0, 0.3)
+    assert np.allclose(G.merge(h, x).get_matrix(), x.get_matrix() @ h.get_matrix(), atol=1e-15)
+    assert np.allclose(G.add(h, rz).get_matrix(), h.get_matrix() + rz.get_matrix(), atol=1e-15)
+    # union order: the first gate's qubits, then the new ones; bit j <-> union[j]
+    m = G.merge(G.H(1), G.CNOT(1, 0))
+    assert m.get_target_index_list() == [1, 0]
+    cnot = np.eye(4)[:, [0, 3, 2, 1]]  # control = bit 0 (qubit 1), target = bit 1 (qubit 0)
+    assert np.allclose(m.get_matrix(), cnot @ np.kron(np.eye(2), h.get_matrix()), atol=1e-15)
+    c = G.to_matrix_gate(G.CZ(3, 1))
+    assert c.get_target_index_list() == [3, 1] and np.array_equal(np.diag(c.get_matrix()), [1, 1, 1, -1])
+    d = G.DenseMatrix([2], G.X(2).get_matrix())
+    d.add_control_qubit(0, 0)
+    t = G.to_matrix_gate(d)
+    assert t.get_target_index_list() == [2, 0]
+    assert np.array_equal(t.get_matrix().real, np.eye(4)[:, [1, 0, 2, 3]])  # flips bit 0 where bit 1 = 0
+    f = G.FusedSWAP(0, 3, 2)
+    assert f.get_target_index_list() == [0, 1, 3, 4]
+    x = np.arange(16)
+    assert np.array_equal(np.argmax(f.get_matrix(), axis=0), (x >> 2) | ((x & 3) << 2))
+    with pytest.raises(ValueError):
+        G.FusedSWAP(0, 1, 2)
+    with pytest.raises(NotImplementedError):
+        G.merge(G.DepolarizingNoise(0, 0.1), h)
