@@ -1262,11 +1262,13 @@ int ev_tiled(const PauliTerm* terms, const std::vector<int>& xidx, UINT n, const
                 if (used[i]) continue;
                 used[i] = 1;
                 size_t j = i + 1;
+                // a pairing bit below tile bit 3 breaks each quarter-warp's run of u0 into pieces that
+                // share banks (two-way conflicts on all three loads): pair only on bits >= 3
                 for (; j < tt.size(); ++j)
-                    if (!used[j] && (tt[i].xloc & tt[j].xloc)) break;
+                    if (!used[j] && (tt[i].xloc & tt[j].xloc & ~7u)) break;
                 if (j < tt.size()) {
                     used[j] = 1;
-                    const UINT common = tt[i].xloc & tt[j].xloc;
+                    const UINT common = tt[i].xloc & tt[j].xloc & ~7u;
                     EvTileTerm e1 = tt[i], e2 = tt[j];
                     e1.pivot = e2.pivot = (UINT)(31 - __builtin_clz(common));
                     pt.push_back(e1);
