@@ -124,3 +124,31 @@ def test_reflection_and_fused_swap(port):
     h = QuantumState(n)
     call("qs_initialize_Haar_random_state", h.data_ptr(), h.dim, None)
     assert abs(h.get_squared_norm() - 1.0) <= 1e-12
+
+
+def test_merged_and_fused_swap_gates_on_device(port):
+    """gate.merge / to_matrix_gate / FusedSWAP (composed on the host) act like their parts."""
+    from qulacs_b200 import gate as G
+    rng = np.random.default_rng(1450)
+    n = 9
+    a = random_state(n, rng)
+    parts = [G.H(2), G.CNOT(2, 7), G.RZ(7, 0.4), G.CZ(0, 2)]
+    m = parts[0]
+    for g in parts[1:]:
+        m = G.merge(m, g)
+    s, t = dev(a), dev(a)
+    for g in parts:
+        g.update_quantum_state(s)
+    m.update_quantum_state(t)
+    assert np.max(np.abs(s.get_vector() - t.get_vector())) <= AMP_TOL
+    u = dev(a)
+    G.to_matrix_gate(G.CNOT(4, 1)).update_quantum_state(u)
+    want = a.copy()
+    port.CNOT_gate(4, 1, want)
+    assert np.max(np.abs(u.get_vector() - want)) <= AMP_TOL
+    f = dev(a)
+    G.FusedSWAP(0, 5, 3).update_quantum_state(f)
+    want = a.copy()
+    for i in range(3):
+        port.SWAP_gate(i, 5 + i, want)
+    assert np.max(np.abs(f.get_vector() - want)) <= AMP_TOL
