@@ -138,6 +138,7 @@ class QuantumCircuit:
     def add_RX_gate(self, t, a): self.add_gate(G.RX(t, a))
     def add_RY_gate(self, t, a): self.add_gate(G.RY(t, a))
     def add_RZ_gate(self, t, a): self.add_gate(G.RZ(t, a))
+    def add_FusedSWAP_gate(self, t0, t1, block_size): self.add_gate(G.FusedSWAP(t0, t1, block_size))
     def add_RotInvX_gate(self, t, a): self.add_gate(G.RotInvX(t, a))
     def add_RotInvY_gate(self, t, a): self.add_gate(G.RotInvY(t, a))
     def add_RotInvZ_gate(self, t, a): self.add_gate(G.RotInvZ(t, a))

@@ -119,6 +119,10 @@ class PauliOperator:
              state.dim, state.stream, C.byref(out))
         return self.coef * out.value
 
+    def get_expectation_value_single_thread(self, state) -> complex:
+        """The reference's single-thread variant; the device reduction has one form."""
+        return self.get_expectation_value(state)
+
 
 class Observable:
     def __init__(self, qubit_count: int):
@@ -159,6 +163,30 @@ class Observable:
 
     def get_qubit_count(self) -> int:
         return self.qubit_count
+
+    def copy(self) -> "Observable":
+        o = Observable(self.qubit_count)
+        o.terms = [t.copy() for t in self.terms]
+        return o
+
+    def is_hermitian(self) -> bool:
+        """Every coefficient real (general_quantum_operator.cpp: HermitianQuantumOperator's check)."""
+        return all(complex(t.get_coef()).imag == 0.0 for t in self.terms)
+
+    def get_matrix(self) -> np.ndarray:
+        """The dense 2^n x 2^n matrix sum_k c_k P_k (bit j of the index <-> qubit j), on the host."""
+        n = self.qubit_count
+        if n > 14:
+            raise NotImplementedError("get_matrix: at most 14 qubits")
+        pm = [np.eye(2), np.array([[0, 1], [1, 0]]), np.array([[0, -1j], [1j, 0]]), np.diag([1, -1])]
+        out = np.zeros((1 << n, 1 << n), dtype=np.complex128)
+        for t in self.terms:
+            ids = dict(zip(t.get_index_list(), t.get_pauli_id_list()))
+            m = np.ones((1, 1), dtype=np.complex128)
+            for q in range(n):
+                m = np.kron(pm[ids.get(q, 0)], m)
+            out += t.get_coef() * m
+        return out
 
     def get_state_dim(self) -> int:
         return 1 << self.qubit_count

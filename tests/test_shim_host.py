@@ -203,3 +203,21 @@ def test_gate_merge_add_to_matrix_and_fused_swap():
         G.FusedSWAP(0, 1, 2)
     with pytest.raises(NotImplementedError):
         G.merge(G.DepolarizingNoise(0, 0.1), h)
+
+
+def test_observable_copy_hermitian_and_matrix():
+    o = Observable(3)
+    o.add_operator(PauliOperator("X 0 Z 2", 0.5))
+    o.add_operator(PauliOperator("Y 1", -0.25))
+    c = o.copy()
+    c.terms[0].change_coef(9.0)
+    assert o.get_term(0).get_coef() == 0.5
+    assert o.is_hermitian()
+    x, y, z = np.array([[0, 1], [1, 0]]), np.array([[0, -1j], [1j, 0]]), np.diag([1, -1])
+    want = 0.5 * np.kron(z, np.kron(np.eye(2), x)) - 0.25 * np.kron(np.eye(2), np.kron(y, np.eye(2)))
+    assert np.allclose(o.get_matrix(), want, atol=0)
+    o.add_operator(PauliOperator("Z 1", 0.1j))
+    assert not o.is_hermitian()
+    c2 = QuantumCircuit(8)
+    c2.add_FusedSWAP_gate(0, 4, 2)
+    assert c2.gate_list[0].get_name() == "FusedSWAP" and c2.gate_list[0].get_target_index_list() == [0, 1, 4, 5]
