@@ -90,3 +90,43 @@ def test_python_errors_map_to_exceptions():
         _lib.check(2, "x")
     with pytest.raises(NotImplementedError):
         _lib.check(5, "x")
+
+
+def _u32p(x):
+    a = np.ascontiguousarray(np.asarray(x, dtype=np.uint32))
+    return a, a.ctypes.data_as(C.c_void_p)
+
+
+def test_added_entry_points_validate_on_host(lib):
+    """The csim forms, state manipulation and density-matrix gates refuse bad arguments before any
+    device work (status 1 = invalid argument, 5 = not supported)."""
+    dim = 1 << 6
+    keep = []
+
+    def u(x):
+        a, p = _u32p(x)
+        keep.append(a)
+        return p
+
+    assert lib.qs_single_qubit_Pauli_gate(0, 4, None, dim, None) == 1          # Pauli id 4
+    assert lib.qs_single_qubit_Pauli_rotation_gate(6, 1, C.c_double(0.1), None, dim, None) == 1  # qubit 6 of 6
+    assert lib.qs_multi_qubit_Pauli_gate_whole_list(u([1] * 7), 7, None, dim, None) == 1  # more ids than qubits
+    assert lib.qs_multi_qubit_control_multi_qubit_diagonal_matrix_gate(
+        u([2]), u([1]), 1, u([2, 3]), 2, None, None, dim, None) == 1          # control is a target
+    assert lib.qs_multi_qubit_control_multi_qubit_diagonal_matrix_gate(
+        u([0]), u([2]), 1, u([1]), 1, None, None, dim, None) == 1             # control value 2
+    assert lib.qs_single_qubit_control_multi_qubit_dense_matrix_gate(1, 0, u([1, 2]), 2, None, None, dim,
+                                                                     None) == 1  # control is a target
+    assert lib.qs_state_permutate_qubit(u([0, 1, 2]), None, None, 3, dim, None) == 1      # not every qubit
+    assert lib.qs_state_permutate_qubit(u([0, 1, 2, 3, 4, 4]), None, None, 6, dim, None) == 1  # repeated
+    assert lib.qs_state_drop_qubits(u([1]), u([2]), 1, None, None, dim, None) == 1        # projection 2
+    assert lib.qs_state_drop_qubits(u(range(6)), u([0] * 6), 6, None, None, dim, None) == 1  # nothing left
+    assert lib.qs_dm_state_partial_trace_from_state_vector(u([0, 0]), 2, None, None, dim, None) == 1
+    assert lib.qs_FusedSWAP_gate(0, 2, 3, None, dim, None) == 1                           # blocks overlap
+    assert lib.qs_FusedSWAP_gate(0, 4, 3, None, dim, None) == 1                           # past qubit 5
+    assert lib.qs_dm_multi_qubit_Pauli_gate_partial_list(u([0, 1]), u([1, 5]), 2, None, 1 << 3, None) == 1
+    assert lib.qs_dm_multi_qubit_Pauli_rotation_gate_partial_list(u(range(13)), u([1] * 13), 13,
+                                                                  C.c_double(0.2), None, 1 << 14, None) == 5
+    assert lib.qs_dm_multi_qubit_control_multi_qubit_dense_matrix_gate(u([0]), u([1]), 1, u([0]), 1, None, None,
+                                                                       1 << 3, None) == 1
+    assert lib.qs_state_tensor_product(None, 1 << 30, None, 1 << 11, None, None) == 5      # 41 qubits
