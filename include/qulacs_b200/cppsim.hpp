@@ -142,6 +142,34 @@ inline CPPCTYPE inner_product(const QuantumState& bra, const QuantumState& ket) 
     return {out[0], out[1]};
 }
 
+// cppsim state::tensor_product / permutate_qubit / drop_qubit (cppsim/state.cpp; csim stat_ops.cpp:111-158):
+// new states the caller owns, as cppsim's return raw new'd pointers.
+namespace state {
+inline CPPCTYPE inner_product(const QuantumState& bra, const QuantumState& ket) { return qulacs_b200::inner_product(bra, ket); }
+inline QuantumState* tensor_product(const QuantumState& left, const QuantumState& right) {
+    auto* out = new QuantumState(left.qubit_count + right.qubit_count, left.get_cuda_stream());
+    check(qs_state_tensor_product(left.data(), left.dim, right.data(), right.dim, out->data(), left.get_cuda_stream()),
+        "tensor_product");
+    return out;
+}
+inline QuantumState* permutate_qubit(const QuantumState& src, const std::vector<UINT>& qubit_order) {
+    auto* out = new QuantumState(src.qubit_count, src.get_cuda_stream());
+    check(qs_state_permutate_qubit(qubit_order.data(), src.data(), out->data(), (UINT)qubit_order.size(), src.dim,
+              src.get_cuda_stream()),
+        "permutate_qubit");
+    return out;
+}
+inline QuantumState* drop_qubit(const QuantumState& src, const std::vector<UINT>& target,
+    const std::vector<UINT>& projection) {
+    if (target.size() != projection.size()) throw std::invalid_argument("drop_qubit: size mismatch");
+    auto* out = new QuantumState(src.qubit_count - (UINT)target.size(), src.get_cuda_stream());
+    check(qs_state_drop_qubits(target.data(), projection.data(), (UINT)target.size(), src.data(), out->data(), src.dim,
+              src.get_cuda_stream()),
+        "drop_qubit");
+    return out;
+}
+}  // namespace state
+
 class DensityMatrix : public QuantumStateBase {
 public:
     explicit DensityMatrix(UINT qubit_count, void* stream = nullptr)

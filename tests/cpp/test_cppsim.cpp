@@ -2,6 +2,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <memory>
 #include <random>
 
 #include "qulacs_b200/cppsim.hpp"
@@ -144,6 +145,19 @@ int main() {
             threw = true;
         }
         EXPECT(threw);
+    }
+    {
+        // state::tensor_product / permutate_qubit / drop_qubit: |1> (x) |0>|1>, right state on the low qubits
+        QuantumState left(1), right(2);
+        left.set_computational_basis(1);
+        right.set_computational_basis(2);  // qubit 1 set
+        std::unique_ptr<QuantumState> t(state::tensor_product(left, right));
+        EXPECT(t->qubit_count == 3 && std::abs(t->get_vector()[0b110] - CPPCTYPE(1.0)) < 1e-15);
+        // dst[i] = src[sum over set bits q of i of 2^order[q]]: src 0b110 comes from i = 0b101
+        std::unique_ptr<QuantumState> p(state::permutate_qubit(*t, {2, 0, 1}));
+        EXPECT(std::abs(p->get_vector()[0b101] - CPPCTYPE(1.0)) < 1e-15);
+        std::unique_ptr<QuantumState> d(state::drop_qubit(*t, {2}, {1}));
+        EXPECT(d->qubit_count == 2 && std::abs(d->get_vector()[0b10] - CPPCTYPE(1.0)) < 1e-15);
     }
     if (failures == 0) std::printf("OK\n");
     return failures == 0 ? 0 : 1;
