@@ -107,8 +107,8 @@ def test_reflection_and_fused_swap(port):
     rng = np.random.default_rng(1440)
     n = 10
     r, a = random_state(n, rng), random_state(n, rng)
-    s = dev(a)
-    call("qs_reflection_gate", dev(r).data_ptr(), s.data_ptr(), s.dim, None)
+    s, rs = dev(a), dev(r)  # both held: a temporary's device buffer would be freed before the call
+    call("qs_reflection_gate", rs.data_ptr(), s.data_ptr(), s.dim, None)
     want = 2 * np.vdot(r, a) * r - a
     assert np.max(np.abs(s.get_vector() - want)) <= AMP_TOL
     s = dev(a)
