@@ -2,11 +2,13 @@
 
 Workload (one step): |0...0> on 30 qubits (16 GiB complex128 state, larger than L2), then 10 layers
 of RX, RY, RZ on every qubit (angles U[0, 2pi), seeded) followed by a CNOT ladder q -> q+1 -- 1190
-gates.  The metric is the circuit's effective HBM bandwidth against the algorithmic 2 x 16 x 2^n
-bytes per gate (the reference's figure), i.e. gates x 2 x 16 x 2^n / circuit time, summed over
-ranks.  The end-to-end figure (``e2e``) runs the same circuit through the public API with the
-observable (256 Pauli strings of weight <= 6) and 1024-shot sampling, reading results back to the
-host, and reports the same unit against the circuit bytes.
+gates.  The value is gates/s through the circuit (1190 / circuit time, summed over ranks); the line
+also carries the circuit time, the physical HBM bandwidth of the staged passes (passes x 2 x 16 x 2^n
+bytes / time) and, named as such, the effective figure gates x 2 x 16 x 2^n / time against the
+reference's per-gate roofline bytes.  The end-to-end figure (``e2e``) runs the same circuit through the
+public API with the observable (256 Pauli strings of weight <= 6) and 1024-shot sampling, reading
+results back to the host, in the same unit.  The reference arm (``--impl reference``) runs the
+reference csim on all host cores over whole layers of the same circuit, in gates/s.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--mode staged|gate_by_gate]
 
@@ -33,7 +35,8 @@ DEPTH = 10
 N_TERMS = 256
 N_SHOTS = 1024
 GATE_SEED, TERM_SEED, SHOT_SEED = 2124, 2125, 2126
-METRIC = "30q circuit time & HBM GB/s (plain c128 layered RX/RY/RZ+CNOT, depth 10)"
+METRIC = ("30q circuit time & HBM GB/s (plain c128 layered RX/RY/RZ+CNOT, depth 10): gates/s through the circuit; "
+          "circuit_s and the physical HBM GB/s beside it")
 
 
 def bytes_per_gate(n: int) -> int:
@@ -161,11 +164,18 @@ def kernel_table(state, n: int, stream, reps: int = 5):
     return out
 
 
-def cpu_reference_gbs(n: int, gates, budget_s: float, threads: int, state=None):
-    """Time the reference csim (oracle/_ref, else the oracle port) gate by gate on host cores."""
+def layer_gates(n: int) -> int:
+    """Gates in one layer of the layered circuit: RX, RY, RZ on every qubit, then n - 1 CNOTs."""
+    return 3 * n + (n - 1)
+
+
+def cpu_reference_layers(n: int, gates, layers: int, threads: int, state=None, first_layer: int = 0):
+    """Time the reference csim (oracle/_ref, else the oracle port) gate by gate on host cores over
+    `layers` WHOLE layers of the layered circuit (every gate kind in its circuit proportion)."""
     os.environ.setdefault("OMP_NUM_THREADS", str(threads))
     os.environ.setdefault("QULACS_NUM_THREADS", str(threads))
     from oracle import oracle as O
+    from oracle import replay as R
     sim = O.reference()
     kind = "reference"
     if sim is None:
@@ -176,47 +186,58 @@ def cpu_reference_gbs(n: int, gates, budget_s: float, threads: int, state=None):
     if s is None:
         s = np.zeros(1 << n, dtype=np.complex128)
         s[0] = 1.0
-        W.run_on_cpu(gates[:2], s, sim)  # first touch of every page, untimed
-    done, t0 = 0, time.perf_counter()
-    i = 2
-    while time.perf_counter() - t0 < budget_s or done < 2:
-        W.run_on_cpu([gates[i % len(gates)]], s, sim)
-        i += 1
-        done += 1
+        R.run_on_cpu(gates[:2], s, sim)  # first touch of every page, untimed
+    per = layer_gates(n)
+    lo = (first_layer % DEPTH) * per
+    work = [gates[(lo + i) % len(gates)] for i in range(layers * per)]
+    t0 = time.perf_counter()
+    R.run_on_cpu(work, s, sim)
     dt = time.perf_counter() - t0
-    return {"value": done * bytes_per_gate(n) / dt / 1e9, "unit": "GB/s", "cores": threads, "kind": kind,
-            "sample": f"{done} gates of the {n}-qubit layered circuit, gate by gate, {dt:.1f} s"}
+    return {"value": len(work) / dt, "unit": "gates/s", "gbs_per_gate": len(work) * bytes_per_gate(n) / dt / 1e9,
+            "seconds": dt, "cores": threads, "kind": kind,
+            "sample": f"{layers} whole layer(s) of the {n}-qubit layered circuit ({len(work)} gates: "
+                      f"{3 * n * layers} rotations, {(n - 1) * layers} CNOTs), gate by gate, {dt:.1f} s"}
 
 
 def run_reference(args, rank: int, world: int):
+    """The reference arm: the reference csim, compiled from its own sources (oracle/_ref), on all host
+    cores, gate by gate.  One step = one whole layer of the benchmark circuit (119 gates at 30 qubits,
+    every gate kind in proportion); value = gates/s over the timed steps, the same unit as this
+    library's arm.  Rank 0 only (the other ranks exit without work)."""
     if rank != 0:
         return
     threads = os.cpu_count() or 1
     os.environ.setdefault("OMP_NUM_THREADS", str(threads))
     os.environ.setdefault("QULACS_NUM_THREADS", str(threads))
     from oracle import oracle as O
+    from oracle import replay as R
     from qulacs_b200 import workloads as W
     n = args.qubits
     gates = W.layered_rotation_circuit(n, DEPTH, GATE_SEED)
-    sim = O.reference() or O.port()
     s = np.zeros(1 << n, dtype=np.complex128)
     s[0] = 1.0
-    W.run_on_cpu(gates[:2], s, sim)  # first touch of every page, untimed
-    per_step_s = 6.0
+    R.run_on_cpu(gates[:2], s, O.reference() or O.port())  # first touch of every page, untimed
     vals = []
     for i in range(args.warmup + args.steps):
-        r = cpu_reference_gbs(n, gates[(i * 7) % len(gates):] + gates, per_step_s, threads, state=s)
+        r = cpu_reference_layers(n, gates, 1, threads, state=s, first_layer=i)
         if i >= args.warmup:
             vals.append(r)
-    value = statistics.median(v["value"] for v in vals)
+    secs = sum(v["seconds"] for v in vals)
+    value = len(vals) * layer_gates(n) / secs
     cb = dict(vals[-1])
     cb["value"] = value
-    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 * bytes_per_gate(n) * len(gates) / (value * 1e9),
+    cb["sample"] = f"{len(vals)} timed steps of one whole layer each ({layer_gates(n)} gates), after " \
+                   f"{args.warmup} warm-up layers"
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "gates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / len(vals),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128 (f64)",
-            "data": "synthetic (seeded)", "config": {"workload": f"layered RX/RY/RZ+CNOT n={n} depth={DEPTH}, gate sample per step"},
-            "cpu_baseline": cb, "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "data": "synthetic (seeded)",
+            "config": {"workload": f"layered RX/RY/RZ+CNOT n={n} depth={DEPTH}: one whole layer of {DEPTH} "
+                                   f"({layer_gates(n)} gates) per step"},
+            "circuit_s_from_layers": len(gates) / value,
+            "gbs_per_gate": value * bytes_per_gate(n) / 1e9,
+            "cpu_baseline": cb, "e2e": {"value": value, "unit": "gates/s", "h2d_bytes_per_step": 0,
+                                        "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
@@ -234,7 +255,7 @@ def fused_comparison(n: int, layers: int, stream, with_gate_by_gate: bool, reps:
     circ = W.to_circuit(gates, n)
     obs = W.to_observable(terms, n)
 
-    def timed(fn):
+    def timed(fn, reps=reps):
         fn()  # warm-up (plan build, first touch)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -249,7 +270,7 @@ def fused_comparison(n: int, layers: int, stream, with_gate_by_gate: bool, reps:
     t_staged = timed(lambda: (plain.set_zero_state(), circ.update_quantum_state(plain, mode="staged")))
     t_gbg = None
     if with_gate_by_gate:
-        t_gbg = timed(lambda: (plain.set_zero_state(), circ.update_quantum_state(plain, mode="gate_by_gate")))
+        t_gbg = timed(lambda: (plain.set_zero_state(), circ.update_quantum_state(plain, mode="gate_by_gate")), 1)
     plain.set_zero_state()
     circ.update_quantum_state(plain, mode="staged")
     fused = Q.QuantumStateC64(n)
@@ -324,13 +345,14 @@ def noise_sampling(n: int = 20, depth: int = 4, p: float = 1e-3, shots: int = 10
            "shots_per_s": shots / gpu_s, "checksum": int(out.sum() % (1 << 31))}
     try:
         from oracle import oracle as O
+        from oracle import replay as R
         port = O.port()
         sample = 1
         t0 = time.perf_counter()
         for _ in range(sample):
             st = np.zeros(1 << n, dtype=np.complex128)
             st[0] = 1
-            W.run_on_cpu([g for g in gates if g[0] != "DEPOL"], st, port)
+            R.run_on_cpu([g for g in gates if g[0] != "DEPOL"], st, port)
         cpu_per = (time.perf_counter() - t0) / sample
         res["cpu_port_s_per_trajectory"] = cpu_per
         res["cpu_port_s_estimate"] = cpu_per * traj.size
@@ -372,6 +394,7 @@ def dm_noisy_circuit(n: int = 13, depth: int = 8, p: float = 1e-3, seed: int = 7
     res["trace"] = rho.get_squared_norm()  # DensityMatrix squared norm = trace (cppsim state_dm.hpp:142)
     try:
         from oracle import oracle as O
+        from oracle import replay as R
         ref = O.reference()
         if ref is None:
             raise RuntimeError("reference csim not built")
@@ -380,7 +403,7 @@ def dm_noisy_circuit(n: int = 13, depth: int = 8, p: float = 1e-3, seed: int = 7
         t0 = time.perf_counter()
         done = 0
         for g in gates:
-            W.run_on_cpu_dm([g], r, ref)
+            R.run_on_cpu_dm([g], r, ref)
             done += 1
             if time.perf_counter() - t0 > 10.0:
                 break
@@ -574,7 +597,7 @@ def main():
         ms = timed_region(step, args.steps, args.warmup, dist, torch.cuda.synchronize, cuda_timer, "cuda")
     launches = lib.qs_launch_count() - launch0[0]
     gb_per_step = len(gates) * bytes_per_gate(n) / 1e9
-    value = world * gb_per_step / (ms / 1e3)
+    value = world * len(gates) / (ms / 1e3)  # gates/s, whole job
 
     # dominant kernel roofline: one HBM pass = 2 x 16 x 2^n algorithmic bytes
     staged_kernel = mode in ("staged", "staged_fused")
@@ -642,15 +665,15 @@ def main():
     # keep the other ranks waiting at the closing barrier
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_reference_gbs(n, gates, 12.0, os.cpu_count() or 1)
+        cpu = cpu_reference_layers(n, gates, 1, os.cpu_count() or 1)
 
     # configs 3-5 beside the headline (each guarded: a failure is reported, not fatal)
     extras = {}
     if world == 1 and not args.no_extras:
         del state
         torch.cuda.synchronize()
-        for key, fn in (("fused", lambda: fused_comparison(args.fused_qubits, args.fused_layers, stream, False)),
-                        ("batched", lambda: batched_throughput(512, 64.0)),
+        for key, fn in (("fused", lambda: fused_comparison(args.fused_qubits, args.fused_layers, stream, True)),
+                        ("batched", lambda: batched_throughput(args.instances, args.budget_gb)),
                         ("serving", lambda: serving_latency(60, 5.0, 96.0, 4)),
                         ("noise", lambda: noise_sampling()),
                         ("density_matrix", lambda: dm_noisy_circuit())):
@@ -661,16 +684,20 @@ def main():
 
     if rank == 0:
         line = {
-            "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "metric": METRIC, "value": value, "unit": "gates/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "c128 (f64)", "data": "synthetic (seeded)",
             "config": {"workload": f"layered RX/RY/RZ+CNOT n={n} depth={DEPTH} ({len(gates)} gates), c128",
                        "exec_mode": mode, "hbm_passes": passes,
                        "l2": f"state {(16 << n) / 2**30:g} GiB > L2 (no flush needed)",
                        "parallelism": f"replicas x{world}"},
+            "circuit_s": ms / 1e3,
+            "hbm_gbs_physical": passes * bytes_per_gate(n) / 1e9 / (ms / 1e3),
+            "effective_gbs": gb_per_step / (ms / 1e3),
+            "effective_gbs_note": "gates x 2 x 16 x 2^n B (the reference's per-gate roofline bytes) / circuit "
+                                  "time; not a bandwidth: a staged pass applies many gates per HBM read+write",
             "fusion": fusion,
             "modes_ms": modes_ms,
-            "circuit_s": ms / 1e3,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                          "frac": achieved / hbm_peak, "peak_kind": peak_kind,
                          "traffic": (STAGED_TRAFFIC_PER_AMP * (1 << n)) if staged_kernel else None,
@@ -684,7 +711,7 @@ def main():
                               "note": "FP64 instr/amplitude: rotation or 1q diagonal 4, 1q dense 8, k-qubit dense "
                                       "4 x 2^k, CNOT/CZ/SWAP 0; nominal 64 FP64 FMA/clk/SM at 1965 MHz"},
             "kernels": kernels,
-            "e2e": {"value": world * gb_per_step / (e2e_ms / 1e3), "unit": "GB/s", "ms_per_step": e2e_ms,
+            "e2e": {"value": world * len(gates) / (e2e_ms / 1e3), "unit": "gates/s", "ms_per_step": e2e_ms,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "includes": "set_zero_state + circuit + <H> (256 strings) + 1024-shot sampling"},
             "energy": energy,

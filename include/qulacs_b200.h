@@ -290,8 +290,10 @@ QS_API int qs_state_sampling(const void* state, QS_ITYPE dim, QS_UINT sampling_c
  * reserved 2.25 MiB array in the library's device image, held by every GPU that loads the library
  * until the process exits.  Limits: dim <= 2^28 and sampling_count <= 16384, else
  * QS_ERR_NOT_SUPPORTED.  Same results as qs_state_sampling_with_uniforms.  The first call on a
- * device looks up the array's device address, so make it before any stream capture.  All calls
- * share the array: calls that overlap on the GPU race.
+ * device looks up the array's device address, so make it before any stream capture.  That address
+ * is kept for the life of the process: after a cudaDeviceReset the library's device image is loaded
+ * again and the kept address is stale, so do not call this entry point after resetting a device.
+ * All calls share the array: calls that overlap on the GPU race.
  */
 QS_API int qs_state_sampling_with_uniforms_noalloc(const void* state, QS_ITYPE dim, const double* uniforms,
     QS_UINT sampling_count, QS_ITYPE* out, void* stream);

@@ -146,27 +146,34 @@ inline CPPCTYPE inner_product(const QuantumState& bra, const QuantumState& ket) 
 // new states the caller owns, as cppsim's return raw new'd pointers.
 namespace state {
 inline CPPCTYPE inner_product(const QuantumState& bra, const QuantumState& ket) { return qulacs_b200::inner_product(bra, ket); }
+// The result is held by a unique_ptr until the C call succeeds, so a rejected call frees its device memory.
 inline QuantumState* tensor_product(const QuantumState& left, const QuantumState& right) {
-    auto* out = new QuantumState(left.qubit_count + right.qubit_count, left.get_cuda_stream());
+    std::unique_ptr<QuantumState> out(new QuantumState(left.qubit_count + right.qubit_count, left.get_cuda_stream()));
+    if (right.get_cuda_stream() != left.get_cuda_stream())  // the right state's last writes must be done
+        check(qs_stream_synchronize(right.get_cuda_stream()), "tensor_product");
     check(qs_state_tensor_product(left.data(), left.dim, right.data(), right.dim, out->data(), left.get_cuda_stream()),
         "tensor_product");
-    return out;
+    return out.release();
 }
 inline QuantumState* permutate_qubit(const QuantumState& src, const std::vector<UINT>& qubit_order) {
-    auto* out = new QuantumState(src.qubit_count, src.get_cuda_stream());
+    if (qubit_order.size() != src.qubit_count)  // cppsim/state.cpp: the order lists every qubit
+        throw std::invalid_argument("permutate_qubit: qubit_order must list every qubit once");
+    std::unique_ptr<QuantumState> out(new QuantumState(src.qubit_count, src.get_cuda_stream()));
     check(qs_state_permutate_qubit(qubit_order.data(), src.data(), out->data(), (UINT)qubit_order.size(), src.dim,
               src.get_cuda_stream()),
         "permutate_qubit");
-    return out;
+    return out.release();
 }
 inline QuantumState* drop_qubit(const QuantumState& src, const std::vector<UINT>& target,
     const std::vector<UINT>& projection) {
     if (target.size() != projection.size()) throw std::invalid_argument("drop_qubit: size mismatch");
-    auto* out = new QuantumState(src.qubit_count - (UINT)target.size(), src.get_cuda_stream());
+    if (target.size() >= src.qubit_count)  // cppsim/state.cpp:70: at least one qubit must remain
+        throw std::invalid_argument("drop_qubit: cannot drop every qubit");
+    std::unique_ptr<QuantumState> out(new QuantumState(src.qubit_count - (UINT)target.size(), src.get_cuda_stream()));
     check(qs_state_drop_qubits(target.data(), projection.data(), (UINT)target.size(), src.data(), out->data(), src.dim,
               src.get_cuda_stream()),
         "drop_qubit");
-    return out;
+    return out.release();
 }
 }  // namespace state
 
@@ -225,22 +232,101 @@ public:
             "add_gate");
     }
     // cppsim QuantumGateBase::update_quantum_state (gate.hpp:159): state vector or density matrix.
+    // One csim-named C-ABI call per gate (the reference's gate classes call csim the same way,
+    // gate_named_one.hpp:41-63, gate_matrix.cpp:69-332); no circuit object is built.
     void update_quantum_state(QuantumStateBase* state) const {
-        qs_circuit_t c = nullptr;
-        check(qs_circuit_create(state->qubit_count, &c), "update_quantum_state");
-        std::unique_ptr<void, void (*)(void*)> guard(c, [](void* p) { qs_circuit_destroy((qs_circuit_t)p); });
-        add_to(c);
-        if (state->is_state_vector())
-            check(qs_circuit_update_quantum_state(c, state->data(), state->dim, QS_EXEC_GATE_BY_GATE,
-                      state->get_cuda_stream()),
-                "update_quantum_state");
-        else
-            check(qs_circuit_update_density_matrix(c, state->data(), state->dim, QS_EXEC_GATE_BY_GATE,
-                      state->get_cuda_stream()),
-                "update_quantum_state");
+        if (state->is_state_vector()) check(apply_state_vector(state->data(), state->dim, state->get_cuda_stream()),
+                                          "update_quantum_state");
+        else check(apply_density_matrix(state->data(), state->dim, state->get_cuda_stream()), "update_quantum_state");
     }
 
 private:
+    std::vector<UINT> pauli_ids() const {
+        std::vector<UINT> ids;
+        for (size_t i = 0; i < targets_.size(); ++i) ids.push_back((UINT)params_[i]);
+        return ids;
+    }
+    int apply_state_vector(void* s, ITYPE dim, void* st) const {
+        const UINT* t = targets_.data();
+        const UINT nt = (UINT)targets_.size();
+        const double* m = params_.data();
+        switch (kind_) {
+            case QS_GATE_RX: return qs_RX_gate(t[0], params_[0], s, dim, st);
+            case QS_GATE_RY: return qs_RY_gate(t[0], params_[0], s, dim, st);
+            case QS_GATE_RZ: return qs_RZ_gate(t[0], params_[0], s, dim, st);
+            case QS_GATE_CNOT: return qs_CNOT_gate(t[0], t[1], s, dim, st);
+            case QS_GATE_CZ: return qs_CZ_gate(t[0], t[1], s, dim, st);
+            case QS_GATE_SWAP: return qs_SWAP_gate(t[0], t[1], s, dim, st);
+            case QS_GATE_PAULI: {
+                const std::vector<UINT> ids = pauli_ids();
+                return qs_multi_qubit_Pauli_gate_partial_list(t, ids.data(), nt, s, dim, st);
+            }
+            case QS_GATE_PAULI_ROTATION: {
+                const std::vector<UINT> ids = pauli_ids();
+                return qs_multi_qubit_Pauli_rotation_gate_partial_list(t, ids.data(), nt, params_[nt], s, dim, st);
+            }
+            case QS_GATE_DIAGONAL:
+                if (nt == 1) return qs_single_qubit_diagonal_matrix_gate(t[0], m, s, dim, st);
+                return qs_multi_qubit_diagonal_matrix_gate(t, nt, m, s, dim, st);
+            case QS_GATE_DENSE:
+                if (controls_.empty()) {
+                    if (nt == 1) return qs_single_qubit_dense_matrix_gate(t[0], m, s, dim, st);
+                    if (nt == 2) return qs_double_qubit_dense_matrix_gate_c(t[0], t[1], m, s, dim, st);
+                    return qs_multi_qubit_dense_matrix_gate(t, nt, m, s, dim, st);
+                }
+                if (nt == 1)
+                    return qs_multi_qubit_control_single_qubit_dense_matrix_gate(controls_.data(), control_values_.data(),
+                        (UINT)controls_.size(), t[0], m, s, dim, st);
+                return qs_multi_qubit_control_multi_qubit_dense_matrix_gate(controls_.data(), control_values_.data(),
+                    (UINT)controls_.size(), t, nt, m, s, dim, st);
+            default: return via_circuit(s, dim, st, true);  // depolarizing: the circuit path reports the error
+        }
+    }
+    int apply_density_matrix(void* r, ITYPE dim, void* st) const {
+        const UINT* t = targets_.data();
+        const UINT nt = (UINT)targets_.size();
+        switch (kind_) {
+            case QS_GATE_RX: return qs_dm_RX_gate(t[0], params_[0], r, dim, st);
+            case QS_GATE_RY: return qs_dm_RY_gate(t[0], params_[0], r, dim, st);
+            case QS_GATE_RZ: return qs_dm_RZ_gate(t[0], params_[0], r, dim, st);
+            case QS_GATE_CNOT: return qs_dm_CNOT_gate(t[0], t[1], r, dim, st);
+            case QS_GATE_CZ: return qs_dm_CZ_gate(t[0], t[1], r, dim, st);
+            case QS_GATE_SWAP: return qs_dm_SWAP_gate(t[0], t[1], r, dim, st);
+            case QS_GATE_PAULI: {
+                const std::vector<UINT> ids = pauli_ids();
+                return qs_dm_multi_qubit_Pauli_gate_partial_list(t, ids.data(), nt, r, dim, st);
+            }
+            case QS_GATE_PAULI_ROTATION: {
+                const std::vector<UINT> ids = pauli_ids();
+                return qs_dm_multi_qubit_Pauli_rotation_gate_partial_list(t, ids.data(), nt, params_[nt], r, dim, st);
+            }
+            case QS_GATE_DEPOLARIZING:
+                if (nt == 1) return qs_dm_depolarizing_noise(t[0], params_[0], r, dim, st);
+                return qs_dm_two_qubit_depolarizing_noise(t[0], t[1], params_[0], r, dim, st);
+            case QS_GATE_DENSE:
+                if (controls_.empty()) {
+                    if (nt == 1) return qs_dm_single_qubit_dense_matrix_gate(t[0], params_.data(), r, dim, st);
+                    return qs_dm_multi_qubit_dense_matrix_gate(t, nt, params_.data(), r, dim, st);
+                }
+                return qs_dm_multi_qubit_control_multi_qubit_dense_matrix_gate(controls_.data(), control_values_.data(),
+                    (UINT)controls_.size(), t, nt, params_.data(), r, dim, st);
+            default: return via_circuit(r, dim, st, false);  // diagonal gates: expanded by the circuit path
+        }
+    }
+    int via_circuit(void* s, ITYPE dim, void* st, bool vector) const {
+        UINT n = 0;
+        while ((ITYPE(1) << n) < dim) ++n;
+        qs_circuit_t c = nullptr;
+        int rc = qs_circuit_create(n, &c);
+        if (rc != QS_OK) return rc;
+        std::unique_ptr<void, void (*)(void*)> guard(c, [](void* p) { qs_circuit_destroy((qs_circuit_t)p); });
+        rc = qs_circuit_add_gate(c, kind_, targets_.data(), (UINT)targets_.size(), controls_.data(),
+            control_values_.data(), (UINT)controls_.size(), params_.data(), (UINT)params_.size());
+        if (rc != QS_OK) return rc;
+        return vector ? qs_circuit_update_quantum_state(c, s, dim, QS_EXEC_GATE_BY_GATE, st)
+                      : qs_circuit_update_density_matrix(c, s, dim, QS_EXEC_GATE_BY_GATE, st);
+    }
+
     int kind_;
     std::vector<UINT> targets_, controls_, control_values_;
     std::vector<double> params_;

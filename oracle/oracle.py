@@ -38,8 +38,17 @@ def build_port() -> str:
     return PORT_SO
 
 
-def build_reference(ref_root: str = "/root/reference") -> str | None:
+def reference_root() -> str:
+    """The reference checkout: $QULACS_REFERENCE_ROOT, else a ``reference`` directory beside the repository."""
+    env = os.environ.get("QULACS_REFERENCE_ROOT")
+    if env:
+        return env
+    return os.path.abspath(os.path.join(HERE, "..", "..", "reference"))
+
+
+def build_reference(ref_root: str | None = None) -> str | None:
     """Compile the reference csim when its sources are present (never on a machine without them)."""
+    ref_root = ref_root or reference_root()
     if not os.path.isdir(os.path.join(ref_root, "src", "csim")):
         return REF_SO if os.path.exists(REF_SO) else None
     subprocess.check_call(["make", "-s", "-j8", "-C", HERE, "ref", f"REF={ref_root}"])

@@ -525,6 +525,8 @@ def tensor_product(state_left, state_right):
         out, fn = QuantumState(n, state_left.stream), "qs_state_tensor_product"
     else:
         raise TypeError("tensor_product needs two QuantumStates or two DensityMatrices")
+    if state_right.stream != state_left.stream:  # the right state's pending writes finish first
+        call("qs_stream_synchronize", state_right.stream)
     call(fn, state_left.data_ptr(), state_left.dim, state_right.data_ptr(), state_right.dim, out.data_ptr(),
          out.stream)
     return out

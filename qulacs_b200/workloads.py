@@ -118,52 +118,6 @@ def to_observable(terms, n: int):
     return obs
 
 
-def run_on_cpu(gates, state: np.ndarray, sim) -> None:
-    """Apply a gate list with a CPU implementation (oracle port or reference csim) in place."""
-    for g in gates:
-        k = g[0]
-        if k == "RX":
-            sim.RX_gate(g[1], g[2], state)
-        elif k == "RY":
-            sim.RY_gate(g[1], g[2], state)
-        elif k == "RZ":
-            sim.RZ_gate(g[1], g[2], state)
-        elif k == "U3":
-            sim.single_qubit_dense_matrix_gate(g[1], u3_matrix(*g[2:5]), state)
-        elif k == "CNOT":
-            sim.CNOT_gate(g[1], g[2], state)
-        elif k == "CZ":
-            sim.CZ_gate(g[1], g[2], state)
-        elif k == "DENSE":
-            sim.multi_qubit_dense_matrix_gate(list(g[1]), g[2], state)
-        else:
-            raise ValueError(k)
-
-
-def run_on_cpu_dm(gates, rho: np.ndarray, sim) -> None:
-    """Apply a gate list to a density matrix with a CPU implementation in place."""
-    for g in gates:
-        k = g[0]
-        if k in ("RX", "RY", "RZ"):
-            sim.dm_single_qubit_dense_matrix_gate(g[1], rotation_matrix(k, g[2]), rho)
-        elif k == "U3":
-            sim.dm_single_qubit_dense_matrix_gate(g[1], u3_matrix(*g[2:5]), rho)
-        elif k == "CNOT":
-            sim.dm_CNOT_gate(g[1], g[2], rho)
-        elif k == "CZ":
-            sim.dm_CZ_gate(g[1], g[2], rho)
-        elif k == "DENSE":
-            sim.dm_multi_qubit_dense_matrix_gate(list(g[1]), g[2], rho)
-        elif k == "DEPOL":
-            qs = list(g[1])
-            if len(qs) == 1:
-                sim.dm_depolarizing_noise(qs[0], g[2], rho)
-            else:
-                sim.dm_two_qubit_depolarizing_noise(qs[0], qs[1], g[2], rho)
-        else:
-            raise ValueError(k)
-
-
 def rotation_matrix(kind: str, a: float) -> np.ndarray:
     """csim RX/RY/RZ matrices (update_ops_pauli_single.cpp:54-120): exp(+i a P / 2)."""
     c, s = math.cos(a / 2), math.sin(a / 2)

@@ -77,6 +77,59 @@ int main() {
         std::vector<UINT> all0(n, 0);
         EXPECT(std::abs(a.get_marginal_probability(all0) - 1.0) < 1e-12);
     }
+    // every gate kind's direct update_quantum_state (one csim-named call) equals the same gate run through
+    // a one-gate circuit, on a state vector and on a density matrix
+    {
+        const UINT n = 5;
+        const double h = 1.0 / std::sqrt(2.0);
+        auto make = [&](int i) -> QuantumGateBase* {
+            switch (i) {
+                case 0: return gate::RX(1, 0.7);
+                case 1: return gate::RY(3, -1.1);
+                case 2: return gate::RZ(0, 2.3);
+                case 3: return gate::CNOT(4, 1);
+                case 4: return gate::CZ(2, 0);
+                case 5: return gate::SWAP(0, 3);
+                case 6: return gate::H(2);
+                case 7: return gate::T(4);
+                case 8: return gate::DenseMatrix({1, 3}, {h, 0, 0, h, 0, h, h, 0, 0, h, -h, 0, h, 0, 0, -h});
+                case 9: return gate::Pauli({0, 2, 4}, {1, 2, 3});
+                case 10: return gate::PauliRotation({1, 3}, {2, 1}, 0.4);
+                case 11: {
+                    QuantumGateBase* g = gate::DenseMatrix(2, {0, CPPCTYPE(0, 1), CPPCTYPE(0, 1), 0});
+                    g->add_control_qubit(4, 1);
+                    return g;
+                }
+                case 12: return gate::DiagonalMatrix({0, 3}, {1, CPPCTYPE(0, 1), -1, CPPCTYPE(0, -1)});
+                default: return nullptr;
+            }
+        };
+        QuantumState a(n), b(n);
+        DensityMatrix ra(n), rb(n);
+        QuantumGateBase* prep = gate::H(0);
+        prep->update_quantum_state(&a);
+        prep->update_quantum_state(&b);
+        prep->update_quantum_state(&ra);
+        prep->update_quantum_state(&rb);
+        delete prep;
+        for (int i = 0; i <= 12; ++i) {
+            std::unique_ptr<QuantumGateBase> g(make(i));
+            g->update_quantum_state(&a);
+            g->update_quantum_state(&ra);
+            QuantumCircuit c(n);
+            c.add_gate(make(i));
+            c.update_quantum_state(&b, QS_EXEC_GATE_BY_GATE);
+            c.update_quantum_state(&rb, QS_EXEC_GATE_BY_GATE);
+            const ComplexVector va = a.get_vector(), vb = b.get_vector();
+            double err = 0;
+            for (size_t k = 0; k < va.size(); ++k) err = std::max(err, std::abs(va[k] - vb[k]));
+            EXPECT(err <= 1e-14);
+            const ComplexVector ma = ra.get_matrix(), mb = rb.get_matrix();
+            err = 0;
+            for (size_t k = 0; k < ma.size(); ++k) err = std::max(err, std::abs(ma[k] - mb[k]));
+            EXPECT(err <= 1e-14);
+        }
+    }
     // sampling a basis state (test/cppsim/test_state.cpp:38-47)
     {
         QuantumState s(10);
@@ -158,6 +211,29 @@ int main() {
         EXPECT(std::abs(p->get_vector()[0b101] - CPPCTYPE(1.0)) < 1e-15);
         std::unique_ptr<QuantumState> d(state::drop_qubit(*t, {2}, {1}));
         EXPECT(d->qubit_count == 2 && std::abs(d->get_vector()[0b10] - CPPCTYPE(1.0)) < 1e-15);
+        // rejected before any allocation (cppsim/state.cpp:70): every qubit dropped, a short order
+        bool threw = false;
+        try {
+            delete state::drop_qubit(*t, {0, 1, 2}, {0, 0, 0});
+        } catch (const std::invalid_argument&) {
+            threw = true;
+        }
+        EXPECT(threw);
+        threw = false;
+        try {
+            delete state::permutate_qubit(*t, {1, 0});
+        } catch (const std::invalid_argument&) {
+            threw = true;
+        }
+        EXPECT(threw);
+        // a bad projection value is rejected by the C ABI and the new state is freed, not leaked
+        threw = false;
+        try {
+            delete state::drop_qubit(*t, {2}, {3});
+        } catch (const std::invalid_argument&) {
+            threw = true;
+        }
+        EXPECT(threw);
     }
     if (failures == 0) std::printf("OK\n");
     return failures == 0 ? 0 : 1;

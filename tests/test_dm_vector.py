@@ -9,6 +9,7 @@ from conftest import AMP_TOL, random_density_matrix, random_unitary
 from qulacs_b200 import QuantumCircuit
 from qulacs_b200 import gate as G
 from qulacs_b200 import workloads as W
+from oracle import replay as R
 
 
 def replay_vector(circ, rho, port):
@@ -28,7 +29,7 @@ def test_noisy_hea_vector_matches_oracle(port, n, seed):
     rng = np.random.default_rng(seed)
     rho0 = random_density_matrix(n, rng)
     want = rho0.copy()
-    W.run_on_cpu_dm(gates, want, port)
+    R.run_on_cpu_dm(gates, want, port)
     got = replay_vector(W.to_circuit(gates, n), rho0, port)
     assert np.max(np.abs(got - want)) <= AMP_TOL
 

@@ -9,6 +9,7 @@ import pytest
 from conftest import random_state
 from qulacs_b200 import workloads as W
 from qulacs_b200._lib import call
+from oracle import replay as R
 
 
 def kmajor_off(r, k):
@@ -46,7 +47,7 @@ def test_fused_blocks_reproduce_circuit(port):
     assert len(blocks) < len(gates)
     s0 = random_state(n, np.random.default_rng(1))
     want = s0.copy()
-    W.run_on_cpu(gates, want, port)
+    R.run_on_cpu(gates, want, port)
     got = s0.copy()
     for qubits, U, _, tile in blocks:
         assert set(qubits) <= set(int(t) for t in tile)
@@ -175,7 +176,7 @@ def test_kernel_dataflow_emulation(port, n, layers, seed):
     circ = W.to_circuit(gates, n)
     s0 = random_state(n, np.random.default_rng(seed))
     want = s0.copy()
-    W.run_on_cpu(gates, want, port)
+    R.run_on_cpu(gates, want, port)
     got = emulate_fused(circ, n, s0)
     assert not np.any(np.isnan(got))
     # bf16 hi + lo operands carry ~16 significant bits per factor (the B operand is exact here)

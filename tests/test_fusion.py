@@ -8,6 +8,7 @@ from conftest import AMP_TOL, random_state, random_unitary
 from qulacs_b200 import QuantumCircuit
 from qulacs_b200 import gate as G
 from qulacs_b200 import workloads as W
+from oracle import replay as R
 
 
 def replay(fused, state, port):
@@ -31,7 +32,7 @@ def test_fused_lists_reproduce_the_circuit(port, k):
         assert len(fused) == len(gates)
     s0 = random_state(n, rng)
     want = s0.copy()
-    W.run_on_cpu(gates, want, port)
+    R.run_on_cpu(gates, want, port)
     got = s0.copy()
     items = [fused[i] for i in range(len(fused))]
     replay(items, got, port)

@@ -7,6 +7,7 @@ from conftest import EV_TOL
 from qulacs_b200 import QuantumState
 from qulacs_b200 import workloads as W
 from qulacs_b200.batch import BatchRunner, run_alone
+from oracle import replay as R
 
 pytestmark = pytest.mark.gpu
 
@@ -34,7 +35,7 @@ def test_batch_matches_alone_and_oracle(port):
         assert abs(e - alone) <= 1e-12  # same states; the reductions chunk the sums differently
         psi = np.zeros(1 << n, dtype=np.complex128)
         psi[0] = 1
-        W.run_on_cpu(gates, psi, port)
+        R.run_on_cpu(gates, psi, port)
         want = sum(c * port.expectation_value(tl, ids, psi) for c, tl, ids in terms)
         assert abs(e - want) <= EV_TOL
 
@@ -52,7 +53,7 @@ def test_batch_states_match_gate_by_gate(port):
     for (circ, _), s, (n, gates, _) in zip(jobs, states, specs):
         psi = np.zeros(1 << n, dtype=np.complex128)
         psi[0] = 1
-        W.run_on_cpu(gates, psi, port)
+        R.run_on_cpu(gates, psi, port)
         v = s.get_vector()
         assert np.max(np.abs(v - psi)) <= 1e-12
         alone = QuantumState(n)
@@ -70,7 +71,7 @@ def test_batch_fused_c64(port):
     for (n, gates, terms), e in zip(specs, got):
         psi = np.zeros(1 << n, dtype=np.complex128)
         psi[0] = 1
-        W.run_on_cpu(gates, psi, port)
+        R.run_on_cpu(gates, psi, port)
         want = sum(c * port.expectation_value(tl, ids, psi) for c, tl, ids in terms)
         assert abs(e - want) <= 1e-4
 
@@ -89,7 +90,7 @@ def test_batch_mixed_sizes_across_the_single_state_threshold(port, precision):
     for (circ, obs), (n, gates, terms), e in zip(jobs, specs, got):
         psi = np.zeros(1 << n, dtype=np.complex128)
         psi[0] = 1
-        W.run_on_cpu(gates, psi, port)
+        R.run_on_cpu(gates, psi, port)
         want = sum(c * port.expectation_value(tl, ids, psi) for c, tl, ids in terms)
         assert abs(e - want) <= (EV_TOL if precision == "c128" else 1e-5), (n, e, want)
 

@@ -8,6 +8,7 @@ import pytest
 from conftest import AMP_TOL, BOUNDARY_EPS, EV_TOL, GOLDEN
 from qulacs_b200 import QuantumState
 from qulacs_b200 import workloads as W
+from oracle import replay as R
 
 pytestmark = pytest.mark.gpu
 
@@ -27,7 +28,7 @@ def test_config1_against_reference_golden(port, mode):
     # full state against the oracle
     want = np.zeros(1 << n, dtype=np.complex128)
     want[0] = 1
-    W.run_on_cpu(gates, want, port)
+    R.run_on_cpu(gates, want, port)
     assert np.max(np.abs(v - want)) <= AMP_TOL
     terms = W.random_pauli_terms(n, 64, 1, 4, int(g["term_seed"]))
     obs = W.to_observable(terms, n)
@@ -65,7 +66,7 @@ def test_random_circuits_against_oracle(port, n, mode):
     circ.update_quantum_state(s, mode=mode)
     want = np.zeros(1 << n, dtype=np.complex128)
     want[0] = 1
-    W.run_on_cpu(gates, want, port)
+    R.run_on_cpu(gates, want, port)
     assert np.max(np.abs(s.get_vector() - want)) <= AMP_TOL
 
 
@@ -93,7 +94,7 @@ def test_cnot_chains_folded_into_dense_ops(port, n, mode):
     circ.update_quantum_state(s, mode=mode)
     want = np.zeros(1 << n, dtype=np.complex128)
     want[0] = 1
-    W.run_on_cpu(gates, want, port)
+    R.run_on_cpu(gates, want, port)
     assert np.max(np.abs(s.get_vector() - want)) <= AMP_TOL
 
 
@@ -126,7 +127,7 @@ def test_forced_fusion_sizes_against_oracle(port, k):
     circ.update_quantum_state(s, mode="staged_fused")
     want = np.zeros(1 << n, dtype=np.complex128)
     want[0] = 1
-    W.run_on_cpu(gates, want, port)
+    R.run_on_cpu(gates, want, port)
     assert np.max(np.abs(s.get_vector() - want)) <= AMP_TOL
     kk, count, passes, est = circ.fusion_info()
     assert kk == k and count == len(circ.fuse(k)) and passes >= 1
@@ -158,7 +159,7 @@ def test_autotuner_records_estimates(port):
     assert est[k] == min(est)
     want = np.zeros(1 << n, dtype=np.complex128)
     want[0] = 1
-    W.run_on_cpu(gates, want, port)
+    R.run_on_cpu(gates, want, port)
     assert np.max(np.abs(s.get_vector() - want)) <= AMP_TOL
     # a second run reuses the schedule
     circ.update_quantum_state(s, mode="staged_fused")

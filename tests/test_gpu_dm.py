@@ -7,6 +7,7 @@ import pytest
 from conftest import AMP_TOL, EV_TOL, GOLDEN, random_density_matrix, random_unitary
 from qulacs_b200 import DensityMatrix, QuantumState, gate as G
 from qulacs_b200 import workloads as W
+from oracle import replay as R
 
 pytestmark = pytest.mark.gpu
 
@@ -92,7 +93,7 @@ def test_noisy_circuits_every_mode_against_oracle(port, mode, n):
     gates = W.noisy_circuit(W.hea_circuit(n, 2, 50 + n), 1e-3) + W.noisy_circuit(W.u3_cz_circuit(n, 2, 60 + n), 0.02)
     rho0 = random_density_matrix(n, rng)
     want = rho0.copy()
-    W.run_on_cpu_dm(gates, want, port)
+    R.run_on_cpu_dm(gates, want, port)
     d = dev(rho0)
     W.to_circuit(gates, n).update_quantum_state(d, mode=mode)
     assert np.max(np.abs(d.get_matrix() - want)) <= AMP_TOL

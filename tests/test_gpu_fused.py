@@ -8,6 +8,7 @@ import pytest
 
 from qulacs_b200 import QuantumState, QuantumStateC64
 from qulacs_b200 import workloads as W
+from oracle import replay as R
 
 pytestmark = pytest.mark.gpu
 
@@ -26,7 +27,7 @@ def test_fused_against_oracle(port, n, kind):
     circ = W.to_circuit(gates, n)
     want = np.zeros(1 << n, dtype=np.complex128)
     want[0] = 1
-    W.run_on_cpu(gates, want, port)
+    R.run_on_cpu(gates, want, port)
     ref = QuantumState(n)
     ref.load(want)
     s = QuantumStateC64(n)

@@ -7,6 +7,7 @@ from conftest import AMP_TOL, BOUNDARY_EPS, random_state
 from oracle.oracle import noise_simulator_execute
 from qulacs_b200 import NoiseSimulator, QuantumState
 from qulacs_b200 import workloads as W
+from oracle import replay as R
 
 pytestmark = pytest.mark.gpu
 
@@ -16,7 +17,7 @@ def test_samples_match_oracle(port, n, p, shots, seed):
     gates = W.noisy_circuit(W.hea_circuit(n, 3, seed) + W.u3_cz_circuit(n, 1, seed + 1), p)
     circ = W.to_circuit(gates, n)
     got = NoiseSimulator(circ, seed=seed).execute(shots)
-    want, near, _ = noise_simulator_execute(gates, n, shots, seed, port, lambda g, s: W.run_on_cpu([g], s, port),
+    want, near, _ = noise_simulator_execute(gates, n, shots, seed, port, lambda g, s: R.run_on_cpu([g], s, port),
                                             eps=BOUNDARY_EPS)
     assert got.shape == want.shape
     assert np.all((got == want) | near)
@@ -32,7 +33,7 @@ def test_trajectory_states_and_initial_state(port):
     init.load(psi0)
     sim = NoiseSimulator(circ, init, seed=seed)
     res = sim.execute_and_get_result(shots)
-    _, _, requests = noise_simulator_execute(gates, n, shots, seed, port, lambda g, s: W.run_on_cpu([g], s, port),
+    _, _, requests = noise_simulator_execute(gates, n, shots, seed, port, lambda g, s: R.run_on_cpu([g], s, port),
                                              init=psi0)
     assert [c for _, c in res.result] == [m for _, m in requests]
     from oracle.oracle import depolarizing_channel, _pauli
@@ -47,7 +48,7 @@ def test_trajectory_states_and_initial_state(port):
                 if any(ids):
                     port.multi_qubit_dense_matrix_gate(list(g[1]), _pauli(ids), want)
             else:
-                W.run_on_cpu([g], want, port)
+                R.run_on_cpu([g], want, port)
         assert np.max(np.abs(state.get_vector() - want)) <= AMP_TOL
     # the all-identity trajectory is the noise-free circuit
     clean = QuantumState(n)

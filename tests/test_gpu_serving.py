@@ -6,6 +6,7 @@ import pytest
 from conftest import EV_TOL
 from qulacs_b200 import workloads as W
 from qulacs_b200.serving import ServingLoop, make_request_mix, run_alone
+from oracle import replay as R
 
 pytestmark = pytest.mark.gpu
 
@@ -37,6 +38,6 @@ def test_mix_equals_alone(port, precision):
             continue
         psi = np.zeros(1 << r.n, dtype=np.complex128)
         psi[0] = 1
-        W.run_on_cpu(r.gates, psi, port)
+        R.run_on_cpu(r.gates, psi, port)
         want = sum(c * port.expectation_value(tl, ids, psi) for c, tl, ids in r.terms)
         assert abs(r.result - want) <= (EV_TOL if precision == "c128" else 1e-4)

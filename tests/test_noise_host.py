@@ -8,6 +8,7 @@ import pytest
 from oracle.oracle import depolarizing_channel, noise_simulator_execute
 from qulacs_b200 import NoiseSimulator
 from qulacs_b200 import workloads as W
+from oracle import replay as R
 
 
 def test_kraus_order_follows_the_reference():
@@ -25,6 +26,6 @@ def test_trajectories_match_oracle(port, n, p, shots, seed):
     circ = W.to_circuit(gates, n)
     got = NoiseSimulator(circ, seed=seed).trajectories(shots)
     _, _, requests = noise_simulator_execute(gates, n, shots, seed, port,
-                                             lambda g, s: W.run_on_cpu([g], s, port))
+                                             lambda g, s: R.run_on_cpu([g], s, port))
     assert [c for _, c in requests] == got.tolist()
     assert int(got.sum()) == shots
