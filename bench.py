@@ -641,6 +641,8 @@ def main():
         e2e_ms = float(t.item())
     h2d = N_TERMS * (8 + 8 + 4) + N_SHOTS * 8 + len(gates) * 64
     d2h = N_TERMS * 8 + N_SHOTS * 8
+    # draws of the last e2e sampling call within 1e-12 of a cumulative boundary (outside the timed region)
+    boundary_draws = state.sampling_boundary_draws(N_SHOTS, SHOT_SEED + e2e_steps - 1, 1e-12)
 
     # the other complex128 execution modes on the same circuit and state (outside the timed region)
     modes_ms = {mode: ms}
@@ -713,7 +715,10 @@ def main():
             "kernels": kernels,
             "e2e": {"value": world * len(gates) / (e2e_ms / 1e3), "unit": "gates/s", "ms_per_step": e2e_ms,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "includes": "set_zero_state + circuit + <H> (256 strings) + 1024-shot sampling"},
+                    "includes": "set_zero_state + circuit + <H> (256 strings) + 1024-shot sampling",
+                    "sampling_boundary_draws": boundary_draws,
+                    "sampling_boundary_note": "of the 1024 draws, those within 1e-12 of a cumulative boundary "
+                                              "of the FP64 prefix (the draws parity with the reference excepts)"},
             "energy": energy,
             "gpu_launches": int(launches),
             "clocks": clk.summary(),

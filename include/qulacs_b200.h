@@ -278,8 +278,16 @@ QS_API int qs_expectation_value_pauli_batch(const QS_ITYPE* x_masks, const QS_IT
  */
 QS_API int qs_state_sampling_with_uniforms(const void* state, QS_ITYPE dim, const double* uniforms,
     QS_UINT sampling_count, QS_ITYPE* out, void* stream);
-/* Same, drawing the uniforms as the reference's Random does (cppsim/utility.hpp:54-80):
- * std::mt19937_64 seeded with `random_seed`, std::uniform_real_distribution<double>(0, 1). */
+/* qs_state_sampling_with_uniforms that also reports which draws lie within `eps` of a cumulative
+ * boundary of the FP64 prefix sums (near_boundary[i] = 1; may be NULL) and how many (near_count; may
+ * be NULL).  Such a draw is the one whose index may differ from the reference's serial prefix sum
+ * (cppsim/state.hpp:909-929) by rounding; parity with the reference excepts exactly these draws. */
+QS_API int qs_state_sampling_with_uniforms_flagged(const void* state, QS_ITYPE dim, const double* uniforms,
+    QS_UINT sampling_count, double eps, QS_ITYPE* out, unsigned char* near_boundary, QS_UINT* near_count,
+    void* stream);
+/* qs_state_sampling_with_uniforms drawing the uniforms as the reference's Random does
+ * (cppsim/utility.hpp:54-80): std::mt19937_64 seeded with `random_seed`,
+ * std::uniform_real_distribution<double>(0, 1). */
 QS_API int qs_state_sampling(const void* state, QS_ITYPE dim, QS_UINT sampling_count,
     QS_UINT random_seed, QS_ITYPE* out, void* stream);
 /*
@@ -458,6 +466,13 @@ QS_API int qs_circuit_update_density_matrix(
  * Synchronises `stream`. */
 QS_API int qs_batch_update_quantum_states(const qs_circuit_t* circuits, void* const* states, QS_UINT count,
     void* stream);
+/* Failure-path check of the batch executor (no reference counterpart; the reference's GPU backend
+ * exits the process on a device error, gpusim/util.cuh:28-42): runs `circuit` on `state` as a
+ * one-circuit batch whose last pass waits on a completion counter that never completes, with the
+ * dependency wait bounded by `wait_limit_us` (1 us .. 2 s; ordinary batches use 2 s).  Returns
+ * QS_ERR_TIMEOUT, leaves the CUDA context usable, and leaves `state` with every pass but the last
+ * applied.  Synchronises `stream`. */
+QS_API int qs_debug_batch_wait_expiry(qs_circuit_t circuit, void* state, QS_UINT wait_limit_us, void* stream);
 /* The same on the fused complex64 tensor-core path: states_c64[i] holds circuits[i]'s 2^n complex64
  * amplitudes (n >= 10).  Missing plans are built on host threads in parallel; the circuits run
  * concurrently on streams forked from `stream` and joined back.  Synchronises `stream`. */

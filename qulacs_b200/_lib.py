@@ -95,6 +95,7 @@ SIGNATURES = {
     "qs_expectation_value_pauli_batch": [P, P, P, U, P, IT, P, P],
     "qs_state_sampling_with_uniforms": [P, IT, P, U, P, P],
     "qs_state_sampling": [P, IT, U, U, P, P],
+    "qs_state_sampling_with_uniforms_flagged": [P, IT, P, U, D, P, P, P, P],
     "qs_reference_uniforms": [U, U, P],
     "qs_state_sampling_with_uniforms_noalloc": [P, IT, P, U, P, P],
     "qs_dm_allocate": [IT, C.POINTER(P)],
@@ -146,6 +147,7 @@ SIGNATURES = {
     "qs_circuit_fusion_info": [P, C.POINTER(I), C.POINTER(U), C.POINTER(U), P],
     "qs_circuit_update_quantum_state_fused_c64": [P, P, IT, P],
     "qs_batch_update_quantum_states": [P, P, U, P],
+    "qs_debug_batch_wait_expiry": [P, P, U, P],
     "qs_batch_expectation_values": [P, P, U, P, P, P, P, P, P],
     "qs_batch_expectation_values_c64": [P, P, U, P, P, P, P, P, P],
     "qs_state_norm_squared_c64": [P, IT, P, P],

@@ -1037,7 +1037,8 @@ extern "C" QS_API int qs_circuit_set_fusion(qs_circuit_t circuit, int k) {
 // pass 1, and so on.  A CTA takes the next item with an atomic counter and, for pass p > 0, waits
 // until all tiles of pass p - 1 of the same circuit are done (acquire load of a per-pass counter).
 // Dependencies only point to earlier queue items, which resident CTAs already hold, so the wait
-// always ends; it is still bounded (about 2 s) and reports QS_ERR_TIMEOUT through an error flag.
+// always ends; it is still bounded (a %globaltimer deadline, 2 s) and reports QS_ERR_TIMEOUT through an
+// error flag, after which the CTA leaves without touching the item.
 namespace qs {
 
 struct BatchRec {
@@ -1048,7 +1049,13 @@ struct BatchRec {
     int dep;       // record of the previous pass of the same circuit, -1 for pass 0
 };
 
-constexpr unsigned kBatchSpinLimit = 1u << 25;  // x ~64 ns sleeps
+constexpr unsigned long long kBatchWaitNs = 2000000000ULL;  // dependency wait limit of a batch launch
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
 
 __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
     unsigned v;
@@ -1057,7 +1064,7 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
 }
 
 __global__ void __launch_bounds__(kStThreads, 3) k_batch_staged(const BatchRec* __restrict__ recs, int nrec,
-    ITYPE total, unsigned long long* head, unsigned* done, int* err) {
+    ITYPE total, unsigned long long* head, unsigned* done, int* err, unsigned long long wait_ns) {
     __shared__ double2 tile[1 << kBatchTileBits];
     __shared__ ITYPE hi_off[1 << (kBatchTileBits - 7)];
     __shared__ ITYPE s_item;
@@ -1080,9 +1087,9 @@ __global__ void __launch_bounds__(kStThreads, 3) k_batch_staged(const BatchRec* 
                 const int dep = recs[lo].dep;
                 if (dep >= 0) {
                     const unsigned need = (unsigned)recs[dep].tiles;
-                    unsigned it = 0;
+                    const unsigned long long t0 = global_ns();
                     while (ld_acquire_u32(done + dep) < need) {
-                        if (++it > kBatchSpinLimit) {
+                        if (global_ns() - t0 > wait_ns) {
                             atomicExch(err, 1);
                             s_abort = 1;
                             break;
@@ -1120,7 +1127,10 @@ static int ensure_batch_plan(Circuit& c, ITYPE dim) {
     return build_plan(c.bgates, c.n, dim, &c.bplan, kBatchTileBits);
 }
 
-int batch_update(Circuit* const* cs, void* const* states, UINT count, cudaStream_t st) {
+// `wait_ns`: the dependency wait limit; `self_dep` >= 0 makes that work record depend on itself (a
+// counter nothing can complete), which only the wait-expiry check below uses.
+int batch_update(Circuit* const* cs, void* const* states, UINT count, cudaStream_t st,
+    unsigned long long wait_ns = kBatchWaitNs, int self_dep = -1) {
     if (count == 0) return QS_OK;
     for (UINT i = 0; i < count; ++i)
         if (cs[i]->n < kPhaseBits) return set_error(QS_ERR_NOT_SUPPORTED, "batch: circuits need at least 4 qubits");
@@ -1185,6 +1195,10 @@ int batch_update(Circuit* const* cs, void* const* states, UINT count, cudaStream
             recs.push_back(r);
         }
     if (recs.empty()) return QS_OK;
+    if (self_dep >= 0) {
+        if (self_dep >= (int)recs.size()) return set_error(QS_ERR_INVALID_ARGUMENT, "batch: no such work record");
+        recs[self_dep].dep = self_dep;
+    }
     const size_t brec = sizeof(BatchRec) * recs.size();
     const size_t bdone = sizeof(unsigned) * recs.size();
     void* buf = nullptr;
@@ -1199,7 +1213,7 @@ int batch_update(Circuit* const* cs, void* const* states, UINT count, cudaStream
     QS_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_staged, kStThreads, 0));
     const ITYPE resident = (ITYPE)std::max(1, per_sm) * sm_count();
     const unsigned grid = (unsigned)std::min<ITYPE>(resident, total);
-    k_batch_staged<<<grid, kStThreads, 0, st>>>(drec, (int)recs.size(), total, dhead, ddone, derr);
+    k_batch_staged<<<grid, kStThreads, 0, st>>>(drec, (int)recs.size(), total, dhead, ddone, derr, wait_ns);
     QS_TRY(check_launch("k_batch_staged"));
     int err = 0;
     QS_CUDA_CHECK(cudaMemcpyAsync(&err, derr, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -1219,4 +1233,29 @@ extern "C" QS_API int qs_batch_update_quantum_states(const qs_circuit_t* circuit
         if (!cs[i] || !states[i]) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "null circuit or state");
     }
     return qs::batch_update(cs.data(), states, count, (cudaStream_t)stream);
+}
+
+// Failure-path check of the batch executor's bounded dependency wait: runs `circuit` on `state` as a
+// one-circuit batch whose last pass waits on its own completion counter, which never completes, with
+// a wait limit of `wait_limit_us`.  Every CTA that takes a tile of that pass gives up after the limit,
+// sets the error flag and leaves, so the call returns QS_ERR_TIMEOUT and the context stays usable; the
+// state is left with all passes but the last applied.
+extern "C" QS_API int qs_debug_batch_wait_expiry(qs_circuit_t circuit, void* state, QS_UINT wait_limit_us,
+    void* stream) {
+    qs::Circuit* c = reinterpret_cast<qs::Circuit*>(circuit);
+    if (!c || !state) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "null circuit or state");
+    if (wait_limit_us == 0 || wait_limit_us > 2000000u)
+        return qs::set_error(QS_ERR_INVALID_ARGUMENT, "wait limit must be 1 us .. 2 s");
+    qs::Circuit* cs[1] = {c};
+    void* ss[1] = {state};
+    // the last record of a one-circuit batch is its last pass
+    UINT passes = 0;
+    {
+        qs::HostPlan H;
+        std::vector<qs::GateRec> fg = qs::fuse_gates(c->gates, qs::batch_block_size(*c));
+        qs::make_host_plan(fg, c->n, &H, qs::kBatchTileBits);
+        passes = (UINT)H.passes.size();
+    }
+    if (passes == 0) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "circuit has no passes");
+    return qs::batch_update(cs, ss, 1, (cudaStream_t)stream, 1000ULL * wait_limit_us, (int)passes - 1);
 }

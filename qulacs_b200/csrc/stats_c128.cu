@@ -3,6 +3,7 @@
 // one partial per CTA written to scratch, then one CTA folds the partials in index order (no
 // floating-point atomics).
 #include <algorithm>
+#include <cstring>
 #include <mutex>
 #include <random>
 #include <vector>
@@ -375,20 +376,29 @@ __global__ void __launch_bounds__(1024) k_scan_sums(const double* __restrict__ s
     }
 }
 
-// One warp per shot.
+// One warp per shot.  With `near` set, near[shot] = 1 when the draw lies within `eps` of one of the two
+// cumulative sums that bracket it (prefix before the sampled index, prefix through it): a draw whose
+// index could differ under another summation order of the same probabilities.
 template <class T>
 __global__ void k_sample(const T* __restrict__ s, ITYPE dim, ITYPE diag_stride, const double* __restrict__ incl,
-    ITYPE nchunks, const double* __restrict__ uniforms, UINT count, ITYPE* __restrict__ out) {
+    ITYPE nchunks, const double* __restrict__ uniforms, UINT count, ITYPE* __restrict__ out, double eps = 0.,
+    unsigned char* __restrict__ near = nullptr) {
     const int lane = threadIdx.x & 31;
     const UINT shot = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (shot >= count) return;
     const double r = uniforms[shot];
     if (!(r > 0.)) {  // lower_bound hits stacked_prob[0] = 0 -> index -1
-        if (lane == 0) out[shot] = ~0ULL;
+        if (lane == 0) {
+            out[shot] = ~0ULL;
+            if (near) near[shot] = r >= -eps;
+        }
         return;
     }
     if (r > incl[nchunks - 1]) {  // past the total -> index dim
-        if (lane == 0) out[shot] = dim;
+        if (lane == 0) {
+            out[shot] = dim;
+            if (near) near[shot] = r - incl[nchunks - 1] <= eps;
+        }
         return;
     }
     // first chunk c with incl[c] >= r
@@ -416,10 +426,11 @@ __global__ void k_sample(const T* __restrict__ s, ITYPE dim, ITYPE diag_stride, 
     const unsigned ball = __ballot_sync(0xffffffffu, end >= r);
     const int owner = ball ? __ffs(ball) - 1 : 31;
     if (lane == owner) {
-        double run = start;
+        double run = start, prev = start;
         ITYPE idx = c0 + kChunk / 32 - 1;
         for (int j = 0; j < kChunk / 32; ++j) {
             if (c0 + j >= dim) break;
+            prev = run;
             run += prob_at(s, c0 + j, diag_stride);
             if (run >= r) {
                 idx = c0 + j;
@@ -427,21 +438,24 @@ __global__ void k_sample(const T* __restrict__ s, ITYPE dim, ITYPE diag_stride, 
             }
         }
         out[shot] = idx < dim ? idx : dim - 1;
+        if (near) near[shot] = (r - prev <= eps) || (run - r <= eps);
     }
 }
 
+// near_host (may be null): per draw, 1 when it lies within eps of a bracketing cumulative sum.
 template <class T>
 int sample_with_uniforms_t(const T* s, ITYPE dim, ITYPE diag_stride, const double* uniforms, UINT count,
-    ITYPE* out, cudaStream_t st) {
+    ITYPE* out, cudaStream_t st, double eps = 0., unsigned char* near_host = nullptr) {
     if (count == 0) return QS_OK;
     const ITYPE nchunks = (dim + kChunk - 1) / kChunk;
-    const size_t bytes = sizeof(double) * (2 * nchunks + count) + sizeof(ITYPE) * count + 1024;
+    const size_t bytes = sizeof(double) * (2 * nchunks + count) + sizeof(ITYPE) * count + count + 1024;
     void* buf;
     QS_TRY(scratch(st, bytes, &buf));
     double* sums = (double*)buf;
     double* incl = sums + nchunks;
     double* du = incl + nchunks;
     ITYPE* dout = (ITYPE*)(du + count);
+    unsigned char* dnear = near_host ? (unsigned char*)(dout + count) : nullptr;
     QS_CUDA_CHECK(cudaMemcpyAsync(du, uniforms, sizeof(double) * count, cudaMemcpyHostToDevice, st));
     k_chunk_sums<T><<<(unsigned)nchunks, 256, 0, st>>>(s, dim, diag_stride, sums);
     QS_TRY(check_launch("k_chunk_sums"));
@@ -449,9 +463,10 @@ int sample_with_uniforms_t(const T* s, ITYPE dim, ITYPE diag_stride, const doubl
     QS_TRY(check_launch("k_scan_sums"));
     const unsigned threads = 256;
     const unsigned blocks = (unsigned)(((ITYPE)count * 32 + threads - 1) / threads);
-    k_sample<T><<<blocks, threads, 0, st>>>(s, dim, diag_stride, incl, nchunks, du, count, dout);
+    k_sample<T><<<blocks, threads, 0, st>>>(s, dim, diag_stride, incl, nchunks, du, count, dout, eps, dnear);
     QS_TRY(check_launch("k_sample"));
     QS_CUDA_CHECK(cudaMemcpyAsync(out, dout, sizeof(ITYPE) * count, cudaMemcpyDeviceToHost, st));
+    if (dnear) QS_CUDA_CHECK(cudaMemcpyAsync(near_host, dnear, count, cudaMemcpyDeviceToHost, st));
     QS_CUDA_CHECK(cudaStreamSynchronize(st));
     return QS_OK;
 }
@@ -665,6 +680,23 @@ QS_API int qs_state_sampling_with_uniforms(const void* state, QS_ITYPE dim, cons
     UINT n;
     QS_TRY(check_dim(dim, &n));
     return sample_with_uniforms((const double2*)state, dim, 0, uniforms, count, out, (cudaStream_t)stream);
+}
+
+// qs_state_sampling_with_uniforms that also reports, per draw, whether it lies within `eps` of a
+// cumulative boundary (near_boundary[i] in {0, 1}, may be NULL) and how many do (near_count, may be NULL).
+QS_API int qs_state_sampling_with_uniforms_flagged(const void* state, QS_ITYPE dim, const double* uniforms,
+    QS_UINT count, double eps, QS_ITYPE* out, unsigned char* near_boundary, QS_UINT* near_count, void* stream) {
+    UINT n;
+    QS_TRY(check_dim(dim, &n));
+    if (!(eps >= 0.)) return set_error(QS_ERR_INVALID_ARGUMENT, "sampling: eps must be >= 0");
+    std::vector<unsigned char> flags(count);
+    QS_TRY(sample_with_uniforms_t<double2>((const double2*)state, dim, 0, uniforms, count, out, (cudaStream_t)stream,
+        eps, flags.data()));
+    UINT c = 0;
+    for (UINT i = 0; i < count; ++i) c += flags[i] ? 1 : 0;
+    if (near_boundary && count) memcpy(near_boundary, flags.data(), count);
+    if (near_count) *near_count = c;
+    return QS_OK;
 }
 
 QS_API int qs_state_sampling(const void* state, QS_ITYPE dim, QS_UINT count, QS_UINT seed, QS_ITYPE* out,

@@ -231,6 +231,25 @@ class QuantumState:
         call("qs_state_sampling_with_uniforms", self._ptr, self.dim, _ptr(u), u.size, _ptr(out), self.stream)
         return out
 
+    def sampling_with_uniforms_flagged(self, uniforms, eps: float = 1e-12):
+        """Indices for the supplied uniforms and, per draw, whether it lies within `eps` of a cumulative
+        boundary of the FP64 prefix sums (the draws whose index may differ from the reference's serial
+        prefix by rounding).  Returns (indices, flags)."""
+        u = np.ascontiguousarray(np.asarray(uniforms, dtype=np.float64))
+        out = np.empty(u.size, dtype=np.uint64)
+        flags = np.zeros(u.size, dtype=np.uint8)
+        cnt = C.c_uint()
+        call("qs_state_sampling_with_uniforms_flagged", self._ptr, self.dim, _ptr(u), u.size, float(eps), _ptr(out),
+             _ptr(flags), C.byref(cnt), self.stream)
+        return out, flags.astype(bool)
+
+    def sampling_boundary_draws(self, sampling_count: int, random_seed: int, eps: float = 1e-12) -> int:
+        """How many of the draws `sampling(sampling_count, random_seed)` makes lie within `eps` of a
+        cumulative boundary."""
+        u = np.empty(int(sampling_count), dtype=np.float64)
+        call("qs_reference_uniforms", int(random_seed) & 0xFFFFFFFF, int(sampling_count), _ptr(u))
+        return int(self.sampling_with_uniforms_flagged(u, eps)[1].sum())
+
     def __del__(self):
         p = getattr(self, "_ptr", None)
         if p:

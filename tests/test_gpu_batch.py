@@ -105,3 +105,28 @@ def test_batch_repeats_a_circuit_and_reuses_plans(precision):
     again = BatchRunner(1 << 30, precision=precision).run(jobs)
     assert first[5] == first[1] and first[6] == first[3]
     assert np.array_equal(first, again)
+
+
+def test_dependency_wait_expires_and_context_stays_usable(port):
+    """The batch kernel's bounded dependency wait, made to run out: the last pass of a one-circuit batch
+    waits on its own completion counter (which nothing can complete) with a 1 ms limit.  The call must
+    return QS_ERR_TIMEOUT, not hang or fault; the passes before it are applied; and a normal batch on
+    the same context afterwards gives the oracle's state."""
+    from qulacs_b200._lib import load
+    lib = load()
+    n = 12
+    gates = W.hea_circuit(n, 8, seed=77)
+    circ = W.to_circuit(gates, n)
+    s = QuantumState(n)
+    rc = lib.qs_debug_batch_wait_expiry(circ._h, s.data_ptr(), 1000, None)
+    assert rc == 4, lib.qs_get_last_error()  # QS_ERR_TIMEOUT
+    assert b"dependency wait expired" in lib.qs_get_last_error()
+    # the context still works: the same circuit as a normal batch matches the oracle
+    psi = np.zeros(1 << n, dtype=np.complex128)
+    psi[0] = 1
+    R.run_on_cpu(gates, psi, port)
+    ok = QuantumState(n)
+    import ctypes as C
+    from qulacs_b200._lib import call
+    call("qs_batch_update_quantum_states", (C.c_void_p * 1)(circ._h), (C.c_void_p * 1)(ok.data_ptr()), 1, None)
+    assert np.max(np.abs(ok.get_vector() - psi)) <= 1e-12

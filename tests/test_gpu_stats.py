@@ -133,3 +133,25 @@ def test_seeded_sampling_matches_reference_rng(port):
     want_u = mt19937_64_uniforms(1234, 256)
     want = port.sampling_with_uniforms(a, want_u)
     assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("n", [6, 14])
+def test_sampling_reports_boundary_draws(port, n):
+    """The flagged sampler reports draws within eps of a cumulative boundary: uniforms planted ON the
+    prefix sums (and 1e-14 beside them) are all flagged, ordinary draws agree with the oracle wherever
+    neither side flags them, and the count equals the number of flags."""
+    rng = np.random.default_rng(40 + n)
+    a = random_state(n, rng)
+    p = a.real ** 2 + a.imag ** 2
+    stacked = np.cumsum(p)  # serial FP64 running sum, cppsim/state.hpp:917-922
+    k = rng.choice((1 << n) - 1, size=16, replace=False)
+    planted = np.concatenate([stacked[k], stacked[k] + 1e-14, stacked[k] - 1e-14])
+    u = np.concatenate([planted, rng.random(512)])
+    s = dev(a)
+    got, flags = s.sampling_with_uniforms_flagged(u, BOUNDARY_EPS)
+    assert flags[:planted.size].all()
+    want, near = port.sampling_with_uniforms(a, u, eps=BOUNDARY_EPS)
+    assert not ((got != want) & ~near & ~flags).any()
+    assert np.array_equal(got[~flags], s.sampling_with_uniforms(u)[~flags])
+    assert s.sampling_boundary_draws(256, 99) == int(
+        s.sampling_with_uniforms_flagged(mt19937_64_uniforms(99, 256))[1].sum())
