@@ -495,6 +495,9 @@ def main():
     ap.add_argument("--fusion-k", type=int, default=-1,
                     help="staged_fused block size (-1: autotuned; pin the autotuner's choice for profiler runs, "
                          "whose instrumented launches distort its timings)")
+    ap.add_argument("--specialize", type=int, default=-1, choices=[-1, 0, 1],
+                    help="specialised pass kernels for the staged modes: 1 on, 0 off (generic pass kernel), "
+                         "-1 by state size (default: on from 22 qubits)")
     ap.add_argument("--no-mode-compare", action="store_true",
                     help="skip timing the other complex128 execution modes beside the headline one")
     ap.add_argument("--qubits", type=int, default=N_QUBITS)
@@ -570,6 +573,7 @@ def main():
     circ = W.to_circuit(gates, n)
     if args.fusion_k >= 0:
         circ.set_fusion(args.fusion_k)
+    circ.set_specialized(args.specialize)
     obs = W.to_observable(terms, n)
     state = Q.QuantumState(n)
     mode = args.mode
@@ -604,7 +608,9 @@ def main():
     fusion = None
     if mode == "staged_fused":
         fk, fcount, passes, fest = circ.fusion_info()
-        fusion = {"k": fk, "gates_after_fusion": fcount, "autotuner_estimates_ms": fest}
+        _, spec, compile_ms = circ.specialized_info()
+        fusion = {"k": fk, "gates_after_fusion": fcount, "autotuner_estimates_ms": fest,
+                  "specialized_passes": spec, "specialize_compile_ms": compile_ms}
     elif mode == "staged":
         passes = circ.pass_count()
     else:
@@ -703,7 +709,9 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                          "frac": achieved / hbm_peak, "peak_kind": peak_kind,
                          "traffic": (STAGED_TRAFFIC_PER_AMP * (1 << n)) if staged_kernel else None,
-                         "kernel": ("k_staged_pass: one HBM pass (2 x 16 x 2^n B) applying ~"
+                         "kernel": (("k_pass_spec (specialised" if (fusion or {}).get("specialized_passes") else
+                                     "k_staged_pass (generic") +
+                                    " pass kernel): one HBM pass (2 x 16 x 2^n B) applying ~"
                                     f"{len(gates) / max(1, passes):.0f} circuit gates" if staged_kernel
                                     else "gate kernels: one HBM pass (2 x 16 x 2^n B) per gate"),
                          "traffic_note": "scaled from the 26-qubit ncu capture by amplitudes" if staged_kernel else None},

@@ -439,6 +439,19 @@ QS_API int qs_circuit_gate_matrix(qs_circuit_t circuit, QS_UINT index, QS_UINT* 
 /* QS_EXEC_STAGED_FUSED: force the block size k (0..6; 0 = no fusion), or -1 (default) to let the
  * autotuner choose k in 0..4 on the next run by timing each candidate's staged passes. */
 QS_API int qs_circuit_set_fusion(qs_circuit_t circuit, int k);
+/* Specialised pass kernels (no reference counterpart): the single-state staged modes can run each HBM
+ * pass as its own kernel, generated from the pass's schedule with every tile qubit, phase bit and gate
+ * matrix entry a compile-time constant, compiled for sm_100a with NVRTC when the plan is built and
+ * cached for the process.  mode 1 = always, 0 = never (the generic pass kernel), -1 = for states of at
+ * least 2^22 amplitudes (default).  Changing the mode drops the circuit's cached schedules. */
+QS_API int qs_circuit_set_specialized(qs_circuit_t circuit, int mode);
+/* Whether the last-built QS_EXEC_STAGED / QS_EXEC_STAGED_FUSED schedules run specialised kernels, and the
+ * wall time of compiling them (ms; 0 when every kernel came from the cache; may be NULL). */
+QS_API int qs_circuit_specialized_info(qs_circuit_t circuit, int* staged, int* staged_fused, double* compile_ms);
+/* CUDA C source of the specialised kernel of pass `pass` of the QS_EXEC_STAGED schedule at dim
+ * amplitudes (host only; dim = 2^qubit_count >= 2^7).  buf == NULL: *size receives length + 1. */
+QS_API int qs_circuit_specialized_source(qs_circuit_t circuit, QS_ITYPE dim, QS_UINT pass, char* buf,
+    QS_ITYPE* size);
 /* The schedule last built for QS_EXEC_STAGED_FUSED: block size (-1 before the first run), gate count
  * after fusion, HBM passes, and the autotuner's estimate per k = 0..4 in ms (estimates_ms[5], may be
  * NULL; < 0 where not tried). */

@@ -27,6 +27,8 @@ def run_on_cpu(gates, state: np.ndarray, sim) -> None:
             sim.CNOT_gate(g[1], g[2], state)
         elif k == "CZ":
             sim.CZ_gate(g[1], g[2], state)
+        elif k == "SWAP":
+            sim.SWAP_gate(g[1], g[2], state)
         elif k == "DENSE":
             sim.multi_qubit_dense_matrix_gate(list(g[1]), g[2], state)
         else:

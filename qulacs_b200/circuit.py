@@ -25,6 +25,7 @@ class QuantumCircuit:
         self._h = h.value
         self.gate_list = []
         self._fusion_k = None
+        self._specialize = None
 
     def get_qubit_count(self) -> int:
         return self.qubit_count
@@ -48,6 +49,8 @@ class QuantumCircuit:
             g._add_to(self._h)
         if self._fusion_k is not None:
             call("qs_circuit_set_fusion", self._h, self._fusion_k)
+        if self._specialize is not None:
+            call("qs_circuit_set_specialized", self._h, self._specialize)
 
     def add_gate(self, gate: G.QuantumGateBase, position: int | None = None) -> None:
         """Append (or insert before ``position``) a copy of ``gate`` (cppsim circuit.cpp:133-165)."""
@@ -207,6 +210,27 @@ class QuantumCircuit:
         """Block size of mode="staged_fused": 0..6, or -1 to let the autotuner choose (default)."""
         call("qs_circuit_set_fusion", self._h, int(k))
         self._fusion_k = int(k)
+
+    def set_specialized(self, mode: int) -> None:
+        """Specialised pass kernels for the "staged" / "staged_fused" modes (each HBM pass compiled with
+        its schedule and gate matrices as constants): 1 always, 0 never, -1 for states of at least 2^22
+        amplitudes (default)."""
+        call("qs_circuit_set_specialized", self._h, int(mode))
+        self._specialize = int(mode)
+
+    def specialized_info(self):
+        """(staged schedule specialised, staged_fused schedule specialised, compile ms)."""
+        a, b, ms = C.c_int(), C.c_int(), C.c_double()
+        call("qs_circuit_specialized_info", self._h, C.byref(a), C.byref(b), C.byref(ms))
+        return bool(a.value), bool(b.value), ms.value
+
+    def specialized_source(self, pass_index: int) -> str:
+        """CUDA C of the specialised kernel of one pass of the "staged" schedule (host only)."""
+        size = C.c_ulonglong(0)
+        call("qs_circuit_specialized_source", self._h, 1 << self.qubit_count, int(pass_index), None, C.byref(size))
+        buf = C.create_string_buffer(size.value)
+        call("qs_circuit_specialized_source", self._h, 1 << self.qubit_count, int(pass_index), buf, C.byref(size))
+        return buf.value.decode()
 
     def fusion_info(self):
         """(k, gates after fusion, HBM passes, autotuner estimates in ms for k = 0..4) of the last

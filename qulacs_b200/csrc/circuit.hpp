@@ -43,6 +43,7 @@ struct Circuit {
     std::vector<GateRec> fgates;
     std::shared_ptr<StagedPlan> fplan;
     std::vector<double> tune_ms;    // autotuner estimate per candidate block size (ms; < 0: not tried)
+    int specialize = -1;            // single-state passes as specialised kernels: 1 on, 0 off, -1 by state size
     // the circuit acting on a density matrix seen as a 2n-qubit vector (circuit.cpp), for the staged
     // executors of qs_circuit_update_density_matrix
     std::shared_ptr<Circuit> dm_vec;

@@ -13,6 +13,7 @@
 // Pauli strings, multi-qubit diagonals) run between passes with the gate-by-gate kernels.
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <complex>
 #include <cstring>
@@ -22,29 +23,10 @@
 
 #include "circuit.hpp"
 #include "qs_internal.cuh"
+#include "staged.hpp"
 
 namespace qs {
 
-constexpr int kLowFixed = 4;        // qubits 0..3 always belong to a tile
-constexpr int kTileBits = 12;       // pass kernel: 2^12 amplitudes = 64 KiB of shared memory per CTA
-constexpr int kBatchTileBits = 11;  // multi-circuit kernel: 2^11 amplitudes = 32 KiB (its persistent loop
-                                    // spills twice as much with the 12-bit tile code)
-constexpr int kStThreads = 128;     // 16 (m = 11) or 32 (m = 12) amplitudes per thread; 1 or 2 cosets per phase
-constexpr int kPhaseBits = 4;       // 16 amplitudes in registers per thread
-
-// ST_CSEL1, ST_D1_IN and ST_D1_OUT are a one-qubit dense gate with a CNOT folded in (see absorb_cnots).
-enum StKind : uint8_t {
-    ST_DENSE1 = 0, ST_DIAG1, ST_RX, ST_RY, ST_CNOT, ST_CZ, ST_SWAP, ST_DENSE2, ST_CSEL1, ST_D1_IN, ST_D1_OUT
-};
-
-struct StOp {
-    uint8_t kind, a, b, pad;  // a, b: register-bit indices 0..3 within the phase; pad: dispatch code
-    uint32_t param;           // index into the parameter pool (double2)
-};
-struct StPhase {
-    uint8_t bits[4];  // tile-local bit positions, ascending
-    uint32_t op_begin, op_count;
-};
 struct StPassArgs {
     int m;                 // tile bits (<= kTileBits)
     int nphases;
@@ -519,6 +501,8 @@ struct DevPass {
     bool folds;  // the pass has CNOT-folded ops
     int gate;
     StPassArgs args;
+    size_t phase_begin = 0;  // the pass's phases in StagedPlan::phases
+    void* spec = nullptr;    // specialised kernel of this pass (pass_codegen.cpp), if compiled
 };
 
 static void launch_pass(double2* state, const DevPass& d, ITYPE tiles, cudaStream_t st) {
@@ -531,6 +515,12 @@ struct StagedPlan {
     ITYPE dim = 0;
     std::vector<DevPass> passes;
     void* dev = nullptr;  // phases | ops | pool
+    // host copies of the schedule (for specialised pass kernels)
+    std::vector<StPhase> phases;
+    std::vector<StOp> ops;
+    std::vector<double2> pool;
+    bool specialized = false;  // every pass has its specialised kernel
+    double compile_ms = 0.;    // wall time of compiling them
     ~StagedPlan() {
         if (dev) cudaFree(dev);
     }
@@ -800,6 +790,9 @@ static int build_plan(const std::vector<GateRec>& gates, UINT n, ITYPE dim, std:
 static int upload_plan(const HostPlan& H, ITYPE dim, std::shared_ptr<StagedPlan>* out) {
     auto P = std::make_shared<StagedPlan>();
     P->dim = dim;
+    P->phases = H.phases;
+    P->ops = H.ops;
+    P->pool = H.pool;
     const std::vector<PassPlan>& passes = H.passes;
     const std::vector<StPhase>& phases = H.phases;
     const std::vector<StOp>& ops = H.ops;
@@ -837,6 +830,7 @@ static int upload_plan(const HostPlan& H, ITYPE dim, std::shared_ptr<StagedPlan>
                 if (high_bits(phases[pp[i].phase_begin + pp[i].nphases - 1])) d.args.io |= 2;
             }
             d.args.phases = dph + pp[i].phase_begin;
+            d.phase_begin = pp[i].phase_begin;
             for (size_t ph = pp[i].phase_begin; ph < pp[i].phase_begin + pp[i].nphases; ++ph)
                 for (uint32_t o = phases[ph].op_begin; o < phases[ph].op_begin + phases[ph].op_count; ++o)
                     d.folds = d.folds || ops[o].kind == ST_CSEL1 || ops[o].kind == ST_D1_IN || ops[o].kind == ST_D1_OUT;
@@ -849,11 +843,6 @@ static int upload_plan(const HostPlan& H, ITYPE dim, std::shared_ptr<StagedPlan>
     return QS_OK;
 }
 
-static int ensure_plan(Circuit& c, ITYPE dim) {
-    if (!c.plan || c.plan->dim != dim) QS_TRY(build_plan(c.gates, c.n, dim, &c.plan));
-    return QS_OK;
-}
-
 static int run_plan(const std::vector<GateRec>& gates, const StagedPlan& P, void* state, ITYPE dim, cudaStream_t st) {
     QS_TRY(staged_allow_smem());
     for (const DevPass& d : P.passes) {
@@ -862,11 +851,74 @@ static int run_plan(const std::vector<GateRec>& gates, const StagedPlan& P, void
             continue;
         }
         const ITYPE tiles = dim >> d.args.m;
+        if (d.spec) {
+            QS_TRY(launch_specialized_pass(d.spec, (double2*)state, tiles, d.args.m, st));
+            continue;
+        }
         launch_pass((double2*)state, d, tiles, st);
         QS_TRY(check_launch("k_staged_pass"));
     }
     return QS_OK;
 }
+
+// The pass as the code generator sees it.
+static PassDesc pass_desc(const StagedPlan& P, const DevPass& d) {
+    PassDesc pd;
+    pd.m = d.args.m;
+    pd.io = d.args.io;
+    for (int j = 0; j < d.args.m; ++j) pd.q[j] = d.args.q[j];
+    pd.phases.assign(P.phases.begin() + d.phase_begin, P.phases.begin() + d.phase_begin + d.args.nphases);
+    pd.ops = P.ops.data();
+    pd.pool = P.pool.data();
+    return pd;
+}
+
+// Specialised kernels for every pass of a plan, compiled on host threads in parallel.  On failure the
+// plan keeps the generic pass kernel for every pass and the error is returned.
+static int specialize_plan(StagedPlan& P) {
+    if (P.specialized) return QS_OK;
+    std::vector<size_t> todo;
+    for (size_t i = 0; i < P.passes.size(); ++i)
+        if (!P.passes[i].single && P.passes[i].args.nphases > 0) todo.push_back(i);
+    std::vector<void*> handles(P.passes.size(), nullptr);
+    std::vector<int> rcs(P.passes.size(), QS_OK);
+    std::vector<std::string> errs(P.passes.size());
+    std::atomic<size_t> next{0};
+    const auto t0 = std::chrono::steady_clock::now();
+    const unsigned nt = std::max(1u, std::min<unsigned>((unsigned)todo.size(), std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    for (unsigned t = 0; t < nt; ++t)
+        pool.emplace_back([&] {
+            for (size_t j; (j = next.fetch_add(1)) < todo.size();) {
+                const size_t i = todo[j];
+                rcs[i] = specialized_pass_kernel(pass_desc(P, P.passes[i]), &handles[i], nullptr);
+                if (rcs[i] != QS_OK) errs[i] = qs_get_last_error();
+            }
+        });
+    for (std::thread& t : pool) t.join();
+    for (size_t i : todo)
+        if (rcs[i] != QS_OK) return set_error(rcs[i], errs[i]);
+    for (size_t i : todo) P.passes[i].spec = handles[i];
+    P.specialized = true;
+    P.compile_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return QS_OK;
+}
+
+// Whether a circuit's single-state passes use specialised kernels: forced on or off per circuit, else
+// for states of at least 2^kSpecializeMinQubits amplitudes (where a pass runs long enough to repay its
+// compile time).
+constexpr UINT kSpecializeMinQubits = 22;
+static bool want_specialized(const Circuit& c, ITYPE dim) {
+    if (c.specialize >= 0) return c.specialize == 1;
+    return dim >= (1ULL << kSpecializeMinQubits);
+}
+
+static int ensure_plan(Circuit& c, ITYPE dim) {
+    if (!c.plan || c.plan->dim != dim) QS_TRY(build_plan(c.gates, c.n, dim, &c.plan));
+    if (want_specialized(c, dim)) QS_TRY(specialize_plan(*c.plan));
+    return QS_OK;
+}
+
 
 int run_staged(Circuit& c, void* state, ITYPE dim, cudaStream_t st) {
     if (c.n < kPhaseBits) {  // too small for a 4-qubit register phase
@@ -940,7 +992,9 @@ static int ensure_fused_plan(Circuit& c, ITYPE dim, cudaStream_t st) {
     if (c.fusion_k >= 0) {
         c.fgates = fuse_gates(c.gates, c.fusion_k);
         c.fused_k = c.fusion_k;
-        return build_plan(c.fgates, c.n, dim, &c.fplan);
+        QS_TRY(build_plan(c.fgates, c.n, dim, &c.fplan));
+        if (want_specialized(c, dim)) QS_TRY(specialize_plan(*c.fplan));
+        return QS_OK;
     }
     c.tune_ms.assign(kTuneMaxK + 1, -1.);
     double best = 0.;
@@ -958,6 +1012,7 @@ static int ensure_fused_plan(Circuit& c, ITYPE dim, cudaStream_t st) {
             c.fused_k = k;
         }
     }
+    if (want_specialized(c, dim)) QS_TRY(specialize_plan(*c.fplan));
     return QS_OK;
 }
 
@@ -1013,6 +1068,77 @@ extern "C" QS_API int qs_circuit_fusion_info(qs_circuit_t circuit, int* k, QS_UI
     if (estimates_ms)
         for (int i = 0; i <= qs::kTuneMaxK; ++i)
             estimates_ms[i] = i < (int)c->tune_ms.size() ? c->tune_ms[i] : -1.;
+    return QS_OK;
+}
+
+// Specialised pass kernels for this circuit's single-state staged modes: 1 = always, 0 = never (the
+// generic pass kernel), -1 = for states of at least 2^22 amplitudes (default).
+extern "C" QS_API int qs_circuit_set_specialized(qs_circuit_t circuit, int mode) {
+    qs::Circuit* c = reinterpret_cast<qs::Circuit*>(circuit);
+    if (!c) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "null circuit");
+    if (mode < -1 || mode > 1) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "specialised mode must be -1, 0 or 1");
+    c->specialize = mode;
+    c->plan.reset();
+    c->fplan.reset();
+    c->fgates.clear();
+    c->fused_k = -1;
+    c->tune_ms.clear();
+    return QS_OK;
+}
+
+// Whether the last-built QS_EXEC_STAGED and QS_EXEC_STAGED_FUSED schedules run specialised kernels, and
+// the wall time their compilation took (ms, both schedules; 0 when served from the kernel cache).
+extern "C" QS_API int qs_circuit_specialized_info(qs_circuit_t circuit, int* staged, int* staged_fused,
+    double* compile_ms) {
+    qs::Circuit* c = reinterpret_cast<qs::Circuit*>(circuit);
+    if (!c || !staged || !staged_fused) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "null argument");
+    *staged = c->plan && c->plan->specialized;
+    *staged_fused = c->fplan && c->fplan->specialized;
+    if (compile_ms)
+        *compile_ms = (c->plan ? c->plan->compile_ms : 0.) + (c->fplan ? c->fplan->compile_ms : 0.);
+    return QS_OK;
+}
+
+// CUDA C source of the specialised kernel of pass `pass` of the circuit's QS_EXEC_STAGED schedule at
+// `dim` amplitudes (host only).  With buf == NULL, *size receives the length + 1; otherwise up to *size
+// bytes are written, NUL-terminated.
+extern "C" QS_API int qs_circuit_specialized_source(qs_circuit_t circuit, QS_ITYPE dim, QS_UINT pass, char* buf,
+    QS_ITYPE* size) {
+    qs::Circuit* c = reinterpret_cast<qs::Circuit*>(circuit);
+    if (!c || !size) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "null argument");
+    if (dim != (1ULL << c->n)) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "dim differs from 2^qubit_count");
+    if (c->n < (UINT)qs::kPhaseBits + 3) return qs::set_error(QS_ERR_NOT_SUPPORTED, "fewer than 7 qubits");
+    qs::HostPlan H;
+    qs::make_host_plan(c->gates, c->n, &H);
+    if (pass >= H.passes.size() || H.passes[pass].single)
+        return qs::set_error(QS_ERR_INVALID_ARGUMENT, "no such staged pass");
+    qs::StagedPlan P;
+    P.phases = H.phases;
+    P.ops = H.ops;
+    P.pool = H.pool;
+    qs::DevPass d{};
+    d.args.m = (int)H.passes[pass].q.size();
+    for (int j = 0; j < d.args.m; ++j) d.args.q[j] = H.passes[pass].q[j];
+    d.args.nphases = (int)H.pp[pass].nphases;
+    d.phase_begin = H.pp[pass].phase_begin;
+    if (d.args.nphases) {
+        auto high_bits = [&](const qs::StPhase& ph) {
+            for (int p = 0; p < 4; ++p)
+                if (ph.bits[p] < qs::kLowFixed) return false;
+            return true;
+        };
+        if (high_bits(H.phases[d.phase_begin])) d.args.io |= 1;
+        if (high_bits(H.phases[d.phase_begin + d.args.nphases - 1])) d.args.io |= 2;
+    }
+    const std::string src = qs::specialized_pass_source(qs::pass_desc(P, d));
+    if (!buf) {
+        *size = src.size() + 1;
+        return QS_OK;
+    }
+    if (*size == 0) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "zero-size buffer");
+    const size_t n = std::min<size_t>(src.size(), (size_t)*size - 1);
+    memcpy(buf, src.data(), n);
+    buf[n] = '\0';
     return QS_OK;
 }
 

@@ -2,7 +2,7 @@
 
 All random draws use numpy's PCG64 (``numpy.random.default_rng(seed)``); the same gate list is
 fed to this library and to the CPU implementations, so both sides see identical inputs.
-A gate is a tuple: ("RX"|"RY"|"RZ", q, angle), ("U3", q, theta, phi, lam), ("CNOT"|"CZ", c, t),
+A gate is a tuple: ("RX"|"RY"|"RZ", q, angle), ("U3", q, theta, phi, lam), ("CNOT"|"CZ", c, t), ("SWAP", a, b),
 ("DENSE", targets, matrix), ("DEPOL", (q,) or (q0, q1), p).
 """
 from __future__ import annotations
@@ -98,6 +98,8 @@ def to_circuit(gates, n: int):
             c.add_gate(G.CNOT(g[1], g[2]))
         elif k == "CZ":
             c.add_gate(G.CZ(g[1], g[2]))
+        elif k == "SWAP":
+            c.add_gate(G.SWAP(g[1], g[2]))
         elif k == "DENSE":
             c.add_gate(G.DenseMatrix(list(g[1]), g[2]))
         elif k == "DEPOL":

@@ -164,3 +164,55 @@ def test_autotuner_records_estimates(port):
     # a second run reuses the schedule
     circ.update_quantum_state(s, mode="staged_fused")
     assert circ.fusion_info()[0] == k
+
+
+@pytest.mark.parametrize("n", [9, 13, 17])
+@pytest.mark.parametrize("mode,k", [("staged", None), ("staged_fused", 0), ("staged_fused", 1), ("staged_fused", 2)])
+def test_specialized_passes_against_oracle(port, n, mode, k):
+    """Every pass as its own compiled kernel (set_specialized(1)): RX/RY/RZ, CNOT ladders, U3, CZ, SWAP,
+    two-qubit dense blocks and CNOT-folded dense ops, HBM-direct and tile round-trip passes, against the
+    oracle; and the same state as the generic pass kernel."""
+    rng = np.random.default_rng(7000 + n)
+    gates = W.layered_rotation_circuit(n, 2, seed=n) + W.u3_cz_circuit(n, 2, seed=n + 1)
+    for _ in range(40):
+        a, b = (int(x) for x in rng.choice(n, size=2, replace=False))
+        r = rng.random()
+        if r < 0.3:
+            m = np.linalg.qr(rng.normal(size=(4, 4)) + 1j * rng.normal(size=(4, 4)))[0]
+            gates.append(("DENSE", (a, b), m))
+        elif r < 0.4:
+            gates.append(("DENSE", (a, b), np.eye(4)[[0, 2, 1, 3]]))  # SWAP as a permutation matrix
+        elif r < 0.5:
+            gates.append(("SWAP", a, b))
+        else:
+            gates.append(("CNOT", a, b))
+            th, ph, la = rng.uniform(0, 2 * np.pi, size=3)
+            gates.append(("U3", b, float(th), float(ph), float(la)))
+    want = np.zeros(1 << n, dtype=np.complex128)
+    want[0] = 1
+    R.run_on_cpu(gates, want, port)
+    out = {}
+    for spec in (1, 0):
+        circ = W.to_circuit(gates, n)
+        circ.set_specialized(spec)
+        if k is not None:
+            circ.set_fusion(k)
+        s = QuantumState(n)
+        circ.update_quantum_state(s, mode=mode)
+        info = circ.specialized_info()
+        assert info[0 if mode == "staged" else 1] == bool(spec)
+        out[spec] = s.get_vector()
+        assert np.max(np.abs(out[spec] - want)) <= AMP_TOL, spec
+    assert np.max(np.abs(out[1] - out[0])) <= 1e-14
+
+
+def test_specialized_kernels_cached_across_circuits():
+    """A second circuit with the same schedule reuses the compiled kernels (no compile time)."""
+    n = 12
+    gates = W.layered_rotation_circuit(n, 3, seed=5)
+    a, b = W.to_circuit(gates, n), W.to_circuit(gates, n)
+    for c in (a, b):
+        c.set_specialized(1)
+        c.update_quantum_state(QuantumState(n), mode="staged")
+    assert a.specialized_info()[0] and b.specialized_info()[0]
+    assert b.specialized_info()[2] < a.specialized_info()[2] or b.specialized_info()[2] < 5.0
