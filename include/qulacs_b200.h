@@ -437,7 +437,9 @@ QS_API int qs_circuit_fuse(qs_circuit_t circuit, int k, qs_circuit_t* out);
 QS_API int qs_circuit_gate_matrix(qs_circuit_t circuit, QS_UINT index, QS_UINT* qubits, QS_UINT* qubit_count,
     double* matrix);
 /* QS_EXEC_STAGED_FUSED: force the block size k (0..6; 0 = no fusion), or -1 (default) to let the
- * autotuner choose k in 0..4 on the next run by timing each candidate's staged passes. */
+ * autotuner choose on the next run: it times each candidate k = 0..6's staged passes (the specialised
+ * kernels when the circuit uses them) with 2^12-amplitude tiles, then the best k with 2^11-amplitude
+ * tiles, and keeps the fastest schedule. */
 QS_API int qs_circuit_set_fusion(qs_circuit_t circuit, int k);
 /* Specialised pass kernels (no reference counterpart): the single-state staged modes can run each HBM
  * pass as its own kernel, generated from the pass's schedule with every tile qubit, phase bit and gate
@@ -453,8 +455,9 @@ QS_API int qs_circuit_specialized_info(qs_circuit_t circuit, int* staged, int* s
 QS_API int qs_circuit_specialized_source(qs_circuit_t circuit, QS_ITYPE dim, QS_UINT pass, char* buf,
     QS_ITYPE* size);
 /* The schedule last built for QS_EXEC_STAGED_FUSED: block size (-1 before the first run), gate count
- * after fusion, HBM passes, and the autotuner's estimate per k = 0..4 in ms (estimates_ms[5], may be
- * NULL; < 0 where not tried). */
+ * after fusion, HBM passes, and the autotuner's estimates in ms (estimates_ms[8], may be NULL; < 0
+ * where not tried): [k] for k = 0..6 with 2^12-amplitude tiles, [7] for the best k with 2^11-amplitude
+ * tiles, the tile shape the schedule uses when [7] is the smallest. */
 QS_API int qs_circuit_fusion_info(qs_circuit_t circuit, int* k, QS_UINT* gate_count, QS_UINT* passes,
     double* estimates_ms);
 /* The circuit acting on a density matrix of n qubits, as a circuit on the 2n-qubit vector

@@ -3,7 +3,8 @@
 Every ``csrc/*.cu`` is compiled by nvcc with ``-gencode arch=compute_100a,code=sm_100a``, every
 ``csrc/*.cpp`` by nvcc's host compiler, and the objects are linked into
 ``qulacs_b200/libqulacs_b200.so`` (CUDA runtime linked statically).  Objects go to
-``qulacs_b200/_build``.  Rebuilds only what changed.
+``qulacs_b200/_build``.  Rebuilds only what changed.  ``csrc/compat/csim_compat.cpp`` becomes
+``qulacs_b200/libcsim_b200.so``: csim's operator names and argument lists over the C ABI.
 """
 from __future__ import annotations
 
@@ -18,6 +19,8 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 OBJ = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libqulacs_b200.so")
+CSIM_LIB = os.path.join(PKG, "libcsim_b200.so")
+CXX = os.environ.get("CXX", "g++")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -55,15 +58,32 @@ def build(verbose: bool = False) -> str:
     srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
     with ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 4)) as ex:
         objs = list(ex.map(lambda s: _compile(s, verbose), srcs))
-    if os.path.exists(LIB) and os.path.getmtime(LIB) >= max(os.path.getmtime(o) for o in objs):
-        return LIB
-    cmd = [NVCC, "-shared", "-o", LIB] + objs + ARCH + ["-cudart", "static", "-lpthread", "-ldl", "-lrt"]
+    if not (os.path.exists(LIB) and os.path.getmtime(LIB) >= max(os.path.getmtime(o) for o in objs)):
+        cmd = [NVCC, "-shared", "-o", LIB] + objs + ARCH + ["-cudart", "static", "-lpthread", "-ldl", "-lrt"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    build_csim_compat(verbose)
+    return LIB
+
+
+def build_csim_compat(verbose: bool = False) -> str:
+    """libcsim_b200.so: csim's function names and argument lists (C++ linkage) over libqulacs_b200.so."""
+    src = os.path.join(CSRC, "compat", "csim_compat.cpp")
+    hdr = os.path.join(ROOT, "include", "qulacs_b200", "csim_compat.hpp")
+    if os.path.exists(CSIM_LIB) and os.path.getmtime(CSIM_LIB) >= max(
+            os.path.getmtime(src), os.path.getmtime(hdr), os.path.getmtime(LIB)):
+        return CSIM_LIB
+    cmd = [CXX, "-std=c++17", "-O2", "-fPIC", "-shared", "-fvisibility=hidden", f"-I{ROOT}/include", src,
+           f"-L{PKG}", "-lqulacs_b200", "-Wl,-rpath,$ORIGIN", "-o", CSIM_LIB]
     if verbose:
         print(" ".join(cmd), flush=True)
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
-        raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
-    return LIB
+        raise RuntimeError(f"libcsim_b200 build failed:\n{r.stdout}\n{r.stderr}")
+    return CSIM_LIB
 
 
 if __name__ == "__main__":

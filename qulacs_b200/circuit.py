@@ -233,10 +233,11 @@ class QuantumCircuit:
         return buf.value.decode()
 
     def fusion_info(self):
-        """(k, gates after fusion, HBM passes, autotuner estimates in ms for k = 0..4) of the last
-        "staged_fused" schedule; k = -1 before the first run."""
+        """(k, gates after fusion, HBM passes, autotuner estimates in ms) of the last "staged_fused"
+        schedule; k = -1 before the first run.  Estimates: [k] for k = 0..6 with 2^12-amplitude tiles,
+        [7] for the best k with 2^11-amplitude tiles (< 0 where not tried)."""
         k, g, p = C.c_int(), C.c_uint(), C.c_uint()
-        est = (C.c_double * 5)()
+        est = (C.c_double * 8)()
         call("qs_circuit_fusion_info", self._h, C.byref(k), C.byref(g), C.byref(p), est)
         return k.value, g.value, p.value, list(est)
 

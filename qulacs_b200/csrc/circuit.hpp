@@ -40,6 +40,7 @@ struct Circuit {
     // FP64-fused gate list and its staged schedule (QS_EXEC_STAGED_FUSED, staged.cu)
     int fusion_k = -1;              // forced block size, or -1: the autotuner chooses
     int fused_k = -1;               // block size of fgates (valid while fplan is set)
+    int fused_tile_bits = 12;       // tile qubits of fplan's passes
     std::vector<GateRec> fgates;
     std::shared_ptr<StagedPlan> fplan;
     std::vector<double> tune_ms;    // autotuner estimate per candidate block size (ms; < 0: not tried)

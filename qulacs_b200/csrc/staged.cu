@@ -929,12 +929,15 @@ int run_staged(Circuit& c, void* state, ITYPE dim, cudaStream_t st) {
     return run_plan(c.gates, *c.plan, state, dim, st);
 }
 
-// ---- FP64 gate fusion + staged passes, block size chosen by measurement.
-// The autotuner fuses the gate list for each candidate block size k (0 = unfused), builds its staged
-// schedule and times every pass's kernel on a scratch buffer of whole tiles (the pass's ops only see
-// tile-local bits, so its tile qubits are remapped to 0..m-1); a pass costs at least its HBM time.
-// Gates left outside passes cost one HBM pass each (dense 5- and 6-qubit kernels more).
-constexpr int kTuneMaxK = 4;
+// ---- FP64 gate fusion + staged passes, block size and tile shape chosen by measurement.
+// The autotuner fuses the gate list for each candidate block size k = 0..6 (0 = unfused), builds its
+// staged schedule with 2^12-amplitude tiles, and times every pass's kernel -- the specialised kernel
+// when the circuit runs specialised passes, else the generic one -- on a scratch buffer of whole tiles
+// (the pass's ops only see tile-local bits, so its tile qubits are remapped to 0..m-1); a pass costs at
+// least its HBM time, and gates left outside passes cost one HBM pass each (dense 5- and 6-qubit
+// kernels more).  The best k is then also tried with 2^11-amplitude tiles (the tile shape).
+constexpr int kTuneMaxK = 6;
+constexpr int kTuneSlots = kTuneMaxK + 2;  // k = 0..6 at 2^12 tiles, then the best k at 2^11 tiles
 constexpr double kTuneHbmBytesPerSec = 6.5e12;  // B200 streaming copy bandwidth
 
 static double single_gate_factor(const GateRec& g) {
@@ -945,15 +948,42 @@ static double single_gate_factor(const GateRec& g) {
 }
 
 static int estimate_plan_ms(const std::vector<GateRec>& gates, const StagedPlan& P, ITYPE dim, cudaStream_t st,
-    double* out_ms) {
+    bool specialized, double* out_ms) {
     const double hbm_ms = 2.0 * 16.0 * (double)dim / kTuneHbmBytesPerSec * 1e3;
-    double total = 0.;
     QS_TRY(staged_allow_smem());
+    // specialised kernels of the remapped passes, compiled on host threads in parallel
+    std::vector<void*> spec(P.passes.size(), nullptr);
+    if (specialized) {
+        std::vector<size_t> todo;
+        for (size_t i = 0; i < P.passes.size(); ++i)
+            if (!P.passes[i].single && P.passes[i].args.nphases > 0) todo.push_back(i);
+        std::vector<int> rcs(P.passes.size(), QS_OK);
+        std::vector<std::string> errs(P.passes.size());
+        std::atomic<size_t> next{0};
+        const unsigned nt =
+            std::max(1u, std::min<unsigned>((unsigned)todo.size(), std::thread::hardware_concurrency()));
+        std::vector<std::thread> pool;
+        for (unsigned t = 0; t < nt; ++t)
+            pool.emplace_back([&] {
+                for (size_t j; (j = next.fetch_add(1)) < todo.size();) {
+                    const size_t i = todo[j];
+                    PassDesc pd = pass_desc(P, P.passes[i]);
+                    for (int b = 0; b < pd.m; ++b) pd.q[b] = (UINT)b;
+                    rcs[i] = specialized_pass_kernel(pd, &spec[i], nullptr);
+                    if (rcs[i] != QS_OK) errs[i] = qs_get_last_error();
+                }
+            });
+        for (std::thread& t : pool) t.join();
+        for (size_t i : todo)
+            if (rcs[i] != QS_OK) return set_error(rcs[i], errs[i]);
+    }
+    double total = 0.;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     QS_CUDA_CHECK(cudaEventCreate(&e0));
     QS_CUDA_CHECK(cudaEventCreate(&e1));
     int rc = QS_OK;
-    for (const DevPass& d : P.passes) {
+    for (size_t i = 0; i < P.passes.size(); ++i) {
+        const DevPass& d = P.passes[i];
         if (d.single) {
             total += hbm_ms * single_gate_factor(gates[d.gate]);
             continue;
@@ -967,11 +997,16 @@ static int estimate_plan_ms(const std::vector<GateRec>& gates, const StagedPlan&
         for (int j = 0; j < a.m; ++j) a.q[j] = (UINT)j;
         DevPass dt = d;
         dt.args = a;
-        launch_pass((double2*)buf, dt, tt, st);  // warm-up
+        auto launch = [&]() -> int {
+            if (spec[i]) return launch_specialized_pass(spec[i], (double2*)buf, tt, a.m, st);
+            launch_pass((double2*)buf, dt, tt, st);
+            return check_launch("k_staged_pass");
+        };
+        rc = launch();  // warm-up
+        if (rc != QS_OK) break;
         cudaEventRecord(e0, st);
-        launch_pass((double2*)buf, dt, tt, st);
+        rc = launch();
         cudaEventRecord(e1, st);
-        rc = check_launch("k_staged_pass");
         if (rc != QS_OK) break;
         if (cudaEventSynchronize(e1) != cudaSuccess) {
             rc = set_error(QS_ERR_CUDA, "autotune: event synchronize failed");
@@ -989,30 +1024,36 @@ static int estimate_plan_ms(const std::vector<GateRec>& gates, const StagedPlan&
 
 static int ensure_fused_plan(Circuit& c, ITYPE dim, cudaStream_t st) {
     if (c.fplan && c.fplan->dim == dim) return QS_OK;
+    const bool spec = want_specialized(c, dim);
     if (c.fusion_k >= 0) {
         c.fgates = fuse_gates(c.gates, c.fusion_k);
         c.fused_k = c.fusion_k;
+        c.fused_tile_bits = kTileBits;
         QS_TRY(build_plan(c.fgates, c.n, dim, &c.fplan));
-        if (want_specialized(c, dim)) QS_TRY(specialize_plan(*c.fplan));
+        if (spec) QS_TRY(specialize_plan(*c.fplan));
         return QS_OK;
     }
-    c.tune_ms.assign(kTuneMaxK + 1, -1.);
+    c.tune_ms.assign(kTuneSlots, -1.);
     double best = 0.;
-    for (int k = 0; k <= kTuneMaxK; ++k) {
+    auto consider = [&](int k, int tile_bits, int slot) -> int {
         std::vector<GateRec> fg = fuse_gates(c.gates, k);
         std::shared_ptr<StagedPlan> P;
-        QS_TRY(build_plan(fg, c.n, dim, &P));
+        QS_TRY(build_plan(fg, c.n, dim, &P, tile_bits));
         double ms = 0.;
-        QS_TRY(estimate_plan_ms(fg, *P, dim, st, &ms));
-        c.tune_ms[k] = ms;
+        QS_TRY(estimate_plan_ms(fg, *P, dim, st, spec, &ms));
+        c.tune_ms[slot] = ms;
         if (!c.fplan || ms < best) {
             best = ms;
             c.fgates.swap(fg);
             c.fplan = P;
             c.fused_k = k;
+            c.fused_tile_bits = tile_bits;
         }
-    }
-    if (want_specialized(c, dim)) QS_TRY(specialize_plan(*c.fplan));
+        return QS_OK;
+    };
+    for (int k = 0; k <= kTuneMaxK; ++k) QS_TRY(consider(k, kTileBits, k));
+    if (c.n > (UINT)kTileBits - 1) QS_TRY(consider(c.fused_k, kTileBits - 1, kTuneMaxK + 1));
+    if (spec) QS_TRY(specialize_plan(*c.fplan));
     return QS_OK;
 }
 
@@ -1056,8 +1097,9 @@ extern "C" QS_API int qs_circuit_staged_stats(qs_circuit_t circuit, QS_UINT* pas
 }
 
 // Block size, gate count and HBM passes of the FP64-fused schedule last built for QS_EXEC_STAGED_FUSED
-// (k = -1 before the first run), and the autotuner's estimate per candidate k = 0..4 (ms; < 0 when
-// not tried, e.g. with a forced k).
+// (k = -1 before the first run), and the autotuner's estimates (ms; < 0 when not tried, e.g. with a
+// forced k): estimates_ms[k] for k = 0..6 with 2^12-amplitude tiles, estimates_ms[7] for the best k
+// with 2^11-amplitude tiles (the schedule uses those tiles when that estimate is the smallest).
 extern "C" QS_API int qs_circuit_fusion_info(qs_circuit_t circuit, int* k, QS_UINT* gate_count, QS_UINT* passes,
     double* estimates_ms) {
     qs::Circuit* c = reinterpret_cast<qs::Circuit*>(circuit);
@@ -1066,7 +1108,7 @@ extern "C" QS_API int qs_circuit_fusion_info(qs_circuit_t circuit, int* k, QS_UI
     *gate_count = c->fplan ? (QS_UINT)c->fgates.size() : 0;
     *passes = c->fplan ? (QS_UINT)c->fplan->passes.size() : 0;
     if (estimates_ms)
-        for (int i = 0; i <= qs::kTuneMaxK; ++i)
+        for (int i = 0; i < qs::kTuneSlots; ++i)
             estimates_ms[i] = i < (int)c->tune_ms.size() ? c->tune_ms[i] : -1.;
     return QS_OK;
 }
