@@ -415,6 +415,68 @@ def dm_noisy_circuit(n: int = 13, depth: int = 8, p: float = 1e-3, seed: int = 7
     return res
 
 
+GPUSIM_SO = os.path.join(ROOT, "baseline", "_ref", "libgpusim_ref.so")
+
+
+def gpusim_baseline(n: int, gates, ours_s: float, reps: int = 2):
+    """The reference's own GPU backend (src/gpusim, compiled for sm_100a by baseline/Makefile) running the
+    same circuit gate by gate through its host wrappers on this B200: one kernel plus one stream
+    synchronise per gate, as the reference's QuantumStateGpu path does.  Timed by the host clock around
+    whole circuits (every wrapper synchronises).  Its amplitudes at the fixture's indices are checked
+    against the reference csim's 30-qubit result when that fixture applies."""
+    import ctypes as C
+    if not os.path.exists(GPUSIM_SO):
+        return {"unavailable": "baseline/_ref/libgpusim_ref.so not built (make -C baseline needs the reference "
+                               "sources)"}
+    lib = C.CDLL(GPUSIM_SO)
+    lib.gs_allocate.restype = C.c_void_p
+    lib.gs_allocate.argtypes = [C.c_ulonglong]
+    lib.gs_norm.restype = C.c_double
+    for f in ("gs_initialize", "gs_release", "gs_norm"):
+        getattr(lib, f).argtypes = [C.c_void_p] + ([C.c_ulonglong] if f != "gs_release" else [])
+    for f in ("gs_RX", "gs_RY", "gs_RZ"):
+        getattr(lib, f).argtypes = [C.c_uint, C.c_double, C.c_void_p, C.c_ulonglong]
+    lib.gs_CNOT.argtypes = [C.c_uint, C.c_uint, C.c_void_p, C.c_ulonglong]
+    if not lib.gs_init():
+        return {"unavailable": "gpusim stream allocation failed"}
+    dim = 1 << n
+    s = lib.gs_allocate(dim)
+    fns = {"RX": lib.gs_RX, "RY": lib.gs_RY, "RZ": lib.gs_RZ}
+
+    def run():
+        lib.gs_initialize(s, dim)
+        for g in gates:
+            if g[0] == "CNOT":
+                lib.gs_CNOT(g[1], g[2], s, dim)
+            else:
+                fns[g[0]](g[1], g[2], s, dim)
+
+    run()  # warm-up
+    times = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        run()
+        times.append(time.perf_counter() - t0)
+    sec = min(times)
+    out = {"workload": f"layered RX/RY/RZ+CNOT n={n} depth={DEPTH} ({len(gates)} gates), gate by gate through "
+                       "gpusim's *_host wrappers (one kernel + one stream synchronise per gate)",
+           "circuit_s": sec, "gates_per_s": len(gates) / sec,
+           "gbs_per_gate": len(gates) * bytes_per_gate(n) / 1e9 / sec,
+           "speedup_of_this_library": sec / ours_s, "norm": lib.gs_norm(s, dim), "reps": reps}
+    fx = os.path.join(ROOT, "tests", "golden", "config2_n30.npz")
+    if n == 30 and os.path.exists(fx):
+        from qulacs_b200._lib import call
+        g = np.load(fx)
+        amp = (C.c_double * 2)()
+        err = 0.0
+        for i, want in zip(g["amp_index"][:512], g["amps"][:512]):
+            call("qs_get_amplitude", C.c_void_p(s), dim, int(i), amp, None)
+            err = max(err, abs(complex(amp[0], amp[1]) - complex(want)))
+        out["max_abs_d_amp_vs_reference_csim"] = err
+    lib.gs_release(s)
+    return out
+
+
 def timed_region(step, steps: int, warmup: int, dist=None, sync=None, make_timer=None, device: str = "cpu") -> float:
     """The timing contract: `warmup` untimed steps, then a barrier with a device synchronize on both
     sides, exactly `steps` timed steps, a synchronize, and the per-step time in ms as the MAX over
@@ -503,6 +565,7 @@ def main():
     ap.add_argument("--qubits", type=int, default=N_QUBITS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-kernel-table", action="store_true")
+    ap.add_argument("--no-gpusim", action="store_true", help="skip the reference GPU backend leg")
     ap.add_argument("--workload", default="plain", choices=["plain", "fused", "batched", "serving", "noise", "dm"],
                     help="fused / batched / serving / noise / dm: only that measurement (configs 3 / 4 / 5, "
                          "NoiseSimulator, noisy density matrix)")
@@ -669,6 +732,14 @@ def main():
             torch.cuda.synchronize()
             modes_ms[other] = e0.elapsed_time(e1) / reps
 
+    # the reference's own GPU backend on the same circuit and device (N = 1 only)
+    gpusim = None
+    if world == 1 and not args.no_gpusim:
+        try:
+            gpusim = gpusim_baseline(n, gates, ms / 1e3)
+        except Exception as e:  # noqa: BLE001
+            gpusim = {"error": f"{type(e).__name__}: {e}"}
+
     # the CPU baseline and the other configurations run at N = 1 only: with N > 1 ranks they would
     # keep the other ranks waiting at the closing barrier
     cpu = None
@@ -731,6 +802,7 @@ def main():
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
+            "gpusim_baseline": gpusim,
             **extras,
         }
         print(json.dumps(line), flush=True)
