@@ -141,7 +141,8 @@ def kernel_table(state, n: int, stream, reps: int = 5):
         (f"dense1 t={n - 1} (k_pair)", 1.0, lambda: call("qs_single_qubit_dense_matrix_gate", n - 1, mp(m1), p, dim, h)),
         ("RZ t=10 (k_diag1)", 1.0, lambda: call("qs_RZ_gate", 10, 0.3, p, dim, h)),
         (f"CNOT {n - 2}->{n - 1} (k_pair swap)", 0.5, lambda: call("qs_CNOT_gate", n - 2, n - 1, p, dim, h)),
-        ("CNOT 0->1 (k_pair swap)", 0.5, lambda: call("qs_CNOT_gate", 0, 1, p, dim, h)),
+        ("CNOT 0->1 (k_perm2_tile, full read + write)", 1.0, lambda: call("qs_CNOT_gate", 0, 1, p, dim, h)),
+        (f"CNOT 2->{n - 1} (k_perm2_tile, full read + write)", 1.0, lambda: call("qs_CNOT_gate", 2, n - 1, p, dim, h)),
         ("CZ 3,17 (k_single negate)", 0.25, lambda: call("qs_CZ_gate", 3, 17, p, dim, h)),
         (f"dense2 {n - 2},{n - 1} (k_dense2)", 1.0, lambda: call("qs_double_qubit_dense_matrix_gate_c", n - 2, n - 1, mp(mats[2]), p, dim, h)),
     ]
@@ -547,6 +548,30 @@ def serving_latency(requests: int, rate: float, budget_gb: float, workers: int, 
     return out
 
 
+def serving_sweep(requests: int, rates, budget_gb: float, workers: int, seed: int = 5005,
+                  precisions=("c128", "c64")):
+    """Config 5 at several arrival rates up to saturation: per rate and precision, achieved jobs/s,
+    p50/p99 latency, the mean and largest expectation batch and the mean number of worker batches on the
+    device at once (continuous batching shows as batches > 1 and several in flight as the rate rises)."""
+    from qulacs_b200.serving import ServingLoop, make_request_mix
+    curve = []
+    for rate in rates:
+        row = {"rate_per_s": rate}
+        for prec in precisions:
+            reqs = make_request_mix(requests, rate, seed)
+            loop = ServingLoop(int(budget_gb * (1 << 30)), workers=workers, precision=prec)
+            try:
+                st = loop.run(reqs)
+            finally:
+                loop.close()
+            row[prec] = {k: st[k] for k in ("jobs_per_s", "p50_ms", "p99_ms", "mean_batch", "max_batch",
+                                              "mean_batches_in_flight")}
+        curve.append(row)
+    return {"workload": f"{requests} requests per rate, Poisson arrivals, mix 70% <H> (n 12-28) / 20% sampling "
+                        f"(n 16-30, 1024 shots) / 10% noisy DM (n 8-13)", "workers": workers,
+            "memory_budget_gb": budget_gb, "curve": curve}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -627,7 +652,7 @@ def main():
             print(json.dumps({"metric": "noisy trajectory sampling: shots/s", **r}), flush=True)
         return
     if args.workload == "serving":
-        r = serving_latency(args.requests, args.rate, args.budget_gb, args.workers)
+        r = serving_sweep(args.requests, (5.0, 20.0, 50.0, 100.0), args.budget_gb, args.workers)
         if rank == 0:
             print(json.dumps({"metric": "serve p99 ms", **r}), flush=True)
         return
@@ -753,7 +778,7 @@ def main():
         torch.cuda.synchronize()
         for key, fn in (("fused", lambda: fused_comparison(args.fused_qubits, args.fused_layers, stream, True)),
                         ("batched", lambda: batched_throughput(args.instances, args.budget_gb)),
-                        ("serving", lambda: serving_latency(60, 5.0, 96.0, 4)),
+                        ("serving", lambda: serving_sweep(60, (5.0, 20.0, 50.0, 100.0), 96.0, 4)),
                         ("noise", lambda: noise_sampling()),
                         ("density_matrix", lambda: dm_noisy_circuit())):
             try:

@@ -489,9 +489,14 @@ QS_API int qs_batch_update_quantum_states(const qs_circuit_t* circuits, void* co
  * QS_ERR_TIMEOUT, leaves the CUDA context usable, and leaves `state` with every pass but the last
  * applied.  Synchronises `stream`. */
 QS_API int qs_debug_batch_wait_expiry(qs_circuit_t circuit, void* state, QS_UINT wait_limit_us, void* stream);
+/* The same check for the complex64 batch kernel (qs_batch_update_quantum_states_fused_c64): its last
+ * pass waits on its own counter, bounded by wait_limit_us; returns QS_ERR_TIMEOUT, context usable. */
+QS_API int qs_debug_batch_wait_expiry_fused_c64(qs_circuit_t circuit, void* state_c64, QS_UINT wait_limit_us,
+    void* stream);
 /* The same on the fused complex64 tensor-core path: states_c64[i] holds circuits[i]'s 2^n complex64
- * amplitudes (n >= 10).  Missing plans are built on host threads in parallel; the circuits run
- * concurrently on streams forked from `stream` and joined back.  Synchronises `stream`. */
+ * amplitudes (n >= 10).  Missing plans are built on host threads in parallel; then every circuit's
+ * passes run in ONE persistent launch (work items: tile pairs of (circuit, pass), a circuit's pass
+ * waiting, bounded, for its previous pass).  Synchronises `stream`. */
 QS_API int qs_batch_update_quantum_states_fused_c64(qs_circuit_t const* circuits, void* const* states_c64,
     QS_UINT count, void* stream);
 /* <P_k> for the Pauli terms of many complex128 states.  Terms of state i are term_offsets[i] ..

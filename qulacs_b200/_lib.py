@@ -148,6 +148,7 @@ SIGNATURES = {
     "qs_circuit_update_quantum_state_fused_c64": [P, P, IT, P],
     "qs_batch_update_quantum_states": [P, P, U, P],
     "qs_debug_batch_wait_expiry": [P, P, U, P],
+    "qs_debug_batch_wait_expiry_fused_c64": [P, P, U, P],
     "qs_circuit_set_specialized": [P, I],
     "qs_circuit_specialized_info": [P, C.POINTER(I), C.POINTER(I), C.POINTER(D)],
     "qs_circuit_specialized_source": [P, IT, U, C.c_char_p, C.POINTER(IT)],

@@ -177,41 +177,115 @@ __device__ __forceinline__ void bulk_load_block(uint32_t dst_a, uint32_t dst_t, 
 // Every in-tile data movement is a table XOR: element (row y, column n) of a block's accumulator goes
 // to byte rowtab[y] ^ coltab[n] of the next B operand (float rowtab[y] ^ coltab[n] of the output
 // tile after the last block).
-__global__ void __launch_bounds__(kFThreads, 1) k_fused_pass(const __grid_constant__ FusedPassArgs a) {
-    extern __shared__ __align__(1024) unsigned char smem[];
-    const int m = a.m;
-    const uint32_t tsize = 1u << m;
-    const uint32_t N = tsize >> kFBlock;  // cosets per block = MMA N
-    const uint32_t bimg = N * 256u;
-    unsigned char* sA = smem;                                  // A hi | A lo   (64 KiB)
-    unsigned char* sB0 = sA + 2 * kAImageBytes;                // tile X: B hi | B lo, then its output tile
-    unsigned char* sB1 = sB0 + 2 * bimg;                       // tile Y
-    uint32_t* tabs = (uint32_t*)(sB1 + 2 * bimg);              // [2][kTabWords]
-    uint64_t* mbar = (uint64_t*)(tabs + 2 * kTabWords);        // [0] MMA X, [1] MMA Y, [2] block record
-    uint32_t* tmem_slot = (uint32_t*)(mbar + 3);
-    int* s_err = (int*)(tmem_slot + 1);
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const uint32_t ncols = 2 * N < 32 ? 32u : 2 * N;  // D_X at column 0, D_Y at column N
+//
+// The per-pair work is written once (fused_pair) and shared by the single-circuit kernel
+// (k_fused_pass: all tile pairs of one pass) and the multi-circuit kernel (k_fused_batch: work items of
+// many circuits' passes).  Shared memory is laid out for the largest tile (N = 128 cosets), so passes
+// of any tile size fit the same layout.
 
+// Shared-memory regions of a fused CTA and the TMEM allocation.
+struct FusedSmem {
+    unsigned char* sA;   // A hi | A lo (64 KiB)
+    unsigned char* sB0;  // tile X: B hi | B lo, then its output tile
+    unsigned char* sB1;  // tile Y
+    uint32_t* tabs;      // [2][kTabWords]
+    uint64_t* mbar;      // [0] MMA X, [1] MMA Y, [2] block record
+    int* s_err;
+    uint32_t tmem, ncols, mb0, mb1, mba, aaddr, taddr;
+};
+// Completion-barrier phases and the record pipeline, identical in every thread of the CTA.
+struct FusedPipe {
+    uint32_t ph0 = 0, ph1 = 0, pha = 0;
+    bool a_pending = false;  // a block record copy is in flight on mba
+    int slot = 0;            // table slot of the current block's record
+    int loads = 0;           // records issued so far (the next one goes to slot loads & 1)
+};
+
+constexpr uint32_t kFNMax = 1u << (kFTileMax - kFBlock);  // 128 cosets per block at the largest tile
+
+__device__ __forceinline__ FusedSmem fused_setup(unsigned char* smem, uint32_t ncols) {
+    FusedSmem S;
+    const uint32_t bimg_max = kFNMax * 256u;
+    S.sA = smem;
+    S.sB0 = S.sA + 2 * kAImageBytes;
+    S.sB1 = S.sB0 + 2 * bimg_max;
+    S.tabs = (uint32_t*)(S.sB1 + 2 * bimg_max);
+    S.mbar = (uint64_t*)(S.tabs + 2 * kTabWords);
+    uint32_t* tmem_slot = (uint32_t*)(S.mbar + 3);
+    S.s_err = (int*)(tmem_slot + 1);
+    S.ncols = ncols;
+    const int tid = threadIdx.x, warp = tid >> 5;
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
                      "r"(ncols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (tid == 0) {
-        for (int i = 0; i < 3; ++i) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar + i)));
+        for (int i = 0; i < 3; ++i) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(S.mbar + i)));
         asm volatile("fence.mbarrier_init.release.cluster;");
-        *s_err = 0;
+        *S.s_err = 0;
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
-    const uint32_t tmem = *tmem_slot;
-    const uint32_t mb0 = smem_u32(mbar), mb1 = smem_u32(mbar + 1), mba = smem_u32(mbar + 2);
-    uint32_t ph0 = 0, ph1 = 0, pha = 0;
-    bool a_pending = false;  // a block record copy is in flight on mba (same in every thread)
+    S.tmem = *tmem_slot;
+    S.mb0 = smem_u32(S.mbar);
+    S.mb1 = smem_u32(S.mbar + 1);
+    S.mba = smem_u32(S.mbar + 2);
+    S.aaddr = smem_u32(S.sA);
+    S.taddr = smem_u32(S.tabs);
+    return S;
+}
+
+// No copy in flight, the error flag published, TMEM freed.
+__device__ __forceinline__ void fused_teardown(const FusedSmem& S, FusedPipe& P, int* err) {
+    if (P.a_pending && !mbar_wait(S.mba, P.pha)) *S.s_err = 1;
+    P.a_pending = false;
+    if (threadIdx.x == 0 && *S.s_err) atomicExch(err, 1);
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    if ((threadIdx.x >> 5) == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(S.tmem), "r"(S.ncols));
+}
+
+__device__ __forceinline__ const unsigned char* fused_record(const FusedPassArgs& a, int b) {
+    return a.records + (size_t)b * kRecordBytes;
+}
+
+// Issue block b's record into the next table slot (one thread copies; every thread tracks the state).
+__device__ __forceinline__ void fused_load_record(const FusedSmem& S, FusedPipe& P, const FusedPassArgs& a, int b,
+                                                  bool set_slot) {
+    const int nslot = P.loads & 1;
+    if (threadIdx.x == 0) bulk_load_block(S.aaddr, S.taddr + nslot * kTabBytes, fused_record(a, b), S.mba);
+    P.a_pending = true;
+    ++P.loads;
+    if (set_slot) P.slot = nslot;
+}
+
+__device__ __forceinline__ void fused_wait_record(const FusedSmem& S, FusedPipe& P) {
+    if (P.a_pending) {
+        if (!mbar_wait(S.mba, P.pha)) *S.s_err = 1;
+        P.pha ^= 1u;
+        P.a_pending = false;
+    }
+}
+
+// One tile pair (TX and, if hasY, TY) through every block of pass `a`.  On entry block 0's record is
+// loaded or in flight in slot P.slot.  `next_pair` (>= 0): another pair of the same pass follows, so
+// block 0's record is reloaded after the last block (tile `next_pair` and its partner are prefetched
+// into L2 meanwhile).  Returns false when a bounded wait expired (the CTA must stop).
+__device__ __forceinline__ bool fused_pair(const FusedPassArgs& a, const FusedSmem& S, FusedPipe& P, ITYPE TX, ITYPE TY, bool hasY,
+                           long long next_pair, ITYPE pair_stride) {
+    const int m = a.m;
+    const uint32_t tsize = 1u << m;
+    const uint32_t N = tsize >> kFBlock;  // cosets per block = MMA N
+    const uint32_t bimg = N * 256u;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t idesc = idesc_bf16(kARows, (int)N);
-    const uint32_t aaddr = smem_u32(sA), taddr = smem_u32(tabs);
+    unsigned char* sB0 = S.sB0;
+    unsigned char* sB1 = S.sB1;
+    const uint32_t* tabs = S.tabs;
 
     // output stores move amplitude pairs (tile bit 0 = qubit 0), 16 B each: pair p = tid + 512 k
     ITYPE lo_off = 0;
@@ -229,7 +303,6 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused_pass(const __grid_consta
             if ((k >> (j - kFTidBits - 1)) & 1) off |= 1ULL << a.q[j];
         return off;
     };
-    auto record = [&](int b) { return a.records + (size_t)b * kRecordBytes; };
 
     // accumulator reads: warp w reads TMEM lanes 32 (w % 4) .. +31 (rows y) and column part w / 4
     const uint32_t y = 32u * (warp & 3) + lane;
@@ -243,7 +316,7 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused_pass(const __grid_consta
 
     // tiles -> B operands straight from HBM: 64-bit offsets of coset n (gn) and block index j (gj);
     // both tiles' loads are in flight together
-    auto gather = [&](ITYPE TX, ITYPE TY, bool hasY, int slot) {
+    auto gather = [&](int slot) {
         const uint64_t* gn = (const uint64_t*)(tabs + slot * kTabWords + kTabGn);
         const ITYPE gj = ((const uint64_t*)(tabs + slot * kTabWords + kTabGj))[g_j];
         const ITYPE bx = tile_base(TX) | gj, by = hasY ? (tile_base(TY) | gj) : bx;
@@ -272,31 +345,44 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused_pass(const __grid_consta
         const uint32_t baddr = smem_u32(sB);
         // shared addresses are below 256 KiB, so the 14-bit start-address field never wraps: the
         // descriptor of K-step s is the K-step-0 descriptor plus its start offset >> 4
-        const uint64_t ahi0 = umma_desc(aaddr), alo0 = umma_desc(aaddr + kAImageBytes);
+        const uint64_t ahi0 = umma_desc(S.aaddr), alo0 = umma_desc(S.aaddr + kAImageBytes);
         const uint64_t bhi0 = umma_desc(baddr), blo0 = umma_desc(baddr + bimg);
 #pragma unroll
         for (int s = 0; s < kAK / 16; ++s) {
             const uint64_t ds = (uint64_t)(((s >> 2) * 1024 + (s & 3) * 32) >> 4);
-            mma_bf16(tmem + dcol, ahi0 + ds, bhi0 + ds, idesc, s > 0 ? 1u : 0u);
-            mma_bf16(tmem + dcol, ahi0 + ds, blo0 + ds, idesc, 1u);
-            mma_bf16(tmem + dcol, alo0 + ds, bhi0 + ds, idesc, 1u);
+            mma_bf16(S.tmem + dcol, ahi0 + ds, bhi0 + ds, idesc, s > 0 ? 1u : 0u);
+            mma_bf16(S.tmem + dcol, ahi0 + ds, blo0 + ds, idesc, 1u);
+            mma_bf16(S.tmem + dcol, alo0 + ds, bhi0 + ds, idesc, 1u);
         }
         asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar_addr)
                      : "memory");
     };
-    // accumulator (TMEM columns dcol..) -> next B operand in sB, or -> complex64 output tile over sB
+    // accumulator (TMEM columns dcol..) -> next B operand in sB, or -> complex64 output tile over sB.
+    // Row bit 0 is the real/imaginary part: lanes 2j and 2j + 1 swap halves of their 16 columns with one
+    // shuffle each, so the even lane holds (re, im) of columns 0..7 of the chunk and the odd lane of
+    // columns 8..15, and each amplitude is stored as one word: bf16x2 hi and lo (re in the low half,
+    // the next operand's K bit 0) or a float2 of the output tile.
     auto move = [&](unsigned char* sB, uint32_t dcol, int slot, bool last) {
         const uint32_t* rt = tabs + slot * kTabWords + kTabRow;
         const uint32_t* ct = tabs + slot * kTabWords + kTabCol;
-        const uint32_t ybase = rt[y];
+        const bool odd = lane & 1;
+        const uint32_t ybase = rt[y & ~1u];  // the pair's real-part row
         float* outt = (float*)sB;
         for (uint32_t cc = c_begin; cc < c_end; cc += 16) {
             float v[16];
-            tmem_ld16(tmem + ((32u * (warp & 3)) << 16) + dcol + cc, v);
-            uint32_t o[16];
+            tmem_ld16(S.tmem + ((32u * (warp & 3)) << 16) + dcol + cc, v);
+            float re[8], im[8];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const uint4 t4 = *(const uint4*)(ct + cc + 4 * q);
+            for (int i = 0; i < 8; ++i) {
+                const float got = __shfl_xor_sync(0xffffffffu, odd ? v[i] : v[8 + i], 1);
+                re[i] = odd ? got : v[i];
+                im[i] = odd ? v[8 + i] : got;
+            }
+            const uint32_t c0 = cc + (odd ? 8u : 0u);
+            uint32_t o[8];
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const uint4 t4 = *(const uint4*)(ct + c0 + 4 * q);
                 o[4 * q] = t4.x ^ ybase;
                 o[4 * q + 1] = t4.y ^ ybase;
                 o[4 * q + 2] = t4.z ^ ybase;
@@ -304,17 +390,14 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused_pass(const __grid_consta
             }
             if (last) {
 #pragma unroll
-                for (int i = 0; i < 16; ++i) outt[o[i]] = v[i];
+                for (int i = 0; i < 8; ++i) *(float2*)(outt + o[i]) = make_float2(re[i], im[i]);
             } else {
 #pragma unroll
-                for (int i = 0; i < 16; ++i) {
-                    uint32_t hl;
-                    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(hl) : "f"(0.f), "f"(v[i]));
-                    const float hf = __uint_as_float(hl << 16);
-                    uint32_t ll;
-                    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(ll) : "f"(0.f), "f"(v[i] - hf));
-                    *(uint16_t*)(sB + o[i]) = (uint16_t)hl;
-                    *(uint16_t*)(sB + bimg + o[i]) = (uint16_t)ll;
+                for (int i = 0; i < 8; ++i) {
+                    uint32_t hi, lo;
+                    split2_bf16(re[i], im[i], &hi, &lo);
+                    *(uint32_t*)(sB + o[i]) = hi;
+                    *(uint32_t*)(sB + bimg + o[i]) = lo;
                 }
             }
         }
@@ -330,86 +413,146 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused_pass(const __grid_consta
             }
         }
     };
-    auto wait_record = [&]() {
-        if (a_pending) {
-            if (!mbar_wait(mba, pha)) *s_err = 1;
-            pha ^= 1u;
-            a_pending = false;
-        }
-    };
 
-    int slot = 0, loads = 0;  // table slot of the current block's record; records issued so far
-    if ((ITYPE)blockIdx.x < a.tiles) {
-        if (tid == 0) bulk_load_block(aaddr, taddr, record(0), mba);
-        a_pending = true;
-        loads = 1;
+    fused_wait_record(S, P);  // block 0's record: its gather tables
+    __syncthreads();
+    if (*S.s_err) return false;
+    gather(P.slot);
+    if (next_pair >= 0) {  // the next pair's 256-byte runs into L2 while this pair's blocks run
+        const ITYPE T2 = (ITYPE)next_pair + (tid >= 256 ? pair_stride : 0);
+        const uint32_t r = (uint32_t)tid & 255u;
+        if (T2 < a.tiles && r < (tsize >> kFLow)) {
+            ITYPE off = 0;
+            for (int j = kFLow; j < m; ++j)
+                if ((r >> (j - kFLow)) & 1u) off |= 1ULL << a.q[j];
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], 256;" ::"l"(a.state + (tile_base(T2) | off))
+                         : "memory");
+        }
     }
+    for (int b = 0; b < a.nblocks; ++b) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        __syncthreads();
+        fused_wait_record(S, P);  // this block's A image and tables
+        if (tid == 0 && !*S.s_err) {
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            issue_mma(sB0, 0, S.mb0);
+            if (hasY) issue_mma(sB1, N, S.mb1);
+        }
+        const bool last = b + 1 == a.nblocks;
+        if (!mbar_wait(S.mb0, P.ph0)) *S.s_err = 1;
+        P.ph0 ^= 1u;
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        move(sB0, 0, P.slot, last);  // while Y's MMAs run
+        if (hasY) {
+            if (!mbar_wait(S.mb1, P.ph1)) *S.s_err = 1;
+            P.ph1 ^= 1u;
+            asm volatile("tcgen05.fence::after_thread_sync;");
+        }
+        __syncthreads();  // both MMAs done: A and the other table slot are free
+        if (*S.s_err) return false;
+        const int nxt = b + 1 < a.nblocks ? b + 1 : (next_pair >= 0 ? 0 : -1);
+        const bool reload = nxt >= 0 && nxt != b;  // a single-block pass keeps its record resident
+        const int cur = P.slot;
+        if (reload) fused_load_record(S, P, a, nxt, true);
+        if (hasY) move(sB1, N, cur, last);  // while the next record lands
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    store_out(TX, sB0);
+    if (hasY) store_out(TY, sB1);
+    __syncthreads();  // the next pair's gather overwrites the output tiles
+    return true;
+}
+
+__global__ void __launch_bounds__(kFThreads, 1) k_fused_pass(const __grid_constant__ FusedPassArgs a) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    const uint32_t N = (1u << a.m) >> kFBlock;
+    FusedSmem S = fused_setup(smem, 2 * N < 32 ? 32u : 2 * N);  // D_X at column 0, D_Y at column N
+    FusedPipe P;
+    if ((ITYPE)blockIdx.x < a.tiles) fused_load_record(S, P, a, 0, true);
     const ITYPE stride = 2 * (ITYPE)gridDim.x;
     for (ITYPE TX = blockIdx.x; TX < a.tiles; TX += stride) {
         const ITYPE TY = TX + gridDim.x;
-        const bool hasY = TY < a.tiles;
         const bool has_next = TX + stride < a.tiles;
-        wait_record();  // block 0's record: its gather tables
-        __syncthreads();
-        if (*s_err) break;
-        gather(TX, TY, hasY, slot);
-        if (has_next) {  // the next pair's 256-byte runs into L2 while this pair's blocks run
-            const ITYPE T2 = TX + stride + (tid >= 256 ? (ITYPE)gridDim.x : 0);
-            const uint32_t r = (uint32_t)tid & 255u;
-            if (T2 < a.tiles && r < (tsize >> kFLow)) {
-                ITYPE off = 0;
-                for (int j = kFLow; j < m; ++j)
-                    if ((r >> (j - kFLow)) & 1u) off |= 1ULL << a.q[j];
-                asm volatile("cp.async.bulk.prefetch.L2.global [%0], 256;" ::"l"(a.state + (tile_base(T2) | off))
-                             : "memory");
-            }
-        }
-        for (int b = 0; b < a.nblocks; ++b) {
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            asm volatile("tcgen05.fence::before_thread_sync;");
-            __syncthreads();
-            wait_record();  // this block's A image and tables
-            if (tid == 0 && !*s_err) {
-                asm volatile("tcgen05.fence::after_thread_sync;");
-                issue_mma(sB0, 0, mb0);
-                if (hasY) issue_mma(sB1, N, mb1);
-            }
-            const bool last = b + 1 == a.nblocks;
-            if (!mbar_wait(mb0, ph0)) *s_err = 1;
-            ph0 ^= 1u;
-            asm volatile("tcgen05.fence::after_thread_sync;");
-            move(sB0, 0, slot, last);  // while Y's MMAs run
-            if (hasY) {
-                if (!mbar_wait(mb1, ph1)) *s_err = 1;
-                ph1 ^= 1u;
-                asm volatile("tcgen05.fence::after_thread_sync;");
-            }
-            __syncthreads();  // both MMAs done: A and the other table slot are free
-            if (*s_err) break;
-            const int nxt = b + 1 < a.nblocks ? b + 1 : (has_next ? 0 : -1);
-            const int nslot = loads & 1;
-            const bool reload = nxt >= 0 && nxt != b;  // a single-block pass keeps its record resident
-            if (reload) {
-                if (tid == 0) bulk_load_block(aaddr, taddr + nslot * kTabBytes, record(nxt), mba);
-                a_pending = true;
-                ++loads;
-            }
-            if (hasY) move(sB1, N, slot, last);  // while the next record lands
-            if (reload) slot = nslot;
-        }
-        if (*s_err) break;
-        asm volatile("tcgen05.fence::before_thread_sync;");
-        __syncthreads();
-        store_out(TX, sB0);
-        if (hasY) store_out(TY, sB1);
-        __syncthreads();  // the next pair's gather overwrites the output tiles
+        if (!fused_pair(a, S, P, TX, TY, TY < a.tiles, has_next ? (long long)(TX + stride) : -1, gridDim.x)) break;
     }
-    if (a_pending && !mbar_wait(mba, pha)) *s_err = 1;  // no copy in flight at exit
-    if (tid == 0 && *s_err) atomicExch(a.err, 1);
-    asm volatile("tcgen05.fence::before_thread_sync;");
-    __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;");
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols));
+    fused_teardown(S, P, a.err);
+}
+
+// ---- many circuits in one persistent launch
+// Work records are (circuit, pass) in pass-round-robin order; a record's work items are its tile pairs
+// (tiles 2i and 2i + 1).  A CTA takes the next item with an atomic counter and, for a pass after a
+// circuit's first, waits until every tile of the circuit's previous pass is done (acquire load of that
+// record's counter, bounded by a %globaltimer deadline).  Items are handed out in queue order and a
+// dependency always points to an earlier record whose items resident CTAs already hold, so the wait
+// ends; on expiry the CTA records an error and leaves.
+struct FusedBatchRec {
+    FusedPassArgs args;  // state, records, m, q, nblocks, tiles
+    ITYPE prefix;        // first work item of this record
+    int dep;             // record of the circuit's previous pass, -1 for its first
+};
+
+__device__ __forceinline__ unsigned ld_acquire_u32_f(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ unsigned long long fused_global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+__global__ void __launch_bounds__(kFThreads, 1) k_fused_batch(const FusedBatchRec* __restrict__ recs, int nrec,
+    ITYPE total, unsigned long long* head, unsigned* done, int* err, unsigned long long wait_ns) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ ITYPE s_item;
+    __shared__ int s_rec, s_abort;
+    FusedSmem S = fused_setup(smem, 2 * kFNMax);
+    FusedPipe P;
+    const int tid = threadIdx.x;
+    while (true) {
+        if (tid == 0) {
+            s_abort = 0;
+            s_item = atomicAdd(head, 1ULL);
+            if (s_item < total) {
+                int lo = 0, hi = nrec - 1;  // last record with prefix <= item
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) / 2;
+                    if (recs[mid].prefix <= s_item) lo = mid;
+                    else hi = mid - 1;
+                }
+                s_rec = lo;
+                const int dep = recs[lo].dep;
+                if (dep >= 0) {
+                    const unsigned need = (unsigned)recs[dep].args.tiles;
+                    const unsigned long long t0 = fused_global_ns();
+                    while (ld_acquire_u32_f(done + dep) < need) {
+                        if (fused_global_ns() - t0 > wait_ns) {
+                            s_abort = 1;
+                            *S.s_err = 1;
+                            break;
+                        }
+                        __nanosleep(128);
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        if (s_item >= total || s_abort) break;
+        const FusedPassArgs a = recs[s_rec].args;
+        const ITYPE TX = 2 * (s_item - recs[s_rec].prefix), TY = TX + 1;
+        const bool hasY = TY < a.tiles;
+        fused_load_record(S, P, a, 0, true);
+        if (!fused_pair(a, S, P, TX, TY, hasY, -1, 0)) break;
+        if (tid == 0) {
+            __threadfence();
+            atomicAdd(done + s_rec, hasY ? 2u : 1u);
+        }
+    }
+    fused_teardown(S, P, err);
 }
 
 __device__ __forceinline__ void split_bf16(float v, __nv_bfloat16_raw* hi, __nv_bfloat16_raw* lo) {
@@ -639,8 +782,11 @@ static void choose_layouts(FusedPass& fp) {
         const std::vector<int> ks = order_with_prefix(bk, locals);
         std::copy(ks.begin(), ks.end(), b0.lay.k_src);
     }
-    // accumulator rows of block b: lanes 0..4 of a warp are rows y bits 0..4.  Pick the 5 row sources
-    // (of 6 block bits + part) and the next block's K / coset orders that minimise bank conflicts.
+    // accumulator rows of block b: lanes 0..4 of a warp are rows y bits 0..4.  Lane bit 0 is always the
+    // real/imaginary part, so lanes 2j and 2j + 1 hold the two parts of one output amplitude and the
+    // device stores them as one word (bf16x2, or float2 after the last block); pick the other 4 lane
+    // sources (of the 6 block bits) and the next block's K / coset orders that minimise the bank
+    // conflicts of those paired stores.
     for (size_t b = 0; b < fp.blocks.size(); ++b) {
         FusedBlock& cb = fp.blocks[b];
         const bool last = b + 1 == fp.blocks.size();
@@ -648,11 +794,12 @@ static void choose_layouts(FusedPass& fp) {
         const std::vector<int> ncos = last ? std::vector<int>() : coset_bits_of(*nb, m);
         int best = 1 << 30;
         BlockLayout best_next;
-        int best_rows[7] = {0, 1, 2, 3, 4, 5, 6};
-        for (int e1 = 0; e1 < 7; ++e1)
-            for (int e2 = e1 + 1; e2 < 7; ++e2) {
-                int rows[7], r = 0;
-                for (int s = 0; s < 7; ++s)
+        int best_rows[7] = {6, 0, 1, 2, 3, 4, 5};
+        for (int e1 = 0; e1 < kFBlock; ++e1)
+            for (int e2 = e1 + 1; e2 < kFBlock; ++e2) {
+                int rows[7], r = 1;
+                rows[0] = 6;
+                for (int s = 0; s < kFBlock; ++s)
                     if (s != e1 && s != e2) rows[r++] = s;
                 rows[5] = e1;
                 rows[6] = e2;
@@ -672,13 +819,22 @@ static void choose_layouts(FusedPass& fp) {
                 }
                 BlockLayout probe = cb.lay;
                 std::copy(rows, rows + 7, probe.row_src);
-                uint32_t words[32];
+                // one paired store instruction: lane l writes the amplitude of row pair l / 2 at column
+                // 0 (even lanes) or 8 (odd lanes); offsets are XOR-linear, so column 0 stands for all
+                const uint32_t u8 = coset_tile_index(cb.lay, 8);
+                uint32_t words[64];
+                int nwords = 0;
                 for (uint32_t lane = 0; lane < 32; ++lane) {
                     uint32_t part;
-                    const uint32_t u = row_tile_index(cb.bits, probe, lane, &part);
-                    words[lane] = last ? (2 * tswz(u) | part) : (b_operand_off(nb->bits, trial_next, u, part) >> 2);
+                    const uint32_t u = row_tile_index(cb.bits, probe, lane & ~1u, &part) ^ ((lane & 1) ? u8 : 0u);
+                    if (last) {  // float2 of (re, im): two words
+                        words[nwords++] = 2 * tswz(u);
+                        words[nwords++] = 2 * tswz(u) + 1;
+                    } else {     // bf16x2 of (re, im): one word
+                        words[nwords++] = b_operand_off(nb->bits, trial_next, u, 0) >> 2;
+                    }
                 }
-                const int cost = bank_degree(words, 32);
+                const int cost = bank_degree(words, nwords);
                 if (cost < best) {
                     best = cost;
                     std::copy(rows, rows + 7, best_rows);
@@ -830,10 +986,10 @@ struct FusedPlanDev {
     }
 };
 
-static size_t fused_smem_bytes(int m) {
-    const size_t tsize = size_t(1) << m, N = tsize >> kFBlock;
-    (void)tsize;
-    return 2 * kAImageBytes + 2 * (2 * N * 256) + 2 * kTabBytes + 64;  // A, two B / output tiles, tables, 3 mbarriers, TMEM slot, flag
+// Shared memory of a fused CTA: A (hi | lo), two B / output tiles laid out for the largest tile (every
+// pass uses the same layout), two table slots, 3 mbarriers, the TMEM slot and the error flag.
+static size_t fused_smem_bytes() {
+    return 2 * kAImageBytes + 2 * (2 * (size_t)kFNMax * 256) + 2 * kTabBytes + 64;
 }
 
 // The kernel's dynamic shared-memory limit is a process-wide attribute: set it once per device to
@@ -848,7 +1004,9 @@ static int fused_allow_smem() {
     if (dev < 0 || dev >= 64) return set_error(QS_ERR_NOT_SUPPORTED, "device index");
     if (!done[dev]) {
         QS_CUDA_CHECK(cudaFuncSetAttribute(k_fused_pass, cudaFuncAttributeMaxDynamicSharedMemorySize,
-            (int)fused_smem_bytes(kFTileMax)));
+            (int)fused_smem_bytes()));
+        QS_CUDA_CHECK(cudaFuncSetAttribute(k_fused_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            (int)fused_smem_bytes()));
         done[dev] = true;
     }
     return QS_OK;
@@ -904,16 +1062,18 @@ static int upload_fused_plan(Circuit& c, ITYPE dim, const FusedPlanHost& H, std:
 
 // Many circuits, each on its own complex64 state: the plans missing from the circuits' caches are
 // built on host threads in parallel (the FP64 block composition and layout search dominate a small
-// circuit's cost), then every circuit's passes are launched round-robin over kBatchStreams streams
-// forked from `st` (a small state occupies few SMs, so circuits run side by side), joined back into
-// `st`, and the completion-wait error flags are read once.
-constexpr int kBatchStreams = 8;
+// circuit's cost), then every circuit's passes run in ONE persistent launch of k_fused_batch (work
+// items: tile pairs of (circuit, pass) records in pass-round-robin order, bounded dependency waits),
+// with one error-flag read.
+constexpr unsigned long long kFusedBatchWaitNs = 2000000000ULL;
 
-int batch_update_fused_c64(Circuit* const* cs, void* const* states, UINT count, cudaStream_t st) {
+int batch_update_fused_c64(Circuit* const* cs, void* const* states, UINT count, cudaStream_t st,
+    unsigned long long wait_ns, int self_dep) {
     for (UINT i = 0; i < count; ++i) {
         if (!cs[i] || !states[i]) return set_error(QS_ERR_INVALID_ARGUMENT, "null circuit or state");
         if (cs[i]->n < 10) return set_error(QS_ERR_NOT_SUPPORTED, "fused path needs at least 10 qubits");
     }
+    if (count == 0) return QS_OK;
     // 1. host plans in parallel
     std::vector<FusedPlanHost> H(count);
     std::vector<int> rc(count, QS_OK), need(count, 0);
@@ -947,49 +1107,49 @@ int batch_update_fused_c64(Circuit* const* cs, void* const* states, UINT count, 
         else QS_TRY(fused_plan_dev(*cs[i], dim, &D[i]));
     }
     QS_TRY(fused_allow_smem());
-    // 3. launches over forked streams
-    cudaEvent_t fork = nullptr;
-    cudaStream_t ss[kBatchStreams] = {};
-    cudaEvent_t joins[kBatchStreams] = {};
-    int out = QS_OK;
-    if (cudaEventCreateWithFlags(&fork, cudaEventDisableTiming) != cudaSuccess || cudaEventRecord(fork, st) != cudaSuccess)
-        out = set_error(QS_ERR_CUDA, "batch fused: event setup failed");
-    for (int k = 0; k < kBatchStreams && out == QS_OK; ++k) {
-        if (cudaStreamCreateWithFlags(&ss[k], cudaStreamNonBlocking) != cudaSuccess ||
-            cudaEventCreateWithFlags(&joins[k], cudaEventDisableTiming) != cudaSuccess ||
-            cudaStreamWaitEvent(ss[k], fork, 0) != cudaSuccess)
-            out = set_error(QS_ERR_CUDA, "batch fused: stream setup failed");
-    }
-    for (UINT i = 0; i < count && out == QS_OK; ++i) {
-        cudaStream_t s = ss[i % kBatchStreams];
-        for (const FusedPassArgs& p0 : D[i]->passes) {
-            FusedPassArgs p = p0;
-            p.state = (float2*)states[i];
-            const unsigned grid = (unsigned)std::min<ITYPE>((p.tiles + 1) / 2, (ITYPE)sm_count());
-            k_fused_pass<<<grid, kFThreads, fused_smem_bytes(p.m), s>>>(p);
-            out = check_launch("k_fused_pass");
-            if (out != QS_OK) break;
+    // 3. work records, pass-round-robin over the circuits
+    size_t maxp = 0;
+    for (UINT i = 0; i < count; ++i) maxp = std::max(maxp, D[i]->passes.size());
+    std::vector<FusedBatchRec> recs;
+    std::vector<int> last(count, -1);
+    ITYPE total = 0;
+    for (size_t p = 0; p < maxp; ++p)
+        for (UINT i = 0; i < count; ++i) {
+            if (p >= D[i]->passes.size()) continue;
+            FusedBatchRec r{};
+            r.args = D[i]->passes[p];
+            r.args.state = (float2*)states[i];
+            r.prefix = total;
+            r.dep = last[i];
+            last[i] = (int)recs.size();
+            total += (r.args.tiles + 1) / 2;  // tile pairs
+            recs.push_back(r);
         }
+    if (recs.empty()) return QS_OK;
+    if (self_dep >= 0) {
+        if (self_dep >= (int)recs.size()) return set_error(QS_ERR_INVALID_ARGUMENT, "batch: no such work record");
+        recs[self_dep].dep = self_dep;
     }
-    for (int k = 0; k < kBatchStreams; ++k) {
-        if (ss[k]) {
-            if (joins[k]) {
-                cudaEventRecord(joins[k], ss[k]);
-                cudaStreamWaitEvent(st, joins[k], 0);
-                cudaEventDestroy(joins[k]);
-            }
-            cudaStreamDestroy(ss[k]);  // released once its work completes
-        }
-    }
-    if (fork) cudaEventDestroy(fork);
-    QS_TRY(out);
-    // 4. completion-wait flags, read once
-    std::vector<int> errs(count, 0);
-    for (UINT i = 0; i < count; ++i)
-        QS_CUDA_CHECK(cudaMemcpyAsync(&errs[i], D[i]->err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    const size_t brec = sizeof(FusedBatchRec) * recs.size(), bdone = sizeof(unsigned) * recs.size();
+    void* buf = nullptr;
+    QS_TRY(scratch(st, brec + bdone + 256, &buf));
+    FusedBatchRec* drec = (FusedBatchRec*)buf;
+    unsigned* ddone = (unsigned*)((char*)buf + brec);
+    unsigned long long* dhead = (unsigned long long*)((char*)buf + ((brec + bdone + 15) / 16 * 16));
+    int* derr = (int*)(dhead + 1);
+    QS_CUDA_CHECK(cudaMemcpyAsync(drec, recs.data(), brec, cudaMemcpyHostToDevice, st));
+    QS_CUDA_CHECK(cudaMemsetAsync(ddone, 0, (brec + bdone + 256) - brec, st));
+    int per_sm = 0;
+    QS_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fused_batch, kFThreads, fused_smem_bytes()));
+    const ITYPE resident = (ITYPE)std::max(1, per_sm) * sm_count();
+    const unsigned grid = (unsigned)std::min<ITYPE>(resident, total);
+    k_fused_batch<<<grid, kFThreads, fused_smem_bytes(), st>>>(drec, (int)recs.size(), total, dhead, ddone, derr,
+        wait_ns);
+    QS_TRY(check_launch("k_fused_batch"));
+    int err = 0;
+    QS_CUDA_CHECK(cudaMemcpyAsync(&err, derr, sizeof(int), cudaMemcpyDeviceToHost, st));
     QS_CUDA_CHECK(cudaStreamSynchronize(st));
-    for (UINT i = 0; i < count; ++i)
-        if (errs[i]) return set_error(QS_ERR_TIMEOUT, "fused pass: tensor-core completion wait expired");
+    if (err) return set_error(QS_ERR_TIMEOUT, "fused batch: a bounded wait expired");
     return QS_OK;
 }
 
@@ -1001,7 +1161,7 @@ int run_fused_c64(Circuit& c, void* state, ITYPE dim, cudaStream_t st) {
     for (const FusedPassArgs& p0 : D->passes) {
         FusedPassArgs p = p0;
         p.state = (float2*)state;
-        const size_t smem = fused_smem_bytes(p.m);
+        const size_t smem = fused_smem_bytes();
         const unsigned grid = (unsigned)std::min<ITYPE>((p.tiles + 1) / 2, (ITYPE)sm_count());  // tile pairs
         k_fused_pass<<<grid, kFThreads, smem, st>>>(p);
         QS_TRY(check_launch("k_fused_pass"));
@@ -1074,7 +1234,26 @@ QS_API int qs_batch_update_quantum_states_fused_c64(qs_circuit_t const* circuits
     QS_UINT count, void* stream) {
     if (!circuits || !states_c64) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "null argument");
     return qs::batch_update_fused_c64(reinterpret_cast<qs::Circuit* const*>(circuits), states_c64, count,
-        (cudaStream_t)stream);
+        (cudaStream_t)stream, qs::kFusedBatchWaitNs, -1);
+}
+
+// Failure-path check of the complex64 batch kernel's bounded dependency wait (the same construction as
+// qs_debug_batch_wait_expiry): `circuit` on `state_c64` as a one-circuit batch whose last pass waits on
+// its own completion counter, with the wait bounded by wait_limit_us.
+QS_API int qs_debug_batch_wait_expiry_fused_c64(qs_circuit_t circuit, void* state_c64, QS_UINT wait_limit_us,
+    void* stream) {
+    qs::Circuit* c = reinterpret_cast<qs::Circuit*>(circuit);
+    if (!c || !state_c64) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "null circuit or state");
+    if (wait_limit_us == 0 || wait_limit_us > 2000000u)
+        return qs::set_error(QS_ERR_INVALID_ARGUMENT, "wait limit must be 1 us .. 2 s");
+    if (c->n < 10) return qs::set_error(QS_ERR_NOT_SUPPORTED, "fused path needs at least 10 qubits");
+    qs::FusedPlanHost H;
+    QS_TRY(qs::fused_plan_host(*c, &H));
+    if (H.passes.empty()) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "circuit has no passes");
+    qs::Circuit* cs[1] = {c};
+    void* ss[1] = {state_c64};
+    return qs::batch_update_fused_c64(cs, ss, 1, (cudaStream_t)stream, 1000ULL * wait_limit_us,
+        (int)H.passes.size() - 1);
 }
 
 QS_API int qs_circuit_fused_block_export(qs_circuit_t circuit, QS_UINT index, QS_UINT* tile_qubits, int* tile_qubit_count,

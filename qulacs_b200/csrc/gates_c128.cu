@@ -114,6 +114,41 @@ __global__ void __launch_bounds__(kThreads) k_pair(
     }
 }
 
+// Two-qubit permutation (CNOT, SWAP) with a qubit below 5, where the pair enumeration of k_pair would
+// use every 32-byte sector at half: each CTA owns 1024 amplitudes -- tile bits 0..8 are qubits 0..8
+// and tile bit 9 is qubit `hq` (the pair's higher qubit when it is >= 9, else 9) -- loads them with
+// fully used 512-byte runs into shared memory, and writes back amplitude x the amplitude at
+// perm(x) (CNOT: x ^ t_bit when x has c_bit; SWAP: x with bits a, b exchanged).  Both qubits are tile
+// bits, so every pair lies inside one tile.  Requires dim >= 1024.
+constexpr int kPermTileBits = 10;
+__global__ void __launch_bounds__(kThreads) k_perm2_tile(double2* __restrict__ s, UINT hq, UINT ca, UINT tb, int swap) {
+    __shared__ double2 tile[1 << kPermTileBits];
+    // global index of tile index x: bits 0..8 in place, tile bit 9 -> qubit hq, the block index in the
+    // remaining bits (zeros inserted at 0..8 and at hq >= 9)
+    const ITYPE base = insert0((ITYPE)blockIdx.x << 9, hq);
+    auto gidx = [&](UINT x) { return base | (ITYPE)(x & 511u) | ((ITYPE)(x >> 9) << hq); };
+    const UINT tid = threadIdx.x;
+#pragma unroll
+    for (int k = 0; k < (1 << kPermTileBits) / kThreads; ++k) {
+        const UINT x = tid + (UINT)k * kThreads;
+        tile[x] = ld_stream(s + gidx(x));
+    }
+    __syncthreads();
+    // tile-local bit of a qubit: q itself below 9, 9 for hq
+    const UINT lc = ca == hq ? 9u : ca, lt = tb == hq ? 9u : tb;
+#pragma unroll
+    for (int k = 0; k < (1 << kPermTileBits) / kThreads; ++k) {
+        const UINT x = tid + (UINT)k * kThreads;
+        UINT y = x;
+        if (swap) {
+            if (((x >> lc) ^ (x >> lt)) & 1u) y = x ^ (1u << lc) ^ (1u << lt);
+        } else if ((x >> lc) & 1u) {
+            y = x ^ (1u << lt);
+        }
+        st_stream(s + gidx(x), tile[y]);
+    }
+}
+
 // Uncontrolled 2x2 on a target t < 5: lane-local amplitudes, partner through shuffles.
 // Requires dim to be a multiple of kThreads * ITEMS.
 template <int ITEMS>
@@ -704,6 +739,11 @@ QS_API int qs_CNOT_gate(QS_UINT c, QS_UINT t, STATE_ARGS) {
     QS_TRY(check_dim(dim, &n));
     const UINT l[2] = {c, t};
     QS_TRY(check_distinct(l, 2, n, "CNOT_gate"));
+    if (std::min(c, t) < 5 && dim >= (1ULL << kPermTileBits)) {
+        const UINT hq = std::max(std::max(c, t), 9u);
+        k_perm2_tile<<<(unsigned)(dim >> kPermTileBits), kThreads, 0, ST>>>(S2, hq, c, t, 0);
+        return check_launch("k_perm2_tile<CNOT>");
+    }
     const ITYPE cm = 1ULL << c;
     const ITYPE items = dim >> 2;
     k_pair<OpSwap, 2><<<blocks_for(items, kThreads * 2), kThreads, 0, ST>>>(
@@ -722,6 +762,11 @@ QS_API int qs_SWAP_gate(QS_UINT a, QS_UINT b, STATE_ARGS) {
     QS_TRY(check_dim(dim, &n));
     const UINT l[2] = {a, b};
     QS_TRY(check_distinct(l, 2, n, "SWAP_gate"));
+    if (std::min(a, b) < 5 && dim >= (1ULL << kPermTileBits)) {
+        const UINT hq = std::max(std::max(a, b), 9u);
+        k_perm2_tile<<<(unsigned)(dim >> kPermTileBits), kThreads, 0, ST>>>(S2, hq, a, b, 1);
+        return check_launch("k_perm2_tile<SWAP>");
+    }
     const ITYPE items = dim >> 2;
     k_pair<OpSwap, 2><<<blocks_for(items, kThreads * 2), kThreads, 0, ST>>>(
         S2, items, make_positions({a, b}), 1ULL << a, 1ULL << b, OpSwap{});

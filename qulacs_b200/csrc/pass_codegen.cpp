@@ -111,6 +111,13 @@ __device__ __forceinline__ D2 ldcs(const D2* p) {
 __device__ __forceinline__ void stcs(D2* p, D2 v) {
     asm volatile("st.global.cs.v2.f64 [%0], {%1, %2};" ::"l"(p), "d"(v.x), "d"(v.y) : "memory");
 }
+// A parameter read at its use (volatile: not hoisted out of the coset loop, where every parameter of
+// the pass would stay live in registers).
+__device__ __forceinline__ D2 ldp(const D2* p) {
+    D2 v;
+    asm volatile("ld.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p));
+    return v;
+}
 __device__ __forceinline__ unsigned swz(unsigned u) { return u ^ (((u >> 4) ^ (u >> 7) ^ (u >> 10)) & 7u); }
 __device__ __forceinline__ u64 ins0(u64 i, unsigned q) { return ((i >> q) << (q + 1)) | (i & ((1ULL << q) - 1ULL)); }
 
@@ -186,6 +193,25 @@ template <int A, int B> __device__ __forceinline__ void r_dense2(D2 (&r)[16], co
             }
         }
 }
+// r_dense2 with the matrix read from a parameter block at each use (volatile loads: only the entries
+// of the row being computed are live).
+template <int A, int B> __device__ __forceinline__ void r_dense2p(D2 (&r)[16], const D2* p) {
+#pragma unroll
+    for (int j = 0; j < 16; ++j)
+        if (!(j & (1 << A)) && !(j & (1 << B))) {
+            const int o[4] = {j, j | (1 << A), j | (1 << B), j | (1 << A) | (1 << B)};
+            D2 v[4];
+#pragma unroll
+            for (int x = 0; x < 4; ++x) v[x] = r[o[x]];
+#pragma unroll
+            for (int y = 0; y < 4; ++y) {
+                D2 acc = cmul(ldp(p + y * 4), v[0]);
+#pragma unroll
+                for (int x = 1; x < 4; ++x) acc = cfma(ldp(p + y * 4 + x), v[x], acc);
+                r[o[y]] = acc;
+            }
+        }
+}
 template <int A, int B> __device__ __forceinline__ void r_csel1(D2 (&r)[16], D2 m0, D2 m1, D2 m2, D2 m3, D2 n0, D2 n1,
                                                                 D2 n2, D2 n3) {
 #pragma unroll
@@ -230,7 +256,17 @@ std::string lit(double v) {
     std::snprintf(buf, sizeof(buf), "%a", v);
     return buf;
 }
-std::string d2(const double2& v) { return "mk(" + lit(v.x) + ", " + lit(v.y) + ")"; }
+// Gate parameters of a generated kernel: written into the source as literals, or (when `bank` is set)
+// referenced as P.v[i] of the kernel's __grid_constant__ parameter block and collected into `bank`, so
+// the kernel depends only on the pass's structure and is shared by circuits that differ in angles.
+struct ParamSink {
+    std::vector<double2>* bank = nullptr;
+    std::string d2(const double2& v) {
+        if (!bank) return "mk(" + lit(v.x) + ", " + lit(v.y) + ")";
+        bank->push_back(v);
+        return "ldp(&P.v[" + std::to_string(bank->size() - 1) + "])";
+    }
+};
 
 std::string u64hex(ITYPE v) {
     char buf[40];
@@ -242,21 +278,31 @@ int gray_bit(int g) { return (g & 1) ? 0 : (g & 2) ? 1 : (g & 4) ? 2 : 3; }
 
 unsigned swz_host(unsigned u) { return u ^ (((u >> 4) ^ (u >> 7) ^ (u >> 10)) & 7u); }
 
-void emit_op(std::ostringstream& o, const StOp& op, const double2* pool) {
+void emit_op(std::ostringstream& o, const StOp& op, const double2* pool, ParamSink& ps) {
     const double2* p = pool + op.param;
     const int a = op.a, b = op.b;
+    auto d2 = [&](const double2& v) { return ps.d2(v); };
     switch (op.kind) {
         case ST_DENSE1:
             o << "      r_dense1<" << a << ">(r, " << d2(p[0]) << ", " << d2(p[1]) << ", " << d2(p[2]) << ", " << d2(p[3])
               << ");\n";
             break;
         case ST_DIAG1: o << "      r_diag1<" << a << ">(r, " << d2(p[0]) << ", " << d2(p[1]) << ");\n"; break;
-        case ST_RX: o << "      r_rx<" << a << ">(r, " << lit(p[0].x) << ", " << lit(p[0].y) << ");\n"; break;
-        case ST_RY: o << "      r_ry<" << a << ">(r, " << lit(p[0].x) << ", " << lit(p[0].y) << ");\n"; break;
+        case ST_RX:
+        case ST_RY:
+            o << "      { const D2 cs = " << d2(p[0]) << "; r_" << (op.kind == ST_RX ? "rx" : "ry") << "<" << a
+              << ">(r, cs.x, cs.y); }\n";
+            break;
         case ST_CNOT: o << "      r_cnot<" << a << ", " << b << ">(r);\n"; break;
         case ST_CZ: o << "      r_cz<" << a << ", " << b << ">(r);\n"; break;
         case ST_SWAP: o << "      r_swap<" << a << ", " << b << ">(r);\n"; break;
         case ST_DENSE2: {
+            if (ps.bank) {  // the 16 entries as one run of the parameter block, read row by row
+                const size_t first = ps.bank->size();
+                for (int i = 0; i < 16; ++i) ps.bank->push_back(p[i]);
+                o << "      r_dense2p<" << a << ", " << b << ">(r, &P.v[" << first << "]);\n";
+                break;
+            }
             o << "      { const D2 m[16] = {";
             for (int i = 0; i < 16; ++i) o << (i ? ", " : "") << d2(p[i]);
             o << "}; r_dense2<" << a << ", " << b << ">(r, m); }\n";
@@ -276,15 +322,22 @@ void emit_op(std::ostringstream& o, const StOp& op, const double2* pool) {
     }
 }
 
-// CUDA C of one pass; mirrors staged_tile (staged.cu) with every schedule quantity a constant.
-std::string pass_source(const PassDesc& d) {
+// Largest parameter block passed to a kernel (within the classic 4 KB kernel-parameter space, with
+// room for the state pointer); a pass with more parameters gets them as literals instead.
+constexpr size_t kMaxParamBytes = 4000;
+
+// CUDA C of one pass; mirrors staged_tile (staged.cu) with every schedule quantity a constant.  With
+// `params`, gate parameters come from the kernel's parameter block (their values appended to *params);
+// without, they are literals.
+std::string pass_source(const PassDesc& d, std::vector<double2>* params) {
     const int m = d.m;
     const unsigned tsize = 1u << m, ncos = tsize >> kPhaseBits;
     const bool hbm_first = d.io & 1, hbm_last = (d.io >> 1) & 1;
     const int rows = 1 << (m - 7);  // tile rows of kStThreads amplitudes
-    std::ostringstream o;
-    o << kPrelude;
-    o << "extern \"C\" __global__ void __launch_bounds__(" << kStThreads << ", 3) k_pass_spec(D2* __restrict__ s) {\n";
+    ParamSink ps;
+    ps.bank = params;
+    std::ostringstream o;  // kernel body (the parameter block's size is known once it is written)
+    o << ") {\n";
     o << "  extern __shared__ D2 tile[];\n  char* tb = reinterpret_cast<char*>(tile);\n";
     o << "  const unsigned tid = threadIdx.x;\n  u64 base = blockIdx.x;\n";
     for (int j = 0; j < m; ++j) o << "  base = ins0(base, " << d.q[j] << "u);\n";
@@ -332,7 +385,7 @@ std::string pass_source(const PassDesc& d) {
             }
             o << "    }\n";
         }
-        for (uint32_t i = 0; i < P.op_count; ++i) emit_op(o, d.ops[P.op_begin + i], d.pool);
+        for (uint32_t i = 0; i < P.op_count; ++i) emit_op(o, d.ops[P.op_begin + i], d.pool, ps);
         if (to_hbm) {
             o << "    { u64 gi = g0;\n";
             for (int g = 0; g < 16; ++g) {
@@ -364,12 +417,18 @@ std::string pass_source(const PassDesc& d) {
         o << "      stcs(s + (base | lo | hi), v[k]);\n    }\n  }\n";
     }
     o << "}\n";
-    return o.str();
+    std::ostringstream h;
+    h << kPrelude;
+    if (params) h << "struct PassParams { D2 v[" << std::max<size_t>(1, params->size()) << "]; };\n";
+    h << "extern \"C\" __global__ void __launch_bounds__(" << kStThreads << ", 3) k_pass_spec(D2* __restrict__ s";
+    if (params) h << ", const __grid_constant__ PassParams P";
+    return h.str() + o.str();
 }
 
 struct Compiled {
     cudaLibrary_t lib = nullptr;
     cudaKernel_t kernel = nullptr;
+    bool has_params = false;  // takes a parameter block after the state pointer
     std::set<int> smem_set;  // devices on which the dynamic shared-memory limit is raised
 };
 
@@ -403,10 +462,17 @@ int compile(const std::string& src, std::vector<char>* cubin) {
 
 }  // namespace
 
-int specialized_pass_kernel(const PassDesc& d, void** kernel, double* compile_ms) {
+int specialized_pass_kernel(const PassDesc& d, void** kernel, std::vector<double2>* params, double* compile_ms) {
     if (d.m < 7 || d.m > kTileBits || d.phases.empty())
         return set_error(QS_ERR_NOT_SUPPORTED, "specialised passes need 7..12 tile qubits and a phase");
-    const std::string src = pass_source(d);
+    params->clear();
+    std::string src = pass_source(d, params);
+    if (params->empty() || params->size() * sizeof(double2) > kMaxParamBytes) {
+        // no parameters (the kernel takes only the state), or too many for a parameter block: literals
+        params->clear();
+        src = pass_source(d, nullptr);
+    }
+    const bool has_params = !params->empty();
     std::shared_ptr<std::mutex> build_mu;
     {
         std::lock_guard<std::mutex> lk(g_mu);
@@ -438,6 +504,7 @@ int specialized_pass_kernel(const PassDesc& d, void** kernel, double* compile_ms
     cudaError_t e = cudaLibraryLoadData(&C->lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0);
     if (e != cudaSuccess) return check_cuda(e, "cudaLibraryLoadData (specialised pass)");
     e = cudaLibraryGetKernel(&C->kernel, C->lib, "k_pass_spec");
+    C->has_params = has_params;
     if (e != cudaSuccess) return check_cuda(e, "cudaLibraryGetKernel (specialised pass)");
     if (compile_ms)
         *compile_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -448,7 +515,7 @@ int specialized_pass_kernel(const PassDesc& d, void** kernel, double* compile_ms
     return QS_OK;
 }
 
-int launch_specialized_pass(void* handle, double2* state, ITYPE tiles, int m, cudaStream_t st) {
+int launch_specialized_pass(void* handle, double2* state, const double2* params, ITYPE tiles, int m, cudaStream_t st) {
     Compiled* C = static_cast<Compiled*>(handle);
     const size_t smem = sizeof(double2) << m;
     int dev = 0;
@@ -464,12 +531,16 @@ int launch_specialized_pass(void* handle, double2* state, ITYPE tiles, int m, cu
             C->smem_set.insert(dev);
         }
     }
-    void* args[] = {&state};
+    void* args[] = {&state, const_cast<double2*>(params)};  // the parameter block is copied at launch
+    if (C->has_params && !params) return set_error(QS_ERR_INVALID_ARGUMENT, "specialised pass: no parameter block");
     e = cudaLaunchKernel((const void*)C->kernel, dim3((unsigned)tiles), dim3(kStThreads), args, smem, st);
     if (e != cudaSuccess) return check_cuda(e, "k_pass_spec launch");
     return check_launch("k_pass_spec");
 }
 
-std::string specialized_pass_source(const PassDesc& d) { return pass_source(d); }
+std::string specialized_pass_source(const PassDesc& d) {
+    std::vector<double2> params;
+    return pass_source(d, &params);
+}
 
 }  // namespace qs

@@ -503,6 +503,7 @@ struct DevPass {
     StPassArgs args;
     size_t phase_begin = 0;  // the pass's phases in StagedPlan::phases
     void* spec = nullptr;    // specialised kernel of this pass (pass_codegen.cpp), if compiled
+    std::vector<double2> spec_params;  // its parameter block
 };
 
 static void launch_pass(double2* state, const DevPass& d, ITYPE tiles, cudaStream_t st) {
@@ -852,7 +853,8 @@ static int run_plan(const std::vector<GateRec>& gates, const StagedPlan& P, void
         }
         const ITYPE tiles = dim >> d.args.m;
         if (d.spec) {
-            QS_TRY(launch_specialized_pass(d.spec, (double2*)state, tiles, d.args.m, st));
+            QS_TRY(launch_specialized_pass(d.spec, (double2*)state, d.spec_params.empty() ? nullptr : d.spec_params.data(),
+                tiles, d.args.m, st));
             continue;
         }
         launch_pass((double2*)state, d, tiles, st);
@@ -881,6 +883,7 @@ static int specialize_plan(StagedPlan& P) {
     for (size_t i = 0; i < P.passes.size(); ++i)
         if (!P.passes[i].single && P.passes[i].args.nphases > 0) todo.push_back(i);
     std::vector<void*> handles(P.passes.size(), nullptr);
+    std::vector<std::vector<double2>> params(P.passes.size());
     std::vector<int> rcs(P.passes.size(), QS_OK);
     std::vector<std::string> errs(P.passes.size());
     std::atomic<size_t> next{0};
@@ -891,14 +894,17 @@ static int specialize_plan(StagedPlan& P) {
         pool.emplace_back([&] {
             for (size_t j; (j = next.fetch_add(1)) < todo.size();) {
                 const size_t i = todo[j];
-                rcs[i] = specialized_pass_kernel(pass_desc(P, P.passes[i]), &handles[i], nullptr);
+                rcs[i] = specialized_pass_kernel(pass_desc(P, P.passes[i]), &handles[i], &params[i], nullptr);
                 if (rcs[i] != QS_OK) errs[i] = qs_get_last_error();
             }
         });
     for (std::thread& t : pool) t.join();
     for (size_t i : todo)
         if (rcs[i] != QS_OK) return set_error(rcs[i], errs[i]);
-    for (size_t i : todo) P.passes[i].spec = handles[i];
+    for (size_t i : todo) {
+        P.passes[i].spec = handles[i];
+        P.passes[i].spec_params = std::move(params[i]);
+    }
     P.specialized = true;
     P.compile_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return QS_OK;
@@ -953,6 +959,7 @@ static int estimate_plan_ms(const std::vector<GateRec>& gates, const StagedPlan&
     QS_TRY(staged_allow_smem());
     // specialised kernels of the remapped passes, compiled on host threads in parallel
     std::vector<void*> spec(P.passes.size(), nullptr);
+    std::vector<std::vector<double2>> sparams(P.passes.size());
     if (specialized) {
         std::vector<size_t> todo;
         for (size_t i = 0; i < P.passes.size(); ++i)
@@ -969,7 +976,7 @@ static int estimate_plan_ms(const std::vector<GateRec>& gates, const StagedPlan&
                     const size_t i = todo[j];
                     PassDesc pd = pass_desc(P, P.passes[i]);
                     for (int b = 0; b < pd.m; ++b) pd.q[b] = (UINT)b;
-                    rcs[i] = specialized_pass_kernel(pd, &spec[i], nullptr);
+                    rcs[i] = specialized_pass_kernel(pd, &spec[i], &sparams[i], nullptr);
                     if (rcs[i] != QS_OK) errs[i] = qs_get_last_error();
                 }
             });
@@ -998,7 +1005,9 @@ static int estimate_plan_ms(const std::vector<GateRec>& gates, const StagedPlan&
         DevPass dt = d;
         dt.args = a;
         auto launch = [&]() -> int {
-            if (spec[i]) return launch_specialized_pass(spec[i], (double2*)buf, tt, a.m, st);
+            if (spec[i])
+                return launch_specialized_pass(spec[i], (double2*)buf, sparams[i].empty() ? nullptr : sparams[i].data(),
+                    tt, a.m, st);
             launch_pass((double2*)buf, dt, tt, st);
             return check_launch("k_staged_pass");
         };

@@ -46,12 +46,15 @@ struct PassDesc {
     const double2* pool = nullptr;
 };
 
-// csrc/pass_codegen.cpp: a kernel for one pass with its tile qubits, phase bits and gate parameters
-// compiled in (NVRTC, sm_100a), cached by source for the life of the process.  `handle` receives the
+// csrc/pass_codegen.cpp: a kernel for one pass with its tile qubits, phase bits and op list compiled
+// in (NVRTC, sm_100a), cached by source for the life of the process.  `handle` receives the
 // cache entry (valid until exit), launched over dim >> m CTAs of kStThreads threads with 16 << m bytes
 // of dynamic shared memory.  QS_ERR_NOT_SUPPORTED when NVRTC cannot be loaded.
-int specialized_pass_kernel(const PassDesc& d, void** handle, double* compile_ms);
-int launch_specialized_pass(void* handle, double2* state, ITYPE tiles, int m, cudaStream_t st);
+// The kernel depends only on the pass's structure: its gate parameters are a kernel-parameter block
+// whose values `params` receives (empty when the pass has too many and they are literals instead), to
+// be passed at every launch.
+int specialized_pass_kernel(const PassDesc& d, void** handle, std::vector<double2>* params, double* compile_ms);
+int launch_specialized_pass(void* handle, double2* state, const double2* params, ITYPE tiles, int m, cudaStream_t st);
 std::string specialized_pass_source(const PassDesc& d);
 
 }  // namespace qs

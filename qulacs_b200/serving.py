@@ -15,7 +15,12 @@ multi-circuit launch plus ONE batched <P> launch; sampling and density-matrix re
 Work of different workers overlaps on the device.  Latency = completion - arrival, per request.
 
 ``precision="c64"`` runs expectation and sampling requests on the fused complex64 tensor-core path
-(reductions in FP64); density-matrix requests stay complex128.
+(reductions in FP64): a batch of expectation requests is one persistent fused launch plus one batched
+<P> launch; density-matrix requests stay complex128.
+
+Served circuits run the generic staged pass kernel, not specialised per-pass kernels: every request
+brings new gate parameters, and compiling a kernel for each would add its compile time to the
+request's latency.
 """
 from __future__ import annotations
 
@@ -51,6 +56,8 @@ class Request:
     arrival: float = 0.0    # seconds after the start of the run
     result: object = None
     t_admit: float = 0.0
+    t_start: float = 0.0    # a worker began its device work
+    batch_id: int = -1      # the worker batch that ran it
     t_done: float = 0.0
 
     def footprint(self, precision: str) -> int:
@@ -170,28 +177,19 @@ class ServingLoop:
         self.outstanding = 0
         self.error = None
         self.batches = []        # sizes of the expectation batches that ran
+        self.nbatches = 0        # worker batches of any kind started
 
     # ---- work execution (worker threads; each has its own stream) ----
     def _run_expectation_batch(self, reqs, stream):
         circs = [W.to_circuit(r.gates, r.n) for r in reqs]
-        if self.precision == "c64":
-            for r, c in zip(reqs, circs):
-                call("qs_initialize_quantum_state_c64", r.ptr, 1 << r.n, stream)
-                call("qs_circuit_update_quantum_state_fused_c64", c._h, r.ptr, 1 << r.n, stream)
-                xm, zm, ny = zip(*[masks(tl, ids) for _, tl, ids in r.terms])
-                vals = np.zeros(len(r.terms))
-                xa, za = np.array(xm, dtype=np.uint64), np.array(zm, dtype=np.uint64)
-                ya = np.array(ny, dtype=np.uint32)
-                call("qs_expectation_value_pauli_batch_c64", _vp(xa), _vp(za), _vp(ya), len(r.terms), r.ptr,
-                     1 << r.n, stream, _vp(vals))
-                r.result = float(np.dot([c for c, _, _ in r.terms], vals))
-            return
         k = len(reqs)
+        c64 = self.precision == "c64"
         for r in reqs:
-            call("qs_initialize_quantum_state", r.ptr, 1 << r.n, stream)
+            call("qs_initialize_quantum_state_c64" if c64 else "qs_initialize_quantum_state", r.ptr, 1 << r.n, stream)
         ch = (C.c_void_p * k)(*[c._h for c in circs])
         st = (C.c_void_p * k)(*[r.ptr for r in reqs])
-        call("qs_batch_update_quantum_states", ch, st, k, stream)
+        call("qs_batch_update_quantum_states_fused_c64" if c64 else "qs_batch_update_quantum_states", ch, st, k,
+             stream)
         xm, zm, ny, offs, coefs = [], [], [], [0], []
         for r in reqs:
             for c, tl, ids in r.terms:
@@ -205,7 +203,8 @@ class ServingLoop:
         xa, za = np.array(xm, dtype=np.uint64), np.array(zm, dtype=np.uint64)
         ya, oa = np.array(ny, dtype=np.uint32), np.array(offs, dtype=np.uint32)
         qa = np.array([r.n for r in reqs], dtype=np.uint32)
-        call("qs_batch_expectation_values", st, _vp(qa), k, _vp(oa), _vp(xa), _vp(za), _vp(ya), _vp(vals), stream)
+        call("qs_batch_expectation_values_c64" if c64 else "qs_batch_expectation_values", st, _vp(qa), k, _vp(oa),
+             _vp(xa), _vp(za), _vp(ya), _vp(vals), stream)
         coefs = np.array(coefs)
         for j, r in enumerate(reqs):
             r.result = float(np.dot(coefs[offs[j]:offs[j + 1]], vals[offs[j]:offs[j + 1]]))
@@ -221,6 +220,7 @@ class ServingLoop:
         else:
             call("qs_initialize_quantum_state", r.ptr, 1 << r.n, stream)
             c.set_fusion(SERVE_FUSION_K)
+            c.set_specialized(0)
             call("qs_circuit_update_quantum_state", c._h, r.ptr, 1 << r.n, EXEC_STAGED_FUSED, stream)
             call("qs_state_sampling_with_uniforms", r.ptr, 1 << r.n, _vp(u), u.size, _vp(out), stream)
         r.result = out
@@ -230,6 +230,7 @@ class ServingLoop:
         dim = 1 << r.n
         call("qs_dm_initialize_quantum_state", r.ptr, dim, stream)
         c.set_fusion(SERVE_FUSION_K)
+        c.set_specialized(0)
         call("qs_circuit_update_density_matrix", c._h, r.ptr, dim, EXEC_STAGED_FUSED, stream)
         e = 0.0
         for coef, tl, ids in r.terms:
@@ -261,6 +262,13 @@ class ServingLoop:
                         batch = [head]
                     for r in batch:
                         self.ready.remove(r)
+                start = time.perf_counter() - t0
+                with self.cv:
+                    bid = self.nbatches
+                    self.nbatches += 1
+                for r in batch:
+                    r.t_start = start
+                    r.batch_id = bid
                 stream = hi.value if max(r.fp for r in batch) <= SMALL_REQUEST_BYTES else lo.value
                 try:
                     if batch[0].kind == "expectation":
@@ -343,9 +351,16 @@ class ServingLoop:
             if lk.size:
                 by_kind[k] = {"count": int(lk.size), "p50_ms": float(np.percentile(lk, 50) * 1e3),
                               "p99_ms": float(np.percentile(lk, 99) * 1e3)}
+        # device work in flight: time-average number of worker batches between their start and completion
+        spans = {}
+        for r in requests:
+            spans[r.batch_id] = (r.t_start, r.t_done)
+        busy = sum(d - s for s, d in spans.values())
         return {"jobs": len(requests), "wall_s": wall, "jobs_per_s": len(requests) / wall if wall else 0.0,
                 "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
-                "mean_batch": float(np.mean(self.batches)) if self.batches else 0.0, "by_kind": by_kind}
+                "mean_batch": float(np.mean(self.batches)) if self.batches else 0.0,
+                "max_batch": int(max(self.batches)) if self.batches else 0,
+                "mean_batches_in_flight": busy / wall if wall else 0.0, "by_kind": by_kind}
 
     def close(self):
         self.arena.close()

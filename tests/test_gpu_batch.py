@@ -130,3 +130,47 @@ def test_dependency_wait_expires_and_context_stays_usable(port):
     from qulacs_b200._lib import call
     call("qs_batch_update_quantum_states", (C.c_void_p * 1)(circ._h), (C.c_void_p * 1)(ok.data_ptr()), 1, None)
     assert np.max(np.abs(ok.get_vector() - psi)) <= 1e-12
+
+
+def test_fused_c64_dependency_wait_expires_and_context_stays_usable(port):
+    """The persistent complex64 batch kernel's bounded dependency wait, made to run out (last pass waits on
+    its own counter, 1 ms limit): QS_ERR_TIMEOUT, no hang or fault, TMEM released; then a normal fused
+    batch on the same context meets the infidelity bar."""
+    from qulacs_b200 import QuantumStateC64
+    from qulacs_b200._lib import load
+    lib = load()
+    n = 14
+    gates = W.hea_circuit(n, 10, seed=78)
+    circ = W.to_circuit(gates, n)
+    s = QuantumStateC64(n)
+    rc = lib.qs_debug_batch_wait_expiry_fused_c64(circ._h, s.data_ptr(), 1000, None)
+    assert rc == 4, lib.qs_get_last_error()  # QS_ERR_TIMEOUT
+    psi = np.zeros(1 << n, dtype=np.complex128)
+    psi[0] = 1
+    R.run_on_cpu(gates, psi, port)
+    ok = QuantumStateC64(n)
+    import ctypes as C
+    from qulacs_b200._lib import call
+    call("qs_batch_update_quantum_states_fused_c64", (C.c_void_p * 1)(circ._h), (C.c_void_p * 1)(ok.data_ptr()),
+         1, None)
+    ref = QuantumState(n)
+    ref.load(psi)
+    assert ok.infidelity(ref) <= 1e-6
+
+
+def test_fused_c64_persistent_batch_equals_each_circuit_alone():
+    """The persistent complex64 batch kernel applies each circuit's passes to its own state exactly as the
+    single-circuit fused kernel does (same block records, same per-tile arithmetic): uneven sizes 10..20,
+    several passes each, bit-identical states."""
+    import ctypes as C
+    from qulacs_b200 import QuantumStateC64
+    from qulacs_b200._lib import call
+    sizes = [10, 14, 11, 20, 13, 16, 10, 18]
+    circs = [W.to_circuit(W.hea_circuit(n, 6 + i % 5, seed=8800 + i), n) for i, n in enumerate(sizes)]
+    batch = [QuantumStateC64(n) for n in sizes]
+    call("qs_batch_update_quantum_states_fused_c64", (C.c_void_p * len(circs))(*[c._h for c in circs]),
+         (C.c_void_p * len(batch))(*[s.data_ptr() for s in batch]), len(circs), None)
+    for c, n, b in zip(circs, sizes, batch):
+        alone = QuantumStateC64(n)
+        c.update_quantum_state(alone)
+        assert np.array_equal(b.get_vector(), alone.get_vector()), n

@@ -86,6 +86,22 @@ def test_two_qubit_named_all_pairs(port):
                 assert np.max(np.abs(s.get_vector() - want)) == 0.0, (name, c, t)
 
 
+@pytest.mark.parametrize("n", [10, 13])
+def test_low_qubit_permutations_tile_kernel(port, n):
+    """CNOT and SWAP with a qubit below 5 on states of >= 2^10 amplitudes run the shared-memory tile
+    kernel (full-sector accesses): every pair with a low qubit, including partners 9 and n - 1."""
+    rng = np.random.default_rng(310 + n)
+    s0 = random_state(n, rng)
+    pairs = [(c, t) for c in range(n) for t in range(n) if c != t and min(c, t) < 5]
+    for c, t in pairs:
+        for name in ("CNOT", "SWAP"):
+            want = s0.copy()
+            getattr(port, name + "_gate")(c, t, want)
+            s = dev(s0)
+            call(f"qs_{name}_gate", c, t, s.data_ptr(), s.dim, None)
+            assert np.max(np.abs(s.get_vector() - want)) == 0.0, (name, c, t)
+
+
 @pytest.mark.parametrize("k", [2, 3, 4, 5, 6])
 def test_multi_qubit_dense(port, k):
     rng = np.random.default_rng(400 + k)

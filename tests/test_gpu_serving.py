@@ -24,6 +24,12 @@ def test_mix_equals_alone(port, precision):
     finally:
         loop.close()
     assert stats["jobs"] == 30 and stats["p99_ms"] >= stats["p50_ms"] > 0
+    # continuous batching happened: some expectation batch held several requests, and requests of
+    # different worker batches were on the device at the same time
+    assert stats["max_batch"] > 1, stats
+    overlapping = [(a.rid, b.rid) for a in reqs for b in reqs
+                   if a.batch_id != b.batch_id and a.t_start < b.t_done and b.t_start < a.t_done]
+    assert overlapping, "no two worker batches overlapped in time"
     for r in reqs:
         alone = run_alone(r, precision)
         if r.kind == "sampling":
