@@ -717,7 +717,7 @@ def main():
     kernels = kernel_table(state, n, stream) if not args.no_kernel_table else None
 
     # end to end through the public API: host gate list already built into the circuit, observable
-    # masks and uniforms from host, results (term values + samples) back to the host
+    # masks, coefficients and uniforms from host, results (energy + samples) back to the host
     e2e_steps = max(1, min(args.steps, 3))
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -733,8 +733,8 @@ def main():
         t = torch.tensor([e2e_ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
-    h2d = N_TERMS * (8 + 8 + 4) + N_SHOTS * 8 + len(gates) * 64
-    d2h = N_TERMS * 8 + N_SHOTS * 8
+    h2d = N_TERMS * (8 + 8 + 4 + 16) + N_SHOTS * 8 + len(gates) * 64  # masks, Y counts, coefficients
+    d2h = 16 + N_SHOTS * 8  # the complex energy and the samples
     # draws of the last e2e sampling call within 1e-12 of a cumulative boundary (outside the timed region)
     boundary_draws = state.sampling_boundary_draws(N_SHOTS, SHOT_SEED + e2e_steps - 1, 1e-12)
 

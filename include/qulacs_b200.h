@@ -272,6 +272,36 @@ QS_API int qs_expectation_value_pauli_batch(const QS_ITYPE* x_masks, const QS_IT
     const QS_UINT* y_counts, QS_UINT term_count, const void* state, QS_ITYPE dim, void* stream,
     double* values);
 /*
+ * sum_k coef_k <P_k> (GeneralQuantumOperator::get_expectation_value,
+ * cppsim/general_quantum_operator.cpp:105-141) with the terms as qs_expectation_value_pauli_batch and
+ * coefs[2k], coefs[2k+1] the real and imaginary parts of coef_k; out[0], out[1] receive the real and
+ * imaginary parts of the sum.  No per-term values are formed: each pass over the state folds every
+ * term it covers into one FP64 sum per thread.  Synchronises `stream` before returning.
+ */
+QS_API int qs_expectation_value_pauli_weighted(const QS_ITYPE* x_masks, const QS_ITYPE* z_masks,
+    const QS_UINT* y_counts, const double* coefs, QS_UINT term_count, const void* state, QS_ITYPE dim,
+    void* stream, double out[2]);
+/* The plan qs_expectation_value_pauli_weighted follows for these terms on a state of dim amplitudes,
+ * host only (diagnostic; no reference counterpart): *passes_out = passes over the state;
+ * kind_counts = terms evaluated {Z-only, bit flips within a thread's registers, partner amplitudes
+ * from shared memory, partner rows selected per thread, one value each outside the passes}. */
+QS_API int qs_expectation_value_pauli_weighted_plan(const QS_ITYPE* x_masks, const QS_ITYPE* z_masks,
+    const QS_UINT* y_counts, QS_UINT term_count, QS_ITYPE dim, QS_UINT* passes_out, QS_UINT kind_counts[5]);
+/* Generated per-pass kernels for qs_expectation_value_pauli_weighted (no reference counterpart): each
+ * pass's term masks compiled into a kernel with NVRTC (sm_100a), the coefficients read from device
+ * memory, so one compile serves every coefficient set of the same strings.  mode 0: generic kernel
+ * only; 1 (default): generate when the same terms are evaluated a second time on >= 20 qubits;
+ * 2: generate at the first evaluation, any size.  Plans and kernels are cached for the process. */
+QS_API int qs_set_expectation_specialized(int mode);
+/* Launches of generated expectation kernels so far, and the total compile time of the last plan
+ * whose kernels were generated (ms). */
+QS_API int qs_expectation_specialized_info(unsigned long long* launches, double* compile_ms_last);
+/* CUDA C source of pass `pass` of the weighted plan for these terms (complex64 state when c64 != 0):
+ * at most out_bytes - 1 characters and a terminating 0 into `out` (may be NULL); *needed receives the
+ * full size including the 0. */
+QS_API int qs_expectation_pass_source(const QS_ITYPE* x_masks, const QS_ITYPE* z_masks, const QS_UINT* y_counts,
+    QS_UINT term_count, QS_ITYPE dim, QS_UINT pass, int c64, char* out, QS_ITYPE out_bytes, QS_ITYPE* needed);
+/*
  * cppsim QuantumStateCpu::sampling (cppsim/state.hpp:909-929) with caller-supplied uniforms in
  * [0, 1): out[c] = lower_bound(stacked_prob, uniforms[c]) - 1 over the FP64 prefix sums of |a_i|^2
  * (so 0 -> 2^64 - 1 and r > norm -> dim, as in the reference).
@@ -542,13 +572,17 @@ QS_API int qs_noise_simulator_execute(qs_circuit_t circuit, const void* initial_
 QS_API int qs_circuit_update_quantum_state_fused_c64(qs_circuit_t circuit, void* state_c64, QS_ITYPE dim, void* stream);
 /* Statistics of a complex64 state with FP64 accumulation (the fused path's reductions): norm, the
  * inner product <bra_c128|ket_c64> (for the infidelity 1 - |<psi|psi_FP64>|^2), batched <P_k>
- * (masks as qs_expectation_value_pauli_batch) and sampling with supplied uniforms. */
+ * (masks as qs_expectation_value_pauli_batch), sum_k coef_k <P_k> and sampling with supplied uniforms. */
 QS_API int qs_state_norm_squared_c64(const void* state_c64, QS_ITYPE dim, void* stream, double* out);
 QS_API int qs_state_inner_product_c128_c64(const void* bra_c128, const void* ket_c64, QS_ITYPE dim,
     void* stream, double out[2]);
 QS_API int qs_expectation_value_pauli_batch_c64(const QS_ITYPE* x_masks, const QS_ITYPE* z_masks,
     const QS_UINT* y_counts, QS_UINT term_count, const void* state_c64, QS_ITYPE dim, void* stream,
     double* values);
+/* qs_expectation_value_pauli_weighted over a complex64 state (FP64 arithmetic). */
+QS_API int qs_expectation_value_pauli_weighted_c64(const QS_ITYPE* x_masks, const QS_ITYPE* z_masks,
+    const QS_UINT* y_counts, const double* coefs, QS_UINT term_count, const void* state_c64, QS_ITYPE dim,
+    void* stream, double out[2]);
 QS_API int qs_state_sampling_with_uniforms_c64(const void* state_c64, QS_ITYPE dim, const double* uniforms,
     QS_UINT sampling_count, QS_ITYPE* out, void* stream);
 /* Number of tile passes and fused blocks of the fused schedule (host only). */

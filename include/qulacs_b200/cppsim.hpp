@@ -595,13 +595,16 @@ public:
         std::vector<ITYPE> xm(k), zm(k);
         std::vector<UINT> ny(k);
         for (UINT i = 0; i < k; ++i) terms_[i].masks(&xm[i], &zm[i], &ny[i]);
-        std::vector<double> vals(k);
-        check(qs_expectation_value_pauli_batch(xm.data(), zm.data(), ny.data(), k, state->data(), state->dim,
-                  state->get_cuda_stream(), vals.data()),
+        std::vector<double> coefs(2 * (size_t)k);
+        for (UINT i = 0; i < k; ++i) {
+            coefs[2 * i] = terms_[i].get_coef().real();
+            coefs[2 * i + 1] = terms_[i].get_coef().imag();
+        }
+        double out[2];
+        check(qs_expectation_value_pauli_weighted(xm.data(), zm.data(), ny.data(), coefs.data(), k, state->data(),
+                  state->dim, state->get_cuda_stream(), out),
             "get_expectation_value");
-        CPPCTYPE s = 0;
-        for (UINT i = 0; i < k; ++i) s += terms_[i].get_coef() * vals[i];
-        return s.real();
+        return out[0];
     }
 
 private:

@@ -93,6 +93,12 @@ SIGNATURES = {
     "qs_expectation_value_multi_qubit_Pauli_operator_whole_list": [P, U, P, IT, P, P],
     "qs_transition_amplitude_multi_qubit_Pauli_operator_whole_list": [P, U, P, P, IT, P, P],
     "qs_expectation_value_pauli_batch": [P, P, P, U, P, IT, P, P],
+    "qs_expectation_value_pauli_weighted": [P, P, P, P, U, P, IT, P, P],
+    "qs_expectation_value_pauli_weighted_c64": [P, P, P, P, U, P, IT, P, P],
+    "qs_expectation_value_pauli_weighted_plan": [P, P, P, U, IT, P, P],
+    "qs_set_expectation_specialized": [C.c_int],
+    "qs_expectation_specialized_info": [P, P],
+    "qs_expectation_pass_source": [P, P, P, U, IT, U, C.c_int, P, IT, P],
     "qs_state_sampling_with_uniforms": [P, IT, P, U, P, P],
     "qs_state_sampling": [P, IT, U, U, P, P],
     "qs_state_sampling_with_uniforms_flagged": [P, IT, P, U, D, P, P, P, P],

@@ -29,6 +29,7 @@
 #include <vector>
 
 #include "../../include/qulacs_b200.h"
+#include "codegen.hpp"
 #include "staged.hpp"
 
 namespace qs {
@@ -436,12 +437,13 @@ std::mutex g_mu;
 std::map<std::string, std::shared_ptr<Compiled>> g_cache;
 std::map<std::string, std::shared_ptr<std::mutex>> g_building;  // one compile per source at a time
 
-int compile(const std::string& src, std::vector<char>* cubin) {
+int compile(const std::string& src, const char* name, std::vector<char>* cubin) {
     Nvrtc* N = nvrtc();
-    if (!N->h) return set_error(QS_ERR_NOT_SUPPORTED, "specialised passes: " + N->error);
+    if (!N->h) return set_error(QS_ERR_NOT_SUPPORTED, "specialised kernels: " + N->error);
     nvrtcProgram_t prog = nullptr;
-    if (N->create(&prog, src.c_str(), "k_pass_spec.cu", 0, nullptr, nullptr) != 0)
-        return set_error(QS_ERR_CUDA, "specialised passes: nvrtcCreateProgram failed");
+    const std::string file = std::string(name) + ".cu";
+    if (N->create(&prog, src.c_str(), file.c_str(), 0, nullptr, nullptr) != 0)
+        return set_error(QS_ERR_CUDA, "specialised kernels: nvrtcCreateProgram failed");
     const char* opts[] = {"--gpu-architecture=sm_100a", "--std=c++17"};
     const int rc = N->compile(prog, 2, opts);
     if (rc != 0) {
@@ -450,7 +452,7 @@ int compile(const std::string& src, std::vector<char>* cubin) {
         std::string log(n, '\0');
         if (n) N->log(prog, &log[0]);
         N->destroy(&prog);
-        return set_error(QS_ERR_CUDA, "specialised passes: NVRTC compile failed: " + log.substr(0, 2000));
+        return set_error(QS_ERR_CUDA, std::string(name) + ": NVRTC compile failed: " + log.substr(0, 2000));
     }
     size_t n = 0;
     N->cubin_size(prog, &n);
@@ -462,17 +464,7 @@ int compile(const std::string& src, std::vector<char>* cubin) {
 
 }  // namespace
 
-int specialized_pass_kernel(const PassDesc& d, void** kernel, std::vector<double2>* params, double* compile_ms) {
-    if (d.m < 7 || d.m > kTileBits || d.phases.empty())
-        return set_error(QS_ERR_NOT_SUPPORTED, "specialised passes need 7..12 tile qubits and a phase");
-    params->clear();
-    std::string src = pass_source(d, params);
-    if (params->empty() || params->size() * sizeof(double2) > kMaxParamBytes) {
-        // no parameters (the kernel takes only the state), or too many for a parameter block: literals
-        params->clear();
-        src = pass_source(d, nullptr);
-    }
-    const bool has_params = !params->empty();
+int nvrtc_kernel(const std::string& src, const char* name, void** kernel, double* compile_ms) {
     std::shared_ptr<std::mutex> build_mu;
     {
         std::lock_guard<std::mutex> lk(g_mu);
@@ -498,14 +490,13 @@ int specialized_pass_kernel(const PassDesc& d, void** kernel, std::vector<double
     }
     const auto t0 = std::chrono::steady_clock::now();
     std::vector<char> cubin;
-    int rc = compile(src, &cubin);
+    int rc = compile(src, name, &cubin);
     if (rc != QS_OK) return rc;
     auto C = std::make_shared<Compiled>();
     cudaError_t e = cudaLibraryLoadData(&C->lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0);
-    if (e != cudaSuccess) return check_cuda(e, "cudaLibraryLoadData (specialised pass)");
-    e = cudaLibraryGetKernel(&C->kernel, C->lib, "k_pass_spec");
-    C->has_params = has_params;
-    if (e != cudaSuccess) return check_cuda(e, "cudaLibraryGetKernel (specialised pass)");
+    if (e != cudaSuccess) return check_cuda(e, "cudaLibraryLoadData (specialised kernel)");
+    e = cudaLibraryGetKernel(&C->kernel, C->lib, name);
+    if (e != cudaSuccess) return check_cuda(e, "cudaLibraryGetKernel (specialised kernel)");
     if (compile_ms)
         *compile_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     std::lock_guard<std::mutex> lk(g_mu);
@@ -515,9 +506,9 @@ int specialized_pass_kernel(const PassDesc& d, void** kernel, std::vector<double
     return QS_OK;
 }
 
-int launch_specialized_pass(void* handle, double2* state, const double2* params, ITYPE tiles, int m, cudaStream_t st) {
+int launch_nvrtc_kernel(void* handle, dim3 grid, dim3 block, void** args, size_t smem, size_t smem_limit,
+    cudaStream_t st, const char* what) {
     Compiled* C = static_cast<Compiled*>(handle);
-    const size_t smem = sizeof(double2) << m;
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return check_cuda(e, "cudaGetDevice");
@@ -526,16 +517,38 @@ int launch_specialized_pass(void* handle, double2* state, const double2* params,
         std::lock_guard<std::mutex> lk(g_mu);
         if (!C->smem_set.count(dev)) {
             e = cudaFuncSetAttribute((const void*)C->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                (int)(sizeof(double2) << kTileBits));
-            if (e != cudaSuccess) return check_cuda(e, "cudaFuncSetAttribute (specialised pass)");
+                (int)smem_limit);
+            if (e != cudaSuccess) return check_cuda(e, "cudaFuncSetAttribute (specialised kernel)");
             C->smem_set.insert(dev);
         }
     }
-    void* args[] = {&state, const_cast<double2*>(params)};  // the parameter block is copied at launch
+    e = cudaLaunchKernel((const void*)C->kernel, grid, block, args, smem, st);
+    if (e != cudaSuccess) return check_cuda(e, what);
+    return check_launch(what);
+}
+
+int specialized_pass_kernel(const PassDesc& d, void** kernel, std::vector<double2>* params, double* compile_ms) {
+    if (d.m < 7 || d.m > kTileBits || d.phases.empty())
+        return set_error(QS_ERR_NOT_SUPPORTED, "specialised passes need 7..12 tile qubits and a phase");
+    params->clear();
+    std::string src = pass_source(d, params);
+    if (params->empty() || params->size() * sizeof(double2) > kMaxParamBytes) {
+        // no parameters (the kernel takes only the state), or too many for a parameter block: literals
+        params->clear();
+        src = pass_source(d, nullptr);
+    }
+    const int rc = nvrtc_kernel(src, "k_pass_spec", kernel, compile_ms);
+    if (rc != QS_OK) return rc;
+    static_cast<Compiled*>(*kernel)->has_params = !params->empty();  // a property of the source
+    return QS_OK;
+}
+
+int launch_specialized_pass(void* handle, double2* state, const double2* params, ITYPE tiles, int m, cudaStream_t st) {
+    Compiled* C = static_cast<Compiled*>(handle);
     if (C->has_params && !params) return set_error(QS_ERR_INVALID_ARGUMENT, "specialised pass: no parameter block");
-    e = cudaLaunchKernel((const void*)C->kernel, dim3((unsigned)tiles), dim3(kStThreads), args, smem, st);
-    if (e != cudaSuccess) return check_cuda(e, "k_pass_spec launch");
-    return check_launch("k_pass_spec");
+    void* args[] = {&state, const_cast<double2*>(params)};  // the parameter block is copied at launch
+    return launch_nvrtc_kernel(handle, dim3((unsigned)tiles), dim3(kStThreads), args, sizeof(double2) << m,
+        sizeof(double2) << kTileBits, st, "k_pass_spec");
 }
 
 std::string specialized_pass_source(const PassDesc& d) {

@@ -6,8 +6,15 @@
 #include <cstring>
 #include <mutex>
 #include <random>
+#include <unordered_map>
+#include <atomic>
+#include <deque>
+#include <map>
+#include <memory>
+#include <thread>
 #include <vector>
 
+#include "ev_spec.hpp"
 #include "qs_internal.cuh"
 
 namespace qs {
@@ -1030,17 +1037,6 @@ constexpr int kEvTileBits = kEvTileBitsDecl;
 constexpr int kEvLowFixed = 4;    // unit vectors of qubits 0..3 in every tile basis (256-byte runs)
 constexpr int kEvMaxTerms = 512;  // terms per pass (shared-memory accumulators)
 
-// A tile is a coset of the span of m basis masks b_j over the index bits, in reduced echelon form:
-// b_j has bit piv_j set and no other basis mask has it.  Tile element u (bit j <-> b_j) of tile T is
-// index rep(T) ^ XOR_{j in u} b_j, rep(T) = T with zeros inserted at the pivots (ascending in
-// `piv_sorted`).  With unit vectors the tile is the usual set of tile qubits.
-struct EvTileArgs {
-    int m;
-    ITYPE b[kEvTileBits];
-    UINT piv_sorted[kEvTileBits];
-    int nterms;
-    int nz;  // the last nz terms are Z-only strings (no bit flip)
-};
 struct EvTileTerm {
     UINT xloc, zloc;  // masks over tile bits
     ITYPE zglob;      // full phase-flip mask (for the base parity)
@@ -1208,6 +1204,81 @@ __global__ void k_fold_cols(const double* __restrict__ part, int rows, int cols,
     if (threadIdx.x == 0) out[out_index[c]] = v;
 }
 
+// A tile basis in reduced echelon form: b[j] has bit piv[j] set and no other mask of the basis has it,
+// so reduce(x) (clear every pivot bit of x with its basis mask) is 0 exactly for x in the span.
+struct EvBasis {
+    std::vector<ITYPE> b;
+    std::vector<int> piv;
+    ITYPE reduce(ITYPE x) const {
+        for (size_t j = 0; j < b.size(); ++j)
+            if ((x >> piv[j]) & 1) x ^= b[j];
+        return x;
+    }
+    void add(ITYPE r) {  // r reduced and nonzero
+        const int p = 63 - __builtin_clzll(r);
+        for (ITYPE& v : b)  // keep every pivot bit in exactly one basis mask
+            if ((v >> p) & 1) v ^= r;
+        b.push_back(r);
+        piv.push_back(p);
+    }
+    // tile coordinates of a mask in the span: bit j <-> basis mask j
+    UINT local_x(ITYPE x) const {
+        UINT l = 0;
+        for (size_t j = 0; j < b.size(); ++j)
+            if ((x >> piv[j]) & 1) l |= 1u << j;
+        return l;
+    }
+    // phase-flip mask over tile coordinates: bit j = parity(b[j] & z)
+    UINT local_z(ITYPE z) const {
+        UINT l = 0;
+        for (size_t j = 0; j < b.size(); ++j)
+            if (__builtin_popcountll(b[j] & z) & 1) l |= 1u << j;
+        return l;
+    }
+    void args(EvTileArgs* a) const {
+        a->m = (int)b.size();
+        for (int j = 0; j < a->m; ++j) {
+            a->b[j] = b[j];
+            a->piv_sorted[j] = (UINT)piv[j];
+        }
+        std::sort(a->piv_sorted, a->piv_sorted + a->m);
+    }
+};
+
+// The basis of one pass: unit vectors of qubits 0..3, then, while fewer than m, the reduced bit-flip
+// mask shared by the most of `todo`'s terms not yet in the span (the first in term order on a tie: a
+// term x joins the span of B + r exactly when reduce_B(x) is 0 or reduce_B(r)), then unit vectors of
+// the lowest free qubits (a tile always has m basis masks).
+EvBasis ev_basis(const PauliTerm* terms, const std::vector<int>& todo, UINT n, int m) {
+    EvBasis B;
+    for (int q = 0; q < kEvLowFixed; ++q) B.add(1ULL << q);
+    std::vector<ITYPE> red(todo.size());
+    for (size_t i = 0; i < todo.size(); ++i) red[i] = B.reduce(terms[todo[i]].x);
+    std::unordered_map<ITYPE, int> freq;
+    while ((int)B.b.size() < m) {
+        freq.clear();
+        ITYPE best = 0;
+        int most = 0;
+        for (ITYPE r : red)
+            if (r) {
+                const int c = ++freq[r];
+                if (c > most) {
+                    most = c;
+                    best = r;
+                }
+            }
+        if (!best) break;
+        B.add(best);
+        for (ITYPE& r : red)
+            if (r) r = B.reduce(r);
+    }
+    for (int q = 0; q < (int)n && (int)B.b.size() < m; ++q) {
+        const ITYPE r = B.reduce(1ULL << q);
+        if (r) B.add(r);
+    }
+    return B;
+}
+
 // Host: cover the terms' bit-flip masks with tiles spanned by qubits 0..3 and up to m - 4 of the terms'
 // own masks (reduced echelon form, see EvTileArgs): a pass evaluates every term whose mask lies in
 // its span from shared memory.  Terms left when a pass would cover fewer than two stay in `rest`
@@ -1221,45 +1292,12 @@ int ev_tiled(const PauliTerm* terms, const std::vector<int>& xidx, UINT n, const
     constexpr size_t kMinCover = 2;  // below this a shared pass is not cheaper than one pass per term
     std::vector<double> hvals;
     while (!todo.empty()) {
-        // basis: unit vectors of qubits 0..3, then reduced term masks (greedy in term order)
-        std::vector<ITYPE> basis;
-        std::vector<int> piv;
-        for (int q = 0; q < kEvLowFixed; ++q) {
-            basis.push_back(1ULL << q);
-            piv.push_back(q);
-        }
-        auto reduce = [&](ITYPE x) {
-            for (size_t j = 0; j < basis.size(); ++j)
-                if ((x >> piv[j]) & 1) x ^= basis[j];
-            return x;
-        };
-        for (int k : todo) {
-            if ((int)basis.size() >= m) break;
-            const ITYPE r = reduce(terms[k].x);
-            if (!r) continue;
-            const int p = 63 - __builtin_clzll(r);
-            for (ITYPE& b : basis)  // keep every pivot bit in exactly one basis mask
-                if ((b >> p) & 1) b ^= r;
-            basis.push_back(r);
-            piv.push_back(p);
-        }
-        // pad with unit vectors of the lowest free qubits (a tile always has m basis masks)
-        for (int q = 0; q < (int)n && (int)basis.size() < m; ++q) {
-            if (reduce(1ULL << q) == 0) continue;
-            const ITYPE r = reduce(1ULL << q);
-            const int p = 63 - __builtin_clzll(r);
-            for (ITYPE& b : basis)
-                if ((b >> p) & 1) b ^= r;
-            basis.push_back(r);
-            piv.push_back(p);
-        }
+        const EvBasis B = ev_basis(terms, todo, n, m);
+        const std::vector<ITYPE>& basis = B.b;
+        const std::vector<int>& piv = B.piv;
+        auto reduce = [&](ITYPE x) { return B.reduce(x); };
         EvTileArgs a{};
-        a.m = (int)basis.size();
-        for (int jj = 0; jj < a.m; ++jj) {
-            a.b[jj] = basis[jj];
-            a.piv_sorted[jj] = (UINT)piv[jj];
-        }
-        std::sort(a.piv_sorted, a.piv_sorted + a.m);
+        B.args(&a);
         std::vector<EvTileTerm> tt;
         std::vector<UINT> outi;
         std::vector<int> left;
@@ -1372,3 +1410,645 @@ template int ev_tiled<float2>(const PauliTerm*, const std::vector<int>&, UINT, c
     double*, std::vector<int>*, std::vector<int>*);
 
 }  // namespace qs
+
+// ---------------------------------------------------------------- sum_k c_k <P_k>, register-resident tiles
+// The weighted expectation value needs no per-term value, so no per-term reduction either: every
+// thread folds each term's contribution into one running complex sum (FP64) across all its tiles, and
+// each CTA writes one partial per pass.  Tiles use the pass bases of the per-term kernel above (2^11
+// amplitudes): tile bits 0..6 are the thread index, tile bits 7..10 index 16 amplitudes held in the
+// thread's registers and also stored to shared memory.  A term with bit-flip mask (xt, xr) over
+// (thread bits, register bits) pairs thread t's amplitude p with amplitude p ^ xr of thread t ^ xt:
+//   xt = 0:          both ends in the thread's own registers (no shared-memory read);
+//   xr != 0 (K its lowest bit): thread t takes its 8 amplitudes with bit K of p clear and reads the
+//                    partner end from shared memory; thread t ^ xt takes the other 8 pairs;
+//   xr = 0:          thread t takes its 8 amplitudes whose bit 0 of p equals bit j of t (j the lowest
+//                    bit of xt); thread t ^ xt the other 8.
+// Each pair {u, u ^ x} is counted once from its own end u (2 Re(conj(a_u) P a_u^x) is the same from
+// either end for a Hermitian string), so each thread reads 8 partner amplitudes per term, not 16.
+// The phase parity of element u splits into the tile base's part (with the full mask), the thread
+// part and the register part; the register part is folded as a +-1 butterfly over the free bits.
+namespace qs {
+
+static_assert(kEvTileBits == kEvBasisBits, "weighted and per-term passes share their tiles");
+
+template <int C>
+__device__ __forceinline__ double ew_part(double2 a, double2 b) {  // Re (C = 0) or Im (C = 1) of a conj(b)
+    return C ? fma(a.y, b.x, -(a.x * b.y)) : fma(a.x, b.x, a.y * b.y);
+}
+// -1.0 when bit j of zr is set, else +1.0
+__device__ __forceinline__ double ew_sgn(UINT zr, int j) {
+    return __hiloint2double((int)(0x3FF00000u | ((zr >> j) << 31)), 0);
+}
+// sum_i v[i] * prod_b s_b^{bit b of i} over 8 values
+__device__ __forceinline__ double ew_fold8(double (&v)[8], double s0, double s1, double s2) {
+    v[0] = fma(s0, v[1], v[0]);
+    v[2] = fma(s0, v[3], v[2]);
+    v[4] = fma(s0, v[5], v[4]);
+    v[6] = fma(s0, v[7], v[6]);
+    v[0] = fma(s1, v[2], v[0]);
+    v[4] = fma(s1, v[6], v[4]);
+    return fma(s2, v[4], v[0]);
+}
+__host__ __device__ constexpr int ew_ins0(int i, int k) { return ((i >> k) << (k + 1)) | (i & ((1 << k) - 1)); }
+__host__ __device__ constexpr int ew_ctz(int x) { return (x & 1) ? 0 : 1 + ew_ctz(x >> 1); }
+__host__ __device__ constexpr int ew_free(int k, int b) { return b < k ? b : b + 1; }  // b-th register bit other than k
+
+// A tile element from shared memory as FP64.
+__device__ __forceinline__ double2 ew_ld(const double2* p) { return *p; }
+__device__ __forceinline__ double2 ew_ld(const float2* p) {
+    const float2 v = *p;
+    return make_double2((double)v.x, (double)v.y);
+}
+// xr != 0, partner row in shared memory: own p (bit K clear) against element p ^ xr of the partner row
+// (rows kRow bytes apart)
+template <int K, int C, class E, int kRow>
+__device__ __forceinline__ double ew_smem(const double2 (&own)[16], const char* prow, UINT xr, UINT zr) {
+    double v[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int p = ew_ins0(i, K);
+        const double2 b = ew_ld((const E*)(prow + ((UINT)p ^ xr) * (UINT)kRow));
+        v[i] = ew_part<C>(own[p], b);
+    }
+    return ew_fold8(v, ew_sgn(zr, ew_free(K, 0)), ew_sgn(zr, ew_free(K, 1)), ew_sgn(zr, ew_free(K, 2)));
+}
+// xr = 0: own p = 2i + bsel against element p of the partner row
+template <int C, class E, int kRow>
+__device__ __forceinline__ double ew_row(const double2 (&own)[16], const char* prow, UINT bsel, UINT zr) {
+    double v[8];
+    const char* pr = prow + bsel * (UINT)kRow;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const double2 a = bsel ? own[2 * i + 1] : own[2 * i];
+        const double2 b = ew_ld((const E*)(pr + i * 2 * kRow));
+        v[i] = ew_part<C>(a, b);
+    }
+    return ew_fold8(v, ew_sgn(zr, 1), ew_sgn(zr, 2), ew_sgn(zr, 3));
+}
+// xt = 0: both ends in registers
+template <int XR, int C>
+__device__ __forceinline__ double ew_reg(const double2 (&own)[16], UINT zr) {
+    constexpr int K = ew_ctz(XR);
+    double v[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int p = ew_ins0(i, K);
+        v[i] = ew_part<C>(own[p], own[p ^ XR]);
+    }
+    return ew_fold8(v, ew_sgn(zr, ew_free(K, 0)), ew_sgn(zr, ew_free(K, 1)), ew_sgn(zr, ew_free(K, 2)));
+}
+// Z-only: sum_p |own[p]|^2 (-1)^{parity(p & zr)}
+__device__ __forceinline__ double ew_diag(const double2 (&own)[16], UINT zr) {
+    double v[16];
+#pragma unroll
+    for (int p = 0; p < 16; ++p) v[p] = fma(own[p].x, own[p].x, own[p].y * own[p].y);
+    const double s0 = ew_sgn(zr, 0), s1 = ew_sgn(zr, 1), s2 = ew_sgn(zr, 2), s3 = ew_sgn(zr, 3);
+#pragma unroll
+    for (int i = 0; i < 16; i += 2) v[i] = fma(s0, v[i + 1], v[i]);
+#pragma unroll
+    for (int i = 0; i < 16; i += 4) v[i] = fma(s1, v[i + 2], v[i]);
+    v[0] = fma(s2, v[4], v[0]);
+    v[8] = fma(s2, v[12], v[8]);
+    return fma(s3, v[8], v[0]);
+}
+
+// 16- (complex128) or 8-byte (complex64) asynchronous copy global -> shared
+template <int B>
+__device__ __forceinline__ void ew_cp_async(unsigned dst, const void* src) {
+    if constexpr (B == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src) : "memory");
+}
+
+template <int TB, class T>
+constexpr size_t ew_smem_bytes() { return 2 * (size_t)(16 << TB) * sizeof(T); }  // two tiles
+
+#define EW_REG_CASE(XR)                                            \
+    case EW_REG + 2 * (XR - 1): v = ew_reg<XR, 0>(own, zr); break; \
+    case EW_REG + 2 * (XR - 1) + 1: v = ew_reg<XR, 1>(own, zr); break;
+#define EW_SMEM_CASE(K)                                                             \
+    case EW_SMEM + 2 * K: v = ew_smem<K, 0, T, kRow>(own, prow, xr, zr); break;     \
+    case EW_SMEM + 2 * K + 1: v = ew_smem<K, 1, T, kRow>(own, prow, xr, zr); break;
+
+// Grid-stride over tiles, two tile buffers in dynamic shared memory: the copies of tile i + 1 are in
+// flight (cp.async) while the terms run over tile i.
+template <class T, int TB>
+__global__ void __launch_bounds__(1 << TB, kEwCtasPerSm) k_ev_weighted(const T* __restrict__ s, ITYPE tiles,
+    const __grid_constant__ EvTileArgs a, const EvWTerm* __restrict__ terms, int nterms,
+    double2* __restrict__ partials) {
+    constexpr int kThreads = 1 << TB;
+    constexpr int kRow = kThreads * (int)sizeof(T);  // bytes between register rows p and p + 1
+    constexpr int kTileBytes = 16 * kRow;
+    extern __shared__ __align__(16) unsigned char ew_tiles[];
+    __shared__ ITYPE hi_off[16];
+    __shared__ double red[2][kThreads / 32];
+    const UINT t = threadIdx.x;
+    if (t < 16) {
+        ITYPE o = 0;
+        for (int j = 0; j < 4; ++j)
+            if ((t >> j) & 1) o ^= a.b[TB + j];
+        hi_off[t] = o;
+    }
+    ITYPE lo_off = 0;
+    for (int j = 0; j < TB; ++j)
+        if ((t >> j) & 1) lo_off ^= a.b[j];
+    auto tile_base = [&](ITYPE ti) {
+        ITYPE base = ti;
+        for (int j = 0; j < a.m; ++j) base = insert0(base, a.piv_sorted[j]);
+        return base;
+    };
+    const unsigned sdst = (unsigned)__cvta_generic_to_shared(ew_tiles) + t * (unsigned)sizeof(T);
+    auto issue = [&](ITYPE ti, int buf) {
+        const ITYPE base = tile_base(ti);
+#pragma unroll
+        for (int p = 0; p < 16; ++p)
+            ew_cp_async<(int)sizeof(T)>(sdst + buf * kTileBytes + p * kRow, s + (base ^ lo_off ^ hi_off[p]));
+    };
+    __syncthreads();  // hi_off
+    if ((ITYPE)blockIdx.x < tiles) issue(blockIdx.x, 0);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    double accr = 0., acci = 0.;
+    int buf = 0;
+    for (ITYPE ti = blockIdx.x; ti < tiles; ti += gridDim.x, buf ^= 1) {
+        if (ti + gridDim.x < tiles) issue(ti + gridDim.x, buf ^ 1);
+        asm volatile("cp.async.commit_group;\ncp.async.wait_group 1;" ::: "memory");
+        __syncthreads();  // every thread's copies of tile ti landed
+        const char* tb = (const char*)ew_tiles + buf * kTileBytes;
+        const ITYPE base = tile_base(ti);
+        double2 own[16];
+#pragma unroll
+        for (int p = 0; p < 16; ++p) own[p] = ew_ld((const T*)(tb + t * sizeof(T) + p * kRow));
+        double2 coef_n = make_double2(0., 0.);
+        ITYPE zglob_n = 0;
+        UINT pk_n = 0;
+        if (nterms > 0) {
+            coef_n = __ldg(&terms[0].coef);
+            zglob_n = __ldg(&terms[0].zglob);
+            pk_n = __ldg(&terms[0].packed);
+        }
+        for (int k = 0; k < nterms; ++k) {
+            // opaque per term: keeps the compiler from hoisting every case's products of the (term-invariant)
+            // amplitudes out of the loop, which would need hundreds of registers
+#pragma unroll
+            for (int p = 0; p < 16; ++p) asm volatile("" : "+d"(own[p].x), "+d"(own[p].y));
+            const double2 coef = coef_n;
+            const ITYPE zglob = zglob_n;
+            const UINT pk = pk_n;
+            if (k + 1 < nterms) {  // the next descriptor in flight during this term
+                coef_n = __ldg(&terms[k + 1].coef);
+                zglob_n = __ldg(&terms[k + 1].zglob);
+                pk_n = __ldg(&terms[k + 1].packed);
+            }
+            const UINT xt = pk & 0xFFu, zt = (pk >> 8) & 0xFFu, xr = (pk >> 16) & 15u, zr = (pk >> 20) & 15u;
+            UINT flip = (UINT)(__popcll(base & zglob) + __popc(t & zt)) & 1u;
+            const char* prow = tb + sizeof(T) * (t ^ xt);
+            double v;
+            switch (pk >> 24) {
+                case EW_Z: v = ew_diag(own, zr); break;
+                EW_SMEM_CASE(0)
+                EW_SMEM_CASE(1)
+                EW_SMEM_CASE(2)
+                EW_SMEM_CASE(3)
+                case EW_ROW:
+                case EW_ROW + 1: {
+                    const UINT bsel = (t >> (__ffs(xt) - 1)) & 1u;
+                    flip ^= bsel & zr;
+                    v = (pk >> 24) == EW_ROW ? ew_row<0, T, kRow>(own, prow, bsel, zr)
+                                             : ew_row<1, T, kRow>(own, prow, bsel, zr);
+                    break;
+                }
+                EW_REG_CASE(1) EW_REG_CASE(2) EW_REG_CASE(3) EW_REG_CASE(4) EW_REG_CASE(5)
+                EW_REG_CASE(6) EW_REG_CASE(7) EW_REG_CASE(8) EW_REG_CASE(9) EW_REG_CASE(10)
+                EW_REG_CASE(11) EW_REG_CASE(12) EW_REG_CASE(13) EW_REG_CASE(14) EW_REG_CASE(15)
+                default: v = 0.; break;
+            }
+            v = __longlong_as_double(__double_as_longlong(v) ^ ((unsigned long long)(flip & 1u) << 63));
+            accr = fma(coef.x, v, accr);
+            acci = fma(coef.y, v, acci);
+        }
+        __syncthreads();  // every thread done with this buffer before the copies of tile ti + 2 overwrite it
+    }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        accr += __shfl_xor_sync(0xffffffffu, accr, o);
+        acci += __shfl_xor_sync(0xffffffffu, acci, o);
+    }
+    if ((t & 31) == 0) {
+        red[0][t >> 5] = accr;
+        red[1][t >> 5] = acci;
+    }
+    __syncthreads();
+    if (t == 0) {
+        double r = 0., i = 0.;
+        for (int w = 0; w < kThreads / 32; ++w) {
+            r += red[0][w];
+            i += red[1][w];
+        }
+        partials[blockIdx.x] = make_double2(r, i);
+    }
+}
+#undef EW_REG_CASE
+#undef EW_SMEM_CASE
+
+__global__ void k_fold_d2(const double2* __restrict__ part, int count, double* __restrict__ out) {
+    __shared__ double sr[32], si[32];
+    double r = 0., i = 0.;
+    for (int j = threadIdx.x; j < count; j += blockDim.x) {
+        r += part[j].x;
+        i += part[j].y;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        r += __shfl_xor_sync(0xffffffffu, r, o);
+        i += __shfl_xor_sync(0xffffffffu, i, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        sr[threadIdx.x >> 5] = r;
+        si[threadIdx.x >> 5] = i;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0., b = 0.;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            a += sr[w];
+            b += si[w];
+        }
+        out[0] = a;
+        out[1] = b;
+    }
+}
+
+// One pass of the weighted kernel: its tile basis (register bits chosen) and term descriptors.
+struct EwPass {
+    EvTileArgs a;
+    size_t first, count;  // range in the descriptor array
+};
+
+// The descriptor of a term for a pass basis, its coefficient field holding the term's factor alone
+// (+-2 for a bit flip, from i^nrot; 1 for Z-only); the coefficient c_k multiplies it per call.
+static EvWTerm ew_term(const PauliTerm& pt, const EvBasis& B) {
+    constexpr UINT tmask = (1u << kEwThreadBits) - 1;
+    const UINT xl = B.local_x(pt.x), zl = B.local_z(pt.z);
+    const UINT xt = xl & tmask, xr = xl >> kEwThreadBits, zt = zl & tmask, zr = zl >> kEwThreadBits;
+    const UINT C = pt.nrot & 1u, r0 = pt.nrot & 3u;
+    double f = (r0 == 1u || r0 == 2u) ? -2.0 : 2.0;  // Re(v i^r): +Re, -Im, -Re, +Im
+    UINT code;
+    if (!pt.x) {
+        code = EW_Z;
+        f = 1.0;  // nrot = 0 for a Z-only string; every element counted once
+    } else if (!xt) {
+        code = EW_REG + 2 * (xr - 1) + C;
+    } else if (xr) {
+        code = EW_SMEM + 2 * (UINT)__builtin_ctz(xr) + C;
+    } else {
+        code = EW_ROW + C;
+    }
+    EvWTerm e{};
+    e.coef = make_double2(f, 0.);
+    e.zglob = pt.z;
+    e.packed = xt | zt << 8 | xr << 16 | zr << 20 | code << 24;
+    return e;
+}
+
+// Reorder basis masks 4..m-1 so the 4 register bits (the last four) hold the most terms entirely
+// (no shared-memory read), then the fewest terms with none of them (the select-based rows).
+static void ew_choose_register_bits(EvBasis* B, const PauliTerm* terms, const std::vector<int>& in) {
+    const int m = (int)B->b.size();
+    std::vector<UINT> xl;
+    for (int k : in) xl.push_back(B->local_x(terms[k].x));
+    int best_set = -1;
+    long best_score = -1;
+    for (int set = 0; set < (1 << m); ++set) {
+        if (__builtin_popcount(set) != 4 || (set & ((1 << kEvLowFixed) - 1))) continue;
+        long reg = 0, row = 0;
+        for (UINT l : xl) {
+            reg += (l & ~(UINT)set) == 0;
+            row += (l & (UINT)set) == 0;
+        }
+        const long score = reg * 4096 - row;
+        if (score > best_score) {
+            best_score = score;
+            best_set = set;
+        }
+    }
+    EvBasis R;
+    for (int j = 0; j < m; ++j)
+        if (!((best_set >> j) & 1)) {
+            R.b.push_back(B->b[j]);
+            R.piv.push_back(B->piv[j]);
+        }
+    for (int j = 0; j < m; ++j)
+        if ((best_set >> j) & 1) {
+            R.b.push_back(B->b[j]);
+            R.piv.push_back(B->piv[j]);
+        }
+    *B = R;
+}
+
+// The plan of sum_k c_k <P_k> for a list of terms on n qubits: pass bases and descriptors (every Z-only
+// term in the first pass), the term behind each descriptor, the terms left for one value each (a pass
+// would cover fewer than two), and the per-pass kernels generated for it.
+struct EwPlan {
+    std::vector<EwPass> passes;
+    std::vector<EvWTerm> desc;
+    std::vector<int> term_of;
+    std::vector<int> rest;
+    std::mutex mu;      // guards the fields below
+    int uses = 0;
+    int spec_state = 0;  // 0 not generated, 1 generated, 2 generation failed
+    std::vector<void*> spec;  // per pass: generated kernel, or nullptr where the generic kernel runs
+    double compile_ms = 0.;
+};
+
+constexpr size_t kEvSpecMaxTerms = 192;  // larger passes keep the generic kernel (code size)
+constexpr UINT kEvSpecMinQubits = 20;    // below this a pass takes microseconds: not worth a compile
+std::atomic<int> g_ev_spec_mode{1};      // 0 off, 1 from the second use of a plan (n >= 20), 2 first use, any n
+std::atomic<long long> g_ev_spec_launches{0};
+std::atomic<double> g_ev_last_compile_ms{0.};
+
+static void ew_build(const PauliTerm* terms, UINT count, UINT n, EwPlan* P) {
+    constexpr size_t kMinCover = 2;
+    std::vector<int> zidx, todo;
+    for (UINT k = 0; k < count; ++k) (terms[k].x == 0 ? zidx : todo).push_back((int)k);
+    if (n < (UINT)kEvTileBits || todo.size() < 4) {
+        for (UINT k = 0; k < count; ++k) P->rest.push_back((int)k);
+        return;
+    }
+    while (!todo.empty()) {
+        EvBasis B = ev_basis(terms, todo, n, kEvTileBits);
+        std::vector<int> in, left;
+        for (int k : todo) (B.reduce(terms[k].x) == 0 ? in : left).push_back(k);
+        if (in.size() < kMinCover) {
+            P->rest.insert(P->rest.end(), todo.begin(), todo.end());
+            break;
+        }
+        ew_choose_register_bits(&B, terms, in);
+        EwPass pass{};
+        B.args(&pass.a);
+        pass.first = P->desc.size();
+        auto add = [&](int k) {
+            P->desc.push_back(ew_term(terms[k], B));
+            P->term_of.push_back(k);
+        };
+        for (int k : in) add(k);
+        if (P->passes.empty()) {  // the Z-only terms ride in the first pass
+            for (int k : zidx) add(k);
+            zidx.clear();
+        }
+        pass.count = P->desc.size() - pass.first;
+        pass.a.nterms = (int)pass.count;
+        P->passes.push_back(pass);
+        todo.swap(left);
+    }
+    P->rest.insert(P->rest.end(), zidx.begin(), zidx.end());
+}
+
+// Plans cached by (qubit count, state type, imaginary coefficients, term masks).
+static std::shared_ptr<EwPlan> ew_plan(const PauliTerm* terms, UINT count, UINT n, bool c64, bool imag) {
+    std::string key;
+    key.reserve(16 + (size_t)count * 20);
+    const UINT head[3] = {n, (UINT)c64, (UINT)imag};
+    key.append((const char*)head, sizeof(head));
+    for (UINT k = 0; k < count; ++k) {
+        key.append((const char*)&terms[k].x, sizeof(ITYPE));
+        key.append((const char*)&terms[k].z, sizeof(ITYPE));
+        key.append((const char*)&terms[k].nrot, sizeof(UINT));
+    }
+    static std::mutex mu;
+    static std::map<std::string, std::shared_ptr<EwPlan>> cache;
+    static std::deque<std::string> order;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+    auto P = std::make_shared<EwPlan>();
+    ew_build(terms, count, n, P.get());
+    cache[key] = P;
+    order.push_back(key);
+    constexpr size_t kMaxPlans = 64;
+    if (order.size() > kMaxPlans) {  // oldest first; a plan in use stays alive through its shared_ptr
+        cache.erase(order.front());
+        order.pop_front();
+    }
+    return P;
+}
+
+// Generate and compile the plan's per-pass kernels (in parallel), once; the first failure's status.
+static int ew_specialize(EwPlan* P, bool c64, bool imag) {
+    std::vector<void*> k(P->passes.size(), nullptr);
+    std::vector<double> ms(P->passes.size(), 0.);
+    std::vector<int> rcs(P->passes.size(), QS_OK);
+    std::atomic<size_t> next{0};
+    auto work = [&] {
+        for (size_t i; (i = next++) < P->passes.size();) {
+            const EwPass& ps = P->passes[i];
+            if (ps.count > kEvSpecMaxTerms) continue;
+            rcs[i] = ev_pass_kernel(P->desc.data() + ps.first, ps.count, c64, imag, &k[i], &ms[i]);
+        }
+    };
+    const unsigned nt = std::max(1u, std::min<unsigned>((unsigned)P->passes.size(), std::min(16u,
+        std::thread::hardware_concurrency())));
+    std::vector<std::thread> pool;
+    for (unsigned i = 1; i < nt; ++i) pool.emplace_back(work);
+    work();
+    for (std::thread& t : pool) t.join();
+    int rc = QS_OK;
+    for (size_t i = 0; i < rcs.size() && rc == QS_OK; ++i) rc = rcs[i];
+    P->spec_state = rc == QS_OK ? 1 : 2;
+    if (rc == QS_OK) {
+        P->spec = k;
+        double total = 0.;
+        for (double v : ms) total += v;
+        P->compile_ms = total;
+        g_ev_last_compile_ms = total;
+    }
+    return rc;
+}
+
+template <class T>
+int ev_weighted(const PauliTerm* terms, const double2* coefs, UINT count, const T* s, ITYPE dim, cudaStream_t st,
+    double out[2]) {
+    UINT n = 0;
+    while ((1ULL << n) < dim) ++n;
+    constexpr bool c64 = sizeof(T) == sizeof(float2);
+    bool imag = false;
+    for (UINT k = 0; k < count; ++k) imag |= coefs[k].y != 0.;
+    std::shared_ptr<EwPlan> P = ew_plan(terms, count, n, c64, imag);
+    double sr = 0., si = 0.;
+    if (!P->passes.empty()) {
+        std::vector<void*> spec;
+        {
+            std::lock_guard<std::mutex> lk(P->mu);
+            ++P->uses;
+            const int mode = g_ev_spec_mode.load();
+            if (P->spec_state == 0 && (mode == 2 || (mode == 1 && n >= kEvSpecMinQubits && P->uses >= 2))) {
+                const int rc = ew_specialize(P.get(), c64, imag);
+                if (rc != QS_OK && mode == 2) return rc;  // required: report; by default the generic kernel runs
+            }
+            if (mode == 2 && P->spec_state == 2)
+                return set_error(QS_ERR_NOT_SUPPORTED, "expectation: kernel generation failed earlier for these terms");
+            if (mode != 0 && P->spec_state == 1) spec = P->spec;
+        }
+        const unsigned grid = (unsigned)std::min<ITYPE>(dim >> kEvTileBits, (ITYPE)sm_count() * kEwCtasPerSm);
+        auto up = [](size_t b) { return (b + 255) / 256 * 256; };
+        // descriptors with their coefficients (generic kernel) and the coefficients alone (generated kernels)
+        std::vector<EvWTerm> desc = P->desc;
+        std::vector<double2> cf(desc.size());
+        for (size_t i = 0; i < desc.size(); ++i) {
+            const double f = desc[i].coef.x;
+            const double2 c = coefs[P->term_of[i]];
+            cf[i] = desc[i].coef = make_double2(c.x * f, c.y * f);
+        }
+        const size_t bd = sizeof(EvWTerm) * desc.size(), bc = sizeof(double2) * cf.size(),
+                     bp = sizeof(double2) * grid * P->passes.size();
+        void* buf;
+        QS_TRY(scratch(st, up(bd) + up(bc) + up(bp) + 256, &buf));
+        EvWTerm* dd = (EvWTerm*)buf;
+        double2* dc = (double2*)((char*)buf + up(bd));
+        double2* dp = (double2*)((char*)buf + up(bd) + up(bc));
+        double* dout = (double*)((char*)buf + up(bd) + up(bc) + up(bp));
+        QS_CUDA_CHECK(cudaMemcpyAsync(dd, desc.data(), bd, cudaMemcpyHostToDevice, st));
+        QS_CUDA_CHECK(cudaMemcpyAsync(dc, cf.data(), bc, cudaMemcpyHostToDevice, st));
+        constexpr size_t smem = ew_smem_bytes<kEwThreadBits, T>();
+        {  // the tile buffers exceed the default 48 KiB of dynamic shared memory: opt in once per device
+            static std::mutex mu;
+            static std::vector<char> ready;
+            int dev = 0;
+            QS_CUDA_CHECK(cudaGetDevice(&dev));
+            std::lock_guard<std::mutex> lock(mu);
+            if ((int)ready.size() <= dev) ready.resize(dev + 1, 0);
+            if (!ready[dev]) {
+                QS_CUDA_CHECK(cudaFuncSetAttribute(k_ev_weighted<T, kEwThreadBits>,
+                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                ready[dev] = 1;
+            }
+        }
+        for (size_t i = 0; i < P->passes.size(); ++i) {
+            const EwPass& ps = P->passes[i];
+            if (!spec.empty() && spec[i]) {
+                QS_TRY(launch_ev_pass(spec[i], s, dim >> kEvTileBits, ps.a, dc + ps.first, dp + i * grid, grid, c64,
+                    st));
+                ++g_ev_spec_launches;
+            } else {
+                k_ev_weighted<T, kEwThreadBits><<<grid, 1 << kEwThreadBits, smem, st>>>(s, dim >> kEvTileBits, ps.a,
+                    dd + ps.first, (int)ps.count, dp + i * grid);
+                QS_TRY(check_launch("k_ev_weighted"));
+            }
+        }
+        k_fold_d2<<<1, 256, 0, st>>>(dp, (int)(grid * P->passes.size()), dout);
+        QS_TRY(check_launch("k_fold_d2"));
+        double h[2];
+        QS_CUDA_CHECK(cudaMemcpyAsync(h, dout, sizeof(h), cudaMemcpyDeviceToHost, st));
+        QS_CUDA_CHECK(cudaStreamSynchronize(st));
+        sr += h[0];
+        si += h[1];
+    }
+    // terms evaluated one value each (ev_batch), weighted on the host
+    if (!P->rest.empty()) {
+        std::vector<PauliTerm> sub;
+        for (int k : P->rest) sub.push_back(terms[k]);
+        std::vector<double> vals(sub.size());
+        QS_TRY(ev_batch<T>(sub.data(), (UINT)sub.size(), s, dim, st, vals.data()));
+        for (size_t i = 0; i < P->rest.size(); ++i) {
+            sr += coefs[P->rest[i]].x * vals[i];
+            si += coefs[P->rest[i]].y * vals[i];
+        }
+    }
+    out[0] = sr;
+    out[1] = si;
+    return QS_OK;
+}
+
+template int ev_weighted<double2>(const PauliTerm*, const double2*, UINT, const double2*, ITYPE, cudaStream_t, double*);
+template int ev_weighted<float2>(const PauliTerm*, const double2*, UINT, const float2*, ITYPE, cudaStream_t, double*);
+
+}  // namespace qs
+
+// Shared argument checks of the batched Pauli entry points.
+static int pauli_terms_from_masks(const QS_ITYPE* x_masks, const QS_ITYPE* z_masks, const QS_UINT* y_counts,
+    QS_UINT term_count, QS_ITYPE dim, const char* what, std::vector<PauliTerm>* terms) {
+    UINT n;
+    QS_TRY(check_dim(dim, &n));
+    terms->assign(term_count, PauliTerm{});
+    for (UINT k = 0; k < term_count; ++k) {
+        if ((x_masks[k] | z_masks[k]) >> n)
+            return set_error(QS_ERR_INVALID_ARGUMENT, std::string(what) + ": mask beyond qubit count");
+        (*terms)[k].x = x_masks[k];
+        (*terms)[k].z = z_masks[k];
+        (*terms)[k].nrot = y_counts[k];
+        (*terms)[k].pivot = x_masks[k] ? (UINT)(63 - __builtin_clzll(x_masks[k])) : 0;
+    }
+    return QS_OK;
+}
+
+QS_API int qs_expectation_value_pauli_weighted(const QS_ITYPE* x_masks, const QS_ITYPE* z_masks,
+    const QS_UINT* y_counts, const double* coefs, QS_UINT term_count, const void* state, QS_ITYPE dim, void* stream,
+    double out[2]) {
+    std::vector<PauliTerm> terms;
+    QS_TRY(pauli_terms_from_masks(x_masks, z_masks, y_counts, term_count, dim, "expectation_value_pauli_weighted",
+        &terms));
+    return ev_weighted<double2>(terms.data(), (const double2*)coefs, term_count, (const double2*)state, dim,
+        (cudaStream_t)stream, out);
+}
+QS_API int qs_expectation_value_pauli_weighted_c64(const QS_ITYPE* x_masks, const QS_ITYPE* z_masks,
+    const QS_UINT* y_counts, const double* coefs, QS_UINT term_count, const void* state, QS_ITYPE dim, void* stream,
+    double out[2]) {
+    std::vector<PauliTerm> terms;
+    QS_TRY(pauli_terms_from_masks(x_masks, z_masks, y_counts, term_count, dim,
+        "expectation_value_pauli_weighted_c64", &terms));
+    return ev_weighted<float2>(terms.data(), (const double2*)coefs, term_count, (const float2*)state, dim,
+        (cudaStream_t)stream, out);
+}
+
+// Host-only plan of qs_expectation_value_pauli_weighted (no device work): passes over the state and
+// how many terms each kind of evaluation takes.
+QS_API int qs_expectation_value_pauli_weighted_plan(const QS_ITYPE* x_masks, const QS_ITYPE* z_masks,
+    const QS_UINT* y_counts, QS_UINT term_count, QS_ITYPE dim, QS_UINT* passes_out, QS_UINT kind_counts[5]) {
+    std::vector<PauliTerm> terms;
+    QS_TRY(pauli_terms_from_masks(x_masks, z_masks, y_counts, term_count, dim,
+        "expectation_value_pauli_weighted_plan", &terms));
+    UINT n;
+    QS_TRY(check_dim(dim, &n));
+    EwPlan P;
+    ew_build(terms.data(), term_count, n, &P);
+    for (int i = 0; i < 5; ++i) kind_counts[i] = 0;
+    for (const EvWTerm& e : P.desc) {
+        const UINT code = e.packed >> 24;
+        kind_counts[code == EW_Z ? 0 : code >= EW_REG ? 1 : code >= EW_ROW ? 3 : 2]++;
+    }
+    kind_counts[4] = (QS_UINT)P.rest.size();
+    *passes_out = (QS_UINT)P.passes.size();
+    return QS_OK;
+}
+
+QS_API int qs_set_expectation_specialized(int mode) {
+    if (mode < 0 || mode > 2) return set_error(QS_ERR_INVALID_ARGUMENT, "expectation specialisation mode must be 0..2");
+    g_ev_spec_mode = mode;
+    return QS_OK;
+}
+
+QS_API int qs_expectation_specialized_info(unsigned long long* launches, double* compile_ms_last) {
+    if (launches) *launches = (unsigned long long)g_ev_spec_launches.load();
+    if (compile_ms_last) *compile_ms_last = g_ev_last_compile_ms.load();
+    return QS_OK;
+}
+
+QS_API int qs_expectation_pass_source(const QS_ITYPE* x_masks, const QS_ITYPE* z_masks, const QS_UINT* y_counts,
+    QS_UINT term_count, QS_ITYPE dim, QS_UINT pass, int c64, char* out, QS_ITYPE out_bytes, QS_ITYPE* needed) {
+    std::vector<PauliTerm> terms;
+    QS_TRY(pauli_terms_from_masks(x_masks, z_masks, y_counts, term_count, dim, "expectation_pass_source", &terms));
+    UINT n;
+    QS_TRY(check_dim(dim, &n));
+    EwPlan P;
+    ew_build(terms.data(), term_count, n, &P);
+    if (pass >= P.passes.size()) return set_error(QS_ERR_INVALID_ARGUMENT, "expectation_pass_source: no such pass");
+    const std::string src = ev_pass_source(P.desc.data() + P.passes[pass].first, P.passes[pass].count, c64 != 0, false);
+    if (needed) *needed = src.size() + 1;
+    if (out && out_bytes) {
+        const size_t m = std::min<size_t>(src.size(), out_bytes - 1);
+        std::memcpy(out, src.data(), m);
+        out[m] = 0;
+    }
+    return QS_OK;
+}

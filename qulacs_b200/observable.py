@@ -1,8 +1,9 @@
 """PauliOperator / Observable (cppsim/pauli_operator.cpp, general_quantum_operator.cpp).
 
-``Observable.get_expectation_value`` evaluates all terms with one batched C-ABI call
-(``qs_expectation_value_pauli_batch``) and sums coef_k <P_k> in FP64 on the host, the sum the
-reference forms in GeneralQuantumOperator::get_expectation_value (general_quantum_operator.cpp:105-141).
+``Observable.get_expectation_value`` evaluates sum_k coef_k <P_k> with one weighted C-ABI call
+(``qs_expectation_value_pauli_weighted``), the sum the reference forms term by term in
+GeneralQuantumOperator::get_expectation_value (general_quantum_operator.cpp:105-141);
+``Observable.term_values`` returns every <P_k> (``qs_expectation_value_pauli_batch``).
 """
 from __future__ import annotations
 
@@ -233,9 +234,79 @@ class Observable:
              vals.ctypes.data_as(C.c_void_p))
         return vals
 
+    def _masks(self):
+        k = len(self.terms)
+        xm = np.zeros(k, dtype=np.uint64)
+        zm = np.zeros(k, dtype=np.uint64)
+        ny = np.zeros(k, dtype=np.uint32)
+        for i, t in enumerate(self.terms):
+            xm[i], zm[i], ny[i] = masks(t.targets, t.ids)
+        return xm, zm, ny
+
+    def weighted_plan(self, qubit_count: int | None = None) -> dict:
+        """How get_expectation_value evaluates these terms on a state of `qubit_count` qubits (host
+        only): passes over the state and terms per kind of evaluation."""
+        n = self.qubit_count if qubit_count is None else int(qubit_count)
+        xm, zm, ny = self._masks()
+        passes = C.c_uint()
+        kinds = (C.c_uint * 5)()
+        call("qs_expectation_value_pauli_weighted_plan", xm.ctypes.data_as(C.c_void_p),
+             zm.ctypes.data_as(C.c_void_p), ny.ctypes.data_as(C.c_void_p), len(self.terms), 1 << n,
+             C.byref(passes), kinds)
+        return {"passes": passes.value, "z_only": kinds[0], "in_registers": kinds[1], "shared_partner": kinds[2],
+                "selected_rows": kinds[3], "one_value_each": kinds[4]}
+
+    def pass_source(self, index: int, qubit_count: int | None = None, c64: bool = False) -> str:
+        """CUDA C of the generated kernel for pass `index` of the weighted plan."""
+        n = self.qubit_count if qubit_count is None else int(qubit_count)
+        xm, zm, ny = self._masks()
+        need = C.c_ulonglong()
+        args = (xm.ctypes.data_as(C.c_void_p), zm.ctypes.data_as(C.c_void_p), ny.ctypes.data_as(C.c_void_p),
+                len(self.terms), 1 << n, index, int(c64))
+        call("qs_expectation_pass_source", *args, None, 0, C.byref(need))
+        buf = C.create_string_buffer(need.value)
+        call("qs_expectation_pass_source", *args, buf, need.value, C.byref(need))
+        return buf.value.decode()
+
+    def get_expectation_value_complex(self, state) -> complex:
+        """sum_k coef_k <P_k> with complex coefficients kept (GeneralQuantumOperator's return)."""
+        if not self.terms:
+            return 0j
+        if not state.is_state_vector():
+            vals = self.term_values(state)
+            return complex(np.sum(np.array([t.coef for t in self.terms], dtype=np.complex128) * vals))
+        xm, zm, ny = self._masks()
+        cf = np.zeros(2 * len(self.terms))
+        for i, t in enumerate(self.terms):
+            c = complex(t.coef)
+            cf[2 * i], cf[2 * i + 1] = c.real, c.imag
+        out = np.zeros(2)
+        fn = "qs_expectation_value_pauli_weighted_c64" if type(state).__name__ == "QuantumStateC64" else \
+            "qs_expectation_value_pauli_weighted"
+        call(fn, xm.ctypes.data_as(C.c_void_p), zm.ctypes.data_as(C.c_void_p), ny.ctypes.data_as(C.c_void_p),
+             cf.ctypes.data_as(C.c_void_p), len(self.terms), state.data_ptr(), state.dim, state.stream,
+             out.ctypes.data_as(C.c_void_p))
+        return complex(out[0], out[1])
+
     def get_expectation_value(self, state) -> float:
-        vals = self.term_values(state)
-        coefs = np.array([t.coef for t in self.terms], dtype=np.complex128)
-        return float(np.real(np.sum(coefs * vals)))
+        """Re sum_k coef_k <P_k>.  For a state vector one weighted device call folds every term's
+        contribution into a single FP64 sum (no per-term values); a density matrix sums term_values."""
+        if not self.terms:
+            return 0.0
+        return self.get_expectation_value_complex(state).real
 
     get_expectation_value_single_thread = get_expectation_value
+
+
+def set_expectation_specialized(mode: int) -> None:
+    """0: generic expectation kernel only; 1 (default): per-pass kernels generated when the same terms
+    are evaluated a second time on >= 20 qubits; 2: generated at the first evaluation, any size."""
+    call("qs_set_expectation_specialized", int(mode))
+
+
+def expectation_specialized_info() -> tuple[int, float]:
+    """(launches of generated expectation kernels so far, compile ms of the last generated plan)."""
+    n = C.c_ulonglong()
+    ms = C.c_double()
+    call("qs_expectation_specialized_info", C.byref(n), C.byref(ms))
+    return n.value, ms.value
