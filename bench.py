@@ -275,6 +275,9 @@ def fused_comparison(n: int, layers: int, stream, with_gate_by_gate: bool, reps:
     plain.set_zero_state()
     circ.update_quantum_state(plain, mode="staged")
     fused = Q.QuantumStateC64(n)
+    circ.set_c64_executor("fp64")  # the other complex64 executor: FP64 passes over the complex64 state
+    t_c64_fp64 = timed(lambda: (fused.set_zero_state(), circ.update_quantum_state(fused)))
+    circ.set_c64_executor("tensor")
     t_fused = timed(lambda: (fused.set_zero_state(), circ.update_quantum_state(fused)))
     fused.set_zero_state()
     circ.update_quantum_state(fused)
@@ -285,6 +288,7 @@ def fused_comparison(n: int, layers: int, stream, with_gate_by_gate: bool, reps:
     passes, blocks = circ.fused_stats()
     out = {"workload": f"U3 + CZ(random matching) n={n} layers={layers} ({len(gates)} gates)",
            "plain_c128_staged_s": t_staged, "plain_c128_gate_by_gate_s": t_gbg, "fused_c64_tc_s": t_fused,
+           "c64_fp64_passes_s": t_c64_fp64,
            "speedup_vs_staged": t_staged / t_fused,
            "speedup_vs_gate_by_gate": (t_gbg / t_fused) if t_gbg else None,
            "infidelity": inf, "abs_dH": abs(float(np.dot(coefs, ev_plain - ev_fused))),
@@ -294,7 +298,8 @@ def fused_comparison(n: int, layers: int, stream, with_gate_by_gate: bool, reps:
     return out
 
 
-def batched_throughput(instances: int, budget_gb: float, seed: int = 4004, precisions=("c128", "c64")):
+def batched_throughput(instances: int, budget_gb: float, seed: int = 4004,
+                       precisions=("c128", "c64", "c64_tensor")):
     """Config 4: hardware-efficient-ansatz instances, n ~ U{10..24}, depth ~ U{4..16}, RY RZ + CZ ring,
     200 strings of weight <= 4 each.  Circuits are built once (outside the timed region, as a variational
     loop reuses them); the timed region is admission + circuit application + <H> for all instances."""
@@ -312,9 +317,12 @@ def batched_throughput(instances: int, budget_gb: float, seed: int = 4004, preci
     out = {"workload": f"{instances} HEA instances, n~U{{10..24}}, depth~U{{4..16}}, 200 strings each",
            "host_build_s": t_build, "memory_budget_gb": budget_gb}
     for prec in precisions:
-        runner = BatchRunner(int(budget_gb * (1 << 30)), precision=prec)
+        # "c64": the default complex64 batch executor (FP64 passes over complex64 tiles when every gate
+        # is stageable); "c64_tensor": the tensor-core blocks forced
+        kw = {"precision": "c64", "c64_executor": "tensor"} if prec == "c64_tensor" else {"precision": prec}
+        runner = BatchRunner(int(budget_gb * (1 << 30)), **kw)
         runner.run(jobs[: min(len(jobs), 64)])  # warm-up: plan building and first launches
-        runner = BatchRunner(int(budget_gb * (1 << 30)), precision=prec)
+        runner = BatchRunner(int(budget_gb * (1 << 30)), **kw)
         t0 = time.perf_counter()
         e = runner.run(jobs)
         dt = time.perf_counter() - t0

@@ -529,6 +529,13 @@ QS_API int qs_debug_batch_wait_expiry_fused_c64(qs_circuit_t circuit, void* stat
  * waiting, bounded, for its previous pass).  Synchronises `stream`. */
 QS_API int qs_batch_update_quantum_states_fused_c64(qs_circuit_t const* circuits, void* const* states_c64,
     QS_UINT count, void* stream);
+/* Many circuits on complex64 states in one persistent launch with a chosen executor: exec 0 = tensor-core
+ * blocks (qs_batch_update_quantum_states_fused_c64), 1 = FP64 passes over the complex64 tiles (the
+ * kernel of qs_batch_update_quantum_states, widening on load and rounding on store; gates of <= 2
+ * qubits, n >= 4), -1 = FP64 passes when every circuit's gates are stageable, else tensor cores.
+ * Synchronises `stream`. */
+QS_API int qs_batch_update_quantum_states_c64(qs_circuit_t const* circuits, void* const* states_c64, QS_UINT count,
+    int exec, void* stream);
 /* <P_k> for the Pauli terms of many complex128 states.  Terms of state i are term_offsets[i] ..
  * term_offsets[i+1]-1 (masks as qs_expectation_value_pauli_batch); values[k] receives <P_k>.  States
  * of fewer than 18 qubits share one launch (jobs of 16 Z-only strings or one bit-flip string);
@@ -570,6 +577,17 @@ QS_API int qs_noise_simulator_execute(qs_circuit_t circuit, const void* initial_
  * composed in FP64 and applied on the tensor cores as split-bf16 products (hi*hi + hi*lo + lo*hi)
  * with FP32 accumulation.  Needs >= 10 qubits and gates of <= 6 qubits (no noise channels). */
 QS_API int qs_circuit_update_quantum_state_fused_c64(qs_circuit_t circuit, void* state_c64, QS_ITYPE dim, void* stream);
+/* Applies the circuit to a complex64 state with the circuit's complex64 executor (see
+ * qs_circuit_set_c64_executor): the tensor-core blocks above, or FP64 passes over the complex64 state
+ * (each tile widened to FP64 in shared memory, gates fused into blocks of <= 2 qubits, rounded back
+ * on the store; >= 4 qubits). */
+QS_API int qs_circuit_update_quantum_state_c64(qs_circuit_t circuit, void* state_c64, QS_ITYPE dim, void* stream);
+/* Complex64 executor of qs_circuit_update_quantum_state_c64: 0 = tensor-core blocks, 1 = FP64 passes,
+ * -1 (default) = the tensor-core blocks when they take the circuit (>= 10 qubits, gates of <= 6
+ * qubits), else the FP64 passes. */
+QS_API int qs_circuit_set_c64_executor(qs_circuit_t circuit, int mode);
+/* The executor of the last complex64 run on this circuit (0 tensor cores, 1 FP64 passes, -1 none). */
+QS_API int qs_circuit_c64_executor_info(qs_circuit_t circuit, int* chosen);
 /* Statistics of a complex64 state with FP64 accumulation (the fused path's reductions): norm, the
  * inner product <bra_c128|ket_c64> (for the infidelity 1 - |<psi|psi_FP64>|^2), batched <P_k>
  * (masks as qs_expectation_value_pauli_batch), sum_k coef_k <P_k> and sampling with supplied uniforms. */

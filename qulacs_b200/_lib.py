@@ -152,6 +152,10 @@ SIGNATURES = {
     "qs_circuit_set_fusion": [P, I],
     "qs_circuit_fusion_info": [P, C.POINTER(I), C.POINTER(U), C.POINTER(U), P],
     "qs_circuit_update_quantum_state_fused_c64": [P, P, IT, P],
+    "qs_circuit_update_quantum_state_c64": [P, P, IT, P],
+    "qs_circuit_set_c64_executor": [P, C.c_int],
+    "qs_circuit_c64_executor_info": [P, P],
+    "qs_batch_update_quantum_states_c64": [P, P, U, C.c_int, P],
     "qs_batch_update_quantum_states": [P, P, U, P],
     "qs_debug_batch_wait_expiry": [P, P, U, P],
     "qs_debug_batch_wait_expiry_fused_c64": [P, P, U, P],

@@ -4,9 +4,10 @@
 waves whose states fit an HBM budget (footprint 16 B x 2^n each, carved from one arena per wave),
 and for each wave applies every circuit in ONE persistent kernel launch
 (``qs_batch_update_quantum_states``) and evaluates every observable term in ONE more launch
-(``qs_batch_expectation_values``).  ``precision="c64"`` runs the wave on the fused complex64
-tensor-core path instead (``qs_batch_update_quantum_states_fused_c64``: plans built on host threads in
-parallel, circuits side by side on several streams; reductions still FP64).
+(``qs_batch_expectation_values``).  ``precision="c64"`` keeps the states in complex64 and runs the wave
+in one persistent launch of the chosen executor (``qs_batch_update_quantum_states_c64``): FP64 passes
+over complex64 tiles (``c64_executor="fp64"``; "auto" takes it whenever every gate is stageable) or
+6-qubit blocks on the tensor cores ("tensor"); reductions are FP64 either way.
 """
 from __future__ import annotations
 
@@ -35,11 +36,15 @@ class BatchStats:
 
 
 class BatchRunner:
-    def __init__(self, memory_budget_bytes: int, precision: str = "c128", stream: int | None = None):
+    def __init__(self, memory_budget_bytes: int, precision: str = "c128", stream: int | None = None,
+                 c64_executor: str = "auto"):
         if precision not in ("c128", "c64"):
             raise ValueError("precision must be c128 or c64")
+        if c64_executor not in ("auto", "tensor", "fp64"):
+            raise ValueError("c64_executor must be auto, tensor or fp64")
         self.budget = int(memory_budget_bytes)
         self.precision = precision
+        self.c64_executor = {"auto": -1, "tensor": 0, "fp64": 1}[c64_executor]
         self.stream = stream
         self.stats = BatchStats()
 
@@ -96,8 +101,8 @@ class BatchRunner:
             k = len(wave)
             states = (C.c_void_p * k)(*ptrs)
             circs = (C.c_void_p * k)(*[jobs[i][0]._h for i in wave])
-            if c64:  # fused tensor-core path: plans built in parallel, circuits side by side on streams
-                call("qs_batch_update_quantum_states_fused_c64", circs, states, k, self.stream)
+            if c64:  # one persistent launch: FP64 passes over complex64 tiles, or tensor-core blocks
+                call("qs_batch_update_quantum_states_c64", circs, states, k, self.c64_executor, self.stream)
             else:  # every circuit in one persistent launch
                 call("qs_batch_update_quantum_states", circs, states, k, self.stream)
             # all terms of all observables in one launch

@@ -193,11 +193,12 @@ class QuantumCircuit:
             raise ValueError("depolarizing noise can be used up to 2 qubits")
 
     def update_quantum_state(self, state, mode: str = "staged") -> None:
-        """Apply the circuit.  A QuantumStateC64 always takes the fused tensor-core path."""
+        """Apply the circuit.  A QuantumStateC64 takes the circuit's complex64 executor (set_c64_executor:
+        6-qubit blocks on the tensor cores, or FP64 passes over the complex64 state)."""
         if state.get_qubit_count() != self.qubit_count:
             raise ValueError("state qubit count differs from the circuit's")
         if type(state).__name__ == "QuantumStateC64":
-            call("qs_circuit_update_quantum_state_fused_c64", self._h, state.data_ptr(), state.dim, state.stream)
+            call("qs_circuit_update_quantum_state_c64", self._h, state.data_ptr(), state.dim, state.stream)
             return
         m = {"gate_by_gate": _lib.EXEC_GATE_BY_GATE, "staged": _lib.EXEC_STAGED,
              "staged_fused": _lib.EXEC_STAGED_FUSED}[mode]
@@ -205,6 +206,20 @@ class QuantumCircuit:
             call("qs_circuit_update_quantum_state", self._h, state.data_ptr(), state.dim, m, state.stream)
         else:
             call("qs_circuit_update_density_matrix", self._h, state.data_ptr(), state.dim, m, state.stream)
+
+    _C64_EXEC = {"auto": -1, "tensor": 0, "fp64": 1}
+
+    def set_c64_executor(self, mode) -> None:
+        """Executor for complex64 states: "tensor" (6-qubit blocks on the tensor cores, >= 10 qubits, gates
+        of <= 6 qubits), "fp64" (FP64 passes over the complex64 state, gates of <= 2 qubits) or "auto"
+        (default: the tensor cores when they take the circuit, else the FP64 passes)."""
+        call("qs_circuit_set_c64_executor", self._h, self._C64_EXEC[mode] if isinstance(mode, str) else int(mode))
+
+    def c64_executor_info(self):
+        """Executor of the last complex64 run: "tensor", "fp64" or None."""
+        ch = C.c_int()
+        call("qs_circuit_c64_executor_info", self._h, C.byref(ch))
+        return {0: "tensor", 1: "fp64"}.get(ch.value)
 
     def set_fusion(self, k: int) -> None:
         """Block size of mode="staged_fused": 0..6, or -1 to let the autotuner choose (default)."""

@@ -53,7 +53,20 @@ struct Circuit {
     int bk = -1;
     std::vector<GateRec> bgates;
     std::shared_ptr<StagedPlan> bplan;
+    // complex64 states: the executor (-1: tensor cores when they take the circuit, else FP64 passes;
+    // 0: 6-qubit blocks on the tensor cores, fused_c64.cu; 1: FP64 passes over the complex64 state,
+    // staged.cu), the executor of the last run, and the FP64 passes' gate list (blocks of <= 2 qubits)
+    // and schedule
+    int c64_exec = -1;
+    int c64_chosen = -1;
+    int ck = -1;
+    std::vector<GateRec> cgates;
+    std::shared_ptr<StagedPlan> cplan;
     void invalidate() {
+        cplan.reset();
+        cgates.clear();
+        ck = -1;
+        c64_chosen = -1;
         dm_vec.reset();
         bplan.reset();
         bgates.clear();
@@ -78,6 +91,20 @@ std::vector<GateRec> dm_vector_gates(const std::vector<GateRec>& G, UINT n);
 int run_staged(Circuit& c, void* state, ITYPE dim, cudaStream_t st);
 int run_staged_fused(Circuit& c, void* state, ITYPE dim, cudaStream_t st);
 int staged_pass_count(Circuit& c, ITYPE dim, UINT* out);
+// staged.cu: the circuit as FP64 passes over a complex64 state (blocks of <= 2 qubits; every gate must
+// be stageable)
+int run_staged_c64(Circuit& c, void* state_c64, ITYPE dim, cudaStream_t st);
+// fused_c64.cu: the tensor-core executor, and whether it takes the circuit
+int run_fused_c64(Circuit& c, void* state, ITYPE dim, cudaStream_t st);
+bool fused_c64_accepts(const Circuit& c);
+// Persistent multi-circuit launches (one state per circuit): staged.cu's FP64 passes over complex128
+// or (c64) complex64 states, and fused_c64.cu's tensor-core blocks over complex64 states.  Dependency
+// waits are bounded by wait_ns; self_dep >= 0 makes that work record wait on itself (expiry checks).
+constexpr unsigned long long kBatchWaitNs = 2000000000ULL;
+int batch_update(Circuit* const* cs, void* const* states, UINT count, cudaStream_t st, unsigned long long wait_ns,
+    int self_dep, bool c64);
+int batch_update_fused_c64(Circuit* const* cs, void* const* states, UINT count, cudaStream_t st,
+    unsigned long long wait_ns, int self_dep);
 
 // fusion.cpp: U <- G U for gate g on block-local bit positions `pos` (targets then controls) of a
 // kb-qubit block matrix U (2^kb x 2^kb, row-major); and the greedy k-qubit fusion of a gate list.

@@ -1173,6 +1173,35 @@ int run_fused_c64(Circuit& c, void* state, ITYPE dim, cudaStream_t st) {
     return QS_OK;
 }
 
+// Whether the tensor-core executor takes the circuit: >= 10 qubits, every gate on <= 6 qubits, no
+// noise channel.
+bool fused_c64_accepts(const Circuit& c) {
+    if (c.n < 10) return false;
+    for (const GateRec& g : c.gates)
+        if (!fusable(g)) return false;
+    return true;
+}
+
+// The executor of a single complex64 run: forced, or the tensor cores whenever they take the circuit,
+// else FP64 passes.  Measured on a B200 over HEA, U3+CZ and layered circuits of 12..30 qubits (depth
+// 4..20), the tensor-core run was the faster or equal one in 13 of 15 and at most 7 % slower in the
+// other two; the FP64 passes take circuits below 10 qubits.  (Batches choose differently, see
+// qs_batch_update_quantum_states_c64: there many circuits fill the device and the FP64 passes' cheaper
+// small tiles win.)
+int choose_c64_executor(Circuit& c, int* exec) {
+    if (c.c64_exec >= 0) {
+        *exec = c.c64_exec;
+    } else if (fused_c64_accepts(c)) {
+        *exec = 0;
+    } else if (c.n >= 4) {  // the FP64 passes hold 16 amplitudes per thread
+        *exec = 1;
+    } else {
+        return set_error(QS_ERR_NOT_SUPPORTED, "complex64 states need at least 4 qubits");
+    }
+    c.c64_chosen = *exec;
+    return QS_OK;
+}
+
 // Host-only export of fused block `index` (in application order): the pass's tile qubits, the
 // block's 6 tile-local bits, its FP64 matrix and its bf16 hi|lo operand image.
 int fused_block_export(Circuit& c, UINT index, UINT* tile_qubits, int* m_out, UINT* bits, double* U_out,
@@ -1222,12 +1251,52 @@ int fused_stats(Circuit& c, UINT* passes, UINT* blocks) {
 
 extern "C" {
 
+QS_API int qs_circuit_set_c64_executor(qs_circuit_t circuit, int mode) {
+    qs::Circuit* c = reinterpret_cast<qs::Circuit*>(circuit);
+    if (!c) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "null circuit");
+    if (mode < -1 || mode > 1) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "complex64 executor must be -1, 0 or 1");
+    c->c64_exec = mode;
+    return QS_OK;
+}
+
+QS_API int qs_circuit_update_quantum_state_c64(qs_circuit_t circuit, void* state_c64, QS_ITYPE dim, void* stream) {
+    qs::Circuit* c = reinterpret_cast<qs::Circuit*>(circuit);
+    if (!c || !state_c64) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "null argument");
+    if (dim != (1ULL << c->n)) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "dim differs from 2^qubit_count");
+    int exec = 0;
+    QS_TRY(qs::choose_c64_executor(*c, &exec));
+    return exec == 0 ? qs::run_fused_c64(*c, state_c64, dim, (cudaStream_t)stream)
+                     : qs::run_staged_c64(*c, state_c64, dim, (cudaStream_t)stream);
+}
+
+QS_API int qs_circuit_c64_executor_info(qs_circuit_t circuit, int* chosen) {
+    qs::Circuit* c = reinterpret_cast<qs::Circuit*>(circuit);
+    if (!c || !chosen) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "null argument");
+    *chosen = c->c64_chosen;
+    return QS_OK;
+}
+
 QS_API int qs_circuit_update_quantum_state_fused_c64(qs_circuit_t circuit, void* state_c64, QS_ITYPE dim, void* stream) {
     qs::Circuit* c = reinterpret_cast<qs::Circuit*>(circuit);
     if (!c) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "null circuit");
     if (dim != (1ULL << c->n))
         return qs::set_error(QS_ERR_INVALID_ARGUMENT, "state dimension does not match the circuit's qubit count");
     return qs::run_fused_c64(*c, state_c64, dim, (cudaStream_t)stream);
+}
+
+QS_API int qs_batch_update_quantum_states_c64(qs_circuit_t const* circuits, void* const* states_c64, QS_UINT count,
+    int exec, void* stream) {
+    if (!circuits || !states_c64) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "null argument");
+    if (exec < -1 || exec > 1) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "complex64 executor must be -1, 0 or 1");
+    auto cs = reinterpret_cast<qs::Circuit* const*>(circuits);
+    for (QS_UINT i = 0; i < count; ++i)
+        if (!cs[i] || !states_c64[i]) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "null circuit or state");
+    if (exec == 0)
+        return qs::batch_update_fused_c64(cs, states_c64, count, (cudaStream_t)stream, qs::kFusedBatchWaitNs, -1);
+    const int rc = qs::batch_update(cs, states_c64, count, (cudaStream_t)stream, qs::kBatchWaitNs, -1, true);
+    if (rc != QS_ERR_NOT_SUPPORTED || exec == 1) return rc;
+    // some circuit has a gate the FP64 passes cannot stage (refused before any launch): tensor cores
+    return qs::batch_update_fused_c64(cs, states_c64, count, (cudaStream_t)stream, qs::kFusedBatchWaitNs, -1);
 }
 
 QS_API int qs_batch_update_quantum_states_fused_c64(qs_circuit_t const* circuits, void* const* states_c64,

@@ -92,6 +92,16 @@ __device__ __forceinline__ double2 ld_stream(const double2* p) {
 __device__ __forceinline__ void st_stream(double2* p, double2 v) {
     asm volatile("st.global.cs.v2.f64 [%0], {%1, %2};" ::"l"(p), "d"(v.x), "d"(v.y) : "memory");
 }
+// An amplitude of a complex128 or complex64 state as FP64, and back (complex64: rounded to nearest).
+__device__ __forceinline__ double2 ld_amp(const double2* p) { return ld_stream(p); }
+__device__ __forceinline__ double2 ld_amp(const float2* p) {
+    const float2 v = __ldcs(p);
+    return make_double2((double)v.x, (double)v.y);
+}
+__device__ __forceinline__ void st_amp(double2* p, double2 v) { st_stream(p, v); }
+__device__ __forceinline__ void st_amp(float2* p, double2 v) {
+    __stcs(p, make_float2(__double2float_rn(v.x), __double2float_rn(v.y)));
+}
 
 struct Mat2 {
     double2 m[4];  // row-major

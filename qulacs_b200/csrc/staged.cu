@@ -227,7 +227,8 @@ __device__ __forceinline__ UINT swz(UINT u) { return u ^ (((u >> 4) ^ (u >> 7) ^
 // lo_off takes tid's bits 0..6 to the tile qubits q[0..6], hi_off[k] takes k's bits to q[7..].
 
 // Global rows of 16 amplitudes per thread from the swizzled tile to HBM (rows k0 .. k0 + 15).
-__device__ __forceinline__ void tile_rows_store(double2* __restrict__ s, const double2* tile, ITYPE off,
+template <class T>
+__device__ __forceinline__ void tile_rows_store(T* __restrict__ s, const double2* tile, ITYPE off,
     const ITYPE* hi_off, UINT tsize, int k0) {
     const UINT tid = threadIdx.x;
     double2 v[16];
@@ -236,14 +237,15 @@ __device__ __forceinline__ void tile_rows_store(double2* __restrict__ s, const d
         if (tid + (UINT)(k0 + k) * kStThreads < tsize) v[k] = tile[swz(tid + (UINT)(k0 + k) * kStThreads)];
 #pragma unroll
     for (int k = 0; k < 16; ++k)
-        if (tid + (UINT)(k0 + k) * kStThreads < tsize) st_stream(s + (off | hi_off[k0 + k]), v[k]);
+        if (tid + (UINT)(k0 + k) * kStThreads < tsize) st_amp(s + (off | hi_off[k0 + k]), v[k]);
 }
 
 // One tile of one pass: load, apply every phase, store.  Shared by the per-pass kernel and the
-// persistent multi-circuit kernel.  `tile` holds 2^m amplitudes (m <= kTileBits).  Ends with a CTA
+// persistent multi-circuit kernel.  `tile` holds 2^m amplitudes (m <= kTileBits) in FP64 whatever the
+// state's type E (complex128, or complex64 widened on load and rounded on store).  Ends with a CTA
 // barrier so the shared buffers can be reused immediately.
-template <int MAX_BITS, bool FOLDS>
-__device__ __forceinline__ void staged_tile(double2* __restrict__ s, const StPassArgs& a, ITYPE T, double2* tile,
+template <int MAX_BITS, bool FOLDS, class E>
+__device__ __forceinline__ void staged_tile(E* __restrict__ s, const StPassArgs& a, ITYPE T, double2* tile,
     ITYPE* hi_off) {
     const int m = a.m;
     const UINT tsize = 1u << m;
@@ -265,17 +267,33 @@ __device__ __forceinline__ void staged_tile(double2* __restrict__ s, const StPas
         __syncthreads();
     }
     if (!hbm_first) {
-        // 16-byte cp.async copies straight into the swizzled tile: every copy of a thread in flight at
-        // once, without holding registers
         const ITYPE off = base | lo_off;
+        if constexpr (sizeof(E) == sizeof(double2)) {
+            // 16-byte cp.async copies straight into the swizzled tile: every copy of a thread in flight at
+            // once, without holding registers
 #pragma unroll
-        for (int k = 0; k < (1 << (MAX_BITS - 7)); ++k)
-            if ((UINT)tid + (UINT)k * kStThreads < tsize) {
-                const unsigned dst = (unsigned)__cvta_generic_to_shared(tile + swz((UINT)tid + (UINT)k * kStThreads));
-                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(s + (off | hi_off[k]))
-                             : "memory");
+            for (int k = 0; k < (1 << (MAX_BITS - 7)); ++k)
+                if ((UINT)tid + (UINT)k * kStThreads < tsize) {
+                    const unsigned dst =
+                        (unsigned)__cvta_generic_to_shared(tile + swz((UINT)tid + (UINT)k * kStThreads));
+                    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(s + (off | hi_off[k]))
+                                 : "memory");
+                }
+            asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
+        } else {
+            // complex64: widened in registers, 4 loads in flight per thread before their stores
+#pragma unroll
+            for (int k0 = 0; k0 < (1 << (MAX_BITS - 7)); k0 += 4) {
+                double2 v[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    if ((UINT)tid + (UINT)(k0 + k) * kStThreads < tsize) v[k] = ld_amp(s + (off | hi_off[k0 + k]));
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    if ((UINT)tid + (UINT)(k0 + k) * kStThreads < tsize)
+                        tile[swz((UINT)tid + (UINT)(k0 + k) * kStThreads)] = v[k];
             }
-        asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
+        }
         __syncthreads();
     }
     const UINT ncos = tsize >> kPhaseBits;  // cosets per phase
@@ -311,7 +329,7 @@ __device__ __forceinline__ void staged_tile(double2* __restrict__ s, const StPas
 #pragma unroll
                 for (int g = 0; g < 16; ++g) {
                     if (g) gi ^= gb[(g & 1) ? 0 : (g & 2) ? 1 : (g & 4) ? 2 : 3];
-                    r[g ^ (g >> 1)] = ld_stream(s + gi);
+                    r[g ^ (g >> 1)] = ld_amp(s + gi);
                 }
             } else {
 #pragma unroll
@@ -327,7 +345,7 @@ __device__ __forceinline__ void staged_tile(double2* __restrict__ s, const StPas
 #pragma unroll
                 for (int g = 0; g < 16; ++g) {
                     if (g) gi ^= gb[(g & 1) ? 0 : (g & 2) ? 1 : (g & 4) ? 2 : 3];
-                    st_stream(s + gi, r[g ^ (g >> 1)]);
+                    st_amp(s + gi, r[g ^ (g >> 1)]);
                 }
             } else {
 #pragma unroll
@@ -348,8 +366,8 @@ __device__ __forceinline__ void staged_tile(double2* __restrict__ s, const StPas
 }
 
 // One CTA per tile; the tile (2^m x 16 bytes, up to 64 KiB) is dynamic shared memory.
-template <bool FOLDS>
-__global__ void __launch_bounds__(kStThreads, 3) k_staged_pass(double2* __restrict__ s, const __grid_constant__ StPassArgs a) {
+template <bool FOLDS, class E>
+__global__ void __launch_bounds__(kStThreads, 3) k_staged_pass(E* __restrict__ s, const __grid_constant__ StPassArgs a) {
     extern __shared__ double2 st_tile[];
     __shared__ ITYPE hi_off[1 << (kTileBits - 7)];
     staged_tile<kTileBits, FOLDS>(s, a, blockIdx.x, st_tile, hi_off);
@@ -364,9 +382,13 @@ static int staged_allow_smem() {
     std::lock_guard<std::mutex> lock(mu);
     if ((int)done.size() <= dev) done.resize(dev + 1, 0);
     if (!done[dev]) {
-        QS_CUDA_CHECK(cudaFuncSetAttribute(k_staged_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        QS_CUDA_CHECK(cudaFuncSetAttribute(k_staged_pass<false, double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
             (int)(sizeof(double2) << kTileBits)));
-        QS_CUDA_CHECK(cudaFuncSetAttribute(k_staged_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        QS_CUDA_CHECK(cudaFuncSetAttribute(k_staged_pass<true, double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            (int)(sizeof(double2) << kTileBits)));
+        QS_CUDA_CHECK(cudaFuncSetAttribute(k_staged_pass<false, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            (int)(sizeof(double2) << kTileBits)));
+        QS_CUDA_CHECK(cudaFuncSetAttribute(k_staged_pass<true, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
             (int)(sizeof(double2) << kTileBits)));
         done[dev] = 1;
     }
@@ -506,10 +528,11 @@ struct DevPass {
     std::vector<double2> spec_params;  // its parameter block
 };
 
-static void launch_pass(double2* state, const DevPass& d, ITYPE tiles, cudaStream_t st) {
-    const size_t smem = sizeof(double2) << d.args.m;
-    if (d.folds) k_staged_pass<true><<<(unsigned)tiles, kStThreads, smem, st>>>(state, d.args);
-    else k_staged_pass<false><<<(unsigned)tiles, kStThreads, smem, st>>>(state, d.args);
+template <class E>
+static void launch_pass(E* state, const DevPass& d, ITYPE tiles, cudaStream_t st) {
+    const size_t smem = sizeof(double2) << d.args.m;  // the tile is FP64 for either state type
+    if (d.folds) k_staged_pass<true, E><<<(unsigned)tiles, kStThreads, smem, st>>>(state, d.args);
+    else k_staged_pass<false, E><<<(unsigned)tiles, kStThreads, smem, st>>>(state, d.args);
 }
 
 struct StagedPlan {
@@ -1075,6 +1098,39 @@ int run_staged_fused(Circuit& c, void* state, ITYPE dim, cudaStream_t st) {
     return run_plan(c.fgates, *c.fplan, state, dim, st);
 }
 
+// ---------------------------------------------------------------- complex64 states, FP64 passes
+// The staged schedule over a complex64 state: each tile is widened to FP64 in shared memory, every
+// phase runs in FP64 (the generic pass kernel's code), and the tile is rounded back on the store, so a
+// pass moves half the bytes of the complex128 pass.  Gates are fused into blocks of at most 2 qubits
+// (a forced QS_EXEC_STAGED_FUSED size of 0..2 is kept) so that every block is a pass op.
+static int c64_block_size(const Circuit& c) { return (c.fusion_k >= 0 && c.fusion_k <= 2) ? c.fusion_k : 2; }
+
+static int ensure_c64_plan(Circuit& c, ITYPE dim) {
+    const int k = c64_block_size(c);
+    if (c.cplan && c.cplan->dim == dim && c.ck == k) return QS_OK;
+    c.cgates = fuse_gates(c.gates, k);
+    c.ck = k;
+    QS_TRY(build_plan(c.cgates, c.n, dim, &c.cplan));
+    for (const DevPass& d : c.cplan->passes)
+        if (d.single) {
+            c.cplan.reset();
+            return set_error(QS_ERR_NOT_SUPPORTED,
+                "complex64 FP64 passes: every gate must be stageable (<= 2 targets and controls together)");
+        }
+    return QS_OK;
+}
+
+int run_staged_c64(Circuit& c, void* state, ITYPE dim, cudaStream_t st) {
+    if (c.n < kPhaseBits) return set_error(QS_ERR_NOT_SUPPORTED, "complex64 FP64 passes need at least 4 qubits");
+    QS_TRY(ensure_c64_plan(c, dim));
+    QS_TRY(staged_allow_smem());
+    for (const DevPass& d : c.cplan->passes) {
+        launch_pass((float2*)state, d, dim >> d.args.m, st);
+        QS_TRY(check_launch("k_staged_pass"));
+    }
+    return QS_OK;
+}
+
 int staged_pass_count(Circuit& c, ITYPE dim, UINT* out) {
     if (c.n < kPhaseBits) {
         *out = (UINT)c.gates.size();
@@ -1220,13 +1276,12 @@ namespace qs {
 
 struct BatchRec {
     StPassArgs args;
-    double2* state;
+    void* state;  // complex128 or complex64 (one type per launch)
     ITYPE tiles;
     ITYPE prefix;  // first work item of this record
     int dep;       // record of the previous pass of the same circuit, -1 for pass 0
 };
 
-constexpr unsigned long long kBatchWaitNs = 2000000000ULL;  // dependency wait limit of a batch launch
 
 __device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;
@@ -1240,6 +1295,7 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
     return v;
 }
 
+template <class E>
 __global__ void __launch_bounds__(kStThreads, 3) k_batch_staged(const BatchRec* __restrict__ recs, int nrec,
     ITYPE total, unsigned long long* head, unsigned* done, int* err, unsigned long long wait_ns) {
     __shared__ double2 tile[1 << kBatchTileBits];
@@ -1247,7 +1303,7 @@ __global__ void __launch_bounds__(kStThreads, 3) k_batch_staged(const BatchRec* 
     __shared__ ITYPE s_item;
     __shared__ int s_rec, s_abort;
     __shared__ StPassArgs s_args;  // the record's pass, copied so the tile code indexes shared memory
-    __shared__ double2* s_state;
+    __shared__ E* s_state;
     const int tid = threadIdx.x;
     while (true) {
         if (tid == 0) {
@@ -1280,7 +1336,7 @@ __global__ void __launch_bounds__(kStThreads, 3) k_batch_staged(const BatchRec* 
         if (s_item >= total || s_abort) break;
         if (tid == 0) {
             s_args = recs[s_rec].args;
-            s_state = recs[s_rec].state;
+            s_state = (E*)recs[s_rec].state;
         }
         __syncthreads();
         staged_tile<kBatchTileBits, true>(s_state, s_args, s_item - recs[s_rec].prefix, tile, hi_off);
@@ -1306,8 +1362,8 @@ static int ensure_batch_plan(Circuit& c, ITYPE dim) {
 
 // `wait_ns`: the dependency wait limit; `self_dep` >= 0 makes that work record depend on itself (a
 // counter nothing can complete), which only the wait-expiry check below uses.
-int batch_update(Circuit* const* cs, void* const* states, UINT count, cudaStream_t st,
-    unsigned long long wait_ns = kBatchWaitNs, int self_dep = -1) {
+int batch_update(Circuit* const* cs, void* const* states, UINT count, cudaStream_t st, unsigned long long wait_ns,
+    int self_dep, bool c64) {
     if (count == 0) return QS_OK;
     for (UINT i = 0; i < count; ++i)
         if (cs[i]->n < kPhaseBits) return set_error(QS_ERR_NOT_SUPPORTED, "batch: circuits need at least 4 qubits");
@@ -1363,7 +1419,7 @@ int batch_update(Circuit* const* cs, void* const* states, UINT count, cudaStream
             if (p >= passes[i].size()) continue;
             BatchRec r{};
             r.args = passes[i][p]->args;
-            r.state = (double2*)states[i];
+            r.state = states[i];
             r.tiles = (1ULL << cs[i]->n) >> r.args.m;
             r.prefix = total;
             r.dep = last[i];
@@ -1387,10 +1443,16 @@ int batch_update(Circuit* const* cs, void* const* states, UINT count, cudaStream
     QS_CUDA_CHECK(cudaMemcpyAsync(drec, recs.data(), brec, cudaMemcpyHostToDevice, st));
     QS_CUDA_CHECK(cudaMemsetAsync(ddone, 0, (brec + bdone + 256) - brec, st));
     int per_sm = 0;
-    QS_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_staged, kStThreads, 0));
+    if (c64)
+        QS_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_staged<float2>, kStThreads, 0));
+    else
+        QS_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_staged<double2>, kStThreads, 0));
     const ITYPE resident = (ITYPE)std::max(1, per_sm) * sm_count();
     const unsigned grid = (unsigned)std::min<ITYPE>(resident, total);
-    k_batch_staged<<<grid, kStThreads, 0, st>>>(drec, (int)recs.size(), total, dhead, ddone, derr, wait_ns);
+    if (c64)
+        k_batch_staged<float2><<<grid, kStThreads, 0, st>>>(drec, (int)recs.size(), total, dhead, ddone, derr, wait_ns);
+    else
+        k_batch_staged<double2><<<grid, kStThreads, 0, st>>>(drec, (int)recs.size(), total, dhead, ddone, derr, wait_ns);
     QS_TRY(check_launch("k_batch_staged"));
     int err = 0;
     QS_CUDA_CHECK(cudaMemcpyAsync(&err, derr, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -1409,7 +1471,7 @@ extern "C" QS_API int qs_batch_update_quantum_states(const qs_circuit_t* circuit
         cs[i] = reinterpret_cast<qs::Circuit*>(circuits[i]);
         if (!cs[i] || !states[i]) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "null circuit or state");
     }
-    return qs::batch_update(cs.data(), states, count, (cudaStream_t)stream);
+    return qs::batch_update(cs.data(), states, count, (cudaStream_t)stream, qs::kBatchWaitNs, -1, false);
 }
 
 // Failure-path check of the batch executor's bounded dependency wait: runs `circuit` on `state` as a
@@ -1434,5 +1496,6 @@ extern "C" QS_API int qs_debug_batch_wait_expiry(qs_circuit_t circuit, void* sta
         passes = (UINT)H.passes.size();
     }
     if (passes == 0) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "circuit has no passes");
-    return qs::batch_update(cs, ss, 1, (cudaStream_t)stream, 1000ULL * wait_limit_us, (int)passes - 1);
+    return qs::batch_update(cs, ss, 1, (cudaStream_t)stream, 1000ULL * wait_limit_us, (int)passes - 1, false);
 }
+

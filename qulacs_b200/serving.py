@@ -14,9 +14,10 @@ continuously: all ready expectation requests at once (up to ``max_batch``) go th
 multi-circuit launch plus ONE batched <P> launch; sampling and density-matrix requests run one each.
 Work of different workers overlaps on the device.  Latency = completion - arrival, per request.
 
-``precision="c64"`` runs expectation and sampling requests on the fused complex64 tensor-core path
-(reductions in FP64): a batch of expectation requests is one persistent fused launch plus one batched
-<P> launch; density-matrix requests stay complex128.
+``precision="c64"`` keeps expectation and sampling requests' states in complex64 (reductions in FP64):
+a batch of expectation requests is one persistent launch of FP64 passes over complex64 tiles (the
+tensor-core blocks when some gate cannot be staged) plus one batched <P> launch; a sampling request
+takes its circuit's complex64 executor; density-matrix requests stay complex128.
 
 Served circuits run the generic staged pass kernel, not specialised per-pass kernels: every request
 brings new gate parameters, and compiling a kernel for each would add its compile time to the
@@ -188,8 +189,10 @@ class ServingLoop:
             call("qs_initialize_quantum_state_c64" if c64 else "qs_initialize_quantum_state", r.ptr, 1 << r.n, stream)
         ch = (C.c_void_p * k)(*[c._h for c in circs])
         st = (C.c_void_p * k)(*[r.ptr for r in reqs])
-        call("qs_batch_update_quantum_states_fused_c64" if c64 else "qs_batch_update_quantum_states", ch, st, k,
-             stream)
+        if c64:  # FP64 passes over complex64 tiles when every gate is stageable, else tensor-core blocks
+            call("qs_batch_update_quantum_states_c64", ch, st, k, -1, stream)
+        else:
+            call("qs_batch_update_quantum_states", ch, st, k, stream)
         xm, zm, ny, offs, coefs = [], [], [], [0], []
         for r in reqs:
             for c, tl, ids in r.terms:
@@ -215,7 +218,7 @@ class ServingLoop:
         u = np.ascontiguousarray(r.uniforms)
         if self.precision == "c64":
             call("qs_initialize_quantum_state_c64", r.ptr, 1 << r.n, stream)
-            call("qs_circuit_update_quantum_state_fused_c64", c._h, r.ptr, 1 << r.n, stream)
+            call("qs_circuit_update_quantum_state_c64", c._h, r.ptr, 1 << r.n, stream)
             call("qs_state_sampling_with_uniforms_c64", r.ptr, 1 << r.n, _vp(u), u.size, _vp(out), stream)
         else:
             call("qs_initialize_quantum_state", r.ptr, 1 << r.n, stream)

@@ -65,9 +65,10 @@ def test_batch_states_match_gate_by_gate(port):
             assert np.max(np.abs(v - alone.get_vector())) <= 1e-14
 
 
-def test_batch_fused_c64(port):
+@pytest.mark.parametrize("executor", ["auto", "tensor", "fp64"])
+def test_batch_fused_c64(port, executor):
     jobs, specs = make_jobs(13, 6, 10, 14)
-    got = BatchRunner(1 << 30, precision="c64").run(jobs)
+    got = BatchRunner(1 << 30, precision="c64", c64_executor=executor).run(jobs)
     for (n, gates, terms), e in zip(specs, got):
         psi = np.zeros(1 << n, dtype=np.complex128)
         psi[0] = 1
@@ -172,5 +173,25 @@ def test_fused_c64_persistent_batch_equals_each_circuit_alone():
          (C.c_void_p * len(batch))(*[s.data_ptr() for s in batch]), len(circs), None)
     for c, n, b in zip(circs, sizes, batch):
         alone = QuantumStateC64(n)
+        c.set_c64_executor("tensor")
         c.update_quantum_state(alone)
         assert np.array_equal(b.get_vector(), alone.get_vector()), n
+
+
+def test_c64_fp64_batch_equals_each_circuit_alone():
+    """The persistent batch kernel over complex64 tiles applies each circuit's FP64 passes to its own state
+    as the single-circuit FP64 passes do, up to the tile shape (2^11 in the batch, 2^12 alone): states
+    agree to complex64 rounding."""
+    import ctypes as C
+    from qulacs_b200 import QuantumStateC64
+    from qulacs_b200._lib import call
+    sizes = [6, 14, 11, 20, 13, 16, 9, 18]
+    circs = [W.to_circuit(W.hea_circuit(n, 4 + i % 5, seed=9900 + i), n) for i, n in enumerate(sizes)]
+    batch = [QuantumStateC64(n) for n in sizes]
+    call("qs_batch_update_quantum_states_c64", (C.c_void_p * len(circs))(*[c._h for c in circs]),
+         (C.c_void_p * len(batch))(*[s.data_ptr() for s in batch]), len(circs), 1, None)
+    for c, n, b in zip(circs, sizes, batch):
+        alone = QuantumStateC64(n)
+        c.set_c64_executor("fp64")
+        c.update_quantum_state(alone)
+        assert np.max(np.abs(b.get_vector() - alone.get_vector())) <= 1e-5, n
