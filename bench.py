@@ -331,6 +331,57 @@ def batched_throughput(instances: int, budget_gb: float, seed: int = 4004,
     return out
 
 
+def graph_replay(reps: int = 20):
+    """Captured CUDA graphs against direct calls (wall time per call, host launch overhead included,
+    since that is what a graph removes): a 16-qubit layered circuit gate by gate (454 launches) and
+    staged, and a batch of 64 HEA circuits (n 10..16) in one persistent launch."""
+    import ctypes as C
+
+    import torch
+
+    import qulacs_b200 as Q
+    from qulacs_b200 import workloads as W
+    from qulacs_b200._lib import call
+    from qulacs_b200.graph import capture_batch, capture_circuit
+
+    def wall(fn):
+        fn()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            fn()
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) / reps * 1e3
+
+    out = {"workload": "16q layered depth 10 (454 gates); 64 HEA circuits n~U{10..16} depth 6", "reps": reps}
+    n = 16
+    circ = W.to_circuit(W.layered_rotation_circuit(n, 10, 7), n)
+    s = Q.QuantumState(n)
+    for mode in ("gate_by_gate", "staged"):
+        direct = wall(lambda: (s.set_zero_state(), circ.update_quantum_state(s, mode=mode)))
+        g = capture_circuit(circ, s, mode=mode)
+        replay = wall(g.launch)
+        out[mode] = {"direct_ms": direct, "graph_ms": replay, "kernels": g.kernel_count()}
+        g.close()
+    rng = np.random.default_rng(8)
+    sizes = [int(rng.integers(10, 17)) for _ in range(64)]
+    circs = [W.to_circuit(W.hea_circuit(m, 6, seed=8000 + i), m) for i, m in enumerate(sizes)]
+    states = [Q.QuantumState(m) for m in sizes]
+    k = len(circs)
+    ch = (C.c_void_p * k)(*[c._h for c in circs])
+    sp = (C.c_void_p * k)(*[x.data_ptr() for x in states])
+
+    def batch_direct():
+        for x in states:
+            x.set_zero_state()
+        call("qs_batch_update_quantum_states", ch, sp, k, None)
+    direct = wall(batch_direct)
+    g = capture_batch(circs, states)
+    out["batch64"] = {"direct_ms": direct, "graph_ms": wall(g.launch), "kernels": g.kernel_count()}
+    g.close()
+    return out
+
+
 def noise_sampling(n: int = 20, depth: int = 4, p: float = 1e-3, shots: int = 1000, seed: int = 6006):
     """NoiseSimulator: HEA circuit with depolarizing noise after every gate (cppsim add_noise_gate rule),
     `shots` trajectories sampled on the device; the oracle port's time for a few trajectories on the
@@ -599,7 +650,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-kernel-table", action="store_true")
     ap.add_argument("--no-gpusim", action="store_true", help="skip the reference GPU backend leg")
-    ap.add_argument("--workload", default="plain", choices=["plain", "fused", "batched", "serving", "noise", "dm"],
+    ap.add_argument("--workload", default="plain",
+                    choices=["plain", "fused", "batched", "serving", "noise", "dm", "graphs"],
                     help="fused / batched / serving / noise / dm: only that measurement (configs 3 / 4 / 5, "
                          "NoiseSimulator, noisy density matrix)")
     ap.add_argument("--instances", type=int, default=4096)
@@ -648,6 +700,11 @@ def main():
         r = batched_throughput(args.instances, args.budget_gb)
         if rank == 0:
             print(json.dumps({"metric": "batched uneven circuits: circuits/s", **r}), flush=True)
+        return
+    if args.workload == "graphs":
+        r = graph_replay()
+        if rank == 0:
+            print(json.dumps({"metric": "captured graph replay vs direct call: ms per call", **r}), flush=True)
         return
     if args.workload == "dm":
         r = dm_noisy_circuit()
@@ -805,6 +862,7 @@ def main():
                         ("batched", lambda: batched_throughput(args.instances, args.budget_gb)),
                         ("serving", lambda: serving_sweep(60, (5.0, 20.0, 50.0, 100.0), 96.0, 4)),
                         ("noise", lambda: noise_sampling()),
+                        ("graphs", lambda: graph_replay()),
                         ("density_matrix", lambda: dm_noisy_circuit())):
             try:
                 extras[key] = fn()

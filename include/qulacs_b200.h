@@ -512,6 +512,31 @@ QS_API int qs_circuit_update_density_matrix(
  * Synchronises `stream`. */
 QS_API int qs_batch_update_quantum_states(const qs_circuit_t* circuits, void* const* states, QS_UINT count,
     void* stream);
+/* ---- captured CUDA graphs (no reference counterpart; the reference launches and synchronises every
+ * gate, gpusim/update_ops_single.cu:126-131) ----
+ * A circuit applied to one device state (mode as qs_circuit_update_quantum_state), or a batch of
+ * circuits applied to their states in one persistent launch (as qs_batch_update_quantum_states, or as
+ * qs_batch_update_quantum_states_c64 with FP64 passes when c64 != 0), recorded once as a CUDA graph
+ * and replayed by qs_graph_launch: host planning, parameter uploads and launches are paid at creation.
+ * With reset_state(s) != 0 the graph first sets each state to |0...0>.  The graph is bound to the
+ * state pointers and to the circuits' gates and parameters at creation (later changes to a circuit
+ * are not seen).  Creation builds plans (and autotunes, and compiles specialised kernels) first and
+ * synchronises `stream`; work that copies from host memory during a run cannot be recorded, since a
+ * replay would read that memory again after the call returned: a dense gate of >= 3 qubits outside the
+ * staged passes (gate by gate, or a QS_EXEC_STAGED_FUSED block of >= 3 qubits: force block size <= 2
+ * with qs_circuit_set_fusion) or a multi-qubit diagonal -> QS_ERR_NOT_SUPPORTED.
+ * A NULL stream is fine (capture then runs on a private stream). */
+typedef struct qs_graph_s* qs_graph_t;
+QS_API int qs_circuit_graph_create(qs_circuit_t circuit, void* state, QS_ITYPE dim, int mode, int reset_state,
+    void* stream, qs_graph_t* out);
+QS_API int qs_batch_graph_create(const qs_circuit_t* circuits, void* const* states, QS_UINT count, int c64,
+    int reset_states, void* stream, qs_graph_t* out);
+/* Replays the graph on `stream`: asynchronous for a circuit graph; a batch graph synchronises `stream`
+ * and returns QS_ERR_TIMEOUT when a bounded dependency wait expired. */
+QS_API int qs_graph_launch(qs_graph_t graph, void* stream);
+/* Kernel launches one replay performs (they are added to qs_launch_count at each replay). */
+QS_API int qs_graph_kernel_count(qs_graph_t graph, QS_ITYPE* kernels);
+QS_API int qs_graph_destroy(qs_graph_t graph);
 /* Failure-path check of the batch executor (no reference counterpart; the reference's GPU backend
  * exits the process on a device error, gpusim/util.cuh:28-42): runs `circuit` on `state` as a
  * one-circuit batch whose last pass waits on a completion counter that never completes, with the

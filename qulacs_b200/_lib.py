@@ -157,6 +157,11 @@ SIGNATURES = {
     "qs_circuit_c64_executor_info": [P, P],
     "qs_batch_update_quantum_states_c64": [P, P, U, C.c_int, P],
     "qs_batch_update_quantum_states": [P, P, U, P],
+    "qs_circuit_graph_create": [P, P, IT, C.c_int, C.c_int, P, P],
+    "qs_batch_graph_create": [P, P, U, C.c_int, C.c_int, P, P],
+    "qs_graph_launch": [P, P],
+    "qs_graph_kernel_count": [P, P],
+    "qs_graph_destroy": [P],
     "qs_debug_batch_wait_expiry": [P, P, U, P],
     "qs_debug_batch_wait_expiry_fused_c64": [P, P, U, P],
     "qs_circuit_set_specialized": [P, I],

@@ -418,6 +418,7 @@ __global__ void __launch_bounds__(kBlkThreads, CP <= 2 ? 2 : 1) k_denseK_blk(dou
 template <int K, int CP>
 static int launch_denseK_blk(const UINT* tl, const double* matrix, double2* s, const Positions& pos, ITYPE fixed,
     ITYPE cosets, cudaStream_t st) {
+    QS_TRY(refuse_if_capturing("a dense gate of 6 qubits"));
     constexpr int D = 1 << K, kBlkCosets = 16 * CP;
     static std::mutex mu;
     static std::vector<char> ready;
@@ -452,6 +453,7 @@ static int launch_denseK_blk(const UINT* tl, const double* matrix, double2* s, c
 template <int K>
 static int launch_denseK_reg(const UINT* tl, const double* matrix, double2* s, ITYPE dim, const Positions& pos,
     ITYPE fixed, ITYPE cosets, cudaStream_t st) {
+    QS_TRY(refuse_if_capturing("a dense gate of 3..5 qubits"));
     constexpr int D = 1 << K;
     static thread_local DenseKArgs<K> a;  // large parameter block, filled on the host
     for (int x = 0; x < D; ++x) {
@@ -526,6 +528,7 @@ __global__ void __launch_bounds__(kGenThreads) k_denseK_gen(double2* __restrict_
 
 static int launch_denseK_gen(const UINT* tl, UINT k, const double* matrix, double2* s, const Positions& pos,
     ITYPE fixed, ITYPE cosets, cudaStream_t st) {
+    QS_TRY(refuse_if_capturing("a dense gate of 7 or more qubits"));
     const size_t D = size_t(1) << k;
     std::vector<double2> ut(D * D);
     for (size_t y = 0; y < D; ++y)
@@ -818,6 +821,7 @@ QS_API int qs_multi_qubit_control_multi_qubit_dense_matrix_gate(const QS_UINT* c
 }
 
 QS_API int qs_multi_qubit_diagonal_matrix_gate(const QS_UINT* tl, QS_UINT k, const double* diag, STATE_ARGS) {
+    QS_TRY(refuse_if_capturing("a multi-qubit diagonal gate"));
     UINT n;
     QS_TRY(check_dim(dim, &n));
     if (k < 1 || k > 20) return set_error(QS_ERR_NOT_SUPPORTED, "multi_qubit_diagonal_matrix_gate: 1..20 targets");

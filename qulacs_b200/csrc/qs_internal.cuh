@@ -43,6 +43,13 @@ int check_distinct(const UINT* list, UINT count, UINT n, const char* what);
 
 // After a launch: returns QS_ERR_CUDA with the launch error, if any.
 int check_launch(const char* kernel);
+// Adjusts the launch counter (graph replays: the kernels a captured graph holds; capture itself: minus
+// the launches it recorded, which did not run).
+void count_launches(long long delta);
+// Graph capture (this thread): calls whose run copies from host memory refuse to be recorded, since a
+// replay would read that host memory again after the call has returned.
+void set_capturing(bool on);
+int refuse_if_capturing(const char* what);
 
 // Per (device, stream) scratch buffer for reduction partials and uploaded matrices.  Grows on
 // demand with cudaMalloc; stream order makes reuse by the next call on the same stream safe.

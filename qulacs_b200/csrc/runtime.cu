@@ -31,6 +31,17 @@ int check_cuda(cudaError_t e, const char* what) {
 
 static std::atomic<unsigned long long> g_launches{0};
 
+static thread_local bool g_capturing = false;
+void set_capturing(bool on) { g_capturing = on; }
+int refuse_if_capturing(const char* what) {
+    if (!g_capturing) return QS_OK;
+    return set_error(QS_ERR_NOT_SUPPORTED, std::string(what) + " copies its matrix from host memory at each run");
+}
+
+void count_launches(long long delta) {
+    g_launches.fetch_add((unsigned long long)delta, std::memory_order_relaxed);
+}
+
 int check_launch(const char* kernel) {
     g_launches.fetch_add(1, std::memory_order_relaxed);
     cudaError_t e = cudaGetLastError();

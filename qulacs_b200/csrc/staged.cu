@@ -17,6 +17,8 @@
 #include <cmath>
 #include <complex>
 #include <cstring>
+#include <memory>
+#include <string>
 #include <mutex>
 #include <thread>
 #include <vector>
@@ -1362,12 +1364,12 @@ static int ensure_batch_plan(Circuit& c, ITYPE dim) {
 
 // `wait_ns`: the dependency wait limit; `self_dep` >= 0 makes that work record depend on itself (a
 // counter nothing can complete), which only the wait-expiry check below uses.
-int batch_update(Circuit* const* cs, void* const* states, UINT count, cudaStream_t st, unsigned long long wait_ns,
-    int self_dep, bool c64) {
-    if (count == 0) return QS_OK;
+// The work records of a batch (plans missing from the circuits' caches built first: FP64 fusion and
+// host planning on host threads in parallel, uploads afterwards) and the number of work items.
+static int batch_records(Circuit* const* cs, void* const* states, UINT count, std::vector<BatchRec>* recs,
+    ITYPE* total_out) {
     for (UINT i = 0; i < count; ++i)
         if (cs[i]->n < kPhaseBits) return set_error(QS_ERR_NOT_SUPPORTED, "batch: circuits need at least 4 qubits");
-    // missing plans: FP64 fusion and host planning on host threads in parallel, uploads afterwards
     {
         std::vector<char> need(count, 0);
         for (UINT i = 0; i < count; ++i) {
@@ -1411,7 +1413,7 @@ int batch_update(Circuit* const* cs, void* const* states, UINT count, cudaStream
         }
         maxp = std::max(maxp, passes[i].size());
     }
-    std::vector<BatchRec> recs;
+    recs->clear();
     std::vector<int> last(count, -1);
     ITYPE total = 0;
     for (size_t p = 0; p < maxp; ++p)
@@ -1423,25 +1425,33 @@ int batch_update(Circuit* const* cs, void* const* states, UINT count, cudaStream
             r.tiles = (1ULL << cs[i]->n) >> r.args.m;
             r.prefix = total;
             r.dep = last[i];
-            last[i] = (int)recs.size();
+            last[i] = (int)recs->size();
             total += r.tiles;
-            recs.push_back(r);
+            recs->push_back(r);
         }
-    if (recs.empty()) return QS_OK;
-    if (self_dep >= 0) {
-        if (self_dep >= (int)recs.size()) return set_error(QS_ERR_INVALID_ARGUMENT, "batch: no such work record");
-        recs[self_dep].dep = self_dep;
+    *total_out = total;
+    return QS_OK;
+}
+
+// Device buffer of a batch launch: records | per-record done counters | (16-byte aligned) work head |
+// error flag.  Everything after the records must be zero before a launch.
+struct BatchLayout {
+    size_t brec, zero_bytes, bytes;
+    explicit BatchLayout(size_t nrec) {
+        brec = sizeof(BatchRec) * nrec;
+        const size_t bdone = sizeof(unsigned) * nrec;
+        bytes = brec + bdone + 256;
+        zero_bytes = bytes - brec;
     }
-    const size_t brec = sizeof(BatchRec) * recs.size();
-    const size_t bdone = sizeof(unsigned) * recs.size();
-    void* buf = nullptr;
-    QS_TRY(scratch(st, brec + bdone + 256, &buf));
-    BatchRec* drec = (BatchRec*)buf;
-    unsigned* ddone = (unsigned*)((char*)buf + brec);
-    unsigned long long* dhead = (unsigned long long*)((char*)buf + ((brec + bdone + 15) / 16 * 16));
-    int* derr = (int*)(dhead + 1);
-    QS_CUDA_CHECK(cudaMemcpyAsync(drec, recs.data(), brec, cudaMemcpyHostToDevice, st));
-    QS_CUDA_CHECK(cudaMemsetAsync(ddone, 0, (brec + bdone + 256) - brec, st));
+    unsigned* done(void* b) const { return (unsigned*)((char*)b + brec); }
+    unsigned long long* head(void* b) const {
+        return (unsigned long long*)((char*)b + ((brec + (bytes - 256 - brec) + 15) / 16 * 16));
+    }
+    int* err(void* b) const { return (int*)(head(b) + 1); }
+};
+
+static int batch_kernel(void* buf, const BatchLayout& L, int nrec, ITYPE total, unsigned long long wait_ns, bool c64,
+    cudaStream_t st) {
     int per_sm = 0;
     if (c64)
         QS_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_staged<float2>, kStThreads, 0));
@@ -1449,18 +1459,187 @@ int batch_update(Circuit* const* cs, void* const* states, UINT count, cudaStream
         QS_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_staged<double2>, kStThreads, 0));
     const ITYPE resident = (ITYPE)std::max(1, per_sm) * sm_count();
     const unsigned grid = (unsigned)std::min<ITYPE>(resident, total);
+    const BatchRec* drec = (const BatchRec*)buf;
     if (c64)
-        k_batch_staged<float2><<<grid, kStThreads, 0, st>>>(drec, (int)recs.size(), total, dhead, ddone, derr, wait_ns);
+        k_batch_staged<float2><<<grid, kStThreads, 0, st>>>(drec, nrec, total, L.head(buf), L.done(buf), L.err(buf), wait_ns);
     else
-        k_batch_staged<double2><<<grid, kStThreads, 0, st>>>(drec, (int)recs.size(), total, dhead, ddone, derr, wait_ns);
-    QS_TRY(check_launch("k_batch_staged"));
+        k_batch_staged<double2><<<grid, kStThreads, 0, st>>>(drec, nrec, total, L.head(buf), L.done(buf), L.err(buf), wait_ns);
+    return check_launch("k_batch_staged");
+}
+
+int batch_update(Circuit* const* cs, void* const* states, UINT count, cudaStream_t st, unsigned long long wait_ns,
+    int self_dep, bool c64) {
+    if (count == 0) return QS_OK;
+    std::vector<BatchRec> recs;
+    ITYPE total = 0;
+    QS_TRY(batch_records(cs, states, count, &recs, &total));
+    if (recs.empty()) return QS_OK;
+    if (self_dep >= 0) {
+        if (self_dep >= (int)recs.size()) return set_error(QS_ERR_INVALID_ARGUMENT, "batch: no such work record");
+        recs[self_dep].dep = self_dep;
+    }
+    const BatchLayout L(recs.size());
+    void* buf = nullptr;
+    QS_TRY(scratch(st, L.bytes, &buf));
+    QS_CUDA_CHECK(cudaMemcpyAsync(buf, recs.data(), L.brec, cudaMemcpyHostToDevice, st));
+    QS_CUDA_CHECK(cudaMemsetAsync(L.done(buf), 0, L.zero_bytes, st));
+    QS_TRY(batch_kernel(buf, L, (int)recs.size(), total, wait_ns, c64, st));
     int err = 0;
-    QS_CUDA_CHECK(cudaMemcpyAsync(&err, derr, sizeof(int), cudaMemcpyDeviceToHost, st));
+    QS_CUDA_CHECK(cudaMemcpyAsync(&err, L.err(buf), sizeof(int), cudaMemcpyDeviceToHost, st));
     QS_CUDA_CHECK(cudaStreamSynchronize(st));
     if (err) return set_error(QS_ERR_TIMEOUT, "batch: dependency wait expired");
     return QS_OK;
 }
 
+// ---------------------------------------------------------------- captured CUDA graphs
+// A circuit (or a batch) applied to fixed device states, recorded once as a CUDA graph and replayed
+// with one cudaGraphLaunch: the host planning, parameter uploads and per-pass launches of a call are
+// paid once.  Plans (and the autotuner, and specialised kernels) are prepared before the capture;
+// the capture records only stream work.  Work that copies from pageable host memory during a run (a
+// dense gate of >= 3 qubits left outside the staged passes, a multi-qubit diagonal) cannot be
+// captured: creation then fails with QS_ERR_NOT_SUPPORTED.
+struct GraphExec {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    void* dev = nullptr;       // batch graphs: work records and counters
+    int* host_err = nullptr;   // batch graphs: the wait-expiry flag, copied back by the graph (pinned)
+    long long kernels = 0;     // kernel launches one replay performs
+    ~GraphExec() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (dev) cudaFree(dev);
+        if (host_err) cudaFreeHost(host_err);
+    }
+};
+
+// Records `work` on a capturing stream (the caller's, or a private one for the legacy default stream)
+// into G.  Capture is thread-local, so other threads' unrelated CUDA calls are not affected.
+template <class F>
+static int capture_graph(cudaStream_t user, GraphExec* G, F work) {
+    cudaStream_t st = user;
+    cudaStream_t own = nullptr;
+    if (!st) {  // the legacy default stream cannot capture
+        QS_TRY(qs_stream_create((void**)&own));
+        st = own;
+    }
+    const unsigned long long l0 = qs_launch_count();
+    cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+        if (own) qs_stream_destroy(own);
+        return check_cuda(e, "cudaStreamBeginCapture");
+    }
+    set_capturing(true);
+    int rc = work(st);
+    set_capturing(false);
+    std::string msg = rc == QS_OK ? std::string() : std::string(qs_get_last_error());
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(st, &g);
+    G->kernels = (long long)(qs_launch_count() - l0);
+    count_launches(-G->kernels);  // recorded, not run
+    if (own) qs_stream_destroy(own);  // with any scratch the capture allocated for it
+    if (rc != QS_OK || e != cudaSuccess || !g) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();  // clear the capture error
+        return set_error(QS_ERR_NOT_SUPPORTED,
+            "graph capture: this work cannot be recorded (" + (msg.empty() ? std::string(cudaGetErrorString(e)) : msg) +
+            ")");
+    }
+    G->graph = g;
+    e = cudaGraphInstantiate(&G->exec, g, 0);
+    if (e != cudaSuccess) return check_cuda(e, "cudaGraphInstantiate");
+    return QS_OK;
+}
+
+}  // namespace qs
+
+extern "C" QS_API int qs_circuit_graph_create(qs_circuit_t circuit, void* state, QS_ITYPE dim, int mode, int reset_state,
+    void* stream, qs_graph_t* out) {
+    qs::Circuit* c = reinterpret_cast<qs::Circuit*>(circuit);
+    if (!c || !state || !out) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "null argument");
+    if (dim != (1ULL << c->n)) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "dim differs from 2^qubit_count");
+    if (mode != QS_EXEC_GATE_BY_GATE && mode != QS_EXEC_STAGED && mode != QS_EXEC_STAGED_FUSED)
+        return qs::set_error(QS_ERR_INVALID_ARGUMENT, "unknown execution mode");
+    cudaStream_t st = (cudaStream_t)stream;
+    // plans, autotuning and specialised kernels first: they synchronise and allocate
+    if (c->n >= (UINT)qs::kPhaseBits) {
+        if (mode == QS_EXEC_STAGED) QS_TRY(qs::ensure_plan(*c, dim));
+        if (mode == QS_EXEC_STAGED_FUSED) QS_TRY(qs::ensure_fused_plan(*c, dim, st));
+    }
+    QS_TRY(qs::staged_allow_smem());
+    auto G = std::make_unique<qs::GraphExec>();
+    QS_TRY(qs::capture_graph(st, G.get(), [&](cudaStream_t cs) -> int {
+        if (reset_state) QS_TRY(qs_initialize_quantum_state(state, dim, cs));
+        if (mode == QS_EXEC_STAGED) return qs::run_staged(*c, state, dim, cs);
+        if (mode == QS_EXEC_STAGED_FUSED) return qs::run_staged_fused(*c, state, dim, cs);
+        for (const qs::GateRec& g : c->gates) QS_TRY(qs::apply_gate_by_gate(g, state, dim, cs));
+        return QS_OK;
+    }));
+    *out = reinterpret_cast<qs_graph_t>(G.release());
+    return QS_OK;
+}
+
+extern "C" QS_API int qs_batch_graph_create(const qs_circuit_t* circuits, void* const* states, QS_UINT count, int c64,
+    int reset_states, void* stream, qs_graph_t* out) {
+    if (!circuits || !states || !out || count == 0) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "null argument");
+    std::vector<qs::Circuit*> cs(count);
+    for (QS_UINT i = 0; i < count; ++i) {
+        cs[i] = reinterpret_cast<qs::Circuit*>(circuits[i]);
+        if (!cs[i] || !states[i]) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "null circuit or state");
+    }
+    std::vector<qs::BatchRec> recs;
+    ITYPE total = 0;
+    QS_TRY(qs::batch_records(cs.data(), states, count, &recs, &total));
+    if (recs.empty()) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "batch graph: no passes to run");
+    auto G = std::make_unique<qs::GraphExec>();
+    const qs::BatchLayout L(recs.size());
+    QS_CUDA_CHECK(cudaMalloc(&G->dev, L.bytes));
+    QS_CUDA_CHECK(cudaMemcpy(G->dev, recs.data(), L.brec, cudaMemcpyHostToDevice));
+    QS_CUDA_CHECK(cudaMallocHost((void**)&G->host_err, sizeof(int)));
+    *G->host_err = 0;
+    void* dev = G->dev;
+    int* host_err = G->host_err;
+    QS_TRY(qs::capture_graph((cudaStream_t)stream, G.get(), [&](cudaStream_t st) -> int {
+        if (reset_states)
+            for (QS_UINT i = 0; i < count; ++i) {
+                const QS_ITYPE dim = 1ULL << cs[i]->n;
+                QS_TRY(c64 ? qs_initialize_quantum_state_c64(states[i], dim, st)
+                           : qs_initialize_quantum_state(states[i], dim, st));
+            }
+        QS_CUDA_CHECK(cudaMemsetAsync(L.done(dev), 0, L.zero_bytes, st));
+        QS_TRY(qs::batch_kernel(dev, L, (int)recs.size(), total, qs::kBatchWaitNs, c64 != 0, st));
+        QS_CUDA_CHECK(cudaMemcpyAsync(host_err, L.err(dev), sizeof(int), cudaMemcpyDeviceToHost, st));
+        return QS_OK;
+    }));
+    *out = reinterpret_cast<qs_graph_t>(G.release());
+    return QS_OK;
+}
+
+extern "C" QS_API int qs_graph_launch(qs_graph_t graph, void* stream) {
+    qs::GraphExec* G = reinterpret_cast<qs::GraphExec*>(graph);
+    if (!G || !G->exec) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "null graph");
+    cudaStream_t st = (cudaStream_t)stream;
+    QS_CUDA_CHECK(cudaGraphLaunch(G->exec, st));
+    qs::count_launches(G->kernels);
+    if (G->host_err) {  // a batch graph: its wait-expiry flag arrives with the graph's last node
+        QS_CUDA_CHECK(cudaStreamSynchronize(st));
+        if (*G->host_err) return qs::set_error(QS_ERR_TIMEOUT, "batch graph: dependency wait expired");
+    }
+    return QS_OK;
+}
+
+extern "C" QS_API int qs_graph_kernel_count(qs_graph_t graph, QS_ITYPE* kernels) {
+    qs::GraphExec* G = reinterpret_cast<qs::GraphExec*>(graph);
+    if (!G || !kernels) return qs::set_error(QS_ERR_INVALID_ARGUMENT, "null argument");
+    *kernels = (QS_ITYPE)G->kernels;
+    return QS_OK;
+}
+
+extern "C" QS_API int qs_graph_destroy(qs_graph_t graph) {
+    delete reinterpret_cast<qs::GraphExec*>(graph);
+    return QS_OK;
+}
+
+namespace qs {
 }  // namespace qs
 
 extern "C" QS_API int qs_batch_update_quantum_states(const qs_circuit_t* circuits, void* const* states, QS_UINT count,
