@@ -522,9 +522,10 @@ QS_API int qs_batch_update_quantum_states(const qs_circuit_t* circuits, void* co
  * state pointers and to the circuits' gates and parameters at creation (later changes to a circuit
  * are not seen).  Creation builds plans (and autotunes, and compiles specialised kernels) first and
  * synchronises `stream`; work that copies from host memory during a run cannot be recorded, since a
- * replay would read that memory again after the call returned: a dense gate of >= 3 qubits outside the
- * staged passes (gate by gate, or a QS_EXEC_STAGED_FUSED block of >= 3 qubits: force block size <= 2
- * with qs_circuit_set_fusion) or a multi-qubit diagonal -> QS_ERR_NOT_SUPPORTED.
+ * replay would read that memory again after the call returned: a dense gate of >= 6 qubits outside the
+ * staged passes (gate by gate, or a QS_EXEC_STAGED_FUSED block of 6 qubits: force a smaller block size
+ * with qs_circuit_set_fusion) or a multi-qubit diagonal -> QS_ERR_NOT_SUPPORTED.  (Dense gates of 3..5
+ * qubits carry their matrices as kernel parameters, which a graph keeps.)
  * A NULL stream is fine (capture then runs on a private stream). */
 typedef struct qs_graph_s* qs_graph_t;
 QS_API int qs_circuit_graph_create(qs_circuit_t circuit, void* state, QS_ITYPE dim, int mode, int reset_state,

@@ -453,7 +453,6 @@ static int launch_denseK_blk(const UINT* tl, const double* matrix, double2* s, c
 template <int K>
 static int launch_denseK_reg(const UINT* tl, const double* matrix, double2* s, ITYPE dim, const Positions& pos,
     ITYPE fixed, ITYPE cosets, cudaStream_t st) {
-    QS_TRY(refuse_if_capturing("a dense gate of 3..5 qubits"));
     constexpr int D = 1 << K;
     static thread_local DenseKArgs<K> a;  // large parameter block, filled on the host
     for (int x = 0; x < D; ++x) {
@@ -466,6 +465,7 @@ static int launch_denseK_reg(const UINT* tl, const double* matrix, double2* s, I
     if (K <= 5) {
         for (int i = 0; i < D * D; ++i) a.m[i] = make_double2(matrix[2 * i], matrix[2 * i + 1]);
     } else {
+        QS_TRY(refuse_if_capturing("a dense gate of 6 qubits"));
         void* buf = nullptr;
         QS_TRY(scratch(st, (size_t)16 * D * D, &buf));
         QS_CUDA_CHECK(cudaMemcpyAsync(buf, matrix, (size_t)16 * D * D, cudaMemcpyHostToDevice, st));

@@ -23,7 +23,7 @@ def test_circuit_graph_equals_direct_call(port, mode):
     gates = W.layered_rotation_circuit(n, 3, seed=31) + W.u3_cz_circuit(n, 2, seed=32)
     circ = W.to_circuit(gates, n)
     if mode == "staged_fused":
-        circ.set_fusion(2)  # blocks of <= 2 qubits stay pass ops; larger ones copy their matrices per run
+        circ.set_fusion(4)  # 3..4-qubit blocks run as dense kernels whose matrices are kernel parameters
     direct = QuantumState(n)
     circ.update_quantum_state(direct, mode=mode)  # plans as the graph uses them
     direct.set_zero_state()
@@ -82,8 +82,8 @@ def test_uncapturable_work_is_refused_and_context_stays_usable():
     n = 10
     rng = np.random.default_rng(35)
     circ = W.to_circuit(W.hea_circuit(n, 2, seed=35), n)
-    u = np.linalg.qr(rng.normal(size=(8, 8)) + 1j * rng.normal(size=(8, 8)))[0]
-    circ.add_gate(G.DenseMatrix([0, 4, 7], u))  # gate by gate: its matrix is copied from host memory
+    u = np.linalg.qr(rng.normal(size=(64, 64)) + 1j * rng.normal(size=(64, 64)))[0]
+    circ.add_gate(G.DenseMatrix([0, 2, 4, 5, 7, 9], u))  # a 6-qubit matrix is copied from host memory per run
     s = QuantumState(n)
     h = C.c_void_p()
     rc = load().qs_circuit_graph_create(circ._h, s.data_ptr(), s.dim, 0, 1, None, C.byref(h))
