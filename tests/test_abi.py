@@ -130,3 +130,35 @@ def test_added_entry_points_validate_on_host(lib):
     assert lib.qs_dm_multi_qubit_control_multi_qubit_dense_matrix_gate(u([0]), u([1]), 1, u([0]), 1, None, None,
                                                                        1 << 3, None) == 1
     assert lib.qs_state_tensor_product(None, 1 << 30, None, 1 << 11, None, None) == 5      # 41 qubits
+
+
+def test_new_entry_points_validate_on_host(lib):
+    """Executor choices, specialisation modes and graph creation reject bad arguments before any CUDA
+    call; a weighted expectation with a mask beyond the qubit count is refused."""
+    from qulacs_b200 import workloads as W
+    circ = W.to_circuit(W.hea_circuit(6, 2, seed=1), 6)
+    assert lib.qs_circuit_set_c64_executor(circ._h, 2) == 1
+    assert lib.qs_circuit_set_c64_executor(None, 0) == 1
+    assert lib.qs_set_expectation_specialized(3) == 1
+    assert lib.qs_set_expectation_specialized(1) == 0
+    h = C.c_void_p()
+    assert lib.qs_circuit_graph_create(None, None, 1 << 6, 1, 1, None, C.byref(h)) == 1
+    assert lib.qs_circuit_graph_create(circ._h, C.c_void_p(16), 1 << 5, 1, 1, None, C.byref(h)) == 1
+    assert b"dim differs" in lib.qs_get_last_error()
+    assert lib.qs_circuit_graph_create(circ._h, C.c_void_p(16), 1 << 6, 7, 1, None, C.byref(h)) == 1
+    assert lib.qs_graph_launch(None, None) == 1
+    assert lib.qs_graph_destroy(None) == 0
+    ch = (C.c_void_p * 1)(circ._h)
+    st = (C.c_void_p * 1)(16)
+    assert lib.qs_batch_update_quantum_states_c64(ch, st, 1, 5, None) == 1
+    assert lib.qs_batch_graph_create(None, None, 0, 0, 1, None, C.byref(h)) == 1
+    x = np.array([1 << 7], dtype=np.uint64)
+    z = np.zeros(1, dtype=np.uint64)
+    y = np.zeros(1, dtype=np.uint32)
+    cf = np.array([1.0, 0.0])
+    out = np.zeros(2)
+    rc = lib.qs_expectation_value_pauli_weighted(x.ctypes.data_as(C.c_void_p), z.ctypes.data_as(C.c_void_p),
+                                                 y.ctypes.data_as(C.c_void_p), cf.ctypes.data_as(C.c_void_p), 1,
+                                                 C.c_void_p(16), 1 << 6, None, out.ctypes.data_as(C.c_void_p))
+    assert rc == 1
+    assert b"mask beyond qubit count" in lib.qs_get_last_error()
