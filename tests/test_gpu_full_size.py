@@ -4,7 +4,8 @@
 * circuit then its inverse returns |0...0> in every execution mode; the norm stays 1;
 * at 30 qubits the three execution modes agree through device inner products (|<a|b>|^2 = 1);
 * <P> of 256 strings (weight <= 6) from the many-strings-per-pass tiles equals the one-string-per-pass
-  kernel on the same state, and sum c_k <P_k> equals the observable's <H>;
+  kernel on the same state, and sum c_k <P_k> equals the observable's <H> from the weighted passes
+  (generic and generated kernels);
 * sampling: seeded draws repeat, lie in [0, 2^n), and a basis state always yields its own index."""
 import gc
 
@@ -66,7 +67,13 @@ def test_layered_circuit_round_trip_and_observables(n):
                        for _, tl, ids in terms])
     assert np.max(np.abs(tiled - single)) <= EV_TOL
     coefs = np.array([c for c, _, _ in terms])
-    assert abs(obs.get_expectation_value(s) - float(coefs @ single)) <= EV_TOL
+    assert abs(obs.get_expectation_value(s) - float(coefs @ single)) <= EV_TOL  # generic pass kernel
+    from qulacs_b200.observable import set_expectation_specialized
+    set_expectation_specialized(2)  # the per-pass generated kernels
+    try:
+        assert abs(obs.get_expectation_value(s) - float(coefs @ single)) <= EV_TOL
+    finally:
+        set_expectation_specialized(1)
 
     a, b = s.sampling(1024, 2126), s.sampling(1024, 2126)
     assert a == b and all(0 <= x < (1 << n) for x in a)
