@@ -1104,7 +1104,8 @@ int run_staged_fused(Circuit& c, void* state, ITYPE dim, cudaStream_t st) {
 // The staged schedule over a complex64 state: each tile is widened to FP64 in shared memory, every
 // phase runs in FP64 (the generic pass kernel's code), and the tile is rounded back on the store, so a
 // pass moves half the bytes of the complex128 pass.  Gates are fused into blocks of at most 2 qubits
-// (a forced QS_EXEC_STAGED_FUSED size of 0..2 is kept) so that every block is a pass op.
+// (a forced QS_EXEC_STAGED_FUSED size of 0..2 is kept) so that every block is a pass op.  The same
+// schedule (it does not depend on the state type) runs the large circuits of a batch.
 static int c64_block_size(const Circuit& c) { return (c.fusion_k >= 0 && c.fusion_k <= 2) ? c.fusion_k : 2; }
 
 static int ensure_c64_plan(Circuit& c, ITYPE dim) {
@@ -1467,13 +1468,40 @@ static int batch_kernel(void* buf, const BatchLayout& L, int nrec, ITYPE total, 
     return check_launch("k_batch_staged");
 }
 
+// Circuits of at least this many qubits leave the persistent launch: a pass of theirs has >= 1024
+// tiles of 2^11 amplitudes, enough to fill the device alone, so they run as their own staged passes
+// with 2^12-amplitude tiles (fewer passes, no dependency waits), on the same stream.
+constexpr UINT kBatchSoloQubits = 21;
+
 int batch_update(Circuit* const* cs, void* const* states, UINT count, cudaStream_t st, unsigned long long wait_ns,
     int self_dep, bool c64) {
     if (count == 0) return QS_OK;
+    std::vector<Circuit*> shared_cs, solo_cs;
+    std::vector<void*> shared_st, solo_st;
+    for (UINT i = 0; i < count; ++i) {
+        const bool solo = self_dep < 0 && cs[i]->n >= kBatchSoloQubits;
+        (solo ? solo_cs : shared_cs).push_back(cs[i]);
+        (solo ? solo_st : shared_st).push_back(states[i]);
+    }
+    // every plan first (a refusal comes before any launch)
+    for (size_t i = 0; i < solo_cs.size(); ++i) QS_TRY(ensure_c64_plan(*solo_cs[i], 1ULL << solo_cs[i]->n));
     std::vector<BatchRec> recs;
     ITYPE total = 0;
-    QS_TRY(batch_records(cs, states, count, &recs, &total));
-    if (recs.empty()) return QS_OK;
+    if (!shared_cs.empty())
+        QS_TRY(batch_records(shared_cs.data(), shared_st.data(), (UINT)shared_cs.size(), &recs, &total));
+    if (!solo_cs.empty()) QS_TRY(staged_allow_smem());
+    for (size_t i = 0; i < solo_cs.size(); ++i) {
+        const ITYPE dim = 1ULL << solo_cs[i]->n;
+        for (const DevPass& d : solo_cs[i]->cplan->passes) {
+            if (c64) launch_pass((float2*)solo_st[i], d, dim >> d.args.m, st);
+            else launch_pass((double2*)solo_st[i], d, dim >> d.args.m, st);
+            QS_TRY(check_launch("k_staged_pass"));
+        }
+    }
+    if (recs.empty()) {
+        QS_CUDA_CHECK(cudaStreamSynchronize(st));
+        return QS_OK;
+    }
     if (self_dep >= 0) {
         if (self_dep >= (int)recs.size()) return set_error(QS_ERR_INVALID_ARGUMENT, "batch: no such work record");
         recs[self_dep].dep = self_dep;
@@ -1496,8 +1524,8 @@ int batch_update(Circuit* const* cs, void* const* states, UINT count, cudaStream
 // with one cudaGraphLaunch: the host planning, parameter uploads and per-pass launches of a call are
 // paid once.  Plans (and the autotuner, and specialised kernels) are prepared before the capture;
 // the capture records only stream work.  Work that copies from pageable host memory during a run (a
-// dense gate of >= 3 qubits left outside the staged passes, a multi-qubit diagonal) cannot be
-// captured: creation then fails with QS_ERR_NOT_SUPPORTED.
+// dense gate of >= 6 qubits left outside the staged passes, a multi-qubit diagonal) refuses to be
+// recorded: creation then fails with QS_ERR_NOT_SUPPORTED.
 struct GraphExec {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;

@@ -195,3 +195,37 @@ def test_c64_fp64_batch_equals_each_circuit_alone():
         c.set_c64_executor("fp64")
         c.update_quantum_state(alone)
         assert np.max(np.abs(b.get_vector() - alone.get_vector())) <= 1e-5, n
+
+
+@pytest.mark.parametrize("precision", ["c128", "c64"])
+def test_large_circuits_of_a_batch_run_their_own_passes(precision):
+    """Circuits of >= 21 qubits leave the persistent launch and run their own staged passes (blocks of
+    <= 2 qubits, 2^12-amplitude tiles) in the same call: each such state equals its circuit run alone
+    with that schedule bit for bit, and the small ones still equal theirs to rounding."""
+    import ctypes as C
+    from qulacs_b200 import QuantumStateC64
+    from qulacs_b200._lib import call
+    sizes = [12, 21, 14, 22]
+    circs = [W.to_circuit(W.hea_circuit(n, 3 + i, seed=9950 + i), n) for i, n in enumerate(sizes)]
+    State = QuantumStateC64 if precision == "c64" else QuantumState
+    batch = [State(n) for n in sizes]
+    k = len(circs)
+    ch = (C.c_void_p * k)(*[c._h for c in circs])
+    sp = (C.c_void_p * k)(*[s.data_ptr() for s in batch])
+    if precision == "c64":
+        call("qs_batch_update_quantum_states_c64", ch, sp, k, 1, None)
+    else:
+        call("qs_batch_update_quantum_states", ch, sp, k, None)
+    for c, n, b in zip(circs, sizes, batch):
+        alone = State(n)
+        if precision == "c64":
+            c.set_c64_executor("fp64")
+            c.update_quantum_state(alone)
+        else:
+            c.set_fusion(2)
+            c.update_quantum_state(alone, mode="staged_fused")
+        if n >= 21:
+            assert np.array_equal(b.get_vector(), alone.get_vector()), n
+        else:
+            tol = 1e-5 if precision == "c64" else 1e-14
+            assert np.max(np.abs(b.get_vector() - alone.get_vector())) <= tol, n
