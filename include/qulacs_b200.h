@@ -570,6 +570,14 @@ QS_API int qs_batch_update_quantum_states_c64(qs_circuit_t const* circuits, void
 QS_API int qs_batch_expectation_values(void* const* states, const QS_UINT* qubit_counts, QS_UINT count,
     const QS_UINT* term_offsets, const QS_ITYPE* x_masks, const QS_ITYPE* z_masks, const QS_UINT* y_counts,
     double* values, void* stream);
+/* sum_k coef_k <P_k> per state (GeneralQuantumOperator::get_expectation_value for many states): terms as
+ * qs_batch_expectation_values, coefs[2k], coefs[2k+1] = Re, Im of coef_k; energies[2i], energies[2i+1]
+ * receive state i's sum.  Small states share one launch as above; each state of >= 18 qubits takes
+ * the weighted passes of qs_expectation_value_pauli_weighted.  c64 != 0: complex64 states.
+ * Synchronises `stream`. */
+QS_API int qs_batch_expectation_weighted(void* const* states, const QS_UINT* qubit_counts, QS_UINT count,
+    const QS_UINT* term_offsets, const QS_ITYPE* x_masks, const QS_ITYPE* z_masks, const QS_UINT* y_counts,
+    const double* coefs, int c64, double* energies, void* stream);
 /* Same for complex64 states (FP64 accumulation). */
 QS_API int qs_batch_expectation_values_c64(void* const* states, const QS_UINT* qubit_counts, QS_UINT count,
     const QS_UINT* term_offsets, const QS_ITYPE* x_masks, const QS_ITYPE* z_masks, const QS_UINT* y_counts,

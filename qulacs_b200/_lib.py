@@ -168,6 +168,7 @@ SIGNATURES = {
     "qs_circuit_specialized_info": [P, C.POINTER(I), C.POINTER(I), C.POINTER(D)],
     "qs_circuit_specialized_source": [P, IT, U, C.c_char_p, C.POINTER(IT)],
     "qs_batch_expectation_values": [P, P, U, P, P, P, P, P, P],
+    "qs_batch_expectation_weighted": [P, P, U, P, P, P, P, P, C.c_int, P, P],
     "qs_batch_expectation_values_c64": [P, P, U, P, P, P, P, P, P],
     "qs_state_norm_squared_c64": [P, IT, P, P],
     "qs_state_inner_product_c128_c64": [P, P, IT, P, P],

@@ -3,8 +3,10 @@
 ``BatchRunner.run(jobs)`` takes (circuit, observable) pairs of any qubit counts, admits them into
 waves whose states fit an HBM budget (footprint 16 B x 2^n each, carved from one arena per wave),
 and for each wave applies every circuit in ONE persistent kernel launch
-(``qs_batch_update_quantum_states``) and evaluates every observable term in ONE more launch
-(``qs_batch_expectation_values``).  ``precision="c64"`` keeps the states in complex64 and runs the wave
+(``qs_batch_update_quantum_states``; circuits of >= 21 qubits, which fill the device alone, run their
+own passes in the same call) and evaluates every energy with ``qs_batch_expectation_weighted`` (the
+small states' terms in one launch, each state of >= 18 qubits through the weighted passes).
+``precision="c64"`` keeps the states in complex64 and runs the wave
 in one persistent launch of the chosen executor (``qs_batch_update_quantum_states_c64``): FP64 passes
 over complex64 tiles (``c64_executor="fp64"``; "auto" takes it whenever every gate is stageable) or
 6-qubit blocks on the tensor cores ("tensor"); reductions are FP64 either way.
@@ -117,19 +119,18 @@ class BatchRunner:
                     coefs.append(t.coef)
                 offs.append(len(xm))
                 nq.append(jobs[i][0].qubit_count)
-            vals = np.zeros(max(1, len(xm)))
             xa = np.ascontiguousarray(np.array(xm, dtype=np.uint64))
             za = np.ascontiguousarray(np.array(zm, dtype=np.uint64))
             ya = np.ascontiguousarray(np.array(ny, dtype=np.uint32))
             oa = np.ascontiguousarray(np.array(offs, dtype=np.uint32))
             qa = np.ascontiguousarray(np.array(nq, dtype=np.uint32))
+            ca = np.ascontiguousarray(np.array(coefs, dtype=np.complex128)).view(np.float64)
+            energies = np.zeros(2 * k)
             vp = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
-            call("qs_batch_expectation_values_c64" if c64 else "qs_batch_expectation_values", states, vp(qa), k,
-                 vp(oa), vp(xa), vp(za), vp(ya), vp(vals), self.stream)
-            coefs = np.array(coefs, dtype=np.complex128)
+            call("qs_batch_expectation_weighted", states, vp(qa), k, vp(oa), vp(xa), vp(za), vp(ya), vp(ca),
+                 int(c64), vp(energies), self.stream)
             for j, i in enumerate(wave):
-                a, b = offs[j], offs[j + 1]
-                out[i] = float(np.real(np.sum(coefs[a:b] * vals[a:b])))
+                out[i] = float(energies[2 * j])
         finally:
             _lib.load().qs_release_quantum_state(arena.value)
 

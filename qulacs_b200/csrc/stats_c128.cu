@@ -899,7 +899,10 @@ __global__ void k_batch_ev_fold(const EvJob* __restrict__ jobs, const double* __
 namespace qs {
 static int batch_ev_impl(void* const* states, const QS_UINT* qubit_counts, QS_UINT count, const QS_UINT* term_offsets,
     const QS_ITYPE* x_masks, const QS_ITYPE* z_masks, const QS_UINT* y_counts, double* values, int c64,
-    cudaStream_t st);
+    cudaStream_t st, bool skip_large = false);
+template <class T>
+int ev_weighted(const PauliTerm* terms, const double2* coefs, UINT count, const T* s, ITYPE dim, cudaStream_t st,
+    double out[2], bool allow_generate);
 }
 extern "C" QS_API int qs_batch_expectation_values(void* const* states, const QS_UINT* qubit_counts, QS_UINT count,
     const QS_UINT* term_offsets, const QS_ITYPE* x_masks, const QS_ITYPE* z_masks, const QS_UINT* y_counts,
@@ -916,9 +919,10 @@ extern "C" QS_API int qs_batch_expectation_values_c64(void* const* states, const
 namespace qs {
 constexpr UINT kBatchEvSingleQubits = 18;  // states at least this large are evaluated on their own
 
+// `skip_large`: leave the terms of states of >= kBatchEvSingleQubits qubits to the caller.
 static int batch_ev_impl(void* const* states, const QS_UINT* qubit_counts, QS_UINT count, const QS_UINT* term_offsets,
     const QS_ITYPE* x_masks, const QS_ITYPE* z_masks, const QS_UINT* y_counts, double* values, int c64,
-    cudaStream_t st) {
+    cudaStream_t st, bool skip_large) {
     if (!states || !qubit_counts || !term_offsets || !values) return set_error(QS_ERR_INVALID_ARGUMENT, "null argument");
     std::vector<EvJob> jobs;
     std::vector<ITYPE> zm;
@@ -930,6 +934,7 @@ static int batch_ev_impl(void* const* states, const QS_UINT* qubit_counts, QS_UI
         if (n < 1 || n > 40) return set_error(QS_ERR_INVALID_ARGUMENT, "batch expectation: bad qubit count");
         const ITYPE dim = 1ULL << n;
         if (n >= kBatchEvSingleQubits) {
+            if (skip_large) continue;
             // a large state: its own passes (Z-only strings 16 per pass, bit-flip strings from
             // span tiles) cost far fewer state reads than one job per bit-flip string
             const UINT k0 = term_offsets[i], nk = term_offsets[i + 1] - k0;
@@ -1022,6 +1027,55 @@ static int batch_ev_impl(void* const* states, const QS_UINT* qubit_counts, QS_UI
     return QS_OK;
 }
 }  // namespace qs
+
+// sum_k c_k <P_k> per state for many states: the small states' terms in the one shared launch above
+// (weighted on the host), each large state through the weighted passes (no per-term values).
+extern "C" QS_API int qs_batch_expectation_weighted(void* const* states, const QS_UINT* qubit_counts, QS_UINT count,
+    const QS_UINT* term_offsets, const QS_ITYPE* x_masks, const QS_ITYPE* z_masks, const QS_UINT* y_counts,
+    const double* coefs, int c64, double* energies, void* stream) {
+    if (!states || !qubit_counts || !term_offsets || !coefs || !energies)
+        return qs::set_error(QS_ERR_INVALID_ARGUMENT, "null argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    for (QS_UINT i = 0; i < count; ++i)
+        if (qubit_counts[i] < 1 || qubit_counts[i] > 40)
+            return qs::set_error(QS_ERR_INVALID_ARGUMENT, "batch expectation: bad qubit count");
+    const QS_UINT nterms = term_offsets[count];
+    std::vector<double> values(nterms, 0.);
+    QS_TRY(qs::batch_ev_impl(states, qubit_counts, count, term_offsets, x_masks, z_masks, y_counts, values.data(), c64,
+        st, true));
+    for (QS_UINT i = 0; i < count; ++i) {
+        const QS_UINT k0 = term_offsets[i], k1 = term_offsets[i + 1];
+        double e[2] = {0., 0.};
+        if (qubit_counts[i] >= qs::kBatchEvSingleQubits) {
+            std::vector<qs::PauliTerm> pt(k1 - k0);
+            for (QS_UINT k = k0; k < k1; ++k) {
+                if ((x_masks[k] | z_masks[k]) >> qubit_counts[i])
+                    return qs::set_error(QS_ERR_INVALID_ARGUMENT, "batch expectation: mask beyond qubit count");
+                pt[k - k0].x = x_masks[k];
+                pt[k - k0].z = z_masks[k];
+                pt[k - k0].nrot = y_counts[k];
+                pt[k - k0].pivot = x_masks[k] ? (QS_UINT)(63 - __builtin_clzll(x_masks[k])) : 0u;
+            }
+            const ITYPE dim = 1ULL << qubit_counts[i];
+            if (k1 > k0) {
+                if (c64)
+                    QS_TRY(qs::ev_weighted<float2>(pt.data(), (const double2*)coefs + k0, k1 - k0, (const float2*)states[i],
+                        dim, st, e, false));
+                else
+                    QS_TRY(qs::ev_weighted<double2>(pt.data(), (const double2*)coefs + k0, k1 - k0,
+                        (const double2*)states[i], dim, st, e, false));
+            }
+        } else {
+            for (QS_UINT k = k0; k < k1; ++k) {
+                e[0] += coefs[2 * k] * values[k];
+                e[1] += coefs[2 * k + 1] * values[k];
+            }
+        }
+        energies[2 * i] = e[0];
+        energies[2 * i + 1] = e[1];
+    }
+    return QS_OK;
+}
 
 // ---------------------------------------------------------------- many terms per HBM pass
 // For terms with a bit flip, one pass per term costs one full read of the state per term.  Here a
@@ -1866,9 +1920,11 @@ static int ew_specialize(EwPlan* P, bool c64, bool imag) {
     return rc;
 }
 
+// `allow_generate`: the per-pass kernels may be generated for these terms (callers that evaluate many
+// different term lists once each, such as the batched energies, pass false: a compile would not pay).
 template <class T>
 int ev_weighted(const PauliTerm* terms, const double2* coefs, UINT count, const T* s, ITYPE dim, cudaStream_t st,
-    double out[2]) {
+    double out[2], bool allow_generate) {
     UINT n = 0;
     while ((1ULL << n) < dim) ++n;
     constexpr bool c64 = sizeof(T) == sizeof(float2);
@@ -1882,7 +1938,8 @@ int ev_weighted(const PauliTerm* terms, const double2* coefs, UINT count, const 
             std::lock_guard<std::mutex> lk(P->mu);
             ++P->uses;
             const int mode = g_ev_spec_mode.load();
-            if (P->spec_state == 0 && (mode == 2 || (mode == 1 && n >= kEvSpecMinQubits && P->uses >= 2))) {
+            if (allow_generate && P->spec_state == 0 &&
+                (mode == 2 || (mode == 1 && n >= kEvSpecMinQubits && P->uses >= 2))) {
                 const int rc = ew_specialize(P.get(), c64, imag);
                 if (rc != QS_OK && mode == 2) return rc;  // required: report; by default the generic kernel runs
             }
@@ -1960,8 +2017,10 @@ int ev_weighted(const PauliTerm* terms, const double2* coefs, UINT count, const 
     return QS_OK;
 }
 
-template int ev_weighted<double2>(const PauliTerm*, const double2*, UINT, const double2*, ITYPE, cudaStream_t, double*);
-template int ev_weighted<float2>(const PauliTerm*, const double2*, UINT, const float2*, ITYPE, cudaStream_t, double*);
+template int ev_weighted<double2>(const PauliTerm*, const double2*, UINT, const double2*, ITYPE, cudaStream_t, double*,
+    bool);
+template int ev_weighted<float2>(const PauliTerm*, const double2*, UINT, const float2*, ITYPE, cudaStream_t, double*,
+    bool);
 
 }  // namespace qs
 
@@ -1989,7 +2048,7 @@ QS_API int qs_expectation_value_pauli_weighted(const QS_ITYPE* x_masks, const QS
     QS_TRY(pauli_terms_from_masks(x_masks, z_masks, y_counts, term_count, dim, "expectation_value_pauli_weighted",
         &terms));
     return ev_weighted<double2>(terms.data(), (const double2*)coefs, term_count, (const double2*)state, dim,
-        (cudaStream_t)stream, out);
+        (cudaStream_t)stream, out, true);
 }
 QS_API int qs_expectation_value_pauli_weighted_c64(const QS_ITYPE* x_masks, const QS_ITYPE* z_masks,
     const QS_UINT* y_counts, const double* coefs, QS_UINT term_count, const void* state, QS_ITYPE dim, void* stream,
@@ -1998,7 +2057,7 @@ QS_API int qs_expectation_value_pauli_weighted_c64(const QS_ITYPE* x_masks, cons
     QS_TRY(pauli_terms_from_masks(x_masks, z_masks, y_counts, term_count, dim,
         "expectation_value_pauli_weighted_c64", &terms));
     return ev_weighted<float2>(terms.data(), (const double2*)coefs, term_count, (const float2*)state, dim,
-        (cudaStream_t)stream, out);
+        (cudaStream_t)stream, out, true);
 }
 
 // Host-only plan of qs_expectation_value_pauli_weighted (no device work): passes over the state and
