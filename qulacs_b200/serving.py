@@ -202,15 +202,15 @@ class ServingLoop:
                 ny.append(y)
                 coefs.append(c)
             offs.append(len(xm))
-        vals = np.zeros(max(1, len(xm)))
         xa, za = np.array(xm, dtype=np.uint64), np.array(zm, dtype=np.uint64)
         ya, oa = np.array(ny, dtype=np.uint32), np.array(offs, dtype=np.uint32)
         qa = np.array([r.n for r in reqs], dtype=np.uint32)
-        call("qs_batch_expectation_values_c64" if c64 else "qs_batch_expectation_values", st, _vp(qa), k, _vp(oa),
-             _vp(xa), _vp(za), _vp(ya), _vp(vals), stream)
-        coefs = np.array(coefs)
+        ca = np.ascontiguousarray(np.array(coefs, dtype=np.complex128)).view(np.float64)
+        energies = np.zeros(2 * k)
+        call("qs_batch_expectation_weighted", st, _vp(qa), k, _vp(oa), _vp(xa), _vp(za), _vp(ya), _vp(ca), int(c64),
+             _vp(energies), stream)
         for j, r in enumerate(reqs):
-            r.result = float(np.dot(coefs[offs[j]:offs[j + 1]], vals[offs[j]:offs[j + 1]]))
+            r.result = float(energies[2 * j])
 
     def _run_sampling(self, r, stream):
         c = W.to_circuit(r.gates, r.n)
