@@ -903,6 +903,10 @@ static int batch_ev_impl(void* const* states, const QS_UINT* qubit_counts, QS_UI
 template <class T>
 int ev_weighted(const PauliTerm* terms, const double2* coefs, UINT count, const T* s, ITYPE dim, cudaStream_t st,
     double out[2], bool allow_generate);
+template <class T>
+int ev_weighted_many(const std::vector<const T*>& s, const std::vector<UINT>& nq,
+    const std::vector<std::vector<PauliTerm>>& terms, const std::vector<const double2*>& coefs, cudaStream_t st,
+    std::vector<double2>* out);
 }
 extern "C" QS_API int qs_batch_expectation_values(void* const* states, const QS_UINT* qubit_counts, QS_UINT count,
     const QS_UINT* term_offsets, const QS_ITYPE* x_masks, const QS_ITYPE* z_masks, const QS_UINT* y_counts,
@@ -1043,36 +1047,51 @@ extern "C" QS_API int qs_batch_expectation_weighted(void* const* states, const Q
     std::vector<double> values(nterms, 0.);
     QS_TRY(qs::batch_ev_impl(states, qubit_counts, count, term_offsets, x_masks, z_masks, y_counts, values.data(), c64,
         st, true));
+    // the large states: every plan, pass and fold in one go
+    std::vector<QS_UINT> large;
+    std::vector<std::vector<qs::PauliTerm>> lterms;
+    std::vector<UINT> lnq;
+    std::vector<const double2*> lcoef;
     for (QS_UINT i = 0; i < count; ++i) {
+        if (qubit_counts[i] < qs::kBatchEvSingleQubits) continue;
         const QS_UINT k0 = term_offsets[i], k1 = term_offsets[i + 1];
+        std::vector<qs::PauliTerm> pt(k1 - k0);
+        for (QS_UINT k = k0; k < k1; ++k) {
+            if ((x_masks[k] | z_masks[k]) >> qubit_counts[i])
+                return qs::set_error(QS_ERR_INVALID_ARGUMENT, "batch expectation: mask beyond qubit count");
+            pt[k - k0].x = x_masks[k];
+            pt[k - k0].z = z_masks[k];
+            pt[k - k0].nrot = y_counts[k];
+            pt[k - k0].pivot = x_masks[k] ? (QS_UINT)(63 - __builtin_clzll(x_masks[k])) : 0u;
+        }
+        large.push_back(i);
+        lterms.push_back(std::move(pt));
+        lnq.push_back(qubit_counts[i]);
+        lcoef.push_back((const double2*)coefs + k0);
+    }
+    std::vector<double2> le;
+    if (c64) {
+        std::vector<const float2*> ls;
+        for (QS_UINT i : large) ls.push_back((const float2*)states[i]);
+        QS_TRY(qs::ev_weighted_many<float2>(ls, lnq, lterms, lcoef, st, &le));
+    } else {
+        std::vector<const double2*> ls;
+        for (QS_UINT i : large) ls.push_back((const double2*)states[i]);
+        QS_TRY(qs::ev_weighted_many<double2>(ls, lnq, lterms, lcoef, st, &le));
+    }
+    for (QS_UINT i = 0; i < count; ++i) {
+        if (qubit_counts[i] >= qs::kBatchEvSingleQubits) continue;
         double e[2] = {0., 0.};
-        if (qubit_counts[i] >= qs::kBatchEvSingleQubits) {
-            std::vector<qs::PauliTerm> pt(k1 - k0);
-            for (QS_UINT k = k0; k < k1; ++k) {
-                if ((x_masks[k] | z_masks[k]) >> qubit_counts[i])
-                    return qs::set_error(QS_ERR_INVALID_ARGUMENT, "batch expectation: mask beyond qubit count");
-                pt[k - k0].x = x_masks[k];
-                pt[k - k0].z = z_masks[k];
-                pt[k - k0].nrot = y_counts[k];
-                pt[k - k0].pivot = x_masks[k] ? (QS_UINT)(63 - __builtin_clzll(x_masks[k])) : 0u;
-            }
-            const ITYPE dim = 1ULL << qubit_counts[i];
-            if (k1 > k0) {
-                if (c64)
-                    QS_TRY(qs::ev_weighted<float2>(pt.data(), (const double2*)coefs + k0, k1 - k0, (const float2*)states[i],
-                        dim, st, e, false));
-                else
-                    QS_TRY(qs::ev_weighted<double2>(pt.data(), (const double2*)coefs + k0, k1 - k0,
-                        (const double2*)states[i], dim, st, e, false));
-            }
-        } else {
-            for (QS_UINT k = k0; k < k1; ++k) {
-                e[0] += coefs[2 * k] * values[k];
-                e[1] += coefs[2 * k + 1] * values[k];
-            }
+        for (QS_UINT k = term_offsets[i]; k < term_offsets[i + 1]; ++k) {
+            e[0] += coefs[2 * k] * values[k];
+            e[1] += coefs[2 * k + 1] * values[k];
         }
         energies[2 * i] = e[0];
         energies[2 * i + 1] = e[1];
+    }
+    for (size_t j = 0; j < large.size(); ++j) {
+        energies[2 * large[j]] = le[j].x;
+        energies[2 * large[j] + 1] = le[j].y;
     }
     return QS_OK;
 }
@@ -2016,6 +2035,104 @@ int ev_weighted(const PauliTerm* terms, const double2* coefs, UINT count, const 
     out[1] = si;
     return QS_OK;
 }
+
+// sum_k c_k <P_k> of many states at once (each with its own terms): the plans are built on host threads
+// in parallel (each term list is evaluated once, so no plan cache and no generated kernels), every
+// pass of every state is launched back to back with the generic pass kernel, one fold per state, and
+// one copy back; terms outside the passes are evaluated afterwards, one value each.
+template <class T>
+int ev_weighted_many(const std::vector<const T*>& s, const std::vector<UINT>& nq,
+    const std::vector<std::vector<PauliTerm>>& terms, const std::vector<const double2*>& coefs, cudaStream_t st,
+    std::vector<double2>* out) {
+    const size_t S = s.size();
+    out->assign(S, make_double2(0., 0.));
+    if (S == 0) return QS_OK;
+    std::vector<EwPlan> plans(S);
+    {
+        std::atomic<size_t> next{0};
+        auto work = [&] {
+            for (size_t i; (i = next++) < S;) ew_build(terms[i].data(), (UINT)terms[i].size(), nq[i], &plans[i]);
+        };
+        const unsigned nt = std::max(1u, std::min<unsigned>((unsigned)S, std::min(16u, std::thread::hardware_concurrency())));
+        std::vector<std::thread> pool;
+        for (unsigned t = 1; t < nt; ++t) pool.emplace_back(work);
+        work();
+        for (std::thread& t : pool) t.join();
+    }
+    std::vector<EvWTerm> desc;
+    std::vector<size_t> desc0(S), part0(S + 1, 0);
+    std::vector<unsigned> grid(S);
+    for (size_t i = 0; i < S; ++i) {
+        desc0[i] = desc.size();
+        for (size_t j = 0; j < plans[i].desc.size(); ++j) {
+            EvWTerm e = plans[i].desc[j];
+            const double f = e.coef.x;
+            const double2 c = coefs[i][plans[i].term_of[j]];
+            e.coef = make_double2(c.x * f, c.y * f);
+            desc.push_back(e);
+        }
+        const ITYPE dim = 1ULL << nq[i];
+        grid[i] = (unsigned)std::min<ITYPE>(dim >> kEvTileBits, (ITYPE)sm_count() * kEwCtasPerSm);
+        part0[i + 1] = part0[i] + (size_t)grid[i] * plans[i].passes.size();
+    }
+    if (!desc.empty()) {
+        auto up = [](size_t b) { return (b + 255) / 256 * 256; };
+        const size_t bd = sizeof(EvWTerm) * desc.size(), bp = sizeof(double2) * part0[S], bo = sizeof(double2) * S;
+        void* buf;
+        QS_TRY(scratch(st, up(bd) + up(bp) + up(bo), &buf));
+        EvWTerm* dd = (EvWTerm*)buf;
+        double2* dp = (double2*)((char*)buf + up(bd));
+        double2* dout = (double2*)((char*)buf + up(bd) + up(bp));
+        QS_CUDA_CHECK(cudaMemcpyAsync(dd, desc.data(), bd, cudaMemcpyHostToDevice, st));
+        QS_CUDA_CHECK(cudaMemsetAsync(dout, 0, bo, st));
+        constexpr size_t smem = ew_smem_bytes<kEwThreadBits, T>();
+        {
+            static std::mutex mu;
+            static std::vector<char> ready;
+            int dev = 0;
+            QS_CUDA_CHECK(cudaGetDevice(&dev));
+            std::lock_guard<std::mutex> lock(mu);
+            if ((int)ready.size() <= dev) ready.resize(dev + 1, 0);
+            if (!ready[dev]) {
+                QS_CUDA_CHECK(cudaFuncSetAttribute(k_ev_weighted<T, kEwThreadBits>,
+                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                ready[dev] = 1;
+            }
+        }
+        for (size_t i = 0; i < S; ++i) {
+            const ITYPE dim = 1ULL << nq[i];
+            for (size_t p = 0; p < plans[i].passes.size(); ++p) {
+                const EwPass& ps = plans[i].passes[p];
+                k_ev_weighted<T, kEwThreadBits><<<grid[i], 1 << kEwThreadBits, smem, st>>>(s[i], dim >> kEvTileBits,
+                    ps.a, dd + desc0[i] + ps.first, (int)ps.count, dp + part0[i] + p * grid[i]);
+                QS_TRY(check_launch("k_ev_weighted"));
+            }
+            if (part0[i + 1] > part0[i]) {
+                k_fold_d2<<<1, 256, 0, st>>>(dp + part0[i], (int)(part0[i + 1] - part0[i]), (double*)(dout + i));
+                QS_TRY(check_launch("k_fold_d2"));
+            }
+        }
+        QS_CUDA_CHECK(cudaMemcpyAsync(out->data(), dout, bo, cudaMemcpyDeviceToHost, st));
+        QS_CUDA_CHECK(cudaStreamSynchronize(st));
+    }
+    for (size_t i = 0; i < S; ++i) {
+        if (plans[i].rest.empty()) continue;
+        std::vector<PauliTerm> sub;
+        for (int k : plans[i].rest) sub.push_back(terms[i][k]);
+        std::vector<double> vals(sub.size());
+        QS_TRY(ev_batch<T>(sub.data(), (UINT)sub.size(), s[i], 1ULL << nq[i], st, vals.data()));
+        for (size_t j = 0; j < sub.size(); ++j) {
+            (*out)[i].x += coefs[i][plans[i].rest[j]].x * vals[j];
+            (*out)[i].y += coefs[i][plans[i].rest[j]].y * vals[j];
+        }
+    }
+    return QS_OK;
+}
+
+template int ev_weighted_many<double2>(const std::vector<const double2*>&, const std::vector<UINT>&,
+    const std::vector<std::vector<PauliTerm>>&, const std::vector<const double2*>&, cudaStream_t, std::vector<double2>*);
+template int ev_weighted_many<float2>(const std::vector<const float2*>&, const std::vector<UINT>&,
+    const std::vector<std::vector<PauliTerm>>&, const std::vector<const double2*>&, cudaStream_t, std::vector<double2>*);
 
 template int ev_weighted<double2>(const PauliTerm*, const double2*, UINT, const double2*, ITYPE, cudaStream_t, double*,
     bool);
