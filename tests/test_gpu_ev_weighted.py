@@ -145,3 +145,20 @@ def test_default_mode_generates_on_second_use():
     e2 = obs.get_expectation_value(s)
     assert expectation_specialized_info()[0] > l0
     assert abs(e1 - e2) <= 1e-12
+
+
+def test_weighted_identity_repeated_and_zero_terms(port, kernels):
+    """An identity term (coef x norm), the same string twice, a zero coefficient and a Y-only string:
+    the weighted sum equals the oracle's."""
+    n = 13
+    rng = np.random.default_rng(9800)
+    a = random_state(n, rng)
+    s = QuantumState(n)
+    s.load(a)
+    terms = W.random_pauli_terms(n, 40, 1, 5, seed=9801)
+    terms += [(0.0, [], []), terms[3], terms[7], (0.0, [2, 9], [2, 2]), (0.0, [0], [2])]
+    coefs = rng.normal(size=len(terms))
+    coefs[5] = 0.0
+    obs = observable(n, terms, coefs)
+    want = oracle_sum(port, a, terms, coefs).real
+    assert abs(obs.get_expectation_value(s) - want) <= EV_TOL * float(np.sum(np.abs(coefs)))
