@@ -189,6 +189,8 @@ struct FusedSmem {
     unsigned char* sB0;  // tile X: B hi | B lo, then its output tile
     unsigned char* sB1;  // tile Y
     uint32_t* tabs;      // [2][kTabWords]
+    uint64_t* dep;       // [kDepChunks][64]: tile-index bits -> global offset (see fused_addr_tables)
+    uint64_t* runoff;    // [256]: 256-byte run index (tile bits 5..12) -> global offset
     uint64_t* mbar;      // [0] MMA X, [1] MMA Y, [2] block record
     int* s_err;
     uint32_t tmem, ncols, mb0, mb1, mba, aaddr, taddr;
@@ -202,6 +204,9 @@ struct FusedPipe {
 };
 
 constexpr uint32_t kFNMax = 1u << (kFTileMax - kFBlock);  // 128 cosets per block at the largest tile
+// Tile indices have at most kDepChunks x 6 bits (the host refuses larger states).
+constexpr int kDepChunks = 4;
+constexpr int kAddrTabBytes = (kDepChunks * 64 + 256) * 8;
 
 __device__ __forceinline__ FusedSmem fused_setup(unsigned char* smem, uint32_t ncols) {
     FusedSmem S;
@@ -210,7 +215,9 @@ __device__ __forceinline__ FusedSmem fused_setup(unsigned char* smem, uint32_t n
     S.sB0 = S.sA + 2 * kAImageBytes;
     S.sB1 = S.sB0 + 2 * bimg_max;
     S.tabs = (uint32_t*)(S.sB1 + 2 * bimg_max);
-    S.mbar = (uint64_t*)(S.tabs + 2 * kTabWords);
+    S.dep = (uint64_t*)(S.tabs + 2 * kTabWords);
+    S.runoff = S.dep + kDepChunks * 64;
+    S.mbar = S.runoff + 256;
     uint32_t* tmem_slot = (uint32_t*)(S.mbar + 3);
     S.s_err = (int*)(tmem_slot + 1);
     S.ncols = ncols;
@@ -247,6 +254,30 @@ __device__ __forceinline__ void fused_teardown(const FusedSmem& S, FusedPipe& P,
     asm volatile("tcgen05.fence::after_thread_sync;");
     if ((threadIdx.x >> 5) == 0)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(S.tmem), "r"(S.ncols));
+}
+
+// A pass's address tables, filled by the whole CTA (a barrier must follow before use): dep[c][v] is
+// the global offset of tile index v << 6c (its bits deposited into the non-tile qubits, in ascending
+// order), so tile T starts at the OR of four lookups; runoff[r] is the offset of 256-byte run r (its
+// bits at tile qubits q[5..m-1]; qubits 0..4 are the run).  This replaces per-pair bit loops over the
+// pass's qubit list.
+__device__ __forceinline__ void fused_addr_tables(const FusedSmem& S, const FusedPassArgs& a) {
+    const int t = threadIdx.x;
+    if (t < kDepChunks * 64) {
+        ITYPE base = (ITYPE)(t & 63) << (6 * (t >> 6));
+        for (int j = 0; j < a.m; ++j) base = insert0(base, a.q[j]);
+        S.dep[t] = base;
+    } else if (t < kDepChunks * 64 + 256) {
+        const uint32_t r = (uint32_t)t - kDepChunks * 64;
+        ITYPE off = 0;
+        for (int j = kFLow; j < a.m; ++j)
+            if ((r >> (j - kFLow)) & 1u) off |= 1ULL << a.q[j];
+        S.runoff[r] = off;
+    }
+}
+
+__device__ __forceinline__ ITYPE fused_tile_base(const FusedSmem& S, ITYPE T) {
+    return S.dep[T & 63] | S.dep[64 + ((T >> 6) & 63)] | S.dep[128 + ((T >> 12) & 63)] | S.dep[192 + ((T >> 18) & 63)];
 }
 
 __device__ __forceinline__ const unsigned char* fused_record(const FusedPassArgs& a, int b) {
@@ -287,22 +318,10 @@ __device__ __forceinline__ bool fused_pair(const FusedPassArgs& a, const FusedSm
     unsigned char* sB1 = S.sB1;
     const uint32_t* tabs = S.tabs;
 
-    // output stores move amplitude pairs (tile bit 0 = qubit 0), 16 B each: pair p = tid + 512 k
-    ITYPE lo_off = 0;
-    for (int j = 1; j <= kFTidBits && j < m; ++j)
-        if ((tid >> (j - 1)) & 1) lo_off |= 1ULL << a.q[j];
+    // output stores move amplitude pairs (tile bit 0 = qubit 0), 16 B each: pair p = tid + 512 k is
+    // amplitude 2 (p % 16) of 256-byte run p / 16
     const uint32_t npairs = tsize >> 1;
-    auto tile_base = [&](ITYPE T) {
-        ITYPE base = T;
-        for (int j = 0; j < m; ++j) base = insert0(base, a.q[j]);
-        return base;
-    };
-    auto pair_off = [&](uint32_t k) {
-        ITYPE off = lo_off;
-        for (int j = kFTidBits + 1; j < m; ++j)
-            if ((k >> (j - kFTidBits - 1)) & 1) off |= 1ULL << a.q[j];
-        return off;
-    };
+    auto tile_base = [&](ITYPE T) { return fused_tile_base(S, T); };
 
     // accumulator reads: warp w reads TMEM lanes 32 (w % 4) .. +31 (rows y) and column part w / 4
     const uint32_t y = 32u * (warp & 3) + lane;
@@ -409,7 +428,7 @@ __device__ __forceinline__ bool fused_pair(const FusedPassArgs& a, const FusedSm
             const uint32_t pidx = tid + k * kFThreads;
             if (pidx < npairs) {
                 const float4 v = *(const float4*)(outt + 2 * tswz(2 * pidx));
-                __stcs((float4*)(a.state + (base | pair_off(k))), v);
+                __stcs((float4*)(a.state + (base | S.runoff[pidx >> 4] | ((pidx & 15u) << 1))), v);
             }
         }
     };
@@ -421,13 +440,9 @@ __device__ __forceinline__ bool fused_pair(const FusedPassArgs& a, const FusedSm
     if (next_pair >= 0) {  // the next pair's 256-byte runs into L2 while this pair's blocks run
         const ITYPE T2 = (ITYPE)next_pair + (tid >= 256 ? pair_stride : 0);
         const uint32_t r = (uint32_t)tid & 255u;
-        if (T2 < a.tiles && r < (tsize >> kFLow)) {
-            ITYPE off = 0;
-            for (int j = kFLow; j < m; ++j)
-                if ((r >> (j - kFLow)) & 1u) off |= 1ULL << a.q[j];
-            asm volatile("cp.async.bulk.prefetch.L2.global [%0], 256;" ::"l"(a.state + (tile_base(T2) | off))
+        if (T2 < a.tiles && r < (tsize >> kFLow))
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], 256;" ::"l"(a.state + (tile_base(T2) | S.runoff[r]))
                          : "memory");
-        }
     }
     for (int b = 0; b < a.nblocks; ++b) {
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -469,6 +484,8 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused_pass(const __grid_consta
     extern __shared__ __align__(1024) unsigned char smem[];
     const uint32_t N = (1u << a.m) >> kFBlock;
     FusedSmem S = fused_setup(smem, 2 * N < 32 ? 32u : 2 * N);  // D_X at column 0, D_Y at column N
+    fused_addr_tables(S, a);
+    __syncthreads();
     FusedPipe P;
     if ((ITYPE)blockIdx.x < a.tiles) fused_load_record(S, P, a, 0, true);
     const ITYPE stride = 2 * (ITYPE)gridDim.x;
@@ -512,6 +529,7 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused_batch(const FusedBatchRe
     __shared__ int s_rec, s_abort;
     FusedSmem S = fused_setup(smem, 2 * kFNMax);
     FusedPipe P;
+    int tab_rec = -1;  // record whose address tables are in shared memory
     const int tid = threadIdx.x;
     while (true) {
         if (tid == 0) {
@@ -543,6 +561,11 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused_batch(const FusedBatchRe
         __syncthreads();
         if (s_item >= total || s_abort) break;
         const FusedPassArgs a = recs[s_rec].args;
+        if (s_rec != tab_rec) {  // every thread left the previous pair's last table use behind a barrier
+            fused_addr_tables(S, a);
+            __syncthreads();
+            tab_rec = s_rec;
+        }
         const ITYPE TX = 2 * (s_item - recs[s_rec].prefix), TY = TX + 1;
         const bool hasY = TY < a.tiles;
         fused_load_record(S, P, a, 0, true);
@@ -885,6 +908,7 @@ int fused_plan_host(const Circuit& c, FusedPlanHost* P) {
     for (const GateRec& g : c.gates)
         if (!fusable(g)) return set_error(QS_ERR_NOT_SUPPORTED, "fused path: gate over more than 6 qubits or a noise channel");
     const int m = (int)std::min<UINT>(kFTileMax, n);
+    if ((int)n - m > 6 * kDepChunks) return set_error(QS_ERR_NOT_SUPPORTED, "fused path: too many tiles");
     const ITYPE low = (1ULL << std::min(kFLow, m)) - 1;
     std::vector<int> pending(c.gates.size());
     for (size_t i = 0; i < c.gates.size(); ++i) pending[i] = (int)i;
@@ -987,9 +1011,10 @@ struct FusedPlanDev {
 };
 
 // Shared memory of a fused CTA: A (hi | lo), two B / output tiles laid out for the largest tile (every
-// pass uses the same layout), two table slots, 3 mbarriers, the TMEM slot and the error flag.
+// pass uses the same layout), two table slots, the pass's address tables, 3 mbarriers, the TMEM slot
+// and the error flag.
 static size_t fused_smem_bytes() {
-    return 2 * kAImageBytes + 2 * (2 * (size_t)kFNMax * 256) + 2 * kTabBytes + 64;
+    return 2 * kAImageBytes + 2 * (2 * (size_t)kFNMax * 256) + 2 * kTabBytes + kAddrTabBytes + 64;
 }
 
 // The kernel's dynamic shared-memory limit is a process-wide attribute: set it once per device to
