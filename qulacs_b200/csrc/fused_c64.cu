@@ -12,9 +12,9 @@
 // Device side: one persistent CTA (512 threads) per SM takes its tiles in pairs that go through the
 // pass's blocks in lockstep and share each block's A image (bulk async copy).  Per block, one thread
 // issues for each tile 8 K-steps x 3 products (A_hi B_hi + A_hi B_lo + A_lo B_hi) of tcgen05.mma
-// M=128 N=128 K=16 into its 128 x 128 FP32 TMEM accumulator and commits to an mbarrier; all warps
-// move the first tile's accumulator (tcgen05.ld) into its next B operand while the second tile's
-// MMAs run.  Tiles are gathered straight from HBM; after the last block each becomes a complex64
+// M=128 N=128 K=16 into its 128 x 128 FP32 TMEM accumulator and commits to an mbarrier; the other
+// warps move one tile's accumulator (tcgen05.ld) into its next B operand while the other tile's MMAs
+// run.  Tiles are gathered straight from HBM; after the last block each becomes a complex64
 // tile stored to HBM.  Every wait is bounded; on expiry the kernel records an error, frees its TMEM
 // and returns.
 #include <algorithm>
@@ -169,9 +169,9 @@ __device__ __forceinline__ void bulk_load_block(uint32_t dst_a, uint32_t dst_t, 
 }
 
 // Two tiles in flight.  A CTA takes its tiles in pairs (X, Y) that go through the pass's blocks in
-// lockstep and share each block's A operand: X's and Y's MMAs are issued back to back into two TMEM
-// accumulators, X's accumulator moves run while Y's MMAs do, and the next block's A image (bulk copy)
-// lands while Y's accumulator moves run.  A tile is gathered straight from HBM into its B operand
+// lockstep and share each block's A operand: X's and Y's MMAs go into two TMEM accumulators, X's
+// accumulator moves run while Y's MMAs do, and Y's moves run while the next block's A image (bulk
+// copy) lands and X's next MMAs run.  A tile is gathered straight from HBM into its B operand
 // (bf16 hi / lo) through 64-bit offset tables; after the last block its accumulator becomes a
 // complex64 tile over its own B region, stored with 16-byte streaming stores.
 // Every in-tile data movement is a table XOR: element (row y, column n) of a block's accumulator goes
@@ -323,12 +323,15 @@ __device__ __forceinline__ bool fused_pair(const FusedPassArgs& a, const FusedSm
     const uint32_t npairs = tsize >> 1;
     auto tile_base = [&](ITYPE T) { return fused_tile_base(S, T); };
 
-    // accumulator reads: warp w reads TMEM lanes 32 (w % 4) .. +31 (rows y) and column part w / 4
+    // accumulator reads: warp w >= 1 reads TMEM lanes 32 (w % 4) .. +31 (rows y); the 16-column chunks
+    // are split over the mover warps of each lane quarter (three in quarter 0: warp 0 issues the MMAs)
     const uint32_t y = 32u * (warp & 3) + lane;
-    const uint32_t parts = N >= 64 ? 4u : N / 16;
-    const uint32_t cw = N / parts;
-    const uint32_t c_begin = (uint32_t)(warp >> 2) < parts ? (warp >> 2) * cw : 0;
-    const uint32_t c_end = (uint32_t)(warp >> 2) < parts ? c_begin + cw : 0;
+    const bool mover = warp != 0;
+    const uint32_t nchunks = N / 16;
+    const uint32_t nq = (warp & 3) == 0 ? 3u : 4u;
+    const uint32_t rq = mover ? ((warp & 3) == 0 ? (uint32_t)(warp >> 2) - 1u : (uint32_t)(warp >> 2)) : 0u;
+    const uint32_t c_begin = mover ? 16u * ((rq * nchunks) / nq) : 0u;
+    const uint32_t c_end = mover ? 16u * (((rq + 1u) * nchunks) / nq) : 0u;
     // gather: thread t owns B rows n = (t & 7) + 8 i and K pair j = bits 3..8 of t
     const uint32_t g_n0 = tid & 7u, g_j = (uint32_t)tid >> 3;
     const uint32_t g_off = kmajor_off(g_n0, 2 * g_j);
@@ -444,33 +447,43 @@ __device__ __forceinline__ bool fused_pair(const FusedPassArgs& a, const FusedSm
             asm volatile("cp.async.bulk.prefetch.L2.global [%0], 256;" ::"l"(a.state + (tile_base(T2) | S.runoff[r]))
                          : "memory");
     }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();  // the gathered B operands are visible to the tensor cores
+    // Block loop, software-pipelined: X(b) is issued as soon as block b's record has landed, while the
+    // mover warps still turn Y's accumulator of block b - 1 into its next operand; Y(b) follows once
+    // that is done, and X's accumulator moves run under Y(b)'s MMAs.  Warp 0 only issues.
     for (int b = 0; b < a.nblocks; ++b) {
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        asm volatile("tcgen05.fence::before_thread_sync;");
-        __syncthreads();
-        fused_wait_record(S, P);  // this block's A image and tables
+        const bool last = b + 1 == a.nblocks;
+        const int cur = P.slot;
+        fused_wait_record(S, P);  // block b's A image and tables (every thread observes the copy)
         if (tid == 0 && !*S.s_err) {
             asm volatile("tcgen05.fence::after_thread_sync;");
-            issue_mma(sB0, 0, S.mb0);
-            if (hasY) issue_mma(sB1, N, S.mb1);
+            issue_mma(sB0, 0, S.mb0);  // sB0 and D_X were released at the previous barrier
         }
-        const bool last = b + 1 == a.nblocks;
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        __syncthreads();  // Y's operand of block b written (and proxy-fenced), D_Y read
+        if (tid == 0 && !*S.s_err && hasY) {
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            issue_mma(sB1, N, S.mb1);
+        }
         if (!mbar_wait(S.mb0, P.ph0)) *S.s_err = 1;
         P.ph0 ^= 1u;
         asm volatile("tcgen05.fence::after_thread_sync;");
-        move(sB0, 0, P.slot, last);  // while Y's MMAs run
+        if (mover) move(sB0, 0, cur, last);  // while Y's MMAs run
         if (hasY) {
             if (!mbar_wait(S.mb1, P.ph1)) *S.s_err = 1;
             P.ph1 ^= 1u;
             asm volatile("tcgen05.fence::after_thread_sync;");
         }
-        __syncthreads();  // both MMAs done: A and the other table slot are free
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        __syncthreads();  // both MMAs done (A and the other table slot free); X's next operand written
         if (*S.s_err) return false;
         const int nxt = b + 1 < a.nblocks ? b + 1 : (next_pair >= 0 ? 0 : -1);
         const bool reload = nxt >= 0 && nxt != b;  // a single-block pass keeps its record resident
-        const int cur = P.slot;
         if (reload) fused_load_record(S, P, a, nxt, true);
-        if (hasY) move(sB1, N, cur, last);  // while the next record lands
+        if (hasY && mover) move(sB1, N, cur, last);  // while the next record lands and X(b + 1) runs
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
