@@ -475,13 +475,24 @@ __device__ __forceinline__ bool fused_pair(const FusedPassArgs& a, const FusedSm
             P.ph1 ^= 1u;
             asm volatile("tcgen05.fence::after_thread_sync;");
         }
+        const int nxt = b + 1 < a.nblocks ? b + 1 : (next_pair >= 0 ? 0 : -1);
+        const bool reload = nxt >= 0 && nxt != b;  // a single-block pass keeps its record resident
+        // Thread 0 has seen both MMA groups complete, so A is free, and the other table slot was
+        // released at the first barrier: the next record's copy starts before the second barrier.
+        // Every thread books it after that barrier, ahead of the error exit, so a teardown waits for it.
+        if (reload && tid == 0) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            bulk_load_block(S.aaddr, S.taddr + (P.loads & 1) * kTabBytes, fused_record(a, nxt), S.mba);
+        }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("tcgen05.fence::before_thread_sync;");
         __syncthreads();  // both MMAs done (A and the other table slot free); X's next operand written
+        if (reload) {
+            P.slot = P.loads & 1;
+            ++P.loads;
+            P.a_pending = true;
+        }
         if (*S.s_err) return false;
-        const int nxt = b + 1 < a.nblocks ? b + 1 : (next_pair >= 0 ? 0 : -1);
-        const bool reload = nxt >= 0 && nxt != b;  // a single-block pass keeps its record resident
-        if (reload) fused_load_record(S, P, a, nxt, true);
         if (hasY && mover) move(sB1, N, cur, last);  // while the next record lands and X(b + 1) runs
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
