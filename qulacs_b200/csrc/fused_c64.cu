@@ -157,12 +157,9 @@ __device__ __forceinline__ void bulk_load_block(uint32_t dst_a, uint32_t dst_t, 
         "{\n.reg .b64 st;\nmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}\n" ::"r"(mbar),
         "r"(2 * kAImageBytes + kTabBytes)
         : "memory");
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                         dst_a + i * (kAImageBytes / 2)),
-                     "l"(rec + i * (kAImageBytes / 2)), "r"(kAImageBytes / 2), "r"(mbar)
-                     : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst_a),
+                 "l"(rec), "r"(2 * kAImageBytes), "r"(mbar)
+                 : "memory");
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst_t),
                  "l"(rec + 2 * kAImageBytes), "r"(kTabBytes), "r"(mbar)
                  : "memory");
