@@ -26,8 +26,6 @@
 #include <thread>
 #include <vector>
 
-#include <cuda_bf16.h>
-
 #include "circuit.hpp"
 #include "qs_internal.cuh"
 
@@ -37,7 +35,6 @@ constexpr int kFTileMax = 13;      // tile qubits (2^13 c64 amplitudes = 64 KiB)
 constexpr int kFLow = 5;            // qubits 0..4 always in a tile
 constexpr int kFBlock = 6;          // qubits per fused block
 constexpr int kFThreads = 512;
-constexpr int kFTidBits = 9;      // log2(kFThreads)
 constexpr int kARows = 128, kAK = 128;           // real-ified block matrix
 constexpr int kAImageBytes = kARows * kAK * 2;   // one bf16 image (hi or lo): 32 KiB
 constexpr long long kWaitLimit = 4000000000LL;   // ~2 s of clock64 at 2 GHz
@@ -72,11 +69,6 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
 // Tile layout swizzle: XOR tile bits 5..12 into bits 1..4 (bit 0 untouched, so amplitude pairs stay
 // adjacent for 16-byte copies), spreading block-bit strides over the shared-memory banks.
 __host__ __device__ __forceinline__ uint32_t tswz(uint32_t u) { return u ^ ((((u >> 5) ^ (u >> 9)) & 15u) << 1); }
-
-__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem_dst)), "l"(gsrc) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // Two floats -> packed bf16 pairs (a in the low half): hi = RN(v), lo = RN(v - hi).
 __device__ __forceinline__ void split2_bf16(float a, float b, uint32_t* hi, uint32_t* lo) {
@@ -142,12 +134,6 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 #pragma unroll
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
-
-__device__ __forceinline__ void split_bf16(float v, __nv_bfloat16_raw* hi, __nv_bfloat16_raw* lo);
-
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait_group() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 // One block record: A image (hi | lo, 64 KiB) into `dst_a` and its index tables into `dst_t`, with bulk
 // async copies completing on `mbar` (issued by one thread; the phase completes when all bytes landed).
@@ -597,19 +583,6 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused_batch(const FusedBatchRe
         }
     }
     fused_teardown(S, P, err);
-}
-
-__device__ __forceinline__ void split_bf16(float v, __nv_bfloat16_raw* hi, __nv_bfloat16_raw* lo) {
-    // round to nearest even: hi = bf16(v), lo = bf16(v - hi)
-    uint32_t u = __float_as_uint(v);
-    uint32_t r = u + 0x7FFFu + ((u >> 16) & 1u);
-    const uint16_t h = (uint16_t)(r >> 16);
-    const float hf = __uint_as_float((uint32_t)h << 16);
-    const float rem = v - hf;
-    uint32_t u2 = __float_as_uint(rem);
-    uint32_t r2 = u2 + 0x7FFFu + ((u2 >> 16) & 1u);
-    hi->x = h;
-    lo->x = (uint16_t)(r2 >> 16);
 }
 
 // ---------------------------------------------------------------- host planning
