@@ -78,17 +78,6 @@ __device__ __forceinline__ double2 cfma(double2 a, double2 b, double2 acc) {
 __device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
 __device__ __forceinline__ double norm2(double2 a) { return fma(a.x, a.x, a.y * a.y); }
 
-__device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
-    return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
-}
-__device__ __forceinline__ float2 cfmaf(float2 a, float2 b, float2 acc) {
-    acc.x = fmaf(a.x, b.x, acc.x);
-    acc.x = fmaf(-a.y, b.y, acc.x);
-    acc.y = fmaf(a.x, b.y, acc.y);
-    acc.y = fmaf(a.y, b.x, acc.y);
-    return acc;
-}
-
 // Streaming 128-bit global accesses: every amplitude is touched once per pass, so loads bypass
 // L1 allocation and stores are marked evict-first in L2.
 __device__ __forceinline__ double2 ld_stream(const double2* p) {
