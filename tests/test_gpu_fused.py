@@ -51,6 +51,26 @@ def test_fused_against_oracle(port, n, kind, executor):
     assert np.mean((got == ref_idx) | near) >= 0.99
 
 
+@pytest.mark.parametrize("n", [26, 31])
+def test_fused_large_tile_indices(n):
+    """Sizes whose tile indices reach the upper 6-bit chunks of the kernel's tile-base tables (26
+    qubits: three chunks; 31: all four): the tensor-core result against the complex128 staged
+    executor, which is itself checked against the reference at 30 qubits."""
+    gates = W.u3_cz_circuit(n, 6, seed=900 + n)
+    circ = W.to_circuit(gates, n)
+    ref = QuantumState(n)
+    circ.update_quantum_state(ref, mode="staged")
+    circ.set_c64_executor("tensor")
+    s = QuantumStateC64(n)
+    circ.update_quantum_state(s)
+    assert circ.c64_executor_info() == "tensor"
+    inf = s.infidelity(ref)
+    assert inf <= INFIDELITY_TOL, inf
+    # the norm drifts by the split-bf16 rounding of every block (1.2e-5 after this circuit's ~25)
+    assert abs(s.get_squared_norm() - 1.0) <= EV_TOL_C64
+    del s, ref
+
+
 def test_fused_schedule_reduces_work():
     n = 20
     circ = W.to_circuit(W.u3_cz_circuit(n, 10, seed=3), n)
